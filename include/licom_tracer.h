@@ -1,0 +1,169 @@
+/*
+ * licom_tracer.h - C ABI of the B200 LICOM3 baroclinic tracer step.
+ *
+ * Drop-in for the tracer path of LICOM3-HIP:
+ *   tracer_(int ii)   replaces  tracer.cpp:1701-1903   (extern "C" void tracer_(int))
+ *   convadj_(void)    replaces  convadj.cpp:290-298    (extern "C" void convadj_())
+ * and the device state those read, which the reference keeps in global d_*
+ * pointers (cuda_data.h:35-345, allocated by cudainit in cuda_init.cpp:372-707).
+ * Here the state lives in a per-domain arena created by lt_create; the two
+ * reference-named shims act on the domain bound with lt_shim_bind.
+ *
+ * Array layout is the reference's: C row-major [n][k][j][i] (Fortran
+ * (i,j,k,n)), i fastest, halo width 2 on each side (imt = nx+4, jmt = ny+4),
+ * j = 0 the northern edge.  ATB carries km+1 levels (Fortran 0:km) and WS km+1
+ * levels.  Every entry point returns an lt_status; nothing prints or exits.
+ */
+#ifndef LICOM_TRACER_H
+#define LICOM_TRACER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LT_OK = 0,
+  LT_E_INVALID = 1,   /* bad argument, size or field id */
+  LT_E_OOM = 2,       /* device memory admission failed */
+  LT_E_CUDA = 3,      /* a CUDA runtime call failed */
+  LT_E_NUMERIC = 4,   /* NaN/Inf found by the step's status scan */
+  LT_E_TIMEOUT = 5,   /* a bounded device wait ran out */
+  LT_E_STATE = 6,     /* call out of order (e.g. step before inputs) */
+  LT_E_NODEVICE = 7   /* no CUDA device visible */
+} lt_status;
+
+/* Field identifiers.  Shapes use km, jmt, imt of the domain. */
+typedef enum {
+  /* prognostic state, f64 */
+  LT_F_AT = 0,        /* [2][km][jmt][imt]  T (degC), S ((psu-35)/1000)  tracer_mod at  */
+  LT_F_ATB,           /* [2][km+1][jmt][imt] previous tracers, level 0 unused  tracer_mod atb */
+  /* dynamics inputs (produced by barotr/bclinc in the model), f64 */
+  LT_F_UTF,           /* [km][jmt][imt] */
+  LT_F_VTF,
+  LT_F_UTL,
+  LT_F_VTL,
+  LT_F_H0F,           /* [jmt][imt] */
+  LT_F_H0L,
+  LT_F_AKT,           /* [2][km][jmt][imt] Canuto diffusivity (readyc.cpp:1569-1572) */
+  /* outputs / persistent side state */
+  LT_F_WS,            /* [km+1][jmt][imt] vertical velocity */
+  LT_F_NET,           /* [2][jmt][imt] surface net flux, halo-updated */
+  LT_F_UTF_OUT,       /* [km][jmt][imt] utf*oncc (the reference scales utf in place) */
+  LT_F_VTF_OUT,
+  LT_F_H0F_OUT,       /* [jmt][imt] h0f*onbc */
+  /* surface forcing, f64 [jmt][imt] */
+  LT_F_SWV, LT_F_NSWV, LT_F_SST, LT_F_SSS, LT_F_FRESH, LT_F_SEAICE,
+  /* horizontal grid, f64 [jmt][imt] */
+  LT_F_TAREA, LT_F_TAREA_R, LT_F_HTW, LT_F_HTS, LT_F_HUN, LT_F_HUE, LT_F_DXU, LT_F_DYU,
+  LT_F_AHF, LT_F_DTN, LT_F_DTS, LT_F_DTE, LT_F_DTW, LT_F_OHBT, LT_F_OHBU,
+  LT_F_AU0, LT_F_AUS, LT_F_AUW, LT_F_AUSW,
+  /* integer masks, i32 [jmt][imt] */
+  LT_F_KMT, LT_F_KMU, LT_F_KMTN, LT_F_KMTS, LT_F_KMTE, LT_F_KMTW,
+  /* vertical, f64 */
+  LT_F_DZP, LT_F_ODZP, LT_F_ODZT,   /* [km] */
+  LT_F_PEN,                         /* [km] shortwave penetration (km-1 used) */
+  LT_F_TO, LT_F_SO,                 /* [km] convadj reference T/S */
+  LT_F_C,                           /* [9][km] convadj density polynomial */
+  LT_F_RESTORE,                     /* [2][km][jmt][imt] restoring target */
+  /* diagnostics, f64 (written when the domain was created with diagnostics) */
+  LT_F_AX, LT_F_AY, LT_F_AZ, LT_F_DZ, LT_F_TEND, LT_F_DT_DIFF, LT_F_DT_CONV,  /* [2][km][jmt][imt] */
+  LT_F_PENETRATE,                   /* [km][jmt][imt] */
+  LT_F_COUNT
+} lt_field;
+
+/* Precision of the step arithmetic.  The state is always f64. */
+typedef enum {
+  LT_PREC_FP64 = 0,   /* plain f64 drop-in: the correctness form */
+  LT_PREC_MIXED = 1   /* f32 flux/stencil/diffusion arithmetic, f64 state and sums */
+} lt_precision;
+
+typedef struct {
+  int nx, ny, km;        /* physical sizes; imt = nx+4, jmt = ny+4 */
+  int precision;         /* lt_precision */
+  int diagnostics;       /* nonzero: write AX..PENETRATE */
+  int ew_cyclic;         /* 1 cyclic east-west, 0 closed */
+  int tripole;           /* 1 tripole north fold, 0 closed north */
+} lt_grid;
+
+/* Scalars read by tracer_ from Fortran module variables (tracer.cpp:1712-1896). */
+typedef struct {
+  double dts;            /* pconst_mod dts */
+  double oncc;           /* pconst_mod oncc */
+  double onbc;           /* pconst_mod onbc */
+  double dwndmix;        /* pconst_mod dwndmix */
+  double gamma;          /* pconst_mod gamma (1/s) */
+  double od0;            /* pconst_mod od0 */
+  double od0cp;          /* pconst_mod od0cp */
+  double ah;             /* hmix_del4 ah */
+  double area_t;         /* grid area_t (global ocean surface area) */
+  int nss;               /* pconst_mod nss */
+  int boundary_restore;  /* pconst_mod boundary_restore (1 = 15-day restoring) */
+} lt_params;
+
+typedef struct lt_domain lt_domain;
+
+/* --- domain lifecycle ---------------------------------------------------- */
+/* Allocates the device arena for one domain on the current device.
+ * Replaces cudainit (cuda_init.cpp:372-707) for the tracer working set. */
+int lt_create(const lt_grid* grid, const lt_params* params, lt_domain** out);
+int lt_destroy(lt_domain* dom);
+int lt_set_params(lt_domain* dom, const lt_params* params);
+/* Bytes one domain of this grid holds on the device (admission control). */
+size_t lt_domain_bytes(const lt_grid* grid);
+
+/* --- data movement (host pointers; synchronous on the domain's stream) --- */
+int lt_set_field(lt_domain* dom, int field, const void* host_src, size_t nbytes);
+int lt_get_field(lt_domain* dom, int field, void* host_dst, size_t nbytes);
+/* Device-to-device variants (pointers into the caller's device memory). */
+int lt_set_field_device(lt_domain* dom, int field, const void* dev_src, size_t nbytes);
+int lt_get_field_device(lt_domain* dom, int field, void* dev_dst, size_t nbytes);
+/* Derive KMU, KMTN/S/E/W, OHBT, OHBU, ODZP, ODZT on the device from KMT
+ * (ghosts filled) and DZP, as boundary.F90:24-52 and grid.F90:1097-1106,
+ * 1343-1346, 2030-2051 do on the host. */
+int lt_derive_masks(lt_domain* dom);
+
+/* --- the step ------------------------------------------------------------ */
+/* Advance nsteps tracer steps with frozen dynamics inputs: each step reads
+ * UTF/VTF/UTL/VTL/H0F/H0L/AKT as given and writes the scaled copies to the
+ * *_OUT fields.  Asynchronous on the domain's stream. */
+int lt_step(lt_domain* dom, int nsteps);
+/* One step taking this step's surface forcing from HOST buffers (swv, nswv,
+ * sst, sss, fresh, seaice; each [jmt][imt] f64, any may be NULL to keep the
+ * resident field) and returning fw_norm2 and the two global tracer integrals
+ * sum(tarea*dzp*vit*tracer) to a host buffer out3 (may be NULL). */
+int lt_step_host(lt_domain* dom, const double* const forcing6[6], double* out3);
+/* Convective adjustment of the current state (convadj.cpp:29-288). */
+int lt_convadj(lt_domain* dom);
+/* Global tracer integrals sum(tarea*dzp*vit*tracer) over the interior, f64,
+ * fixed-order pairwise tree (deterministic). out2[0] = T, out2[1] = S. */
+int lt_tracer_content(lt_domain* dom, double* out2);
+/* fw_norm2 of the last step (tracer.cpp:1862-1865). */
+int lt_fw_norm2(lt_domain* dom, double* out);
+int lt_sync(lt_domain* dom);
+/* Scan AT for NaN/Inf; LT_E_NUMERIC if any. */
+int lt_check_numeric(lt_domain* dom, long long* bad_count);
+/* Elapsed device time (ms) of the last lt_step call, CUDA events. */
+int lt_last_step_ms(lt_domain* dom, float* ms);
+
+/* --- reference-named shims ---------------------------------------------- */
+/* Bind the domain the shims act on (the reference uses process globals). */
+int lt_shim_bind(lt_domain* dom);
+/* tracer.cpp:1701: one step with the reference's side effects on the bound
+ * domain: UTF/VTF/H0F scaled in place, VTL left holding S with halo. */
+void tracer_(int ii);
+/* convadj.cpp:290: convective adjustment of the bound domain. */
+void convadj_(void);
+
+/* --- errors, device ------------------------------------------------------ */
+const char* lt_last_error(void);
+int lt_device_count(int* count);
+/* Library version/build id string. */
+const char* lt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LICOM_TRACER_H */

@@ -1,0 +1,60 @@
+// lt_fields.h - shapes of the lt_field identifiers (host/device agnostic).
+#pragma once
+#include "../../include/licom_tracer.h"
+
+namespace lt {
+
+enum FieldShape {
+  SH_TRACER3 = 0,   // [2][km][jmt][imt]
+  SH_TRACERB,       // [2][km+1][jmt][imt]
+  SH_LEVEL3,        // [km][jmt][imt]
+  SH_W3,            // [km+1][jmt][imt]
+  SH_SURF2,         // [jmt][imt]
+  SH_SURF2N,        // [2][jmt][imt]
+  SH_MASK2,         // [jmt][imt] int32
+  SH_COL1,          // [km]
+  SH_COEF9          // [9][km]
+};
+
+inline int field_shape(int f) {
+  switch (f) {
+    case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE: case LT_F_AX: case LT_F_AY: case LT_F_AZ:
+    case LT_F_DZ: case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV:
+      return SH_TRACER3;
+    case LT_F_ATB: return SH_TRACERB;
+    case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
+    case LT_F_PENETRATE:
+      return SH_LEVEL3;
+    case LT_F_WS: return SH_W3;
+    case LT_F_NET: return SH_SURF2N;
+    case LT_F_KMT: case LT_F_KMU: case LT_F_KMTN: case LT_F_KMTS: case LT_F_KMTE: case LT_F_KMTW:
+      return SH_MASK2;
+    case LT_F_DZP: case LT_F_ODZP: case LT_F_ODZT: case LT_F_PEN: case LT_F_TO: case LT_F_SO:
+      return SH_COL1;
+    case LT_F_C: return SH_COEF9;
+    default: return SH_SURF2;
+  }
+}
+
+inline bool field_is_int(int f) { return field_shape(f) == SH_MASK2; }
+
+inline long field_count(int f, int imt, int jmt, int km) {
+  const long A = (long)imt * jmt;
+  switch (field_shape(f)) {
+    case SH_TRACER3: return 2 * A * km;
+    case SH_TRACERB: return 2 * A * (km + 1);
+    case SH_LEVEL3: return A * km;
+    case SH_W3: return A * (km + 1);
+    case SH_SURF2: case SH_MASK2: return A;
+    case SH_SURF2N: return 2 * A;
+    case SH_COL1: return km;
+    case SH_COEF9: return 9L * km;
+  }
+  return 0;
+}
+
+inline size_t field_bytes(int f, int imt, int jmt, int km) {
+  return (size_t)field_count(f, imt, jmt, km) * (field_is_int(f) ? 4 : 8);
+}
+
+}  // namespace lt

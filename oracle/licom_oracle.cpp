@@ -1,0 +1,810 @@
+// licom_oracle.cpp - CPU FP64 restatement of the LICOM3-HIP baroclinic tracer
+// step.  TEST INFRASTRUCTURE ONLY: it is the checker the GPU path is compared
+// against, never part of the product.
+//
+// What it follows (paths are within the reference project):
+//   orchestration and index ranges: tracer.cpp:1701-1903 (tracer_)
+//   continuity                      tracer.cpp:980-1150 (tracer_1_0, tracer_1,
+//                                   upwell_2, operators_div, upwell_3, upwell_4),
+//                                   upwell.F90:26-109, grid.F90:1936-1993
+//   tspas advection                 tracer.cpp:83-119, 291-921, advection.F90:153-431
+//   biharmonic tracer diffusion     tracer.cpp:1238-1362, hmix_del4.F90:626-757
+//   vertical terms, forcing         tracer.cpp:1395-1699
+//   implicit vertical diffusion     tracer.cpp:923-978, invtri.F90:5-65
+//   halo and tripole fold           POP_HaloMod.F90:2716-3139, 5602-5680,
+//                                   POP_BlocksMod.F90:284-375
+//   convective adjustment           convadj.cpp:29-288
+//
+// Arithmetic keeps the reference's operation order term by term (so that a
+// build with -ffp-contract=off reproduces the reference's own code compiled
+// the same way bit for bit); the loop structure, storage and naming are this
+// file's own.  The only reduction, the SSS-normalisation sum, runs in the
+// reference's sequential j-major order.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+#include "../include/licom_tracer.h"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+enum Kind { K3N = 0, KB3N, K3, KW, K2, K2N, K2I, K1, K1C };
+
+struct FieldInfo { int kind; bool is_int; };
+
+FieldInfo field_info(int f) {
+  switch (f) {
+    case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE:
+    case LT_F_AX: case LT_F_AY: case LT_F_AZ: case LT_F_DZ: case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV:
+      return {K3N, false};
+    case LT_F_ATB: return {KB3N, false};
+    case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
+    case LT_F_PENETRATE:
+      return {K3, false};
+    case LT_F_WS: return {KW, false};
+    case LT_F_NET: return {K2N, false};
+    case LT_F_KMT: case LT_F_KMU: case LT_F_KMTN: case LT_F_KMTS: case LT_F_KMTE: case LT_F_KMTW:
+      return {K2I, true};
+    case LT_F_DZP: case LT_F_ODZP: case LT_F_ODZT: case LT_F_PEN: case LT_F_TO: case LT_F_SO:
+      return {K1, false};
+    case LT_F_C: return {K1C, false};
+    default: return {K2, false};
+  }
+}
+
+struct Oracle {
+  int nx, ny, km, imt, jmt;
+  long A, F, FB;
+  int ew_cyclic = 1, tripole = 1, diagnostics = 1;
+  lt_params p{};
+  std::vector<double> fd[LT_F_COUNT];
+  std::vector<int> fi[LT_F_COUNT];
+  // scratch of the reference kernels
+  std::vector<double> vit, at00, atmax, atmin, uk, vk, wka, wkb, wkd, wkc, work, stf, tf, adv_tt, d2tk,
+      u_wface, v_sface, ori, temp11, vtl_work;
+  double fw_norm2 = 0.0;
+  int ist = 0;
+
+  long count(int f) const {
+    switch (field_info(f).kind) {
+      case K3N: return 2 * F;
+      case KB3N: return 2 * FB;
+      case K3: return F;
+      case KW: return FB;
+      case K2N: return 2 * A;
+      case K2: case K2I: return A;
+      case K1: return km;
+      case K1C: return 9L * km;
+    }
+    return 0;
+  }
+
+  Oracle(int nx_, int ny_, int km_) : nx(nx_), ny(ny_), km(km_) {
+    imt = nx + 4; jmt = ny + 4;
+    A = (long)imt * jmt; F = A * km; FB = A * (km + 1);
+    for (int f = 0; f < LT_F_COUNT; ++f) {
+      if (field_info(f).is_int) fi[f].assign(count(f), 0);
+      else fd[f].assign(count(f), 0.0);
+    }
+    for (auto* v : {&vit, &at00, &atmax, &atmin, &uk, &vk, &wka, &wkb, &wkd, &wkc, &tf, &adv_tt, &d2tk,
+                    &u_wface, &v_sface, &ori})
+      v->assign(F, 0.0);
+    work.assign(A, 0.0); stf.assign(A, 0.0); temp11.assign(A, 0.0);
+  }
+
+  // index helpers
+  long c3(int k, int j, int i) const { return (long)k * A + (long)j * imt + i; }
+  long c2(int j, int i) const { return (long)j * imt + i; }
+};
+
+// ------------------------------------------------------------------ halo
+// Global-domain, single-block ghost update (POP_HaloUpdate3DR8 with
+// POP_gridHorzLocCenter / POP_fieldKindScalar).  Message order of the
+// reference: east/west local copies of physical rows, then the tripole buffer
+// (top haloWidth+1 physical rows), symmetric averaging of its first row for
+// i = 1..nx/2-1 with partner nx-i, and the copy-out into ghost rows j=1,2 and
+// the top physical row j=3 (1-based) for every column including E-W ghosts.
+// A closed boundary sends no message, so its ghost cells are left as they are.
+void halo_r8(double* a, int nz, int imt, int jmt, int ew_cyclic, int tripole) {
+  const int nx = imt - 4;
+  std::vector<double> buf((size_t)(nx + 1) * 3);
+  for (int z = 0; z < nz; ++z) {
+    double* s = a + (long)z * imt * jmt;
+    if (ew_cyclic) {
+      for (int jf = 3; jf <= jmt - 2; ++jf) {        // physical rows, Fortran numbering
+        double* row = s + (long)(jf - 1) * imt;
+        for (int h = 1; h <= 2; ++h) {
+          row[h - 1] = row[(nx + 2) - 2 + h - 1];      // east msg: ie-hw+h -> h
+          row[(nx + 2) + h - 1] = row[3 + h - 2];      // west msg: ib+h-1 -> ie+h
+        }
+      }
+    }
+    if (!tripole) continue;
+    for (int r = 1; r <= 3; ++r)
+      for (int g = 1; g <= nx; ++g) buf[(size_t)(r - 1) * (nx + 1) + g] = s[(long)(2 + r - 1) * imt + (g + 2) - 1];
+    for (int g = 1; g <= nx / 2 - 1; ++g) {
+      const int gd = nx - g;
+      const double x1 = buf[g], x2 = buf[gd];
+      const double xavg = 0.5 * (x1 + x2);
+      buf[g] = xavg;
+      buf[gd] = xavg;
+    }
+    buf[nx] = 1.0 * buf[nx];
+    for (int jf = 1; jf <= 3; ++jf) {
+      for (int iF = 1; iF <= imt; ++iF) {
+        int ig = iF - 2;                            // POP_BlocksMod global index
+        if (ig < 1) ig = ew_cyclic ? ig + nx : 0;
+        else if (ig > nx) ig = ew_cyclic ? ig - nx : 0;
+        int isrc = nx - ig + 1 - 1;
+        const int jsrc = (2 + 3 - jf) - 1;
+        if (isrc == 0) isrc = nx;
+        if (jsrc > 0) s[(long)(jf - 1) * imt + iF - 1] = buf[(size_t)(jsrc - 1) * (nx + 1) + isrc];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ the step
+void tracer_call(Oracle& o) {
+  const int km = o.km, imt = o.imt, jmt = o.jmt;
+  const long A = o.A, F = o.F, FB = o.FB;
+  const lt_params& p = o.p;
+  double* at = o.fd[LT_F_AT].data();
+  double* atb = o.fd[LT_F_ATB].data();
+  double* utf = o.fd[LT_F_UTF].data();
+  double* vtf = o.fd[LT_F_VTF].data();
+  double* utl = o.fd[LT_F_UTL].data();
+  double* vtl = o.fd[LT_F_VTL].data();
+  double* h0f = o.fd[LT_F_H0F].data();
+  double* h0l = o.fd[LT_F_H0L].data();
+  double* akt = o.fd[LT_F_AKT].data();
+  double* ws = o.fd[LT_F_WS].data();
+  double* net = o.fd[LT_F_NET].data();
+  const double* swv = o.fd[LT_F_SWV].data();
+  const double* nswv = o.fd[LT_F_NSWV].data();
+  const double* sst = o.fd[LT_F_SST].data();
+  const double* sss = o.fd[LT_F_SSS].data();
+  const double* fresh = o.fd[LT_F_FRESH].data();
+  const double* seaice = o.fd[LT_F_SEAICE].data();
+  const double* tarea = o.fd[LT_F_TAREA].data();
+  const double* tarea_r = o.fd[LT_F_TAREA_R].data();
+  const double* htw = o.fd[LT_F_HTW].data();
+  const double* hts = o.fd[LT_F_HTS].data();
+  const double* hun = o.fd[LT_F_HUN].data();
+  const double* hue = o.fd[LT_F_HUE].data();
+  const double* ahf = o.fd[LT_F_AHF].data();
+  const double* dtn = o.fd[LT_F_DTN].data();
+  const double* dts_c = o.fd[LT_F_DTS].data();
+  const double* dte = o.fd[LT_F_DTE].data();
+  const double* dtw = o.fd[LT_F_DTW].data();
+  const double* ohbt = o.fd[LT_F_OHBT].data();
+  const double* ohbu = o.fd[LT_F_OHBU].data();
+  const double* au0 = o.fd[LT_F_AU0].data();
+  const double* aus = o.fd[LT_F_AUS].data();
+  const double* auw = o.fd[LT_F_AUW].data();
+  const double* ausw = o.fd[LT_F_AUSW].data();
+  const int* kmt = o.fi[LT_F_KMT].data();
+  const int* kmtn = o.fi[LT_F_KMTN].data();
+  const int* kmts = o.fi[LT_F_KMTS].data();
+  const int* kmte = o.fi[LT_F_KMTE].data();
+  const int* kmtw = o.fi[LT_F_KMTW].data();
+  const double* dzp = o.fd[LT_F_DZP].data();
+  const double* odzp = o.fd[LT_F_ODZP].data();
+  const double* odzt = o.fd[LT_F_ODZT].data();
+  const double* pen = o.fd[LT_F_PEN].data();
+  const double* restore = o.fd[LT_F_RESTORE].data();
+  double* ax = o.fd[LT_F_AX].data();
+  double* ay = o.fd[LT_F_AY].data();
+  double* az = o.fd[LT_F_AZ].data();
+  double* dzd = o.fd[LT_F_DZ].data();
+  double* tend = o.fd[LT_F_TEND].data();
+  double* dt_diff = o.fd[LT_F_DT_DIFF].data();
+  double* penetrate = o.fd[LT_F_PENETRATE].data();
+  double* vit = o.vit.data();
+  double *at00 = o.at00.data(), *atmax = o.atmax.data(), *atmin = o.atmin.data();
+  double *uk = o.uk.data(), *vk = o.vk.data(), *wka = o.wka.data(), *wkb = o.wkb.data(), *wkd = o.wkd.data();
+  double *wkc = o.wkc.data(), *work = o.work.data(), *stf = o.stf.data(), *tf = o.tf.data();
+  double *adv_tt = o.adv_tt.data(), *d2tk = o.d2tk.data(), *uw = o.u_wface.data(), *vs = o.v_sface.data();
+  double *ori = o.ori.data(), *temp11 = o.temp11.data();
+  const double dts = p.dts;
+
+  // vit from kmt (boundary.F90:44-52)
+#pragma omp parallel for
+  for (int k = 0; k < km; ++k)
+    for (long a = 0; a < A; ++a) vit[(long)k * A + a] = (k < kmt[a]) ? 1.0 : 0.0;
+
+  auto C = [&](int k, int j, int i) { return (long)k * A + (long)j * imt + i; };
+  auto Q = [&](int j, int i) { return (long)j * imt + i; };
+
+  std::fill(o.at00.begin(), o.at00.end(), 0.0);
+  std::fill(o.atmax.begin(), o.atmax.end(), 0.0);
+  std::fill(o.atmin.begin(), o.atmin.end(), 0.0);
+  std::fill(o.uk.begin(), o.uk.end(), 0.0);
+  std::fill(o.vk.begin(), o.vk.end(), 0.0);
+
+  // tracer_1_0: h0f *= onbc; stf = mean sea level of the two time levels
+  for (long a = 0; a < A; ++a) {
+    h0f[a] = h0f[a] * p.onbc;
+    stf[a] = 0.5 * h0f[a] + 0.5 * h0l[a];
+  }
+  // tracer_1: scale utf/vtf, time-mean velocities, T->U interpolation of stf
+#pragma omp parallel for
+  for (int k = 0; k < km; ++k)
+    for (int j = 0; j < jmt; ++j)
+      for (int i = 0; i < imt; ++i) {
+        const long c = C(k, j, i);
+        utf[c] = utf[c] * p.oncc;
+        vtf[c] = vtf[c] * p.oncc;
+        wkd[c] = 0.5 * utf[c] + 0.5 * utl[c];
+        wkb[c] = 0.5 * vtf[c] + 0.5 * vtl[c];
+        wka[c] = 0.0;
+      }
+  for (int j = 0; j < jmt; ++j)
+    for (int i = 0; i < imt; ++i) {
+      double v = 0.0;
+      if (j < jmt - 1 && i >= 1)
+        v = au0[Q(j, i)] * stf[Q(j, i)] + aus[Q(j, i)] * stf[Q(j + 1, i)] + auw[Q(j, i)] * stf[Q(j, i - 1)] +
+            ausw[Q(j, i)] * stf[Q(j + 1, i - 1)];
+      work[Q(j, i)] = v;
+    }
+  // upwell_2: U-point velocities corrected for the free surface
+#pragma omp parallel for
+  for (int k = 0; k < km; ++k)
+    for (int j = 0; j < jmt - 1; ++j)
+      for (int i = 1; i < imt; ++i) {
+        const long c = C(k, j, i);
+        uk[c] = (1.0 + work[Q(j, i)] * ohbu[Q(j, i)]) * wkd[c];
+        vk[c] = (1.0 + work[Q(j, i)] * ohbu[Q(j, i)]) * wkb[c];
+      }
+  // operators_div: horizontal divergence on T cells above the bottom
+#pragma omp parallel for
+  for (int k = 0; k < km; ++k)
+    for (int j = 1; j < jmt; ++j)
+      for (int i = 0; i < imt - 1; ++i) {
+        if (!(k <= kmt[Q(j, i)] - 1)) continue;
+        const double east = (uk[C(k, j, i + 1)] + uk[C(k, j - 1, i + 1)]) * htw[Q(j, i + 1)];
+        const double west = (uk[C(k, j, i)] + uk[C(k, j - 1, i)]) * htw[Q(j, i)];
+        const double south = (vk[C(k, j, i + 1)] + vk[C(k, j, i)]) * hts[Q(j, i)];
+        const double north = (vk[C(k, j - 1, i + 1)] + vk[C(k, j - 1, i)]) * hts[Q(j - 1, i)];
+        wka[C(k, j, i)] = 0.5 * (east - west + south - north) * tarea_r[Q(j, i)];
+      }
+  // upwell_3 / upwell_4: column divergence, w by upward integration, rescale
+#pragma omp parallel for
+  for (int j = 0; j < jmt; ++j)
+    for (int i = 0; i < imt; ++i) {
+      const long a = Q(j, i);
+      work[a] = 0.0;
+      if (!(j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1)) continue;
+      for (int k = 0; k < km; ++k) work[a] = work[a] - dzp[k] * wka[k * A + a] * vit[k * A + a];
+      for (int k = 1; k < km; ++k)
+        ws[k * A + a] = vit[k * A + a] * (ws[(k - 1) * A + a] + dzp[k - 1] * (work[a] * ohbt[a] + wka[(k - 1) * A + a]));
+      work[a] = 1.0 / (1.0 + stf[a] * ohbt[a]);
+      for (int k = 1; k < km; ++k) ws[k * A + a] = ws[k * A + a] * work[a];
+    }
+  o.ist += 1;
+
+  for (int n = 0; n < 2; ++n) {
+    const double* atn = at + n * F;
+    double* atbn = atb + n * FB;
+    std::fill(o.tf.begin(), o.tf.end(), 0.0);
+    std::fill(o.adv_tt.begin(), o.adv_tt.end(), 0.0);
+    // advection_tracer_1_0 (tspas): face transports
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 0; j < jmt; ++j)
+        for (int i = 0; i < imt; ++i) {
+          if (i >= 1 && i < imt - 1) vs[C(k, j, i)] = (wkb[C(k, j, i)] + wkb[C(k, j, i + 1)]) * hts[Q(j, i)] * 0.25;
+          if (j >= 1 && j < jmt - 1) uw[C(k, j, i)] = (wkd[C(k, j - 1, i)] + wkd[C(k, j, i)]) * htw[Q(j, i)] * 0.25;
+        }
+    // advection_tracer_2: predictor at00 and masked 7-point extrema
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 1; j < jmt - 1; ++j)
+        for (int i = 1; i < imt - 1; ++i) {
+          const long c = C(k, j, i), a = Q(j, i);
+          const double tr = tarea_r[a];
+          const double x0 = (atn[c + 1] + atn[c]) * uw[c + 1] * tr - (atn[c] + atn[c - 1]) * uw[c] * tr;
+          const double y0 = ((atn[c + imt] + atn[c]) * vs[c] - (atn[c] + atn[c - imt]) * vs[c - imt]) * tr;
+          const double xy1 = -dts * (atn[c + 1] - atn[c]) * 2.0 * tr * uw[c + 1] * uw[c + 1] / (htw[a + 1] * hun[a + 1]);
+          const double xy2 = dts * (atn[c] - atn[c - 1]) * 2.0 * tr * uw[c] * uw[c] / (htw[a] * hun[a]);
+          const double xy3 = -dts * (atn[c + imt] - atn[c]) * 2.0 * tr * vs[c] * vs[c] / (hts[a] * hue[a]);
+          const double xy4 = dts * (atn[c] - atn[c - imt]) * 2.0 * tr * vs[c - imt] * vs[c - imt] / (hts[a - imt] * hue[a - imt]);
+          const double cx = -atn[c] * (uw[c + 1] - uw[c]) * tr * 2.0;
+          const double cy = -atn[c] * (vs[c] - vs[c - imt]) * tr * 2.0;
+          double za, zb1, zb2, zc;
+          if (k == 0) {
+            za = -0.5 * odzp[0] * ws[A + a] * (atn[A + a] + atn[a]);
+            zb1 = 0.0;
+            zb2 = 0.5 * odzp[0] * ws[A + a] * ws[A + a] * odzt[1] * (atn[a] - atn[A + a]) * dts;
+            zc = odzp[0] * atn[a] * ws[A + a];
+          } else if (k == km - 1) {
+            za = 0.5 * odzp[km - 1] * ws[c] * (atn[c] + atn[c - A]);
+            zb1 = -0.5 * odzp[km - 1] * ws[c] * ws[c] * odzt[km - 1] * (atn[c - A] - atn[c]) * dts;
+            zb2 = 0.0;
+            zc = -odzp[km - 1] * atn[c] * ws[c];
+          } else {
+            za = 0.5 * odzp[k] * ws[c] * (atn[c] + atn[c - A]) - 0.5 * odzp[k] * ws[c + A] * (atn[c] + atn[c + A]);
+            zb1 = -0.5 * odzp[k] * ws[c] * ws[c] * odzt[k] * (atn[c - A] - atn[c]) * dts;
+            zb2 = 0.5 * odzp[k] * ws[c + A] * ws[c + A] * odzt[k + 1] * (atn[c] - atn[c + A]) * dts;
+            zc = -odzp[k] * atn[c] * (ws[c] - ws[c + A]);
+          }
+          const double xx = -(x0 + xy1 + xy2 + cx);
+          const double yy = -(y0 + xy3 + xy4 + cy);
+          const double zz = -(zb1 + zb2 + za + zc);
+          at00[c] = atn[c] + (xx + yy + zz) * dts;
+          // masked extrema: land contributes -1e10 to the max, +1e10 to the min
+          auto mx = [&](long q) { return atn[q] * vit[q] + (1.0 - vit[q]) * -1.0e10; };
+          auto mn = [&](long q) { return atn[q] * vit[q] + (1.0 - vit[q]) * 1.0e10; };
+          const long nb[4] = {c - imt, c + imt, c - 1, c + 1};
+          double vmax = mx(c), vmin = mn(c);
+          for (long q : nb) { const double v = mx(q); if (vmax < v) vmax = v; }
+          for (long q : nb) { const double v = mn(q); if (vmin > v) vmin = v; }
+          if (k == 0) {
+            const double v = mx(c + A); if (vmax < v) vmax = v;
+            const double w = mn(c + A); if (vmin > w) vmin = w;
+          } else if (k == km - 1) {
+            const double v = mx(c - A); if (vmax < v) vmax = v;
+            const double w = mn(c - A); if (vmin > w) vmin = w;
+          } else {
+            const double v = mx(c - A); if (vmax < v) vmax = v;
+            const double w = mn(c - A); if (vmin > w) vmin = w;
+            const double v2 = mx(c + A); if (vmax < v2) vmax = v2;
+            const double w2 = mn(c + A); if (vmin > w2) vmin = w2;
+          }
+          atmax[c] = vmax;
+          atmin[c] = vmin;
+        }
+    // advection_tracer_3: limited fluxes (upwind where the predictor leaves
+    // the local bounds at this cell or the neighbour across the face)
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 1; j < jmt - 1; ++j)
+        for (int i = 1; i < imt - 1; ++i) {
+          const long c = C(k, j, i), a = Q(j, i);
+          const double tr = tarea_r[a];
+          auto out = [&](long q) { return at00[q] > atmax[q] || at00[q] < atmin[q]; };
+          const bool self = out(c);
+          const bool edge_k = (k == 0 || k == km - 1);
+          // horizontal faces: at the top and bottom level the neighbour test is
+          // guarded alone; at inner levels the guard covers the whole test
+          auto lim = [&](long q, bool guard) { return edge_k ? (self || (out(q) && guard)) : ((self || out(q)) && guard); };
+          double xy1, xy2, xy3, xy4, zb1, zb2;
+          if (lim(c + 1, i <= imt - 3)) xy1 = -(atn[c + 1] - atn[c]) * std::fabs(uw[c + 1]) * tr;
+          else xy1 = -dts * (atn[c + 1] - atn[c]) * 2.0 * tr * uw[c + 1] * uw[c + 1] / (htw[a + 1] * hun[a + 1]);
+          if (lim(c - 1, i >= 2)) xy2 = (atn[c] - atn[c - 1]) * std::fabs(uw[c]) * tr;
+          else xy2 = dts * (atn[c] - atn[c - 1]) * 2.0 * tr * uw[c] * uw[c] / (htw[a] * hun[a]);
+          if (lim(c + imt, j <= jmt - 3)) xy3 = -(atn[c + imt] - atn[c]) * std::fabs(vs[c]) * tr;
+          else xy3 = -dts * (atn[c + imt] - atn[c]) * 2.0 * tr * vs[c] * vs[c] / (hts[a] * hue[a]);
+          if (lim(c - imt, j >= 2)) xy4 = (atn[c] - atn[c - imt]) * std::fabs(vs[c - imt]) * tr;
+          else xy4 = dts * (atn[c] - atn[c - imt]) * 2.0 * tr * vs[c - imt] * vs[c - imt] / (hts[a - imt] * hue[a - imt]);
+          double za, zc;
+          if (k == 0) {
+            zb1 = 0.0;
+            if (self || (out(c + A) && k <= km - 2)) zb2 = 0.5 * std::fabs(ws[c + A]) * odzp[k] * (atn[c] - atn[c + A]);
+            else zb2 = 0.5 * odzp[0] * ws[A + a] * ws[A + a] * odzt[1] * (atn[a] - atn[A + a]) * dts;
+            za = -0.5 * odzp[0] * ws[A + a] * (atn[A + a] + atn[a]);
+            zc = odzp[0] * atn[a] * ws[A + a];
+          } else if (k == km - 1) {
+            if (self || out(c - A)) zb1 = -0.5 * std::fabs(ws[c]) * odzp[k] * (atn[c - A] - atn[c]);
+            else zb1 = -0.5 * odzp[k] * ws[c] * ws[c] * odzt[k] * (atn[c - A] - atn[c]) * dts;
+            zb2 = 0.0;
+            za = 0.5 * odzp[km - 1] * ws[c] * (atn[c] + atn[c - A]);
+            zc = -odzp[km - 1] * atn[c] * ws[c];
+          } else {
+            if ((self || out(c - A)) && k >= 1) zb1 = -0.5 * std::fabs(ws[c]) * odzp[k] * (atn[c - A] - atn[c]);
+            else zb1 = -0.5 * odzp[k] * ws[c] * ws[c] * odzt[k] * (atn[c - A] - atn[c]) * dts;
+            if ((self || out(c + A)) && k <= km - 2) zb2 = 0.5 * std::fabs(ws[c + A]) * odzp[k] * (atn[c] - atn[c + A]);
+            else zb2 = 0.5 * odzp[k] * ws[c + A] * ws[c + A] * odzt[k + 1] * (atn[c] - atn[c + A]) * dts;
+            za = 0.5 * odzp[k] * ws[c] * (atn[c] + atn[c - A]) - 0.5 * odzp[k] * ws[c + A] * (atn[c] + atn[c + A]);
+            zc = -odzp[k] * atn[c] * (ws[c] - ws[c + A]);
+          }
+          const double cx = -atn[c] * (uw[c + 1] - uw[c]) * tr * 2.0;
+          const double cy = -atn[c] * (vs[c] - vs[c - imt]) * tr * 2.0;
+          const double x0 = (atn[c + 1] + atn[c]) * uw[c + 1] * tr - (atn[c] + atn[c - 1]) * uw[c] * tr;
+          const double y0 = ((atn[c + imt] + atn[c]) * vs[c] - (atn[c] + atn[c - imt]) * vs[c - imt]) * tr;
+          const double xx = -(x0 + xy1 + xy2 + cx);
+          const double yy = -(y0 + xy3 + xy4 + cy);
+          const double zz = -(za + zb1 + zb2 + zc);
+          adv_tt[c] = xx + yy + zz;
+          ax[n * F + c] = xx;
+          ay[n * F + c] = yy;
+          az[n * F + c] = zz;
+        }
+    // tracer_del4_1: first masked Laplacian of atb, scaled by ahf
+    std::fill(o.d2tk.begin(), o.d2tk.end(), 0.0);
+    auto lap = [&](const double* fld, long c, long a, int k) {
+      double h = 0.0, cc = 0.0;
+      if (k <= kmt[a] - 1) {
+        if (k <= kmtn[a] - 1) { h += dtn[a] * fld[c - imt]; cc -= dtn[a]; }
+        if (k <= kmts[a] - 1) { h += dts_c[a] * fld[c + imt]; cc -= dts_c[a]; }
+        if (k <= kmte[a] - 1) { h += dte[a] * fld[c + 1]; cc -= dte[a]; }
+        if (k <= kmtw[a] - 1) { h += dtw[a] * fld[c - 1]; cc -= dtw[a]; }
+      }
+      return std::pair<double, double>(h, cc);
+    };
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 1; j < jmt - 1; ++j)
+        for (int i = 1; i < imt - 1; ++i) {
+          const long c = C(k, j, i), a = Q(j, i);
+          const double* lvl = atbn + A;  // tracer level k lives at atb level k+1
+          auto hc = lap(lvl, c, a, k);
+          d2tk[c] = ahf[a] * (hc.second * lvl[c] + hc.first);
+        }
+    // tracer_del4_2: advective tendency, surface mixing floor, second Laplacian
+    double* aktn = akt + n * F;
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 1; j < jmt - 1; ++j)
+        for (int i = 1; i < imt - 1; ++i) {
+          const long c = C(k, j, i), a = Q(j, i);
+          const bool inner = (j >= 2 && j < jmt - 2 && i >= 2 && i < imt - 2);
+          if (inner) tf[c] = adv_tt[c] * vit[c];
+          if (n == 0 && aktn[a] < p.dwndmix) aktn[a] = p.dwndmix;
+          wkc[c] = aktn[c];
+          auto hc = lap(d2tk, c, a, k);
+          const double h = inner ? p.ah * (hc.second * d2tk[c] + hc.first) : 0.0;
+          tf[c] += h;
+        }
+    // tracer_5: shortwave penetration (T), explicit half of vertical
+    // diffusion (aidif = 0.5), salt surface flux (S)
+    const double aidif = 0.5;
+#pragma omp parallel for
+    for (int j = 2; j < jmt - 2; ++j)
+      for (int i = 2; i < imt - 2; ++i) {
+        const long a = Q(j, i);
+        if (n == 0) {
+          for (int k = 1; k < km - 1; ++k) {
+            const long c = C(k, j, i);
+            const double w1 = swv[a] * pen[k - 1] * vit[c];
+            const double w2 = swv[a] * pen[k] * vit[c + A];
+            tf[c] = tf[c] + (w1 - w2) * odzp[k];
+            penetrate[c] = (w1 - w2) * odzp[k];
+          }
+          const double w1 = swv[a] * pen[0] * vit[A + a];
+          const double w2 = swv[a] * pen[km - 2] * vit[(km - 1) * A + a];
+          tf[a] = tf[a] - odzp[0] * w1;
+          tf[(km - 1) * A + a] = tf[(km - 1) * A + a] + odzp[km - 1] * w2;
+          penetrate[a] = -w1 * odzp[0];
+          penetrate[(km - 1) * A + a] = w2 * odzp[km - 1];
+        }
+        for (int k = 1; k < km - 1; ++k) {
+          const long c = C(k, j, i);
+          const double w1 = wkc[c - A] * (atbn[c] - atbn[c + A]) * odzt[k] * vit[c];
+          const double w2 = wkc[c] * (atbn[c + A] - atbn[c + 2 * A]) * odzt[k + 1] * vit[c + A];
+          tf[c] = tf[c] + odzp[k] * (w1 - w2) * 0.5;
+          dzd[n * F + c] = odzp[k] * (w1 - w2) * 0.5;
+        }
+        const double w1 = wkc[a] * (atbn[A + a] - atbn[2 * A + a]) * odzt[1] * vit[A + a];
+        const double w2 = wkc[(km - 2) * A + a] * (atbn[(km - 1) * A + a] - atbn[km * A + a]) * odzt[km - 1] *
+                          vit[(km - 1) * A + a];
+        tf[a] = tf[a] - odzp[0] * w1 * 0.5;
+        tf[(km - 1) * A + a] = tf[(km - 1) * A + a] + odzp[km - 1] * w2 * (1.0 - aidif);
+        dzd[n * F + a] = -odzp[0] * w1 * 0.5;
+        dzd[n * F + (km - 1) * A + a] = odzp[km - 1] * w2 * 0.5;
+      }
+    if (n == 1) {
+      const double* atbS_top = atb + FB + A;   // S at the surface, previous time level
+      for (int j = 0; j < jmt; ++j)
+        for (int i = 0; i < imt; ++i) {
+          const long a = Q(j, i);
+          if (kmt[a] > 0) {
+            stf[a] = fresh[a] * 34.7 * p.od0 / 1000.0 + p.gamma * (sss[a] - atbS_top[a]) * seaice[a] / odzp[0] +
+                     p.gamma * 30.0 / 365.0 / 4.0 * 50.0 * (sss[a] - atbS_top[a]) / odzp[0] * (1.0 - seaice[a]);
+            tf[a] = tf[a] + stf[a] * (1.0 - aidif) * odzp[0];
+            net[A + a] = stf[a] * odzp[0];
+          }
+          temp11[a] = tarea[a] * net[A + a] * vit[a];
+        }
+    }
+    // SSS normalisation: global salt flux removed uniformly (mpi3.F90:26)
+    double err_norm2 = 0.0;
+    if (n == 1) {
+      double err_norm1 = 0.0;
+      for (int j = 2; j < jmt - 2; ++j)
+        for (int i = 2; i < imt - 2; ++i) err_norm1 = err_norm1 + temp11[Q(j, i)];
+      err_norm2 = -err_norm1 / p.area_t;
+      o.fw_norm2 = err_norm2;
+    }
+    // tracer_6: SSS norm (S); heat flux, its half-step tendency and net (T)
+    for (int j = 0; j < jmt; ++j)
+      for (int i = 0; i < imt; ++i) {
+        const long a = Q(j, i);
+        if (n == 1) {
+          tf[a] = tf[a] + err_norm2 * vit[a];
+        } else if (kmt[a] > 0) {
+          stf[a] = ((swv[a] + nswv[a]) * p.od0cp + seaice[a] * p.gamma * (sst[a] - atb[A + a]) / odzp[0]);
+          tf[a] = tf[a] + stf[a] * odzp[0] * 0.5;
+          net[a] = stf[a] * odzp[0];
+        }
+      }
+    halo_r8(net, 2, imt, jmt, o.ew_cyclic, o.tripole);
+    // tracer_7: restoring (boundary_restore == 1), 15-day time scale
+    if (p.boundary_restore == 1) {
+      const double lamda = 1.0 / (15.0 * 86400.0);
+#pragma omp parallel for
+      for (int k = 1; k < km; ++k)
+        for (int j = 2; j < jmt - 2; ++j)
+          for (int i = 2; i < imt - 2; ++i) {
+            const long c = C(k, j, i);
+            tf[c] = tf[c] + vit[c] * (restore[n * F + c] - atbn[c + A]) * lamda;
+          }
+    }
+    // tracer_8: explicit update into vtl (used as scratch), copy to ori
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 0; j < jmt; ++j)
+        for (int i = 0; i < imt; ++i) {
+          const long c = C(k, j, i);
+          if (j >= 2 && j < jmt - 2 && i >= 2 && i < imt - 2) vtl[c] = atn[c] + dts * tf[c];
+          ori[c] = vtl[c];
+        }
+    // invtrit: implicit half of vertical diffusion, Thomas sweep per column
+#pragma omp parallel for
+    for (int j = 2; j < jmt - 2; ++j) {
+      std::vector<double> a8(km), b8(km), c8(km), d8(km), e8(km + 1), f8(km + 1);
+      for (int i = 2; i < imt - 2; ++i) {
+        const long a = Q(j, i);
+        const int kz = kmt[a];
+        if (kz <= 0) continue;
+        for (int k = 1; k < kz; ++k) {
+          a8[k] = wkc[(k - 1) * A + a] * odzt[k] * odzp[k] * dts * 0.5;
+          d8[k] = vtl[k * A + a];
+        }
+        for (int k = 1; k < kz - 1; ++k) {
+          c8[k] = wkc[k * A + a] * odzt[k + 1] * odzp[k] * dts * 0.5;
+          b8[k] = 1.0 + a8[k] + c8[k];
+          e8[k] = 0.0;
+          f8[k] = 0.0;
+        }
+        a8[0] = odzp[0] * dts * 0.5;
+        c8[0] = wkc[a] * odzt[1] * odzp[0] * dts * 0.5;
+        b8[0] = 1.0 + c8[0];
+        d8[0] = vtl[a];
+        e8[0] = 0.0;
+        f8[0] = 0.0;
+        b8[kz - 1] = 1.0 + a8[kz - 1];
+        c8[kz - 1] = odzp[kz - 1] * dts * 0.5;
+        e8[kz] = 0.0;
+        f8[kz] = 0.0;
+        for (int k = kz - 1; k >= 0; --k) {
+          const double g0 = 1.0 / (b8[k] - c8[k] * e8[k + 1]);
+          e8[k] = a8[k] * g0;
+          f8[k] = (d8[k] + c8[k] * f8[k + 1]) * g0;
+        }
+        vtl[a] = (e8[0] * stf[a] + f8[0]) * vit[a];
+        for (int k = 1; k < kz; ++k) vtl[k * A + a] = (e8[k] * vtl[(k - 1) * A + a] + f8[k]) * vit[k * A + a];
+      }
+    }
+    halo_r8(vtl, km, imt, jmt, o.ew_cyclic, o.tripole);
+    // tracer_9: diagnostics and state update (all points incl. ghosts)
+#pragma omp parallel for
+    for (int k = 0; k < km; ++k)
+      for (int j = 0; j < jmt; ++j)
+        for (int i = 0; i < imt; ++i) {
+          const long c = C(k, j, i), a = Q(j, i);
+          if (k == 0) dt_diff[n * F + c] = (vtl[c] - ori[c]) / dts * vit[c] - stf[a] * 0.5 * odzp[0];
+          else dt_diff[n * F + c] = (vtl[c] - ori[c]) / dts * vit[c];
+          tend[n * F + c] = (vtl[c] - at[n * F + c]) / dts * vit[c];
+          at[n * F + c] = vtl[c];
+          atbn[c + A] = at[n * F + c];
+        }
+  }
+}
+
+// convadj_cu: per-column convective adjustment (convadj.cpp:29-288)
+void convadj_call(Oracle& o) {
+  const int km = o.km, imt = o.imt, jmt = o.jmt;
+  const long A = o.A, F = o.F, FB = o.FB;
+  double* at = o.fd[LT_F_AT].data();
+  double* atb = o.fd[LT_F_ATB].data();
+  double* tend = o.fd[LT_F_TEND].data();
+  double* dt_conv = o.fd[LT_F_DT_CONV].data();
+  const double* to = o.fd[LT_F_TO].data();
+  const double* so = o.fd[LT_F_SO].data();
+  const double* cc = o.fd[LT_F_C].data();
+  const double* dzp = o.fd[LT_F_DZP].data();
+  const int* kmt = o.fi[LT_F_KMT].data();
+  const double c2dtts = o.p.dts;
+  auto rho = [&](double t, double s, int l) {  // l: 0-based level of the coefficients
+    return (cc[l] + (cc[3 * km + l] + cc[6 * km + l] * s) * s + (cc[2 * km + l] + cc[7 * km + l] * s + cc[5 * km + l] * t) * t) * t +
+           (cc[1 * km + l] + (cc[4 * km + l] + cc[8 * km + l] * s) * s) * s;
+  };
+#pragma omp parallel for
+  for (int j = 0; j < jmt; ++j) {
+    std::vector<double> rhoup(km, 0.0), rholo(km, 0.0);
+    for (int i = 0; i < imt; ++i) {
+      const long a = (long)j * imt + i;
+      auto T = [&](int l) -> double& { return at[(long)l * A + a]; };       // l 0-based level
+      auto S = [&](int l) -> double& { return at[F + (long)l * A + a]; };
+      const int kcon = kmt[a];
+      std::fill(rhoup.begin(), rhoup.end(), 0.0);
+      std::fill(rholo.begin(), rholo.end(), 0.0);
+      if (kcon != 0) {
+        int lcon = 0;
+        for (int l = 0; l < km - 1; ++l) {
+          const int l1 = l + 1;
+          rhoup[l1] = rho(T(l1) - to[l1], S(l1) - so[l1], l1);
+          rholo[l] = rho(T(l) - to[l1], S(l) - so[l1], l1);
+        }
+        for (int k = kcon - 1; k >= 1; --k)
+          if (rholo[k - 1] > rhoup[k]) lcon = k;
+        if (lcon != 0) {
+          // levels below are 1-based as in the reference's mixing loops
+          for (;;) {
+            int lcona = lcon, lconb = lcon + 1;
+            double dztsum = dzp[lcona - 1] + dzp[lconb - 1];
+            double trasum[2];
+            for (int n = 0; n < 2; ++n) {
+              double* X = at + n * F;
+              trasum[n] = X[(long)(lcona - 1) * A + a] * dzp[lcona - 1] + X[(long)(lconb - 1) * A + a] * dzp[lconb - 1];
+              const double tramix = trasum[n] / dztsum;
+              X[(long)(lcona - 1) * A + a] = tramix;
+              X[(long)(lconb - 1) * A + a] = tramix;
+            }
+            for (;;) {  // grow the mixed layer down or up while unstable
+              if (lconb != kcon) {
+                const int l1 = lconb + 1;
+                rholo[lconb - 1] = rho(T(lconb - 1) - to[l1 - 1], S(lconb - 1) - so[l1 - 1], l1 - 1);
+                if (rholo[lconb - 1] > rhoup[l1 - 1]) {
+                  lconb = lconb + 1;
+                  dztsum = dztsum + dzp[lconb - 1];
+                  for (int n = 0; n < 2; ++n) {
+                    double* X = at + n * F;
+                    trasum[n] = trasum[n] + X[(long)(lconb - 1) * A + a] * dzp[lconb - 1];
+                    const double tramix = trasum[n] / dztsum;
+                    for (int lm = lcona - 1; lm < lconb; ++lm) X[(long)lm * A + a] = tramix;
+                  }
+                  continue;
+                }
+              }
+              if (lcona > 1) {
+                const int l1 = lcona - 1;
+                rholo[l1 - 1] = rho(T(l1 - 1) - to[lcona - 1], S(l1 - 1) - so[lcona - 1], lcona - 1);
+                rhoup[lcona - 1] = rho(T(lcona - 1) - to[lcona - 1], S(lcona - 1) - so[lcona - 1], lcona - 1);
+                if (rholo[lcona - 2] > rhoup[lcona - 1]) {
+                  lcona = lcona - 1;
+                  dztsum = dztsum + dzp[lcona - 1];
+                  for (int n = 0; n < 2; ++n) {
+                    double* X = at + n * F;
+                    trasum[n] = trasum[n] + X[(long)(lcona - 1) * A + a] * dzp[lcona - 1];
+                    const double tramix = trasum[n] / dztsum;
+                    for (int lm = lcona; lm <= lconb; ++lm) X[(long)(lm - 1) * A + a] = tramix;
+                  }
+                  continue;
+                }
+              }
+              break;
+            }
+            if (lconb == kcon) break;
+            lcon = lconb;
+            bool done = false;
+            for (;;) {  // search deeper for the next unstable interface
+              lcon = lcon + 1;
+              if (lcon == kcon) { done = true; break; }
+              if (rholo[lcon - 1] <= rhoup[lcon]) continue;
+              break;
+            }
+            if (done) break;
+          }
+        }
+      }
+      // (convadj.cpp:258-276) tendency diagnostics and atb = at, for every column
+      for (int n = 0; n < 2; ++n)
+        for (int k = 0; k < km; ++k) {
+          const long c = n * F + (long)k * A + a;
+          const double vitk = (k < kmt[a]) ? 1.0 : 0.0;
+          dt_conv[c] = (at[c] - atb[n * FB + (long)(k + 1) * A + a]) / c2dtts * vitk;
+          tend[c] += dt_conv[c];
+          atb[n * FB + (long)(k + 1) * A + a] = at[c];
+        }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void* or_create(int nx, int ny, int km) {
+  if (nx < 4 || ny < 4 || km < 3) return nullptr;
+  return new Oracle(nx, ny, km);
+}
+void or_destroy(void* h) { delete static_cast<Oracle*>(h); }
+int or_set_params(void* h, const lt_params* p, int ew_cyclic, int tripole) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  o.p = *p; o.ew_cyclic = ew_cyclic; o.tripole = tripole;
+  return 0;
+}
+long or_field_count(void* h, int f) {
+  if (f < 0 || f >= LT_F_COUNT) return -1;
+  return static_cast<Oracle*>(h)->count(f);
+}
+int or_set_field(void* h, int f, const void* src, size_t nbytes) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  if (f < 0 || f >= LT_F_COUNT) return LT_E_INVALID;
+  const bool isint = field_info(f).is_int;
+  const size_t need = (size_t)o.count(f) * (isint ? sizeof(int) : sizeof(double));
+  if (nbytes != need) return LT_E_INVALID;
+  if (isint) std::memcpy(o.fi[f].data(), src, nbytes);
+  else std::memcpy(o.fd[f].data(), src, nbytes);
+  return 0;
+}
+int or_get_field(void* h, int f, void* dst, size_t nbytes) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  if (f < 0 || f >= LT_F_COUNT) return LT_E_INVALID;
+  const bool isint = field_info(f).is_int;
+  const size_t need = (size_t)o.count(f) * (isint ? sizeof(int) : sizeof(double));
+  if (nbytes != need) return LT_E_INVALID;
+  if (isint) std::memcpy(dst, o.fi[f].data(), nbytes);
+  else std::memcpy(dst, o.fd[f].data(), nbytes);
+  return 0;
+}
+// One literal tracer_ call: utf/vtf/h0f are scaled in place and vtl is left
+// holding S, as in the reference.
+int or_tracer_call(void* h) {
+  tracer_call(*static_cast<Oracle*>(h));
+  return 0;
+}
+// nsteps steps with frozen dynamics: before each step utf, vtf, utl, vtl, h0f
+// are restored from the given copies (the model's bclinc/barotr would supply
+// fresh ones), then one tracer_ call runs; afterwards UTF/VTF/H0F hold the
+// scaled values of the last step, copied to the *_OUT fields.
+int or_step(void* h, int nsteps) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const std::vector<double> utf0 = o.fd[LT_F_UTF], vtf0 = o.fd[LT_F_VTF], utl0 = o.fd[LT_F_UTL],
+                            vtl0 = o.fd[LT_F_VTL], h0f0 = o.fd[LT_F_H0F];
+  for (int s = 0; s < nsteps; ++s) {
+    o.fd[LT_F_UTF] = utf0; o.fd[LT_F_VTF] = vtf0; o.fd[LT_F_UTL] = utl0; o.fd[LT_F_VTL] = vtl0;
+    o.fd[LT_F_H0F] = h0f0;
+    tracer_call(o);
+  }
+  o.fd[LT_F_UTF_OUT] = o.fd[LT_F_UTF];
+  o.fd[LT_F_VTF_OUT] = o.fd[LT_F_VTF];
+  o.fd[LT_F_H0F_OUT] = o.fd[LT_F_H0F];
+  o.fd[LT_F_UTF] = utf0; o.fd[LT_F_VTF] = vtf0; o.fd[LT_F_VTL] = vtl0; o.fd[LT_F_H0F] = h0f0;
+  return 0;
+}
+int or_convadj(void* h) {
+  convadj_call(*static_cast<Oracle*>(h));
+  return 0;
+}
+double or_fw_norm2(void* h) { return static_cast<Oracle*>(h)->fw_norm2; }
+// sum(tarea*dzp*vit*tracer) over the interior, sequential order
+int or_tracer_content(void* h, double* out2) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const double* at = o.fd[LT_F_AT].data();
+  for (int n = 0; n < 2; ++n) {
+    double s = 0.0;
+    for (int k = 0; k < o.km; ++k)
+      for (int j = 2; j < o.jmt - 2; ++j)
+        for (int i = 2; i < o.imt - 2; ++i) {
+          const long a = (long)j * o.imt + i;
+          if (k < o.fi[LT_F_KMT][a]) s += o.fd[LT_F_TAREA][a] * o.fd[LT_F_DZP][k] * at[n * o.F + (long)k * o.A + a];
+        }
+    out2[n] = s;
+  }
+  return 0;
+}
+// standalone halo (tests): nz levels of [jmt][imt]
+int or_halo(double* a, int nz, int imt, int jmt, int ew_cyclic, int tripole) {
+  halo_r8(a, nz, imt, jmt, ew_cyclic, tripole);
+  return 0;
+}
+int or_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+}  // extern "C"
