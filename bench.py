@@ -1,0 +1,325 @@
+"""Benchmark: LICOM3 baroclinic tracer step on B200.
+
+Metric: tracer cell-steps/s (nx*ny*km physical cells, land included, halo
+excluded, both T and S advanced per step) on the 0.1-degree grid
+3600 x 2302 x 55, seeded synthetic inputs of that shape (no NetCDF here).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--impl ours|reference] [--grid NX NY KM]
+
+One JSON line on rank 0.  Under torchrun each rank advances an independent
+replica of the domain on its own GPU (the path has no cross-domain exchange on
+one device: replicas only, weak scaling); the timed region is bracketed by a
+barrier and a device synchronize and the max over ranks is reported.
+``--impl reference`` times the reference algorithm on the host cores (the FP64
+CPU restatement, bit-exact with the reference's own tracer.cpp) on a bounded
+sample of the same workload.
+"""
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(REPO, "licom3-hip_b200")
+PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# algorithmic bytes per cell-step (compulsory traffic of the whole step, both
+# tracers; 2-D/1-D coefficients not counted) and of the fused column kernel
+STEP_BYTES = {"fp64": 136.0, "mixed": 100.0}
+TRACER_KERNEL_BYTES = {"fp64": 104.0, "mixed": 80.0}
+
+
+def load_package():
+    if "licom3_hip_b200" in sys.modules:
+        return sys.modules["licom3_hip_b200"]
+    spec = importlib.util.spec_from_file_location("licom3_hip_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["licom3_hip_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--grid", type=int, nargs=3, default=[3600, 2302, 55])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
+    return ap.parse_args()
+
+
+def workload(args):
+    nx, ny, km = args.grid
+    deep = km >= 50
+    return dict(nx=nx, ny=ny, km=km, umax=0.3 if deep else 0.1, dz_top=5.0 if deep else 10.0,
+                dz_bot=300.0 if deep else 250.0, cap_north=0, forced=1)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(PEAKS) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_rate(lt, args, steps, warmup, budget_s=20.0):
+    """The reference algorithm on the host: the FP64 CPU restatement
+    (oracle/licom_oracle.cpp, OpenMP over all host cores), which is bit-exact
+    with the reference's own tracer.cpp compiled for the CPU.  Runs on a
+    bounded sample of the workload: the same generators on a patch of the
+    grid with the full column depth.  Returns (cell-steps/s, details)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle
+    cores = cpu_cores()
+    nx, ny, km = args.grid
+    w = workload(args)
+    snx, sny = max(72, nx // 5), max(48, ny // 5)
+    snx += snx % 2
+    syn = lt.Synth(snx, sny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+    fields = syn.all_fields()
+    o = pyoracle.Oracle(snx, sny, km, syn.params, threads=cores)
+    o.load(fields)
+    o.sum_order(0)
+    for _ in range(warmup):
+        o.step(1)
+    done, t_total = 0, 0.0
+    while done < steps:
+        t0 = time.perf_counter()
+        o.step(1)
+        t_total += time.perf_counter() - t0
+        done += 1
+        if t_total > budget_s:
+            break
+    cells = snx * sny * km
+    rate = cells * done / t_total
+    sample = "%dx%dx%d patch (1/25 of the horizontal grid, full depth), %d step(s) after %d warm-up" % (
+        snx, sny, km, done, warmup)
+    return rate, {"unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": sample,
+                  "value": rate}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def reduce_max(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda:%d" % local)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        pg.barrier()
+        torch.cuda.synchronize(local)
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    lt = load_package()
+    if rank == 0:
+        rate, cb = cpu_reference_rate(lt, args, args.steps, args.warmup, budget_s=120.0)
+        nx, ny, km = args.grid
+        line = {"impl": "reference", "metric": "tracer cell-steps/s (0.1deg 3600x2302x55, FP64)", "value": rate,
+                "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": nx * ny * km / rate * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators, configuration shapes)",
+                "config": {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
+                           "device": "host cores"},
+                "cpu_baseline": cb,
+                "e2e": {"value": rate, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_ours(args):
+    world, rank, local, pg = dist_setup(args)
+    lt = load_package()
+    lt.set_device(local)
+    nx, ny, km = args.grid
+    w = workload(args)
+    prec = lt.PREC_MIXED if args.precision == "mixed" else lt.PREC_FP64
+    syn = lt.Synth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+    dom = syn.domain(precision=prec)
+    cells = nx * ny * km
+
+    # ---- device-resident throughput (value)
+    dom.step(args.warmup)
+    dom.sync()
+    barrier(pg, local)
+    dom.profile(True)
+    n0 = lt.launch_count()
+    with ClockSampler(local) as clk:
+        dom.step(args.steps)
+        dom.sync()
+    launches = lt.launch_count() - n0
+    barrier(pg, local)
+    ms = reduce_max(pg, dom.last_step_ms(), local)
+    nprof, phases = dom.phase_ms()
+    dom.profile(False)
+    value = cells * args.steps * world / (ms * 1e-3)
+
+    # ---- roofline of the dominant kernel (the fused tracer column kernel)
+    hbm, hbm_kind = peaks()
+    t_tracer = phases["tracer"] / max(nprof, 1)            # ms per launch
+    kbytes = TRACER_KERNEL_BYTES[args.precision] * cells   # algorithmic bytes per launch
+    achieved = kbytes / (t_tracer * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "tracer column kernel", "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
+                "algorithmic_bytes_per_launch": kbytes, "traffic": None,
+                "step_frac": STEP_BYTES[args.precision] * cells / (ms / args.steps * 1e-3) / 1e9 / hbm,
+                "phase_ms_per_step": {k: v / max(nprof, 1) for k, v in phases.items()}}
+
+    # ---- end to end through the C ABI with host buffers: every step copies
+    # that step's surface forcing (6 fields) from pinned host memory and
+    # reads the step's fw_norm2 back
+    import torch
+    A = (nx + 4) * (ny + 4)
+    pinned = torch.empty(6 * A, dtype=torch.float64, pin_memory=True)
+    names = ("SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE")
+    for m, nm in enumerate(names):
+        pinned[m * A:(m + 1) * A] = torch.from_numpy(dom.get(nm).ravel())
+    base = pinned.data_ptr()
+    ptrs = [base + m * A * 8 for m in range(6)]
+    fw = C.c_double()
+    e2e_steps = args.e2e_steps or args.steps
+    dom.step_host_ptrs(ptrs, fw)
+    barrier(pg, local)
+    dom.mark(0)
+    for _ in range(e2e_steps):
+        dom.step_host_ptrs(ptrs, fw)
+    dom.mark(1)
+    dom.sync()
+    barrier(pg, local)
+    ms_e2e = reduce_max(pg, dom.last_step_ms(), local)
+    e2e = {"value": cells * e2e_steps * world / (ms_e2e * 1e-3), "unit": "cell-steps/s",
+           "h2d_bytes_per_step": 6 * A * 8, "d2h_bytes_per_step": 8,
+           "api": "lt_step_host (C ABI), pinned host forcing"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _, cpu = cpu_reference_rate(lt, args, 2, 0)
+
+    if rank == 0:
+        line = {"metric": "tracer cell-steps/s (0.1deg 3600x2302x55, %s)" % args.precision.upper(),
+                "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "f32 arithmetic, f64 state",
+                "data": "synthetic (seeded generators with the configuration's shapes and distributions)",
+                "config": {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
+                           "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary(), "fw_norm2": fw.value}
+        print(json.dumps(line), flush=True)
+    dom.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -132,9 +132,10 @@ int lt_derive_masks(lt_domain* dom);
 int lt_step(lt_domain* dom, int nsteps);
 /* One step taking this step's surface forcing from HOST buffers (swv, nswv,
  * sst, sss, fresh, seaice; each [jmt][imt] f64, any may be NULL to keep the
- * resident field) and returning fw_norm2 and the two global tracer integrals
- * sum(tarea*dzp*vit*tracer) to a host buffer out3 (may be NULL). */
-int lt_step_host(lt_domain* dom, const double* const forcing6[6], double* out3);
+ * resident field; pinned memory makes the copies asynchronous) and returning
+ * fw_norm2 (fw_norm2_out) and, if content2_out is not NULL, the two global
+ * tracer integrals sum(tarea*dzp*vit*tracer).  Synchronous. */
+int lt_step_host(lt_domain* dom, const double* const forcing6[6], double* fw_norm2_out, double* content2_out);
 /* Convective adjustment of the current state (convadj.cpp:29-288). */
 int lt_convadj(lt_domain* dom);
 /* Global tracer integrals sum(tarea*dzp*vit*tracer) over the interior, f64,
@@ -147,6 +148,17 @@ int lt_sync(lt_domain* dom);
 int lt_check_numeric(lt_domain* dom, long long* bad_count);
 /* Elapsed device time (ms) of the last lt_step call, CUDA events. */
 int lt_last_step_ms(lt_domain* dom, float* ms);
+/* Record the start (which = 0) or end (which = 1) event that lt_last_step_ms
+ * measures, on the domain's stream, around any sequence of calls. */
+int lt_mark(lt_domain* dom, int which);
+/* Per-phase device timing: lt_profile(dom, 1) records CUDA events around the
+ * six launch phases of each step (surface fluxes, SSS-norm sum, net halo,
+ * continuity, tracer column kernel, state halo); lt_phase_ms sums them over
+ * the recorded steps into ms[0..5] and returns the number of steps. */
+int lt_profile(lt_domain* dom, int on);
+int lt_phase_ms(lt_domain* dom, float* ms, int nphase);
+/* Kernels this library has launched in this process (all domains). */
+long long lt_launch_count(void);
 
 /* --- reference-named shims ---------------------------------------------- */
 /* Bind the domain the shims act on (the reference uses process globals). */
@@ -157,9 +169,21 @@ void tracer_(int ii);
 /* convadj.cpp:290: convective adjustment of the bound domain. */
 void convadj_(void);
 
+/* --- field metadata ------------------------------------------------------ */
+/* Upper-case name of a field id without the LT_F_ prefix ("AT", "ATB", ...). */
+const char* lt_field_name(int field);
+/* Element count of a field for physical sizes nx, ny, km; -1 if invalid. */
+long lt_field_count(int field, int nx, int ny, int km);
+/* 1 for the int32 mask fields, 0 for f64 fields. */
+int lt_field_is_int(int field);
+
 /* --- errors, device ------------------------------------------------------ */
 const char* lt_last_error(void);
 int lt_device_count(int* count);
+/* Make device dev current for this library's CUDA runtime on the calling
+ * thread (the library carries its own runtime; other runtimes in the
+ * process keep their own current device). */
+int lt_set_device(int dev);
 /* Library version/build id string. */
 const char* lt_version(void);
 

@@ -1,0 +1,331 @@
+"""LICOM3 baroclinic tracer step on B200 (sm_100a) - host-side interface.
+
+This package mirrors, in Python, the interface LICOM3-HIP's host code uses
+for the tracer path (``tracer_(ii)`` and ``convadj_()`` from stepon.cpp:69,77
+acting on device-resident state) on top of the C ABI declared in
+``include/licom_tracer.h`` and ``include/licom_synth.h``.  The compute path is
+``liblicom_tracer.so`` (hand-written CUDA for sm_100a); nothing here computes a
+tracer step on the CPU.  Importing fails loudly when the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblicom_tracer.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("liblicom_tracer.so is not built; run python licom3-hip_b200/build.py")
+
+lib = C.CDLL(LIB_PATH)
+
+LT_OK, LT_E_INVALID, LT_E_OOM, LT_E_CUDA, LT_E_NUMERIC, LT_E_TIMEOUT, LT_E_STATE, LT_E_NODEVICE = range(8)
+PREC_FP64, PREC_MIXED = 0, 1
+
+
+class LtError(RuntimeError):
+    def __init__(self, code, where):
+        msg = lib.lt_last_error().decode(errors="replace")
+        super().__init__("%s failed with status %d: %s" % (where, code, msg))
+        self.code = code
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("km", C.c_int), ("precision", C.c_int),
+                ("diagnostics", C.c_int), ("ew_cyclic", C.c_int), ("tripole", C.c_int)]
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("dts", "oncc", "onbc", "dwndmix", "gamma", "od0", "od0cp", "ah", "area_t")] + [
+        ("nss", C.c_int), ("boundary_restore", C.c_int)]
+
+
+class SynthConfig(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("km", C.c_int), ("lat_s", C.c_double), ("lat_n", C.c_double),
+                ("dz_top", C.c_double), ("dz_bot", C.c_double), ("depth", C.c_double), ("umax", C.c_double),
+                ("seed", C.c_uint64), ("forced", C.c_int), ("cap_north", C.c_int), ("cap_south", C.c_int),
+                ("ew_cyclic", C.c_int), ("tripole", C.c_int), ("land_frac", C.c_double), ("member", C.c_uint32),
+                ("tpert", C.c_double), ("ah_bihar", C.c_double)]
+
+
+_vp, _sz, _i = C.c_void_p, C.c_size_t, C.c_int
+_SIGS = {
+    "lt_create": ([C.POINTER(Grid), C.POINTER(Params), C.POINTER(_vp)], _i),
+    "lt_destroy": ([_vp], _i),
+    "lt_set_params": ([_vp, C.POINTER(Params)], _i),
+    "lt_domain_bytes": ([C.POINTER(Grid)], _sz),
+    "lt_set_field": ([_vp, _i, _vp, _sz], _i),
+    "lt_get_field": ([_vp, _i, _vp, _sz], _i),
+    "lt_set_field_device": ([_vp, _i, _vp, _sz], _i),
+    "lt_get_field_device": ([_vp, _i, _vp, _sz], _i),
+    "lt_derive_masks": ([_vp], _i),
+    "lt_step": ([_vp, _i], _i),
+    "lt_step_host": ([_vp, C.POINTER(_vp), C.POINTER(C.c_double), C.POINTER(C.c_double)], _i),
+    "lt_profile": ([_vp, _i], _i),
+    "lt_mark": ([_vp, _i], _i),
+    "lt_phase_ms": ([_vp, C.POINTER(C.c_float), _i], _i),
+    "lt_launch_count": ([], C.c_longlong),
+    "lt_set_device": ([_i], _i),
+    "lt_convadj": ([_vp], _i),
+    "lt_tracer_content": ([_vp, C.POINTER(C.c_double)], _i),
+    "lt_fw_norm2": ([_vp, C.POINTER(C.c_double)], _i),
+    "lt_sync": ([_vp], _i),
+    "lt_check_numeric": ([_vp, C.POINTER(C.c_longlong)], _i),
+    "lt_last_step_ms": ([_vp, C.POINTER(C.c_float)], _i),
+    "lt_shim_bind": ([_vp], _i),
+    "tracer_": ([_i], None),
+    "convadj_": ([], None),
+    "lt_last_error": ([], C.c_char_p),
+    "lt_device_count": ([C.POINTER(_i)], _i),
+    "lt_version": ([], C.c_char_p),
+    "lt_field_name": ([_i], C.c_char_p),
+    "lt_field_count": ([_i, _i, _i, _i], C.c_long),
+    "lt_field_is_int": ([_i], _i),
+    "lt_synth_defaults": ([C.POINTER(SynthConfig)], None),
+    "lt_synth_build": ([C.POINTER(SynthConfig), C.POINTER(_vp)], _i),
+    "lt_synth_free": ([_vp], _i),
+    "lt_synth_params": ([_vp, C.POINTER(Params)], _i),
+    "lt_synth_grid": ([_vp, C.POINTER(Grid)], _i),
+    "lt_synth_field": ([_vp, _i, _vp, _sz], _i),
+    "lt_synth_field_count": ([_vp, _i], C.c_long),
+    "lt_synth_upload": ([_vp, _vp], _i),
+}
+for _name, (_args, _res) in _SIGS.items():
+    _fn = getattr(lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
+
+FIELDS = []
+_f = 0
+while True:
+    _nm = lib.lt_field_name(_f)
+    if _nm is None:
+        break
+    FIELDS.append(_nm.decode())
+    _f += 1
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+INT_FIELDS = {n for n in FIELDS if lib.lt_field_is_int(FIELD_ID[n])}
+# inputs a caller supplies (everything except step outputs and diagnostics)
+# (WS and NET are model state the step reads and rewrites; they start at zero)
+INPUT_FIELDS = [n for n in FIELDS if n not in (
+    "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE")]
+
+
+def _check(rc, where):
+    if rc != LT_OK:
+        raise LtError(rc, where)
+
+
+def field_shape(name, nx, ny, km):
+    imt, jmt = nx + 4, ny + 4
+    n = lib.lt_field_count(FIELD_ID[name], nx, ny, km)
+    shapes = {2 * km * jmt * imt: (2, km, jmt, imt), 2 * (km + 1) * jmt * imt: (2, km + 1, jmt, imt),
+              km * jmt * imt: (km, jmt, imt), (km + 1) * jmt * imt: (km + 1, jmt, imt),
+              jmt * imt: (jmt, imt), 2 * jmt * imt: (2, jmt, imt), km: (km,), 9 * km: (9, km)}
+    return shapes[n]
+
+
+def field_dtype(name):
+    return np.int32 if name in INT_FIELDS else np.float64
+
+
+def set_device(dev):
+    _check(lib.lt_set_device(int(dev)), "lt_set_device")
+
+
+def launch_count():
+    return lib.lt_launch_count()
+
+
+def device_count():
+    n = C.c_int(0)
+    lib.lt_device_count(C.byref(n))
+    return n.value
+
+
+class TracerDomain:
+    """One LICOM tracer domain resident on the current CUDA device.
+
+    Replaces the reference's global device state (cuda_data.h, cudainit in
+    cuda_init.cpp:372-707) for the tracer path, with explicit lifetime.
+    """
+
+    def __init__(self, nx, ny, km, params, precision=PREC_FP64, diagnostics=False, ew_cyclic=True, tripole=True):
+        self.nx, self.ny, self.km = nx, ny, km
+        self.grid = Grid(nx, ny, km, precision, int(bool(diagnostics)), int(bool(ew_cyclic)), int(bool(tripole)))
+        self.params = params
+        h = _vp()
+        _check(lib.lt_create(C.byref(self.grid), C.byref(params), C.byref(h)), "lt_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.lt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def shape(self, name):
+        return field_shape(name, self.nx, self.ny, self.km)
+
+    def set(self, name, array):
+        a = np.ascontiguousarray(array, dtype=field_dtype(name))
+        _check(lib.lt_set_field(self.h, FIELD_ID[name], a.ctypes.data, a.nbytes), "lt_set_field(%s)" % name)
+
+    def get(self, name):
+        a = np.empty(self.shape(name), dtype=field_dtype(name))
+        _check(lib.lt_get_field(self.h, FIELD_ID[name], a.ctypes.data, a.nbytes), "lt_get_field(%s)" % name)
+        return a
+
+    def set_device(self, name, ptr, nbytes):
+        _check(lib.lt_set_field_device(self.h, FIELD_ID[name], ptr, nbytes), "lt_set_field_device(%s)" % name)
+
+    def derive_masks(self):
+        _check(lib.lt_derive_masks(self.h), "lt_derive_masks")
+
+    def step(self, nsteps=1):
+        _check(lib.lt_step(self.h, nsteps), "lt_step")
+
+    def step_host(self, forcing=None):
+        """One step with host forcing arrays (dict name->array for SWV, NSWV,
+        SST, SSS, FRESH, SEAICE); returns (fw_norm2, T content, S content)."""
+        arr = (_vp * 6)()
+        keep = []
+        for m, nm in enumerate(("SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE")):
+            if forcing is not None and nm in forcing:
+                a = np.ascontiguousarray(forcing[nm], dtype=np.float64)
+                keep.append(a)
+                arr[m] = a.ctypes.data
+        fw = C.c_double()
+        cont = (C.c_double * 2)()
+        _check(lib.lt_step_host(self.h, arr, C.byref(fw), cont), "lt_step_host")
+        return fw.value, cont[0], cont[1]
+
+    def step_host_ptrs(self, ptrs, fw_out):
+        """Step with forcing at raw host addresses (6 ints, 0 = keep) and the
+        fw_norm2 written to a ctypes double; the timed end-to-end path."""
+        arr = (_vp * 6)(*ptrs)
+        _check(lib.lt_step_host(self.h, arr, C.byref(fw_out), None), "lt_step_host")
+
+    def mark(self, which):
+        _check(lib.lt_mark(self.h, int(which)), "lt_mark")
+
+    def profile(self, on=True):
+        _check(lib.lt_profile(self.h, int(on)), "lt_profile")
+
+    PHASES = ("surface", "sss_sum", "net_halo", "continuity", "tracer", "state_halo")
+
+    def phase_ms(self):
+        ms = (C.c_float * 6)()
+        n = lib.lt_phase_ms(self.h, ms, 6)
+        if n < 0:
+            _check(-n, "lt_phase_ms")
+        return n, dict(zip(self.PHASES, list(ms)))
+
+    def convadj(self):
+        _check(lib.lt_convadj(self.h), "lt_convadj")
+
+    def tracer_content(self):
+        out = (C.c_double * 2)()
+        _check(lib.lt_tracer_content(self.h, out), "lt_tracer_content")
+        return tuple(out)
+
+    def fw_norm2(self):
+        v = C.c_double()
+        _check(lib.lt_fw_norm2(self.h, C.byref(v)), "lt_fw_norm2")
+        return v.value
+
+    def sync(self):
+        _check(lib.lt_sync(self.h), "lt_sync")
+
+    def check_numeric(self):
+        bad = C.c_longlong(0)
+        rc = lib.lt_check_numeric(self.h, C.byref(bad))
+        if rc not in (LT_OK, LT_E_NUMERIC):
+            _check(rc, "lt_check_numeric")
+        return bad.value
+
+    def last_step_ms(self):
+        v = C.c_float()
+        _check(lib.lt_last_step_ms(self.h, C.byref(v)), "lt_last_step_ms")
+        return v.value
+
+    def bind_shim(self):
+        _check(lib.lt_shim_bind(self.h), "lt_shim_bind")
+
+
+def tracer_(ii=0):
+    """tracer.cpp:1701 - one tracer step on the domain bound with bind_shim()."""
+    lib.tracer_(int(ii))
+    err = lib.lt_last_error()
+    return err.decode() if err else ""
+
+
+def convadj_():
+    """convadj.cpp:290 - convective adjustment of the bound domain."""
+    lib.convadj_()
+
+
+class Synth:
+    """Seeded synthetic domain (grid, masks, state, velocities, mixing, forcing)."""
+
+    def __init__(self, nx=360, ny=196, km=30, **kw):
+        cfg = SynthConfig()
+        lib.lt_synth_defaults(C.byref(cfg))
+        cfg.nx, cfg.ny, cfg.km = nx, ny, km
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        h = _vp()
+        _check(lib.lt_synth_build(C.byref(cfg), C.byref(h)), "lt_synth_build")
+        self.h = h
+        self.nx, self.ny, self.km = nx, ny, km
+        p = Params()
+        _check(lib.lt_synth_params(self.h, C.byref(p)), "lt_synth_params")
+        self.params = p
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib.lt_synth_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def field(self, name):
+        a = np.empty(field_shape(name, self.nx, self.ny, self.km), dtype=field_dtype(name))
+        _check(lib.lt_synth_field(self.h, FIELD_ID[name], a.ctypes.data, a.nbytes), "lt_synth_field(%s)" % name)
+        return a
+
+    def inputs(self):
+        return {n: self.field(n) for n in INPUT_FIELDS}
+
+    def all_fields(self):
+        """Every field of the domain (outputs and diagnostics zero)."""
+        return {n: self.field(n) for n in FIELDS}
+
+    def upload(self, dom):
+        """Fill a TracerDomain: 2-D/1-D inputs from the host, 3-D inputs
+        generated on the device (bit-identical to field())."""
+        _check(lib.lt_synth_upload(self.h, dom.h), "lt_synth_upload")
+
+    def domain(self, precision=PREC_FP64, diagnostics=False, device_fill=True):
+        dom = TracerDomain(self.nx, self.ny, self.km, self.params, precision=precision, diagnostics=diagnostics,
+                           ew_cyclic=bool(self.cfg.ew_cyclic), tripole=bool(self.cfg.tripole))
+        if device_fill:
+            self.upload(dom)
+        else:
+            for n, a in self.inputs().items():
+                dom.set(n, a)
+        return dom

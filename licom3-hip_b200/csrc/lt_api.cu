@@ -1,0 +1,521 @@
+// lt_api.cu - C ABI of the tracer step: per-domain device arena (replacing the
+// reference's global d_* state, cuda_data.h / cuda_init.cpp:372-707), field
+// transfer, the step sequence and the reference-named shims.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <mutex>
+#include <new>
+#include <vector>
+#include "lt_common.cuh"
+
+constexpr int LT_NPHASE = 6;       // surface, sss sum, net halo, continuity, tracer, state halo
+constexpr int LT_PROF_STEPS = 512;  // steps whose phase events are kept
+
+struct lt_domain {
+  lt::Arena a;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int profile = 0;
+  int prof_steps = 0;
+  std::vector<cudaEvent_t> prof_ev;   // [LT_PROF_STEPS][LT_NPHASE + 1]
+  std::vector<void*> allocations;
+  int slots = 0;
+  int steps_done = 0;
+  bool have_state = false;
+  bool owns_stream = false;
+};
+
+namespace lt {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+static std::atomic<long long> g_launches{0};
+long long launch_counter() { return g_launches.load(); }
+void count_launches(int n) { g_launches += n; }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error("CUDA error %d (%s) in %s", (int)e, cudaGetErrorString(e), what);
+  return e == cudaErrorMemoryAllocation ? LT_E_OOM : LT_E_CUDA;
+}
+
+namespace {
+
+lt_domain* g_shim = nullptr;
+
+// device pointer of a field in the arena (current state buffer for AT/ATB)
+void* field_ptr(lt_domain* d, int f, int which_state) {
+  Arena& a = d->a;
+  switch (f) {
+    case LT_F_AT: return a.at[which_state];
+    case LT_F_ATB: return a.atb[which_state];
+    case LT_F_UTF: return a.utf;
+    case LT_F_VTF: return a.vtf;
+    case LT_F_UTL: return a.utl;
+    case LT_F_VTL: return a.vtl;
+    case LT_F_H0F: return a.h0f;
+    case LT_F_H0L: return a.h0l;
+    case LT_F_AKT: return a.akt;
+    case LT_F_WS: return a.ws;
+    case LT_F_NET: return a.net;
+    case LT_F_UTF_OUT: return a.utf_out;
+    case LT_F_VTF_OUT: return a.vtf_out;
+    case LT_F_H0F_OUT: return a.h0f_out;
+    case LT_F_SWV: return a.swv;
+    case LT_F_NSWV: return a.nswv;
+    case LT_F_SST: return a.sst;
+    case LT_F_SSS: return a.sss;
+    case LT_F_FRESH: return a.fresh;
+    case LT_F_SEAICE: return a.seaice;
+    case LT_F_TAREA: return a.tarea;
+    case LT_F_TAREA_R: return a.tarea_r;
+    case LT_F_HTW: return a.htw;
+    case LT_F_HTS: return a.hts;
+    case LT_F_HUN: return a.hun;
+    case LT_F_HUE: return a.hue;
+    case LT_F_DXU: return a.dxu;
+    case LT_F_DYU: return a.dyu;
+    case LT_F_AHF: return a.ahf;
+    case LT_F_DTN: return a.dtn;
+    case LT_F_DTS: return a.dts;
+    case LT_F_DTE: return a.dte;
+    case LT_F_DTW: return a.dtw;
+    case LT_F_OHBT: return a.ohbt;
+    case LT_F_OHBU: return a.ohbu;
+    case LT_F_AU0: return a.au0;
+    case LT_F_AUS: return a.aus;
+    case LT_F_AUW: return a.auw;
+    case LT_F_AUSW: return a.ausw;
+    case LT_F_KMT: return a.kmt;
+    case LT_F_KMU: return a.kmu;
+    case LT_F_KMTN: return a.kmtn;
+    case LT_F_KMTS: return a.kmts;
+    case LT_F_KMTE: return a.kmte;
+    case LT_F_KMTW: return a.kmtw;
+    case LT_F_DZP: return a.dzp;
+    case LT_F_ODZP: return a.odzp;
+    case LT_F_ODZT: return a.odzt;
+    case LT_F_PEN: return a.pen;
+    case LT_F_TO: return a.to;
+    case LT_F_SO: return a.so;
+    case LT_F_C: return a.cc;
+    case LT_F_RESTORE: return a.restore;
+    case LT_F_AX: return a.ax;
+    case LT_F_AY: return a.ay;
+    case LT_F_AZ: return a.az;
+    case LT_F_DZ: return a.dzd;
+    case LT_F_TEND: return a.tend;
+    case LT_F_DT_DIFF: return a.dt_diff;
+    case LT_F_DT_CONV: return a.dt_conv;
+    case LT_F_PENETRATE: return a.penetrate;
+  }
+  return nullptr;
+}
+
+bool grid_ok(const lt_grid* g) {
+  if (!g) return false;
+  if (g->nx < 8 || g->ny < 8 || g->km < 3 || g->km > 256) return false;
+  if (g->tripole && (g->nx % 2)) return false;
+  if (g->precision != LT_PREC_FP64 && g->precision != LT_PREC_MIXED) return false;
+  return true;
+}
+
+struct Plan {
+  size_t off = 0;
+  std::vector<std::pair<void**, size_t>> items;
+  void add(void** p, size_t bytes) { items.push_back({p, bytes}); off += (bytes + 255) / 256 * 256; }
+};
+
+void plan_arena(Arena& a, Plan& pl) {
+  const size_t A = a.A, F = a.F, FB = a.FB, km = a.km;
+  auto D = [&](double** p, size_t n) { pl.add(reinterpret_cast<void**>(p), n * sizeof(double)); };
+  auto I = [&](int** p, size_t n) { pl.add(reinterpret_cast<void**>(p), n * sizeof(int)); };
+  D(&a.at[0], 2 * F); D(&a.at[1], 2 * F); D(&a.atb[0], 2 * FB); D(&a.atb[1], 2 * FB);
+  D(&a.utf, F); D(&a.vtf, F); D(&a.utl, F); D(&a.vtl, F); D(&a.akt, 2 * F);
+  D(&a.utf_out, F); D(&a.vtf_out, F); D(&a.ws, FB); D(&a.uwf, F); D(&a.vsf, F);
+  D(&a.h0f, A); D(&a.h0l, A); D(&a.h0f_out, A); D(&a.net, 2 * A);
+  double** two_d[] = {&a.swv, &a.nswv, &a.sst, &a.sss, &a.fresh, &a.seaice, &a.tarea, &a.tarea_r, &a.htw,
+                      &a.hts, &a.hun, &a.hue, &a.dxu, &a.dyu, &a.ahf, &a.dtn, &a.dts, &a.dte, &a.dtw,
+                      &a.ohbt, &a.ohbu, &a.au0, &a.aus, &a.auw, &a.ausw, &a.stf_ssh};
+  for (auto p : two_d) D(p, A);
+  D(&a.stf_n, 2 * A);
+  int** masks[] = {&a.kmt, &a.kmu, &a.kmtn, &a.kmts, &a.kmte, &a.kmtw};
+  for (auto p : masks) I(p, A);
+  D(&a.dzp, km); D(&a.odzp, km); D(&a.odzt, km); D(&a.pen, km); D(&a.to, km); D(&a.so, km); D(&a.cc, 9 * km);
+  D(&a.red_part, tree_sum_part_elems((long)a.A * a.km) + 16);
+  D(&a.scalars, 16);
+  I(&a.status, 16);
+  if (a.p.boundary_restore == 1) D(&a.restore, 2 * F);
+  if (a.diagnostics) {
+    D(&a.ax, 2 * F); D(&a.ay, 2 * F); D(&a.az, 2 * F); D(&a.dzd, 2 * F);
+    D(&a.tend, 2 * F); D(&a.dt_diff, 2 * F); D(&a.dt_conv, 2 * F); D(&a.penetrate, F);
+    D(&a.fold_save, 2 * km * (size_t)a.imt);
+  } else {
+    D(&a.dt_conv, 2 * F);  // convadj writes it
+    D(&a.tend, 2 * F);     // convadj accumulates into it
+  }
+  D(&a.col_scratch, (size_t)a.col_scratch_slots * km * a.nv_scratch * TTHREADS);
+}
+
+void init_arena_dims(Arena& a, const lt_grid* g, const lt_params* p) {
+  std::memset(&a, 0, sizeof(a));
+  a.nx = g->nx; a.ny = g->ny; a.km = g->km;
+  a.imt = g->nx + 4; a.jmt = g->ny + 4;
+  a.A = (long)a.imt * a.jmt; a.F = a.A * a.km; a.FB = a.A * (a.km + 1);
+  a.ew_cyclic = g->ew_cyclic; a.tripole = g->tripole;
+  a.diagnostics = g->diagnostics; a.precision = g->precision;
+  if (p) a.p = *p;
+  a.nv_scratch = a.diagnostics ? 3 : 2;
+}
+
+long slots_for(const Arena& a, int sms) {
+  const long ntiles = (long)((a.imt + TX - 1) / TX) * ((a.jmt + TY - 1) / TY);
+  long s = (long)sms * 4;
+  if (s > 2 * ntiles) s = 2 * ntiles;
+  return s;
+}
+
+int run_step(lt_domain* d) {
+  Arena& a = d->a;
+  cudaStream_t s = d->stream;
+  int rc;
+  cudaEvent_t* ev = nullptr;
+  if (d->profile && d->prof_steps < LT_PROF_STEPS) {
+    ev = &d->prof_ev[(size_t)d->prof_steps * (LT_NPHASE + 1)];
+    d->prof_steps++;
+  }
+  auto mark = [&](int ph) { if (ev) cudaEventRecord(ev[ph], s); };
+  mark(0);
+  if ((rc = launch_surface(a, s))) return rc;
+  mark(1);
+  if ((rc = launch_interior_sum_sss(a, s))) return rc;
+  mark(2);
+  if ((rc = launch_halo_r8(a.net, 2, a.imt, a.jmt, a.ew_cyclic, a.tripole, s))) return rc;
+  mark(3);
+  if ((rc = launch_continuity_fp64(a, s))) return rc;
+  mark(4);
+  if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
+  mark(5);
+  if ((rc = launch_halo_state(a, s))) return rc;
+  mark(6);
+  a.cur ^= 1;
+  d->steps_done++;
+  return LT_OK;
+}
+
+}  // namespace
+}  // namespace lt
+
+using namespace lt;
+
+extern "C" {
+
+const char* lt_last_error(void) { return lt::g_err; }
+
+static const char* const k_field_names[LT_F_COUNT] = {
+    "AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "NET", "UTF_OUT", "VTF_OUT", "H0F_OUT",
+    "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE", "DXU", "DYU",
+    "AHF", "DTN", "DTS", "DTE", "DTW", "OHBT", "OHBU", "AU0", "AUS", "AUW", "AUSW", "KMT", "KMU", "KMTN", "KMTS",
+    "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND",
+    "DT_DIFF", "DT_CONV", "PENETRATE"};
+
+const char* lt_field_name(int f) { return (f >= 0 && f < LT_F_COUNT) ? k_field_names[f] : nullptr; }
+long lt_field_count(int f, int nx, int ny, int km) {
+  if (f < 0 || f >= LT_F_COUNT || nx < 1 || ny < 1 || km < 1) return -1;
+  return lt::field_count(f, nx + 4, ny + 4, km);
+}
+int lt_field_is_int(int f) { return (f >= 0 && f < LT_F_COUNT) ? (int)lt::field_is_int(f) : 0; }
+
+const char* lt_version(void) { return "licom3-hip_b200 tracer 0.1 (sm_100a)"; }
+
+int lt_set_device(int dev) {
+  cudaError_t e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  return LT_OK;
+}
+
+long long lt_launch_count(void) { return lt::launch_counter(); }
+
+int lt_profile(lt_domain* d, int on) {
+  if (!d) return LT_E_INVALID;
+  if (on && d->prof_ev.empty()) {
+    d->prof_ev.resize((size_t)LT_PROF_STEPS * (LT_NPHASE + 1));
+    for (auto& e : d->prof_ev) LT_CUDA_OK(cudaEventCreate(&e));
+  }
+  d->profile = on;
+  d->prof_steps = 0;
+  return LT_OK;
+}
+
+int lt_phase_ms(lt_domain* d, float* ms, int nphase) {
+  if (!d || !ms || nphase < LT_NPHASE) return LT_E_INVALID;
+  for (int p = 0; p < LT_NPHASE; ++p) ms[p] = 0.0f;
+  if (d->prof_steps == 0) return LT_OK;
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  for (int st = 0; st < d->prof_steps; ++st) {
+    cudaEvent_t* ev = &d->prof_ev[(size_t)st * (LT_NPHASE + 1)];
+    for (int p = 0; p < LT_NPHASE; ++p) {
+      float t = 0.0f;
+      LT_CUDA_OK(cudaEventElapsedTime(&t, ev[p], ev[p + 1]));
+      ms[p] += t;
+    }
+  }
+  return d->prof_steps;
+}
+
+int lt_device_count(int* count) {
+  if (!count) return LT_E_INVALID;
+  cudaError_t e = cudaGetDeviceCount(count);
+  if (e != cudaSuccess) { *count = 0; return LT_E_NODEVICE; }
+  return LT_OK;
+}
+
+size_t lt_domain_bytes(const lt_grid* g) {
+  if (!grid_ok(g)) return 0;
+  Arena a;
+  lt_params p{};
+  init_arena_dims(a, g, &p);
+  a.col_scratch_slots = slots_for(a, 148);
+  Plan pl;
+  plan_arena(a, pl);
+  return pl.off;
+}
+
+int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
+  if (!out || !grid_ok(g) || !p) { set_error("lt_create: invalid grid or params"); return LT_E_INVALID; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("lt_create: no CUDA device");
+    return LT_E_NODEVICE;
+  }
+  lt_domain* d = new (std::nothrow) lt_domain;
+  if (!d) return LT_E_OOM;
+  init_arena_dims(d->a, g, p);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  d->a.col_scratch_slots = slots_for(d->a, sms);
+  d->slots = (int)d->a.col_scratch_slots;
+  Plan pl;
+  plan_arena(d->a, pl);
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  if (pl.off + (64u << 20) > free_b) {
+    set_error("lt_create: domain needs %zu bytes, %zu free", pl.off, free_b);
+    delete d;
+    return LT_E_OOM;
+  }
+  char* base = nullptr;
+  cudaError_t e = cudaMalloc(&base, pl.off);
+  if (e != cudaSuccess) {
+    set_error("lt_create: cudaMalloc(%zu) failed: %s", pl.off, cudaGetErrorString(e));
+    delete d;
+    return LT_E_OOM;
+  }
+  d->allocations.push_back(base);
+  size_t off = 0;
+  for (auto& it : pl.items) {
+    *it.first = base + off;
+    off += (it.second + 255) / 256 * 256;
+  }
+  cudaMemset(base, 0, pl.off);
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaFree(base);
+    delete d;
+    return LT_E_CUDA;
+  }
+  d->owns_stream = true;
+  cudaEventCreate(&d->ev0);
+  cudaEventCreate(&d->ev1);
+  cudaDeviceSynchronize();
+  *out = d;
+  return LT_OK;
+}
+
+int lt_destroy(lt_domain* d) {
+  if (!d) return LT_E_INVALID;
+  if (g_shim == d) g_shim = nullptr;
+  cudaStreamSynchronize(d->stream);
+  for (void* p : d->allocations) cudaFree(p);
+  if (d->ev0) cudaEventDestroy(d->ev0);
+  if (d->ev1) cudaEventDestroy(d->ev1);
+  for (auto e : d->prof_ev) cudaEventDestroy(e);
+  if (d->owns_stream) cudaStreamDestroy(d->stream);
+  delete d;
+  return LT_OK;
+}
+
+int lt_set_params(lt_domain* d, const lt_params* p) {
+  if (!d || !p) return LT_E_INVALID;
+  if (p->boundary_restore == 1 && !d->a.restore) {
+    set_error("lt_set_params: boundary_restore needs a domain created with it");
+    return LT_E_STATE;
+  }
+  d->a.p = *p;
+  return LT_OK;
+}
+
+static int xfer(lt_domain* d, int f, void* ptr, size_t nbytes, cudaMemcpyKind kind, bool set) {
+  if (!d || !ptr || f < 0 || f >= LT_F_COUNT) { set_error("bad field transfer"); return LT_E_INVALID; }
+  const size_t need = lt::field_bytes(f, d->a.imt, d->a.jmt, d->a.km);
+  if (nbytes != need) {
+    set_error("field %d: %zu bytes given, %zu expected", f, nbytes, need);
+    return LT_E_INVALID;
+  }
+  void* dev = field_ptr(d, f, d->a.cur);
+  if (!dev) { set_error("field %d not held by this domain (diagnostics/restore off)", f); return LT_E_STATE; }
+  if (set) {
+    LT_CUDA_OK(cudaMemcpyAsync(dev, ptr, nbytes, kind, d->stream));
+    if (f == LT_F_AT || f == LT_F_ATB) {  // both state buffers start equal
+      LT_CUDA_OK(cudaMemcpyAsync(field_ptr(d, f, d->a.cur ^ 1), ptr, nbytes, kind, d->stream));
+    }
+  } else {
+    LT_CUDA_OK(cudaMemcpyAsync(ptr, dev, nbytes, kind, d->stream));
+  }
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  return LT_OK;
+}
+
+int lt_set_field(lt_domain* d, int f, const void* src, size_t nbytes) {
+  return xfer(d, f, const_cast<void*>(src), nbytes, cudaMemcpyHostToDevice, true);
+}
+int lt_get_field(lt_domain* d, int f, void* dst, size_t nbytes) {
+  return xfer(d, f, dst, nbytes, cudaMemcpyDeviceToHost, false);
+}
+int lt_set_field_device(lt_domain* d, int f, const void* src, size_t nbytes) {
+  return xfer(d, f, const_cast<void*>(src), nbytes, cudaMemcpyDeviceToDevice, true);
+}
+int lt_get_field_device(lt_domain* d, int f, void* dst, size_t nbytes) {
+  return xfer(d, f, dst, nbytes, cudaMemcpyDeviceToDevice, false);
+}
+
+int lt_derive_masks(lt_domain* d) {
+  if (!d) return LT_E_INVALID;
+  int rc = launch_derive_masks(d->a, d->stream);
+  if (rc) return rc;
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  return LT_OK;
+}
+
+int lt_step(lt_domain* d, int nsteps) {
+  if (!d || nsteps < 0) return LT_E_INVALID;
+  LT_CUDA_OK(cudaEventRecord(d->ev0, d->stream));
+  for (int s = 0; s < nsteps; ++s) {
+    int rc = run_step(d);
+    if (rc) return rc;
+  }
+  LT_CUDA_OK(cudaEventRecord(d->ev1, d->stream));
+  return LT_OK;
+}
+
+int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2_out, double* content2_out) {
+  if (!d) return LT_E_INVALID;
+  Arena& a = d->a;
+  double* dst[6] = {a.swv, a.nswv, a.sst, a.sss, a.fresh, a.seaice};
+  const size_t bytes = sizeof(double) * a.A;
+  if (forcing6)
+    for (int m = 0; m < 6; ++m)
+      if (forcing6[m]) LT_CUDA_OK(cudaMemcpyAsync(dst[m], forcing6[m], bytes, cudaMemcpyHostToDevice, d->stream));
+  int rc = run_step(d);
+  if (rc) return rc;
+  if (content2_out) {
+    if ((rc = launch_tracer_content(a, d->stream))) return rc;
+    LT_CUDA_OK(cudaMemcpyAsync(content2_out, a.scalars + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  }
+  if (fw_norm2_out) LT_CUDA_OK(cudaMemcpyAsync(fw_norm2_out, a.scalars, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  return LT_OK;
+}
+
+int lt_convadj(lt_domain* d) {
+  if (!d) return LT_E_INVALID;
+  int rc = launch_convadj(d->a, d->stream);
+  if (rc) return rc;
+  return LT_OK;
+}
+
+int lt_tracer_content(lt_domain* d, double* out2) {
+  if (!d || !out2) return LT_E_INVALID;
+  int rc = launch_tracer_content(d->a, d->stream);
+  if (rc) return rc;
+  LT_CUDA_OK(cudaMemcpyAsync(out2, d->a.scalars + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  return LT_OK;
+}
+
+int lt_fw_norm2(lt_domain* d, double* out) {
+  if (!d || !out) return LT_E_INVALID;
+  LT_CUDA_OK(cudaMemcpyAsync(out, d->a.scalars, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  return LT_OK;
+}
+
+int lt_sync(lt_domain* d) {
+  if (!d) return LT_E_INVALID;
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  return LT_OK;
+}
+
+int lt_check_numeric(lt_domain* d, long long* bad) {
+  if (!d) return LT_E_INVALID;
+  int rc = launch_check_numeric(d->a, d->stream);
+  if (rc) return rc;
+  int h = 0;
+  LT_CUDA_OK(cudaMemcpyAsync(&h, d->a.status, sizeof(int), cudaMemcpyDeviceToHost, d->stream));
+  LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+  if (bad) *bad = h;
+  if (h) { set_error("%d non-finite tracer values", h); return LT_E_NUMERIC; }
+  return LT_OK;
+}
+
+int lt_mark(lt_domain* d, int which) {
+  if (!d || (which != 0 && which != 1)) return LT_E_INVALID;
+  LT_CUDA_OK(cudaEventRecord(which ? d->ev1 : d->ev0, d->stream));
+  return LT_OK;
+}
+
+int lt_last_step_ms(lt_domain* d, float* ms) {
+  if (!d || !ms) return LT_E_INVALID;
+  LT_CUDA_OK(cudaEventSynchronize(d->ev1));
+  LT_CUDA_OK(cudaEventElapsedTime(ms, d->ev0, d->ev1));
+  return LT_OK;
+}
+
+int lt_shim_bind(lt_domain* d) {
+  g_shim = d;
+  return LT_OK;
+}
+
+// tracer.cpp:1701 - one step with the reference's visible side effects on the
+// bound domain: utf/vtf/h0f scaled in place, vtl left holding S.
+void tracer_(int ii) {
+  (void)ii;
+  lt_domain* d = g_shim;
+  if (!d) { set_error("tracer_: no domain bound (lt_shim_bind)"); return; }
+  Arena& a = d->a;
+  if (run_step(d)) return;
+  const size_t fb = sizeof(double) * a.F;
+  cudaMemcpyAsync(a.utf, a.utf_out, fb, cudaMemcpyDeviceToDevice, d->stream);
+  cudaMemcpyAsync(a.vtf, a.vtf_out, fb, cudaMemcpyDeviceToDevice, d->stream);
+  cudaMemcpyAsync(a.h0f, a.h0f_out, sizeof(double) * a.A, cudaMemcpyDeviceToDevice, d->stream);
+  launch_vtl_clobber(a, d->stream);
+  cudaStreamSynchronize(d->stream);
+}
+
+// convadj.cpp:290
+void convadj_(void) {
+  lt_domain* d = g_shim;
+  if (!d) { set_error("convadj_: no domain bound (lt_shim_bind)"); return; }
+  launch_convadj(d->a, d->stream);
+  cudaStreamSynchronize(d->stream);
+}
+
+}  // extern "C"

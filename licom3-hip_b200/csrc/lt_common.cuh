@@ -1,0 +1,91 @@
+// lt_common.cuh - device arena and launch parameters shared by the tracer
+// step's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/licom_tracer.h"
+#include "lt_fields.h"
+
+namespace lt {
+
+// Column tile of the fused tracer kernel: TX columns along i (one warp) by TY
+// rows along j; one thread per column.
+constexpr int TX = 32;
+constexpr int TY = 4;
+constexpr int TTHREADS = TX * TY;
+
+// Everything the step kernels touch, as raw device pointers (dense
+// [n][k][j][i] layout of the reference, i fastest).
+struct Arena {
+  int nx, ny, km, imt, jmt;
+  long A, F, FB;
+  int ew_cyclic, tripole, diagnostics, precision;
+  lt_params p;
+
+  // state, ping-pong: index cur holds the state the next step reads
+  double* at[2];
+  double* atb[2];
+  int cur;
+
+  // dynamics inputs (frozen across lt_step calls) and step outputs
+  double *utf, *vtf, *utl, *vtl, *h0f, *h0l, *akt;
+  double *utf_out, *vtf_out, *h0f_out;
+  double *ws, *net;
+  // surface forcing and grid
+  double *swv, *nswv, *sst, *sss, *fresh, *seaice;
+  double *tarea, *tarea_r, *htw, *hts, *hun, *hue, *dxu, *dyu, *ahf, *dtn, *dts, *dte, *dtw, *ohbt, *ohbu;
+  double *au0, *aus, *auw, *ausw;
+  int *kmt, *kmu, *kmtn, *kmts, *kmte, *kmtw;
+  double *dzp, *odzp, *odzt, *pen, *to, *so, *cc, *restore;
+  // diagnostics (null when off)
+  double *ax, *ay, *az, *dzd, *tend, *dt_diff, *dt_conv, *penetrate;
+
+  // step scratch
+  double *uwf, *vsf;          // face transports u_wface, v_sface [km][jmt][imt]
+  double *stf_ssh;            // [jmt][imt] 0.5*(h0f*onbc + h0l)
+  double *stf_n;              // [2][jmt][imt] surface flux per tracer (T, S)
+  double *red_part;           // partial sums of the deterministic reductions
+  double *scalars;            // [0] err_norm2 (fw_norm2), [1..2] tracer content, [3..] spare
+  double *col_scratch;        // per-slot Thomas sweep storage
+  double *fold_save;          // [2][km][2][imt] pre-fold values of the top physical row (diagnostics)
+  int *status;                // [4] device status words
+  long col_scratch_slots;
+  int nv_scratch;             // values per level per column in col_scratch
+};
+
+#define LT_CUDA_OK(call)                                   \
+  do {                                                     \
+    cudaError_t e_ = (call);                               \
+    if (e_ != cudaSuccess) return lt::cuda_fail(e_, #call); \
+  } while (0)
+
+// after a kernel launch: check the launch and count it
+#define LT_LAUNCHED()                    \
+  do {                                   \
+    LT_CUDA_OK(cudaGetLastError());      \
+    lt::count_launches(1);               \
+  } while (0)
+
+int cuda_fail(cudaError_t e, const char* what);
+// process-wide count of kernels launched by this library
+long long launch_counter();
+void count_launches(int n);
+void set_error(const char* fmt, ...);
+
+// host launchers (defined in the step translation units)
+int launch_surface(const Arena& a, cudaStream_t s);
+int launch_continuity_fp64(const Arena& a, cudaStream_t s);
+int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots);
+int launch_halo_state(const Arena& a, cudaStream_t s);
+int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripole, cudaStream_t s);
+int launch_tree_sum(const double* x, long n, double* part, double* out, cudaStream_t s);
+int launch_interior_sum_sss(const Arena& a, cudaStream_t s);
+int launch_tracer_content(const Arena& a, cudaStream_t s);
+int launch_convadj(const Arena& a, cudaStream_t s);
+int launch_check_numeric(const Arena& a, cudaStream_t s);
+int launch_derive_masks(const Arena& a, cudaStream_t s);
+int launch_vtl_clobber(const Arena& a, cudaStream_t s);
+int tracer_slots(const Arena& a);
+size_t tree_sum_part_elems(long n);
+
+}  // namespace lt

@@ -1,0 +1,829 @@
+// lt_step_fp64.cu - the plain FP64 tracer step (the drop-in form).
+//
+// Compiled with -fmad=false: every floating-point expression keeps the
+// operation order of the reference kernels it replaces (cited per kernel), so
+// results match the FP64 CPU oracle bit for bit.
+//
+// Launch sequence of one step (replacing tracer.cpp:1701-1903):
+//   k_surface       surface fluxes of both tracers, SSH mean, net, the
+//                   surface mixing floor, SSS-norm terms       (tracer_1_0, tracer_5/6 surface parts)
+//   tree sum        deterministic SSS-normalisation sum         (tracer.cpp:1849-1868)
+//   halo(net)       in-GPU ghost fill                           (pop_haloupdate_tracer1)
+//   k_continuity    uk/vk, divergence, w by upward integration,
+//                   face transports, scaled utf/vtf             (tracer_1, upwell_2..4, advection_tracer_1_0)
+//   k_tracer64      per column tile, both tracers: tspas predictor/limiter,
+//                   biharmonic diffusion, shortwave, explicit and implicit
+//                   vertical diffusion, surface terms, update   (advection_tracer_2/3, tracer_del4_1/2,
+//                                                                tracer_5..9, invtrit)
+//   k_halo_state    ghost fill + fold of the new state          (pop_haloupdate_tracer2, tracer_9 for ghosts)
+#include <cstdio>
+#include "lt_common.cuh"
+#include "lt_halo.cuh"
+
+namespace lt {
+
+namespace {
+
+__device__ __forceinline__ long q2(int j, int i, int imt) { return (long)j * imt + i; }
+
+// ------------------------------------------------------------------ surface
+// One thread per column.  tracer_1_0 (tracer.cpp:1081-1093): h0f*onbc and the
+// SSH mean stf; tracer_del4_2's surface floor on akt(T) (tracer.cpp:1315-1317);
+// salt flux of tracer_5 (tracer.cpp:1480-1520) and heat flux of tracer_6
+// (tracer.cpp:1545-1565) from the previous time level; net (both tracers).
+__global__ void k_surface(Arena a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.imt || j >= a.jmt) return;
+  const long q = q2(j, i, a.imt);
+  const lt_params& p = a.p;
+  const double h0 = a.h0f[q] * p.onbc;
+  a.h0f_out[q] = h0;
+  const double ssh = 0.5 * h0 + 0.5 * a.h0l[q];
+  a.stf_ssh[q] = ssh;
+  if (i >= 1 && i < a.imt - 1 && j >= 1 && j < a.jmt - 1) {
+    if (a.akt[q] < p.dwndmix) a.akt[q] = p.dwndmix;
+  }
+  double sT = ssh, sS = ssh;
+  if (a.kmt[q] > 0) {
+    const double* atb = a.atb[a.cur];
+    const double odzp0 = a.odzp[0];
+    const double s_top = atb[a.FB + a.A + q];
+    sS = a.fresh[q] * 34.7 * p.od0 / 1000.0 + p.gamma * (a.sss[q] - s_top) * a.seaice[q] / odzp0 +
+         p.gamma * 30.0 / 365.0 / 4.0 * 50.0 * (a.sss[q] - s_top) / odzp0 * (1.0 - a.seaice[q]);
+    a.net[a.A + q] = sS * odzp0;
+    const double t_top = atb[a.A + q];
+    sT = ((a.swv[q] + a.nswv[q]) * p.od0cp + a.seaice[q] * p.gamma * (a.sst[q] - t_top) / odzp0);
+    a.net[q] = sT * odzp0;
+  }
+  a.stf_n[q] = sT;
+  a.stf_n[a.A + q] = sS;
+}
+
+// --------------------------------------------------------- deterministic sum
+// Fixed binary tree: blocks of 2048 consecutive terms, pairs (t, t+stride) for
+// stride = 1024..1, zero padding; repeated on the block sums until one value.
+constexpr int RB = 1024;
+
+template <class Term>
+__global__ void k_tree_first(Term term, long n, double* part) {
+  __shared__ double s[2 * RB];
+  const long base = (long)blockIdx.x * 2 * RB;
+  const int t = threadIdx.x;
+  s[t] = (base + t < n) ? term(base + t) : 0.0;
+  s[t + RB] = (base + t + RB < n) ? term(base + t + RB) : 0.0;
+  for (int stride = RB; stride > 0; stride >>= 1) {
+    __syncthreads();
+    if (t < stride) s[t] = s[t] + s[t + stride];
+  }
+  if (t == 0) part[blockIdx.x] = s[0];
+}
+
+struct ArrayTerm {
+  const double* x;
+  __device__ double operator()(long m) const { return x[m]; }
+};
+
+// SSS-norm term of interior column m (row-major over j=2..jmt-3, i=2..imt-3):
+// tarea*net(S)*vit(k=0) (tracer.cpp:1522-1525)
+struct SssTerm {
+  const double* tarea;
+  const double* net_s;
+  const int* kmt;
+  int nx, imt;
+  __device__ double operator()(long m) const {
+    const int j = 2 + (int)(m / nx), i = 2 + (int)(m % nx);
+    const long q = (long)j * imt + i;
+    return tarea[q] * net_s[q] * (kmt[q] > 0 ? 1.0 : 0.0);
+  }
+};
+
+__global__ void k_finish_sss(double* scalars, const double* sum, double area_t) {
+  scalars[0] = -sum[0] / area_t;
+}
+
+template <class Term>
+int tree_sum(Term term, long n, double* part, double* out, cudaStream_t s) {
+  long nb = (n + 2 * RB - 1) / (2 * RB);
+  if (nb < 1) nb = 1;
+  k_tree_first<<<(unsigned)nb, RB, 0, s>>>(term, n, part);
+  LT_LAUNCHED();
+  double* cur = part;
+  double* nxt = part + nb;
+  while (nb > 1) {
+    const long nb2 = (nb + 2 * RB - 1) / (2 * RB);
+    k_tree_first<<<(unsigned)nb2, RB, 0, s>>>(ArrayTerm{cur}, nb, nxt);
+    LT_LAUNCHED();
+    cur = nxt;
+    nxt = nxt + nb2;
+    nb = nb2;
+  }
+  LT_CUDA_OK(cudaMemcpyAsync(out, cur, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return LT_OK;
+}
+
+// ------------------------------------------------------------------ halo
+// In-place ghost fill of nz levels (e.g. net), one block per level.
+__global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripole) {
+  extern __shared__ double top[];
+  double* lvl = f + (long)blockIdx.x * imt * jmt;
+  for (int i = threadIdx.x; i < imt; i += blockDim.x) top[i] = lvl[2L * imt + i];
+  __syncthreads();
+  HaloCells hc{imt, jmt, tripole};
+  const long nc = hc.count();
+  for (long m = threadIdx.x; m < nc; m += blockDim.x) {
+    int j, i;
+    hc.cell(m, j, i);
+    double v;
+    if (halo_cell_value(lvl, top, j, i, imt, jmt, ew_cyclic, tripole, v)) lvl[(long)j * imt + i] = v;
+  }
+}
+
+// ------------------------------------------------------------- continuity
+// One thread per T column of a TX x TY tile.  Per level: U-point velocities
+// of the tile plus one column east and one row north are staged in shared
+// memory; the thread forms
+//   wkd = 0.5*utf*oncc + 0.5*utl, uk = (1 + work*ohbu)*wkd   (tracer_1, upwell_2)
+//   wka = masked divergence of (uk, vk)                          (operators_div)
+//   u_wface, v_sface face transports                             (advection_tracer_1_0)
+// and keeps wka in shared memory for the second, upward pass
+//   ws(k) = vit*(ws(k-1) + dzp(k-1)*(W*ohbt + wka(k-1))) * 1/(1+stf*ohbt)   (upwell_3/4)
+constexpr int CX = TX + 1, CY = TY + 1;  // U-point region: i in [x0, x0+TX], j in [y0-1, y0+TY-1]
+
+__global__ void __launch_bounds__(TTHREADS) k_continuity(Arena a) {
+  extern __shared__ double sh[];
+  double* s_wkd = sh;                 // [CY][CX]
+  double* s_wkb = s_wkd + CY * CX;
+  double* s_uk = s_wkb + CY * CX;
+  double* s_vk = s_uk + CY * CX;
+  double* s_fac = s_vk + CY * CX;     // 1 + work*ohbu per U point
+  double* s_wka = s_fac + CY * CX;    // [km][TTHREADS]
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A;
+  const lt_params& p = a.p;
+  const bool own = (i < imt && j < jmt);
+
+  // free-surface factor at the staged U points: tgrid_to_ugrid(stf) (grid.F90:1975-1990)
+  for (int m = tid; m < CY * CX; m += TTHREADS) {
+    const int uj = y0 - 1 + m / CX, ui = x0 + m % CX;
+    double fac = 0.0;
+    if (uj >= 0 && uj < jmt - 1 && ui >= 1 && ui < imt) {
+      const long q = q2(uj, ui, imt);
+      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
+                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
+      fac = 1.0 + work * a.ohbu[q];
+    }
+    s_fac[m] = fac;
+  }
+  const long qo = own ? q2(j, i, imt) : 0;
+  const int kz = own ? a.kmt[qo] : 0;
+  const bool wcol = own && j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1;
+  double W = 0.0;
+
+  for (int k = 0; k < km; ++k) {
+    __syncthreads();
+    for (int m = tid; m < CY * CX; m += TTHREADS) {
+      const int uj = y0 - 1 + m / CX, ui = x0 + m % CX;
+      double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
+      if (uj >= 0 && uj < jmt && ui < imt) {
+        const long c = (long)k * A + q2(uj, ui, imt);
+        wkd = 0.5 * (a.utf[c] * p.oncc) + 0.5 * a.utl[c];
+        wkb = 0.5 * (a.vtf[c] * p.oncc) + 0.5 * a.vtl[c];
+        if (uj < jmt - 1 && ui >= 1) {
+          uk = s_fac[m] * wkd;
+          vk = s_fac[m] * wkb;
+        }
+      }
+      s_wkd[m] = wkd; s_wkb[m] = wkb; s_uk[m] = uk; s_vk[m] = vk;
+    }
+    __syncthreads();
+    if (!own) continue;
+    const long c = (long)k * A + qo;
+    const int m0 = (ty + 1) * CX + tx;      // U point (j, i)
+    const int mn = ty * CX + tx;            // U point (j-1, i)
+    a.utf_out[c] = a.utf[c] * p.oncc;
+    a.vtf_out[c] = a.vtf[c] * p.oncc;
+    if (j >= 1 && j < jmt - 1) a.uwf[c] = (s_wkd[mn] + s_wkd[m0]) * a.htw[qo] * 0.25;
+    if (i >= 1 && i < imt - 1) a.vsf[c] = (s_wkb[m0] + s_wkb[m0 + 1]) * a.hts[qo] * 0.25;
+    double wka = 0.0;
+    if (j >= 1 && i < imt - 1 && k <= kz - 1) {
+      const double east = (s_uk[m0 + 1] + s_uk[mn + 1]) * a.htw[qo + 1];
+      const double west = (s_uk[m0] + s_uk[mn]) * a.htw[qo];
+      const double south = (s_vk[m0 + 1] + s_vk[m0]) * a.hts[qo];
+      const double north = (s_vk[mn + 1] + s_vk[mn]) * a.hts[qo - imt];
+      wka = 0.5 * (east - west + south - north) * a.tarea_r[qo];
+    }
+    s_wka[k * TTHREADS + tid] = wka;
+    if (wcol) W = W - a.dzp[k] * wka * (k < kz ? 1.0 : 0.0);
+  }
+  if (!wcol) return;
+  const double ohbt = a.ohbt[qo];
+  const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
+  double wsp = a.ws[qo];  // level 0 is never written by the step
+  for (int k = 1; k < km; ++k) {
+    const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + s_wka[(k - 1) * TTHREADS + tid]));
+    a.ws[(long)k * A + qo] = raw * fac;
+    wsp = raw;
+  }
+}
+
+// ------------------------------------------------------------- tracer march
+// Shared-memory regions of a TX x TY column tile:
+//   H2: rows y0-2..y0+TY+1, cols x0-2..x0+TX+1   (RY x RX)   tracer, atb, kmt
+//   H1: rows y0-1..y0+TY,   cols x0-1..x0+TX     (QY x QX)   predictor, extrema, w, d2tk
+constexpr int RX = TX + 4, RY = TY + 4, QX = TX + 2, QY = TY + 2;
+constexpr int UWN = QY * RX;          // u_wface: H1 rows, cols x0-2..x0+TX+1
+constexpr int VSN = (QY + 1) * QX;    // v_sface: rows y0-2..y0+TY, H1 cols
+
+struct TSmem {
+  double at[4][RY * RX];
+  double a00[3][QY * QX], amx[3][QY * QX], amn[3][QY * QX];
+  double ws[3][QY * QX];
+  double uw[2][UWN], vs[2][VSN];
+  double atb[RY * RX];
+  double d2[QY * QX];
+  double tr[QY * QX], hw[UWN], hs[VSN];
+  double dtn[QY * QX], dts[QY * QX], dte[QY * QX], dtw[QY * QX], ahf[QY * QX];
+  int kmt[RY * RX];
+};
+
+__device__ __forceinline__ int slot4(int k) { return k & 3; }
+__device__ __forceinline__ int slot3(int k) { return k % 3; }
+
+// load one level of a [km][jmt][imt] field over region rows r0.., cols c0..
+// (ny x nxr), zero outside the domain
+__device__ __forceinline__ void load_region(double* dst, const double* lvl, int r0, int c0, int nyr, int nxr,
+                                            int imt, int jmt) {
+  for (int m = threadIdx.x; m < nyr * nxr; m += TTHREADS) {
+    const int gj = r0 + m / nxr, gi = c0 + m % nxr;
+    dst[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? lvl[(long)gj * imt + gi] : 0.0;
+  }
+}
+
+// tspas predictor at00 and masked extrema at level kk for every H1 point
+// (advection_tracer_2, tracer.cpp:291-547).  s_at slots hold kk-1, kk, kk+1.
+__device__ void predictor_level(TSmem& S, const Arena& a, int kk, int x0, int y0) {
+  const int km = a.km, imt = a.imt, jmt = a.jmt;
+  const double dts = a.p.dts;
+  const double* odzp = a.odzp;
+  const double* odzt = a.odzt;
+  const double* at_c = S.at[slot4(kk)];
+  const double* at_u = kk > 0 ? S.at[slot4(kk - 1)] : nullptr;        // level above
+  const double* at_d = kk < km - 1 ? S.at[slot4(kk + 1)] : nullptr;   // level below
+  const double* ws_c = S.ws[slot3(kk)];
+  const double* ws_d = kk < km - 1 ? S.ws[slot3(kk + 1)] : nullptr;
+  const double* uw = S.uw[kk & 1];
+  const double* vs = S.vs[kk & 1];
+  double* o00 = S.a00[slot3(kk)];
+  double* omx = S.amx[slot3(kk)];
+  double* omn = S.amn[slot3(kk)];
+  for (int m = threadIdx.x; m < QY * QX; m += TTHREADS) {
+    const int hj = m / QX, hi = m % QX;
+    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+    if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) {
+      o00[m] = 0.0; omx[m] = 0.0; omn[m] = 0.0;
+      continue;
+    }
+    const int r = (hj + 1) * RX + (hi + 1);   // H2 index of this point
+    const int u = hj * RX + (hi + 1);          // uw index of column gi (row gj)
+    const int v = (hj + 1) * QX + hi;          // vs index of row gj
+    const double tr = S.tr[m];
+    const double c = at_c[r], e = at_c[r + 1], w = at_c[r - 1], s = at_c[r + RX], n = at_c[r - RX];
+    const double ue = uw[u + 1], uwc = uw[u];
+    const double vsc = vs[v], vn = vs[v - QX];
+    const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
+    const double y0v = ((s + c) * vsc - (c + n) * vn) * tr;
+    const double xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / S.hw[u + 1];
+    const double xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / S.hw[u];
+    const double xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / S.hs[v];
+    const double xy4 = dts * (c - n) * 2.0 * tr * vn * vn / S.hs[v - QX];
+    const double cx = -c * (ue - uwc) * tr * 2.0;
+    const double cy = -c * (vsc - vn) * tr * 2.0;
+    double za, zb1, zb2, zc;
+    const double wk = ws_c[m];
+    if (kk == 0) {
+      const double w1 = ws_d[m], ad = at_d[r];
+      za = -0.5 * odzp[0] * w1 * (ad + c);
+      zb1 = 0.0;
+      zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
+      zc = odzp[0] * c * w1;
+    } else if (kk == km - 1) {
+      const double au = at_u[r];
+      za = 0.5 * odzp[km - 1] * wk * (c + au);
+      zb1 = -0.5 * odzp[km - 1] * wk * wk * odzt[km - 1] * (au - c) * dts;
+      zb2 = 0.0;
+      zc = -odzp[km - 1] * c * wk;
+    } else {
+      const double au = at_u[r], ad = at_d[r], w1 = ws_d[m];
+      za = 0.5 * odzp[kk] * wk * (c + au) - 0.5 * odzp[kk] * w1 * (c + ad);
+      zb1 = -0.5 * odzp[kk] * wk * wk * odzt[kk] * (au - c) * dts;
+      zb2 = 0.5 * odzp[kk] * w1 * w1 * odzt[kk + 1] * (c - ad) * dts;
+      zc = -odzp[kk] * c * (wk - w1);
+    }
+    const double xx = -(x0v + xy1 + xy2 + cx);
+    const double yy = -(y0v + xy3 + xy4 + cy);
+    const double zz = -(zb1 + zb2 + za + zc);
+    o00[m] = c + (xx + yy + zz) * dts;
+    // masked 7-point extrema, land weighted to -/+1e10 (tracer.cpp:418-546)
+    auto vitk = [&](int kl, int rr) { return (kl < S.kmt[rr]) ? 1.0 : 0.0; };
+    auto mxv = [&](double t, double vt) { return t * vt + (1.0 - vt) * -1.0e10; };
+    auto mnv = [&](double t, double vt) { return t * vt + (1.0 - vt) * 1.0e10; };
+    const double vc = vitk(kk, r), vn_ = vitk(kk, r - RX), vs_ = vitk(kk, r + RX), vw = vitk(kk, r - 1),
+                 ve = vitk(kk, r + 1);
+    double hi_ = mxv(c, vc), lo_ = mnv(c, vc), t;
+    t = mxv(n, vn_); if (hi_ < t) hi_ = t;
+    t = mxv(s, vs_); if (hi_ < t) hi_ = t;
+    t = mxv(w, vw); if (hi_ < t) hi_ = t;
+    t = mxv(e, ve); if (hi_ < t) hi_ = t;
+    t = mnv(n, vn_); if (lo_ > t) lo_ = t;
+    t = mnv(s, vs_); if (lo_ > t) lo_ = t;
+    t = mnv(w, vw); if (lo_ > t) lo_ = t;
+    t = mnv(e, ve); if (lo_ > t) lo_ = t;
+    if (kk > 0) {
+      const double au = at_u[r], vu = vitk(kk - 1, r);
+      t = mxv(au, vu); if (hi_ < t) hi_ = t;
+      t = mnv(au, vu); if (lo_ > t) lo_ = t;
+    }
+    if (kk < km - 1) {
+      const double ad = at_d[r], vd = vitk(kk + 1, r);
+      t = mxv(ad, vd); if (hi_ < t) hi_ = t;
+      t = mnv(ad, vd); if (lo_ > t) lo_ = t;
+    }
+    omx[m] = hi_;
+    omn[m] = lo_;
+  }
+}
+
+// first masked Laplacian of atb at level kk on H1 (tracer_del4_1, tracer.cpp:1238-1293)
+__device__ void del4_first(TSmem& S, const Arena& a, int kk, int x0, int y0) {
+  for (int m = threadIdx.x; m < QY * QX; m += TTHREADS) {
+    const int hj = m / QX, hi = m % QX;
+    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+    if (!(gi >= 1 && gi < a.imt - 1 && gj >= 1 && gj < a.jmt - 1)) { S.d2[m] = 0.0; continue; }
+    const int r = (hj + 1) * RX + (hi + 1);
+    double h = 0.0, cc = 0.0;
+    if (kk <= S.kmt[r] - 1) {
+      if (kk <= S.kmt[r - RX] - 1) { h += S.dtn[m] * S.atb[r - RX]; cc -= S.dtn[m]; }
+      if (kk <= S.kmt[r + RX] - 1) { h += S.dts[m] * S.atb[r + RX]; cc -= S.dts[m]; }
+      if (kk <= S.kmt[r + 1] - 1) { h += S.dte[m] * S.atb[r + 1]; cc -= S.dte[m]; }
+      if (kk <= S.kmt[r - 1] - 1) { h += S.dtw[m] * S.atb[r - 1]; cc -= S.dtw[m]; }
+    }
+    S.d2[m] = S.ahf[m] * (cc * S.atb[r] + h);
+  }
+}
+
+template <bool DIAG>
+__global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long ntiles) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TSmem& S = *reinterpret_cast<TSmem*>(smem_raw);
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A, F = a.F, FB = a.FB;
+  const lt_params& p = a.p;
+  const double dts = p.dts;
+  const double aidif = 0.5;
+  const double* __restrict__ odzp = a.odzp;
+  const double* __restrict__ odzt = a.odzt;
+  const int NV = a.nv_scratch;
+  double* scr = a.col_scratch + (long)blockIdx.x * km * NV * TTHREADS;
+
+  for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x) {
+    const long tile = w >> 1;
+    const int n = (int)(w & 1);
+    const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * TY;
+    const int i = x0 + tx, j = y0 + ty;
+    const double* at_in = a.at[a.cur] + n * F;
+    const double* atb_in = a.atb[a.cur] + n * FB;
+    double* at_out = a.at[a.cur ^ 1] + n * F;
+    double* atb_out = a.atb[a.cur ^ 1] + n * FB;
+    const double* akt = a.akt + n * F;
+
+    __syncthreads();  // previous tile finished with shared memory
+    // ---- per-tile 2-D statics
+    for (int m = tid; m < RY * RX; m += TTHREADS) {
+      const int gj = y0 - 2 + m / RX, gi = x0 - 2 + m % RX;
+      S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[q2(gj, gi, imt)] : 0;
+    }
+    for (int m = tid; m < QY * QX; m += TTHREADS) {
+      const int gj = y0 - 1 + m / QX, gi = x0 - 1 + m % QX;
+      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
+      const long q = in ? q2(gj, gi, imt) : 0;
+      S.tr[m] = in ? a.tarea_r[q] : 0.0;
+      S.dtn[m] = in ? a.dtn[q] : 0.0;
+      S.dts[m] = in ? a.dts[q] : 0.0;
+      S.dte[m] = in ? a.dte[q] : 0.0;
+      S.dtw[m] = in ? a.dtw[q] : 0.0;
+      S.ahf[m] = in ? a.ahf[q] : 0.0;
+    }
+    for (int m = tid; m < UWN; m += TTHREADS) {
+      const int gj = y0 - 1 + m / RX, gi = x0 - 2 + m % RX;
+      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
+      S.hw[m] = in ? a.htw[q2(gj, gi, imt)] * a.hun[q2(gj, gi, imt)] : 1.0;
+    }
+    for (int m = tid; m < VSN; m += TTHREADS) {
+      const int gj = y0 - 2 + m / QX, gi = x0 - 1 + m % QX;
+      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
+      S.hs[m] = in ? a.hts[q2(gj, gi, imt)] * a.hue[q2(gj, gi, imt)] : 1.0;
+    }
+    // ---- prologue: levels km-1 and km-2 of the tracer, w and faces at km-1
+    load_region(S.at[slot4(km - 1)], at_in + (long)(km - 1) * A, y0 - 2, x0 - 2, RY, RX, imt, jmt);
+    load_region(S.at[slot4(km - 2)], at_in + (long)(km - 2) * A, y0 - 2, x0 - 2, RY, RX, imt, jmt);
+    load_region(S.ws[slot3(km - 1)], a.ws + (long)(km - 1) * A, y0 - 1, x0 - 1, QY, QX, imt, jmt);
+    load_region(S.uw[(km - 1) & 1], a.uwf + (long)(km - 1) * A, y0 - 1, x0 - 2, QY, RX, imt, jmt);
+    load_region(S.vs[(km - 1) & 1], a.vsf + (long)(km - 1) * A, y0 - 2, x0 - 1, QY + 1, QX, imt, jmt);
+    __syncthreads();
+    predictor_level(S, a, km - 1, x0, y0);
+
+    const bool own = (i < imt && j < jmt);
+    const bool ring = own && i >= 1 && i < imt - 1 && j >= 1 && j < jmt - 1;
+    const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
+    const long qo = own ? q2(j, i, imt) : 0;
+    const int kz = own ? a.kmt[qo] : 0;
+    const int rc = (ty + 2) * RX + (tx + 2);     // own cell in H2
+    const int hc = (ty + 1) * QX + (tx + 1);     // own cell in H1
+    const int uc = (ty + 1) * RX + (tx + 2);     // own column in uw
+    const int vc = (ty + 2) * QX + (tx + 1);     // own row in vs
+    const double swv = (inner && n == 0) ? a.swv[qo] : 0.0;
+    const double stf = own ? a.stf_n[n * A + qo] : 0.0;
+    double atb_kp1 = 0.0;                                       // tracer level k+1 of atb
+    double atb_k = own ? atb_in[(long)km * A + qo] : 0.0;       // level km-1
+    double wkc_k = 0.0;
+    double e_prev = 0.0, f_prev = 0.0;
+
+    for (int k = km - 1; k >= 0; --k) {
+      // ---- phase A: loads for this level
+      __syncthreads();
+      if (k >= 2) load_region(S.at[slot4(k - 2)], at_in + (long)(k - 2) * A, y0 - 2, x0 - 2, RY, RX, imt, jmt);
+      if (k >= 1) {
+        load_region(S.ws[slot3(k - 1)], a.ws + (long)(k - 1) * A, y0 - 1, x0 - 1, QY, QX, imt, jmt);
+        load_region(S.uw[(k - 1) & 1], a.uwf + (long)(k - 1) * A, y0 - 1, x0 - 2, QY, RX, imt, jmt);
+        load_region(S.vs[(k - 1) & 1], a.vsf + (long)(k - 1) * A, y0 - 2, x0 - 1, QY + 1, QX, imt, jmt);
+      }
+      load_region(S.atb, atb_in + (long)(k + 1) * A, y0 - 2, x0 - 2, RY, RX, imt, jmt);
+      const double atb_km1 = (own && k >= 1) ? atb_in[(long)k * A + qo] : 0.0;  // tracer level k-1
+      const double wkc_km1 = (own && k >= 1) ? akt[(long)(k - 1) * A + qo] : 0.0;
+      if (k == km - 1) wkc_k = 0.0;
+      __syncthreads();
+      // ---- phase B: predictor one level up, first Laplacian at this level
+      if (k >= 1) predictor_level(S, a, k - 1, x0, y0);
+      del4_first(S, a, k, x0, y0);
+      __syncthreads();
+      // ---- phase C: own column
+      if (ring) {
+        const double* at_c = S.at[slot4(k)];
+        const double* at_u = k > 0 ? S.at[slot4(k - 1)] : nullptr;
+        const double* at_d = k < km - 1 ? S.at[slot4(k + 1)] : nullptr;
+        const double* o00 = S.a00[slot3(k)];
+        const double* omx = S.amx[slot3(k)];
+        const double* omn = S.amn[slot3(k)];
+        auto out = [&](const double* a0, const double* mx, const double* mn, int m) {
+          return a0[m] > mx[m] || a0[m] < mn[m];
+        };
+        const double tr = S.tr[hc];
+        const double c = at_c[rc], e = at_c[rc + 1], w = at_c[rc - 1], s = at_c[rc + RX], nn = at_c[rc - RX];
+        const double* uw = S.uw[k & 1];
+        const double* vs = S.vs[k & 1];
+        const double ue = uw[uc + 1], uwc = uw[uc], vsc = vs[vc], vn = vs[vc - QX];
+        const bool self = out(o00, omx, omn, hc);
+        const bool edge_k = (k == 0 || k == km - 1);
+        auto lim = [&](int m, bool guard) {
+          const bool nb = out(o00, omx, omn, m);
+          return edge_k ? (self || (nb && guard)) : ((self || nb) && guard);
+        };
+        double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
+        if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
+        else xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / S.hw[uc + 1];
+        if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
+        else xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / S.hw[uc];
+        if (lim(hc + QX, j <= jmt - 3)) xy3 = -(s - c) * fabs(vsc) * tr;
+        else xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / S.hs[vc];
+        if (lim(hc - QX, j >= 2)) xy4 = (c - nn) * fabs(vn) * tr;
+        else xy4 = dts * (c - nn) * 2.0 * tr * vn * vn / S.hs[vc - QX];
+        const double wk = S.ws[slot3(k)][hc];
+        if (k == 0) {
+          const double w1 = S.ws[slot3(1)][hc], ad = at_d[rc];
+          zb1 = 0.0;
+          if (self || (out(S.a00[slot3(1)], S.amx[slot3(1)], S.amn[slot3(1)], hc) && k <= km - 2))
+            zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
+          else
+            zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
+          za = -0.5 * odzp[0] * w1 * (ad + c);
+          zc = odzp[0] * c * w1;
+        } else if (k == km - 1) {
+          const double au = at_u[rc];
+          if (self || out(S.a00[slot3(k - 1)], S.amx[slot3(k - 1)], S.amn[slot3(k - 1)], hc))
+            zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
+          else
+            zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
+          zb2 = 0.0;
+          za = 0.5 * odzp[km - 1] * wk * (c + au);
+          zc = -odzp[km - 1] * c * wk;
+        } else {
+          const double au = at_u[rc], ad = at_d[rc], w1 = S.ws[slot3(k + 1)][hc];
+          if ((self || out(S.a00[slot3(k - 1)], S.amx[slot3(k - 1)], S.amn[slot3(k - 1)], hc)) && k >= 1)
+            zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
+          else
+            zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
+          if ((self || out(S.a00[slot3(k + 1)], S.amx[slot3(k + 1)], S.amn[slot3(k + 1)], hc)) && k <= km - 2)
+            zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
+          else
+            zb2 = 0.5 * odzp[k] * w1 * w1 * odzt[k + 1] * (c - ad) * dts;
+          za = 0.5 * odzp[k] * wk * (c + au) - 0.5 * odzp[k] * w1 * (c + ad);
+          zc = -odzp[k] * c * (wk - w1);
+        }
+        const double cx = -c * (ue - uwc) * tr * 2.0;
+        const double cy = -c * (vsc - vn) * tr * 2.0;
+        const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
+        const double y0v = ((s + c) * vsc - (c + nn) * vn) * tr;
+        const double xx = -(x0v + xy1 + xy2 + cx);
+        const double yy = -(y0v + xy3 + xy4 + cy);
+        const double zz = -(za + zb1 + zb2 + zc);
+        const double adv = xx + yy + zz;
+        const long cg = (long)k * A + qo;
+        if (DIAG) {
+          a.ax[n * F + cg] = xx;
+          a.ay[n * F + cg] = yy;
+          a.az[n * F + cg] = zz;
+        }
+        if (inner) {
+          const double vit_k = k < kz ? 1.0 : 0.0;
+          const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
+          double tf = adv * vit_k;
+          // second Laplacian (tracer_del4_2)
+          {
+            const int r = rc;
+            double h = 0.0, cc = 0.0;
+            if (k <= S.kmt[r] - 1) {
+              if (k <= S.kmt[r - RX] - 1) { h += S.dtn[hc] * S.d2[hc - QX]; cc -= S.dtn[hc]; }
+              if (k <= S.kmt[r + RX] - 1) { h += S.dts[hc] * S.d2[hc + QX]; cc -= S.dts[hc]; }
+              if (k <= S.kmt[r + 1] - 1) { h += S.dte[hc] * S.d2[hc + 1]; cc -= S.dte[hc]; }
+              if (k <= S.kmt[r - 1] - 1) { h += S.dtw[hc] * S.d2[hc - 1]; cc -= S.dtw[hc]; }
+            }
+            tf += p.ah * (cc * S.d2[hc] + h);
+          }
+          // shortwave penetration, temperature only (tracer_5)
+          if (n == 0) {
+            if (k >= 1 && k < km - 1) {
+              const double w1 = swv * a.pen[k - 1] * vit_k;
+              const double w2 = swv * a.pen[k] * vit_kp1;
+              tf = tf + (w1 - w2) * odzp[k];
+              if (DIAG) a.penetrate[cg] = (w1 - w2) * odzp[k];
+            } else if (k == 0) {
+              const double w1 = swv * a.pen[0] * ((1 < kz) ? 1.0 : 0.0);
+              tf = tf - odzp[0] * w1;
+              if (DIAG) a.penetrate[cg] = -w1 * odzp[0];
+            } else {
+              const double w2 = swv * a.pen[km - 2] * vit_k;
+              tf = tf + odzp[km - 1] * w2;
+              if (DIAG) a.penetrate[cg] = w2 * odzp[km - 1];
+            }
+          }
+          // explicit half of the vertical diffusion (tracer_5)
+          if (k >= 1 && k < km - 1) {
+            const double w1 = wkc_km1 * (atb_km1 - atb_k) * odzt[k] * vit_k;
+            const double w2 = wkc_k * (atb_k - atb_kp1) * odzt[k + 1] * vit_kp1;
+            tf = tf + odzp[k] * (w1 - w2) * 0.5;
+            if (DIAG) a.dzd[n * F + cg] = odzp[k] * (w1 - w2) * 0.5;
+          } else if (k == 0) {
+            const double w1 = wkc_k * (atb_k - atb_kp1) * odzt[1] * vit_kp1;
+            tf = tf - odzp[0] * w1 * 0.5;
+            if (DIAG) a.dzd[n * F + cg] = -odzp[0] * w1 * 0.5;
+          } else {
+            const double w2 = wkc_km1 * (atb_km1 - atb_k) * odzt[km - 1] * vit_k;
+            tf = tf + odzp[km - 1] * w2 * (1.0 - aidif);
+            if (DIAG) a.dzd[n * F + cg] = odzp[km - 1] * w2 * 0.5;
+          }
+          // surface fluxes (tracer_5 salt, tracer_6 SSS norm / heat)
+          if (k == 0) {
+            if (n == 1) {
+              if (kz > 0) tf = tf + stf * (1.0 - aidif) * odzp[0];
+              tf = tf + a.scalars[0] * vit_k;
+            } else if (kz > 0) {
+              tf = tf + stf * odzp[0] * 0.5;
+            }
+          }
+          // restoring (tracer_7, boundary_restore == 1)
+          if (p.boundary_restore == 1 && k >= 1) {
+            const double lamda = 1.0 / (15.0 * 86400.0);
+            tf = tf + vit_k * (a.restore[n * F + cg] - atb_k) * lamda;
+          }
+          // explicit update (tracer_8) and one elimination step of the
+          // implicit sweep (invtrit, tracer.cpp:923-978)
+          const double d8 = c + dts * tf;
+          double ev = 0.0, fv = d8;
+          if (k < kz) {
+            double a8, c8, b8;
+            if (k >= 1) a8 = wkc_km1 * odzt[k] * odzp[k] * dts * 0.5;
+            else a8 = odzp[0] * dts * 0.5;
+            if (k == kz - 1) {
+              c8 = odzp[kz - 1] * dts * 0.5;
+              b8 = 1.0 + a8;
+            } else if (k >= 1) {
+              c8 = wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
+              b8 = 1.0 + a8 + c8;
+            } else {
+              c8 = wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
+              b8 = 1.0 + c8;
+            }
+            if (k == kz - 1) { e_prev = 0.0; f_prev = 0.0; }
+            const double g0 = 1.0 / (b8 - c8 * e_prev);
+            ev = a8 * g0;
+            fv = (d8 + c8 * f_prev) * g0;
+            e_prev = ev;
+            f_prev = fv;
+          }
+          double* sl = scr + (long)k * NV * TTHREADS;
+          sl[tid] = ev;
+          sl[TTHREADS + tid] = fv;
+          if (DIAG) sl[2 * TTHREADS + tid] = d8;
+        }
+      }
+      atb_kp1 = atb_k;
+      atb_k = atb_km1;
+      wkc_k = wkc_km1;
+    }
+    // ---- substitution, top down, and the new state of the inner cells
+    if (inner) {
+      double x = 0.0;
+      const double stf_c = stf;
+      for (int k = 0; k < km; ++k) {
+        const double* sl = scr + (long)k * NV * TTHREADS;
+        const double ev = sl[tid], fv = sl[TTHREADS + tid];
+        const long cg = (long)k * A + qo;
+        double v;
+        if (k < kz) {
+          const double vit_k = 1.0;
+          v = (k == 0) ? (ev * stf_c + fv) * vit_k : (ev * x + fv) * vit_k;
+          x = v;
+        } else {
+          v = fv;
+        }
+        if (DIAG) {
+          const double d8 = sl[2 * TTHREADS + tid];
+          const double vit_k = k < kz ? 1.0 : 0.0;
+          const double at_old = at_in[cg];
+          a.tend[n * F + cg] = (v - at_old) / dts * vit_k;
+          if (k == 0) a.dt_diff[n * F + cg] = (v - d8) / dts * vit_k - stf_c * 0.5 * odzp[0];
+          else a.dt_diff[n * F + cg] = (v - d8) / dts * vit_k;
+          if (j == 2 && a.tripole) a.fold_save[((long)(n * km + k)) * imt + i] = d8;
+        }
+        at_out[cg] = v;
+        atb_out[(long)(k + 1) * A + qo] = v;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------- state halo
+// One block per (level, tracer): ghost cells of the new state take the halo
+// values (pop_haloupdate_tracer2 then tracer_9 for every point); cells the
+// halo does not reach take the vtl input, which is what the reference's
+// scratch use of vtl leaves there (tracer.cpp:1629-1653, 1895).
+// Launched once per tracer (temperature first), so the salinity pass can read
+// the temperature's final ghost values, which is what vtl holds in the
+// reference between the two passes.
+template <bool DIAG>
+__global__ void k_halo_state(Arena a, int n) {
+  extern __shared__ double top[];
+  const int k = blockIdx.x;
+  const int imt = a.imt, jmt = a.jmt;
+  const long A = a.A, F = a.F, FB = a.FB;
+  double* lvl = a.at[a.cur ^ 1] + n * F + (long)k * A;
+  double* lvlb = a.atb[a.cur ^ 1] + n * FB + (long)(k + 1) * A;
+  const double* old = a.at[a.cur] + n * F + (long)k * A;
+  const double* vin = a.vtl + (long)k * A;
+  const double* tnew = a.at[a.cur ^ 1] + (long)k * A;  // temperature after its halo (n == 1 only)
+  for (int i = threadIdx.x; i < imt; i += blockDim.x) top[i] = lvl[2L * imt + i];
+  __syncthreads();
+  HaloCells hc{imt, jmt, a.tripole};
+  const long nc = hc.count();
+  const double dts = a.p.dts;
+  for (long m = threadIdx.x; m < nc; m += blockDim.x) {
+    int j, i;
+    hc.cell(m, j, i);
+    const long q = (long)j * imt + i;
+    double v;
+    const bool filled = halo_cell_value(lvl, top, j, i, imt, jmt, a.ew_cyclic, a.tripole, v);
+    if (!filled) v = vin[q];
+    if (DIAG) {
+      const double vit = k < a.kmt[q] ? 1.0 : 0.0;
+      const bool inner = (i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2);
+      double ori;
+      if (inner) ori = a.fold_save[((long)(n * a.km + k)) * imt + i];
+      else if (n == 0 || !filled) ori = vin[q];
+      else ori = tnew[q];
+      a.tend[n * F + (long)k * A + q] = (v - old[q]) / dts * vit;
+      if (k == 0)
+        a.dt_diff[n * F + q] = (v - ori) / dts * vit - a.stf_n[n * A + q] * 0.5 * a.odzp[0];
+      else
+        a.dt_diff[n * F + (long)k * A + q] = (v - ori) / dts * vit;
+    }
+    lvl[q] = v;
+    lvlb[q] = v;
+  }
+}
+
+__global__ void k_vtl_clobber(Arena a) {
+  // tracer_ leaves vtl holding S with its halo (tracer.cpp:1891-1893)
+  const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.F) return;
+  a.vtl[m] = a.at[a.cur][a.F + m];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+int launch_surface(const Arena& a, cudaStream_t s) {
+  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
+  k_surface<<<g, b, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+size_t tree_sum_part_elems(long n) {
+  size_t tot = 0;
+  long nb = (n + 2 * RB - 1) / (2 * RB);
+  if (nb < 1) nb = 1;
+  tot += nb;
+  while (nb > 1) { nb = (nb + 2 * RB - 1) / (2 * RB); tot += nb; }
+  return tot + 4;
+}
+
+int launch_interior_sum_sss(const Arena& a, cudaStream_t s) {
+  SssTerm t{a.tarea, a.net + a.A, a.kmt, a.nx, a.imt};
+  int rc = tree_sum(t, (long)a.nx * a.ny, a.red_part, a.scalars + 4, s);
+  if (rc) return rc;
+  k_finish_sss<<<1, 1, 0, s>>>(a.scalars, a.scalars + 4, a.p.area_t);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_tree_sum(const double* x, long n, double* part, double* out, cudaStream_t s) {
+  return tree_sum(ArrayTerm{x}, n, part, out, s);
+}
+
+int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripole, cudaStream_t s) {
+  k_halo_r8<<<nz, 256, imt * sizeof(double), s>>>(f, imt, jmt, ew_cyclic, tripole);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_continuity_fp64(const Arena& a, cudaStream_t s) {
+  dim3 g((a.imt + TX - 1) / TX, (a.jmt + TY - 1) / TY);
+  const size_t sm = sizeof(double) * (5 * CY * CX + (size_t)a.km * TTHREADS);
+  static bool attr = false;
+  if (!attr) {
+    LT_CUDA_OK(cudaFuncSetAttribute(k_continuity, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  k_continuity<<<g, TTHREADS, sm, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int tracer_slots(const Arena& a) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long ntiles = (long)((a.imt + TX - 1) / TX) * ((a.jmt + TY - 1) / TY);
+  long slots = (long)sms * 4;
+  if (slots > 2 * ntiles) slots = 2 * ntiles;
+  return (int)slots;
+}
+
+int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots) {
+  const int ntx = (a.imt + TX - 1) / TX;
+  const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
+  const size_t sm = sizeof(TSmem);
+  static bool attr = false;
+  if (!attr) {
+    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
+  if (a.diagnostics) k_tracer64<true><<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
+  else k_tracer64<false><<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_halo_state(const Arena& a, cudaStream_t s) {
+  for (int n = 0; n < 2; ++n) {
+    if (a.diagnostics) k_halo_state<true><<<a.km, 256, a.imt * sizeof(double), s>>>(a, n);
+    else k_halo_state<false><<<a.km, 256, a.imt * sizeof(double), s>>>(a, n);
+    LT_LAUNCHED();
+  }
+  return LT_OK;
+}
+
+int launch_vtl_clobber(const Arena& a, cudaStream_t s) {
+  const long nb = (a.F + 255) / 256;
+  k_vtl_clobber<<<(unsigned)nb, 256, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+}  // namespace lt

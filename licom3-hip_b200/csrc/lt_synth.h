@@ -118,7 +118,7 @@ LT_HD double cell_akt(const CellTables& t, int n, int k, int j, int i) {
 }
 
 // ------------------------------------------------------------- host side
-#if !defined(__CUDA_ARCH__)
+// host-only builders below (parsed by every pass, called from host code only)
 
 enum HaloLoc { HALO_CENTER = 0, HALO_SWCORNER = 1 };
 
@@ -195,7 +195,11 @@ struct SynthConfig {
   double smooth_cells_1deg = 8.0;       // smoothing radius at 1 degree
   int ncc = 1, nbb = 60;
   double dts = 1800.0;
-  double ah_bihar = -1.0e17;
+  // Biharmonic tracer diffusivity (m^4/s).  0 selects the value -1e17 at the
+  // 36-column (10 degree) global grid scaled by (36/nx)^4, i.e. by the fourth
+  // power of the grid spacing, which keeps ah*dts*64/dx^4 (the forward-step
+  // stability number of del4) the same at every resolution.
+  double ah_bihar = 0.0;
   double dwndmix = 1.0e-3;
   double gamma_days = 30.0;
   double tnoise = 0.1, snoise_psu = 0.01;
@@ -401,7 +405,11 @@ inline Domain build_domain(const SynthConfig& c) {
       int m = km + 1;
       for (int dj = -1; dj <= 1; ++dj)
         for (int di = -1; di <= 1; ++di) {
-          const int jj = j + dj, ii = i + di;
+          const int jj = j + dj;
+          int ii = i + di;
+          // beyond the outer ghost columns the cyclic domain continues
+          if (c.ew_cyclic && ii < 0) ii += nx;
+          if (c.ew_cyclic && ii >= imt) ii -= nx;
           const int v = (jj < 0 || jj >= jmt || ii < 0 || ii >= imt) ? 0 : d.kmt[(long)jj * imt + ii];
           m = std::min(m, v);
         }
@@ -482,7 +490,12 @@ inline Domain build_domain(const SynthConfig& c) {
   d.gamma = 1.0 / (c.gamma_days * 86400.0);
   d.od0 = 1.0 / 1026.0;
   d.od0cp = 1.0 / (1026.0 * 3996.0);
-  d.ah = c.ah_bihar;
+  if (c.ah_bihar != 0.0) {
+    d.ah = c.ah_bihar;
+  } else {
+    const double r = 36.0 / (double)nx;
+    d.ah = -1.0e17 * (r * r) * (r * r);
+  }
   d.nss = (int)std::lround(86400.0 / c.dts);
   d.area_t = 0.0;
   for (int j = 2; j < jmt - 2; ++j)
@@ -559,6 +572,6 @@ inline void fill_akt(const Domain& d, double* akt) {
           akt[n * F + (long)k * A + (long)j * d.imt + i] = cell_akt(t, n, k, j, i);
 }
 
-#endif  // !__CUDA_ARCH__
+
 
 }  // namespace lt

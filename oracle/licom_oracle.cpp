@@ -70,6 +70,7 @@ struct Oracle {
       u_wface, v_sface, ori, temp11, vtl_work;
   double fw_norm2 = 0.0;
   int ist = 0;
+  bool tree_sum = false;  // SSS-norm sum in the device's tree order instead of sequential
 
   long count(int f) const {
     switch (field_info(f).kind) {
@@ -102,6 +103,28 @@ struct Oracle {
   long c3(int k, int j, int i) const { return (long)k * A + (long)j * imt + i; }
   long c2(int j, int i) const { return (long)j * imt + i; }
 };
+
+// The device's deterministic sum order (alternative to the reference's
+// sequential loop): blocks of 2048 consecutive terms zero-padded, each reduced
+// by pairing element t with t+stride for stride = 1024, 512, ..., 1; the
+// block sums are reduced the same way until one value remains.
+double device_tree_sum(std::vector<double> x) {
+  const size_t RB = 1024;
+  if (x.empty()) x.push_back(0.0);
+  for (;;) {
+    const size_t nb = (x.size() + 2 * RB - 1) / (2 * RB);
+    std::vector<double> part(nb);
+    std::vector<double> s(2 * RB);
+    for (size_t b = 0; b < nb; ++b) {
+      for (size_t t = 0; t < 2 * RB; ++t) s[t] = (b * 2 * RB + t < x.size()) ? x[b * 2 * RB + t] : 0.0;
+      for (size_t stride = RB; stride > 0; stride >>= 1)
+        for (size_t t = 0; t < stride; ++t) s[t] = s[t] + s[t + stride];
+      part[b] = s[0];
+    }
+    if (nb == 1) return part[0];
+    x.swap(part);
+  }
+}
 
 // ------------------------------------------------------------------ halo
 // Global-domain, single-block ghost update (POP_HaloUpdate3DR8 with
@@ -507,8 +530,16 @@ void tracer_call(Oracle& o) {
     double err_norm2 = 0.0;
     if (n == 1) {
       double err_norm1 = 0.0;
-      for (int j = 2; j < jmt - 2; ++j)
-        for (int i = 2; i < imt - 2; ++i) err_norm1 = err_norm1 + temp11[Q(j, i)];
+      if (o.tree_sum) {
+        std::vector<double> terms;
+        terms.reserve((size_t)(jmt - 4) * (imt - 4));
+        for (int j = 2; j < jmt - 2; ++j)
+          for (int i = 2; i < imt - 2; ++i) terms.push_back(temp11[Q(j, i)]);
+        err_norm1 = device_tree_sum(terms);
+      } else {
+        for (int j = 2; j < jmt - 2; ++j)
+          for (int i = 2; i < imt - 2; ++i) err_norm1 = err_norm1 + temp11[Q(j, i)];
+      }
       err_norm2 = -err_norm1 / p.area_t;
       o.fw_norm2 = err_norm2;
     }
@@ -795,6 +826,10 @@ int or_tracer_content(void* h, double* out2) {
 // standalone halo (tests): nz levels of [jmt][imt]
 int or_halo(double* a, int nz, int imt, int jmt, int ew_cyclic, int tripole) {
   halo_r8(a, nz, imt, jmt, ew_cyclic, tripole);
+  return 0;
+}
+int or_set_sum_order(void* h, int tree) {
+  static_cast<Oracle*>(h)->tree_sum = tree != 0;
   return 0;
 }
 int or_set_threads(int n) {

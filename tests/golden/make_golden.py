@@ -1,0 +1,57 @@
+"""Generate tests/golden/reference_digests.json from the reference's own code.
+
+Runs LICOM3-HIP's tracer.cpp and convadj.cpp, compiled for the CPU by
+oracle/Makefile (target ``ref``) from the reference tree, on seeded synthetic
+inputs at the reference's built-in block size (36 x 40 physical, 55 levels)
+and records SHA-256 digests of every output field plus fw_norm2.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "tests"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+import numpy as np  # noqa: E402
+from conftest import load_package  # noqa: E402
+import pyoracle  # noqa: E402
+
+CASES = [(1, 5, 20240611), (0, 3, 7), (1, 2, 99)]
+OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
+              "DT_DIFF", "DT_CONV", "PENETRATE"]
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main():
+    lt = load_package()
+    out = {}
+    for forced, nsteps, seed in CASES:
+        syn = lt.Synth(36, 40, 55, forced=forced, cap_north=0, cap_south=3, dz_top=5.0, dz_bot=300.0, seed=seed)
+        inp = syn.all_fields()
+        ref = pyoracle.Reference(syn.params)
+        ref.load(inp)
+        for s in range(nsteps):
+            ref.tracer_call(s)
+        ref.convadj()
+        key = "forced%d_steps%d_seed%d" % (forced, nsteps, seed)
+        out[key] = {
+            "inputs": {"AT": digest(inp["AT"]), "UTF": digest(inp["UTF"])},
+            "outputs": {n: digest(ref.get(n)) for n in OUT_FIELDS},
+            "fw_norm2": ref.fw_norm2(),
+            "surface_T_sample": ref.get("AT")[0, 0, 20, 5:15].tolist(),
+        }
+    with open(os.path.join(HERE, "reference_digests.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print("wrote", len(out), "cases")
+
+
+if __name__ == "__main__":
+    main()
