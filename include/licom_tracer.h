@@ -157,6 +157,9 @@ int lt_mark(lt_domain* dom, int which);
  * the recorded steps into ms[0..5] and returns the number of steps. */
 int lt_profile(lt_domain* dom, int on);
 int lt_phase_ms(lt_domain* dom, float* ms, int nphase);
+/* Select the tracer column kernel: 1 = TMA-fed pipeline (default where the
+ * row pitch allows 16-byte strides), 0 = plain-load variant. */
+int lt_use_tma(lt_domain* dom, int on);
 /* Kernels this library has launched in this process (all domains). */
 long long lt_launch_count(void);
 

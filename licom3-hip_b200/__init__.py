@@ -64,6 +64,7 @@ _SIGS = {
     "lt_step_host": ([_vp, C.POINTER(_vp), C.POINTER(C.c_double), C.POINTER(C.c_double)], _i),
     "lt_profile": ([_vp, _i], _i),
     "lt_mark": ([_vp, _i], _i),
+    "lt_use_tma": ([_vp, _i], _i),
     "lt_phase_ms": ([_vp, C.POINTER(C.c_float), _i], _i),
     "lt_launch_count": ([], C.c_longlong),
     "lt_set_device": ([_i], _i),
@@ -217,6 +218,9 @@ class TracerDomain:
         fw_norm2 written to a ctypes double; the timed end-to-end path."""
         arr = (_vp * 6)(*ptrs)
         _check(lib.lt_step_host(self.h, arr, C.byref(fw_out), None), "lt_step_host")
+
+    def use_tma(self, on=True):
+        _check(lib.lt_use_tma(self.h, int(on)), "lt_use_tma")
 
     def mark(self, which):
         _check(lib.lt_mark(self.h, int(which)), "lt_mark")

@@ -4,11 +4,14 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <new>
 #include <vector>
 #include "lt_common.cuh"
+#include "lt_tracer_tma.cuh"
+#include <cudaTypedefs.h>
 
 constexpr int LT_NPHASE = 6;       // surface, sss sum, net halo, continuity, tracer, state halo
 constexpr int LT_PROF_STEPS = 512;  // steps whose phase events are kept
@@ -25,6 +28,9 @@ struct lt_domain {
   int steps_done = 0;
   bool have_state = false;
   bool owns_stream = false;
+  bool use_tma = false;       // tracer kernel fed by TMA boxes (needs 16-byte row pitch)
+  int tma_grid = 0;           // persistent CTAs of the TMA tracer kernel
+  lt::TracerMaps maps;
 };
 
 namespace lt {
@@ -51,9 +57,26 @@ namespace {
 
 lt_domain* g_shim = nullptr;
 
+// f32 device storage of a field in a mixed-precision domain, else null
+float* field_ptr32(lt_domain* d, int f) {
+  Arena& a = d->a;
+  switch (f) {
+    case LT_F_UTF: return a.utf32;
+    case LT_F_VTF: return a.vtf32;
+    case LT_F_UTL: return a.utl32;
+    case LT_F_VTL: return a.vtl32;
+    case LT_F_AKT: return a.akt32;
+    case LT_F_WS: return a.ws32;
+    case LT_F_UTF_OUT: return a.utf_out32;
+    case LT_F_VTF_OUT: return a.vtf_out32;
+  }
+  return nullptr;
+}
+
 // device pointer of a field in the arena (current state buffer for AT/ATB)
 void* field_ptr(lt_domain* d, int f, int which_state) {
   Arena& a = d->a;
+  if (float* p = field_ptr32(d, f)) return p;
   switch (f) {
     case LT_F_AT: return a.at[which_state];
     case LT_F_ATB: return a.atb[which_state];
@@ -125,6 +148,8 @@ bool grid_ok(const lt_grid* g) {
   if (g->nx < 8 || g->ny < 8 || g->km < 3 || g->km > 256) return false;
   if (g->tripole && (g->nx % 2)) return false;
   if (g->precision != LT_PREC_FP64 && g->precision != LT_PREC_MIXED) return false;
+  // the mixed kernel takes its f32 fields by TMA: row pitch a multiple of 16 bytes
+  if (g->precision == LT_PREC_MIXED && ((g->nx + 4) % 4)) return false;
   return true;
 }
 
@@ -138,9 +163,15 @@ void plan_arena(Arena& a, Plan& pl) {
   const size_t A = a.A, F = a.F, FB = a.FB, km = a.km;
   auto D = [&](double** p, size_t n) { pl.add(reinterpret_cast<void**>(p), n * sizeof(double)); };
   auto I = [&](int** p, size_t n) { pl.add(reinterpret_cast<void**>(p), n * sizeof(int)); };
+  auto S = [&](float** p, size_t n) { pl.add(reinterpret_cast<void**>(p), n * sizeof(float)); };
   D(&a.at[0], 2 * F); D(&a.at[1], 2 * F); D(&a.atb[0], 2 * FB); D(&a.atb[1], 2 * FB);
-  D(&a.utf, F); D(&a.vtf, F); D(&a.utl, F); D(&a.vtl, F); D(&a.akt, 2 * F);
-  D(&a.utf_out, F); D(&a.vtf_out, F); D(&a.ws, FB); D(&a.uwf, F); D(&a.vsf, F);
+  if (a.precision == LT_PREC_MIXED) {
+    S(&a.utf32, F); S(&a.vtf32, F); S(&a.utl32, F); S(&a.vtl32, F); S(&a.akt32, 2 * F);
+    S(&a.utf_out32, F); S(&a.vtf_out32, F); S(&a.ws32, FB); S(&a.wkd32, F); S(&a.wkb32, F);
+  } else {
+    D(&a.utf, F); D(&a.vtf, F); D(&a.utl, F); D(&a.vtl, F); D(&a.akt, 2 * F);
+    D(&a.utf_out, F); D(&a.vtf_out, F); D(&a.ws, FB); D(&a.uwf, F); D(&a.vsf, F); D(&a.wka, F);
+  }
   D(&a.h0f, A); D(&a.h0l, A); D(&a.h0f_out, A); D(&a.net, 2 * A);
   double** two_d[] = {&a.swv, &a.nswv, &a.sst, &a.sss, &a.fresh, &a.seaice, &a.tarea, &a.tarea_r, &a.htw,
                       &a.hts, &a.hun, &a.hue, &a.dxu, &a.dyu, &a.ahf, &a.dtn, &a.dts, &a.dte, &a.dtw,
@@ -183,6 +214,49 @@ long slots_for(const Arena& a, int sms) {
   return s;
 }
 
+}  // namespace
+
+bool make_tensor_map_3d(CUtensorMap* map, const void* base, int esize, long nx, long ny, long nz, int bx, int by) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", reinterpret_cast<void**>(&encode), cudaEnableDefault,
+                                &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !encode)
+      return false;
+  }
+  if ((nx * esize) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) % 16) != 0 || (bx * esize) % 16 != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)(nx * esize), (cuuint64_t)(nx * ny * esize)};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = encode(map, esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                            const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+bool build_tracer_maps(const Arena& a, TracerMaps* m) {
+  const long imt = a.imt, jmt = a.jmt, km = a.km;
+  bool ok = true;
+  for (int b = 0; b < 2; ++b) {
+    ok = ok && make_tensor_map_3d(&m->at[b], a.at[b], 8, imt, jmt, 2 * km, SW, TY + 4);
+    ok = ok && make_tensor_map_3d(&m->atb[b], a.atb[b], 8, imt, jmt, 2 * (km + 1), SW, TY + 4);
+  }
+  const bool mx = a.precision == LT_PREC_MIXED;
+  const int es = mx ? 4 : 8;
+  ok = ok && make_tensor_map_3d(&m->ws, mx ? (const void*)a.ws32 : a.ws, es, imt, jmt, km + 1, SW, TY + 2);
+  // f64: face transports u_wface (rows y0-1..) and v_sface (rows y0-2..);
+  // mixed: the U-point means wkd, wkb (rows y0-2..), faces formed in the kernel
+  ok = ok && make_tensor_map_3d(&m->uw, mx ? (const void*)a.wkd32 : a.uwf, es, imt, jmt, km, SW, mx ? TY + 3 : TY + 2);
+  ok = ok && make_tensor_map_3d(&m->vs, mx ? (const void*)a.wkb32 : a.vsf, es, imt, jmt, km, SW, TY + 3);
+  ok = ok && make_tensor_map_3d(&m->akt, mx ? (const void*)a.akt32 : a.akt, es, imt, jmt, 2 * km, TX, TY);
+  return ok;
+}
+
+namespace {
+
 int run_step(lt_domain* d) {
   Arena& a = d->a;
   cudaStream_t s = d->stream;
@@ -200,9 +274,19 @@ int run_step(lt_domain* d) {
   mark(2);
   if ((rc = launch_halo_r8(a.net, 2, a.imt, a.jmt, a.ew_cyclic, a.tripole, s))) return rc;
   mark(3);
-  if ((rc = launch_continuity_fp64(a, s))) return rc;
-  mark(4);
-  if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
+  if (a.precision == LT_PREC_MIXED) {
+    if ((rc = launch_continuity_mixed(a, s))) return rc;
+    mark(4);
+    if ((rc = launch_tracer_tma_mixed(a, d->maps, s, d->tma_grid))) return rc;
+  } else {
+    if ((rc = launch_continuity_fp64(a, s))) return rc;
+    mark(4);
+    if (d->use_tma) {
+      if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid))) return rc;
+    } else {
+      if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
+    }
+  }
   mark(5);
   if ((rc = launch_halo_state(a, s))) return rc;
   mark(6);
@@ -335,6 +419,12 @@ int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
   d->owns_stream = true;
   cudaEventCreate(&d->ev0);
   cudaEventCreate(&d->ev1);
+  // TMA-fed tracer kernel where the row pitch is a multiple of 16 bytes
+  d->use_tma = build_tracer_maps(d->a, &d->maps);
+  // one persistent CTA per resident slot: the f64 kernel fits 3 per SM, the
+  // mixed kernel 4 (its __launch_bounds__ and shared-memory footprint)
+  const long per_sm = d->a.precision == LT_PREC_MIXED ? 4 : 3;
+  d->tma_grid = (int)std::min<long>(d->a.col_scratch_slots, (long)sms * per_sm);
   cudaDeviceSynchronize();
   *out = d;
   return LT_OK;
@@ -372,6 +462,23 @@ static int xfer(lt_domain* d, int f, void* ptr, size_t nbytes, cudaMemcpyKind ki
   }
   void* dev = field_ptr(d, f, d->a.cur);
   if (!dev) { set_error("field %d not held by this domain (diagnostics/restore off)", f); return LT_E_STATE; }
+  if (float* d32 = field_ptr32(d, f)) {
+    // f32 storage (mixed precision): the boundary stays f64, converted on the device
+    const long n = (long)(nbytes / sizeof(double));
+    double* tmp = nullptr;
+    LT_CUDA_OK(cudaMallocAsync(reinterpret_cast<void**>(&tmp), nbytes, d->stream));
+    int rc = LT_OK;
+    if (set) {
+      if (cudaMemcpyAsync(tmp, ptr, nbytes, kind, d->stream) != cudaSuccess) rc = LT_E_CUDA;
+      if (!rc) rc = launch_f64_to_f32(tmp, d32, n, d->stream);
+    } else {
+      rc = launch_f32_to_f64(d32, tmp, n, d->stream);
+      if (!rc && cudaMemcpyAsync(ptr, tmp, nbytes, kind, d->stream) != cudaSuccess) rc = LT_E_CUDA;
+    }
+    cudaFreeAsync(tmp, d->stream);
+    LT_CUDA_OK(cudaStreamSynchronize(d->stream));
+    return rc;
+  }
   if (set) {
     LT_CUDA_OK(cudaMemcpyAsync(dev, ptr, nbytes, kind, d->stream));
     if (f == LT_F_AT || f == LT_F_ATB) {  // both state buffers start equal
@@ -489,6 +596,16 @@ int lt_last_step_ms(lt_domain* d, float* ms) {
   return LT_OK;
 }
 
+int lt_use_tma(lt_domain* d, int on) {
+  if (!d) return LT_E_INVALID;
+  if (on && !build_tracer_maps(d->a, &d->maps)) {
+    set_error("lt_use_tma: row pitch of this domain does not allow TMA boxes");
+    return LT_E_INVALID;
+  }
+  d->use_tma = on != 0;
+  return LT_OK;
+}
+
 int lt_shim_bind(lt_domain* d) {
   g_shim = d;
   return LT_OK;
@@ -502,11 +619,18 @@ void tracer_(int ii) {
   if (!d) { set_error("tracer_: no domain bound (lt_shim_bind)"); return; }
   Arena& a = d->a;
   if (run_step(d)) return;
-  const size_t fb = sizeof(double) * a.F;
-  cudaMemcpyAsync(a.utf, a.utf_out, fb, cudaMemcpyDeviceToDevice, d->stream);
-  cudaMemcpyAsync(a.vtf, a.vtf_out, fb, cudaMemcpyDeviceToDevice, d->stream);
+  if (a.precision == LT_PREC_MIXED) {
+    const size_t fb = sizeof(float) * a.F;
+    cudaMemcpyAsync(a.utf32, a.utf_out32, fb, cudaMemcpyDeviceToDevice, d->stream);
+    cudaMemcpyAsync(a.vtf32, a.vtf_out32, fb, cudaMemcpyDeviceToDevice, d->stream);
+    launch_f64_to_f32(a.at[a.cur] + a.F, a.vtl32, a.F, d->stream);
+  } else {
+    const size_t fb = sizeof(double) * a.F;
+    cudaMemcpyAsync(a.utf, a.utf_out, fb, cudaMemcpyDeviceToDevice, d->stream);
+    cudaMemcpyAsync(a.vtf, a.vtf_out, fb, cudaMemcpyDeviceToDevice, d->stream);
+    launch_vtl_clobber(a, d->stream);
+  }
   cudaMemcpyAsync(a.h0f, a.h0f_out, sizeof(double) * a.A, cudaMemcpyDeviceToDevice, d->stream);
-  launch_vtl_clobber(a, d->stream);
   cudaStreamSynchronize(d->stream);
 }
 

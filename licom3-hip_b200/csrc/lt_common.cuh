@@ -42,6 +42,12 @@ struct Arena {
 
   // step scratch
   double *uwf, *vsf;          // face transports u_wface, v_sface [km][jmt][imt]
+  double *wka;                // horizontal divergence [km][jmt][imt]
+  // mixed precision: f32 storage of the dynamics inputs, mixing and the
+  // derived fields (the f64 pointers above are null for these; the
+  // horizontal divergence lives only in registers of the continuity march)
+  float *utf32, *vtf32, *utl32, *vtl32, *akt32, *ws32, *utf_out32, *vtf_out32;
+  float *wkd32, *wkb32;       // U-point mean velocities wkd, wkb; the tracer kernel forms the faces from them
   double *stf_ssh;            // [jmt][imt] 0.5*(h0f*onbc + h0l)
   double *stf_n;              // [2][jmt][imt] surface flux per tracer (T, S)
   double *red_part;           // partial sums of the deterministic reductions
@@ -85,6 +91,9 @@ int launch_convadj(const Arena& a, cudaStream_t s);
 int launch_check_numeric(const Arena& a, cudaStream_t s);
 int launch_derive_masks(const Arena& a, cudaStream_t s);
 int launch_vtl_clobber(const Arena& a, cudaStream_t s);
+int launch_continuity_mixed(const Arena& a, cudaStream_t s);
+int launch_f64_to_f32(const double* x, float* y, long n, cudaStream_t s);
+int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s);
 int tracer_slots(const Arena& a);
 size_t tree_sum_part_elems(long n);
 

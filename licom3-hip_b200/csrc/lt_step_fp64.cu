@@ -19,6 +19,7 @@
 #include <cstdio>
 #include "lt_common.cuh"
 #include "lt_halo.cuh"
+#include "lt_tracer_tma.cuh"
 
 namespace lt {
 
@@ -42,7 +43,11 @@ __global__ void k_surface(Arena a) {
   const double ssh = 0.5 * h0 + 0.5 * a.h0l[q];
   a.stf_ssh[q] = ssh;
   if (i >= 1 && i < a.imt - 1 && j >= 1 && j < a.jmt - 1) {
-    if (a.akt[q] < p.dwndmix) a.akt[q] = p.dwndmix;
+    if (a.akt) {
+      if (a.akt[q] < p.dwndmix) a.akt[q] = p.dwndmix;
+    } else if (a.akt32[q] < (float)p.dwndmix) {
+      a.akt32[q] = (float)p.dwndmix;
+    }
   }
   double sT = ssh, sS = ssh;
   if (a.kmt[q] > 0) {
@@ -225,6 +230,82 @@ __global__ void __launch_bounds__(TTHREADS) k_continuity(Arena a) {
   double wsp = a.ws[qo];  // level 0 is never written by the step
   for (int k = 1; k < km; ++k) {
     const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + s_wka[(k - 1) * TTHREADS + tid]));
+    a.ws[(long)k * A + qo] = raw * fac;
+    wsp = raw;
+  }
+}
+
+// Continuity in two fully parallel passes (used when the arena holds a wka
+// buffer).  k_cont_level: one thread per cell of one level; U-point
+// velocities of a 32 x 8 block plus one column east and one row north staged
+// in shared memory; writes the scaled utf/vtf, both face transports and the
+// masked divergence wka (tracer_1, upwell_2, operators_div,
+// advection_tracer_1_0).  k_cont_column: one thread per column; the column
+// divergence W in level order and w by upward integration (upwell_3/4).
+__global__ void __launch_bounds__(256) k_cont_level(Arena a) {
+  constexpr int BX = 32, BY = 8, UX = BX + 1, UY = BY + 1;
+  __shared__ double s_wkd[UY * UX], s_wkb[UY * UX], s_uk[UY * UX], s_vk[UY * UX];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, k = blockIdx.z;
+  const int imt = a.imt, jmt = a.jmt;
+  const long lvl = (long)k * a.A;
+  const lt_params& p = a.p;
+  for (int m = tid; m < UY * UX; m += BX * BY) {
+    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+    double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
+    if (uj >= 0 && uj < jmt && ui < imt) {
+      const long q = q2(uj, ui, imt);
+      const long c = lvl + q;
+      wkd = 0.5 * (a.utf[c] * p.oncc) + 0.5 * a.utl[c];
+      wkb = 0.5 * (a.vtf[c] * p.oncc) + 0.5 * a.vtl[c];
+      if (uj < jmt - 1 && ui >= 1) {
+        const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
+                            a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
+        const double fac = 1.0 + work * a.ohbu[q];
+        uk = fac * wkd;
+        vk = fac * wkb;
+      }
+    }
+    s_wkd[m] = wkd; s_wkb[m] = wkb; s_uk[m] = uk; s_vk[m] = vk;
+  }
+  __syncthreads();
+  const int i = x0 + tx, j = y0 + ty;
+  if (i >= imt || j >= jmt) return;
+  const long qo = q2(j, i, imt);
+  const long c = lvl + qo;
+  const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
+  a.utf_out[c] = a.utf[c] * p.oncc;
+  a.vtf_out[c] = a.vtf[c] * p.oncc;
+  if (j >= 1 && j < jmt - 1) a.uwf[c] = (s_wkd[mn] + s_wkd[m0]) * a.htw[qo] * 0.25;
+  if (i >= 1 && i < imt - 1) a.vsf[c] = (s_wkb[m0] + s_wkb[m0 + 1]) * a.hts[qo] * 0.25;
+  double wka = 0.0;
+  if (j >= 1 && i < imt - 1 && k <= a.kmt[qo] - 1) {
+    const double east = (s_uk[m0 + 1] + s_uk[mn + 1]) * a.htw[qo + 1];
+    const double west = (s_uk[m0] + s_uk[mn]) * a.htw[qo];
+    const double south = (s_vk[m0 + 1] + s_vk[m0]) * a.hts[qo];
+    const double north = (s_vk[mn + 1] + s_vk[mn]) * a.hts[qo - imt];
+    wka = 0.5 * (east - west + south - north) * a.tarea_r[qo];
+  }
+  a.wka[c] = wka;
+}
+
+__global__ void __launch_bounds__(256) k_cont_column(Arena a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  if (!(j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1)) return;
+  const long qo = q2(j, i, imt);
+  const long A = a.A;
+  const int kz = a.kmt[qo];
+  double W = 0.0;
+#pragma unroll 8
+  for (int k = 0; k < km; ++k) W = W - a.dzp[k] * a.wka[(long)k * A + qo] * (k < kz ? 1.0 : 0.0);
+  const double ohbt = a.ohbt[qo];
+  const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
+  double wsp = a.ws[qo];
+#pragma unroll 8
+  for (int k = 1; k < km; ++k) {
+    const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + a.wka[(long)(k - 1) * A + qo]));
     a.ws[(long)k * A + qo] = raw * fac;
     wsp = raw;
   }
@@ -677,6 +758,417 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
   }
 }
 
+// -------------------------------------------- tracer march, TMA pipeline
+// Same arithmetic as k_tracer64 (term for term), data staged by TMA boxes.
+// Four level slots (k+1 .. k-2 in use; the slot freed after step k receives
+// level k-3), predictor ring and first Laplacian in shared memory; the 2-D
+// metric terms are read through L1 (the same 2-D values serve every level), so
+// three CTAs fit on an SM.
+constexpr int NSX = 4;
+struct ExSmem {
+  LevelSlot<double> slot[NSX];
+  double a00[3][HN], amx[3][HN], amn[3][HN];
+  double d2[HN];
+  int kmt[(TY + 4) * SW];
+  uint64_t bar[NSX];
+};
+
+__device__ void predictor_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0) {
+  const int km = a.km, imt = a.imt, jmt = a.jmt;
+  const double dts = a.p.dts;
+  const double* odzp = a.odzp;
+  const double* odzt = a.odzt;
+  const LevelSlot<double>& Lc = S.slot[kk % NSX];
+  const double* at_c = Lc.at;
+  const double* at_u = kk > 0 ? S.slot[(kk - 1) % NSX].at : nullptr;
+  const double* at_d = kk < km - 1 ? S.slot[(kk + 1) % NSX].at : nullptr;
+  const double* ws_c = Lc.ws;
+  const double* ws_d = kk < km - 1 ? S.slot[(kk + 1) % NSX].ws : nullptr;
+  const double* uw = Lc.uw;
+  const double* vs = Lc.vs;
+  double* o00 = S.a00[kk % 3];
+  double* omx = S.amx[kk % 3];
+  double* omn = S.amn[kk % 3];
+  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
+    const int hj = m / HQX, hi = m % HQX;
+    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+    if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) {
+      o00[m] = 0.0; omx[m] = 0.0; omn[m] = 0.0;
+      continue;
+    }
+    const int r = r2(hj, hi), u = ru(hj, hi), v = rv(hj, hi);
+    const long q = (long)gj * imt + gi;
+    const double tr = __ldg(a.tarea_r + q);
+    const double hwe = __ldg(a.htw + q + 1) * __ldg(a.hun + q + 1), hww = __ldg(a.htw + q) * __ldg(a.hun + q);
+    const double hss = __ldg(a.hts + q) * __ldg(a.hue + q), hsn = __ldg(a.hts + q - imt) * __ldg(a.hue + q - imt);
+    const double c = at_c[r], e = at_c[r + 1], w = at_c[r - 1], s = at_c[r + SW], n = at_c[r - SW];
+    const double ue = uw[u + 1], uwc = uw[u];
+    const double vsc = vs[v], vn = vs[v - SW];
+    const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
+    const double y0v = ((s + c) * vsc - (c + n) * vn) * tr;
+    const double xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
+    const double xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
+    const double xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
+    const double xy4 = dts * (c - n) * 2.0 * tr * vn * vn / hsn;
+    const double cx = -c * (ue - uwc) * tr * 2.0;
+    const double cy = -c * (vsc - vn) * tr * 2.0;
+    double za, zb1, zb2, zc;
+    const double wk = ws_c[u];
+    if (kk == 0) {
+      const double w1 = ws_d[u], ad = at_d[r];
+      za = -0.5 * odzp[0] * w1 * (ad + c);
+      zb1 = 0.0;
+      zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
+      zc = odzp[0] * c * w1;
+    } else if (kk == km - 1) {
+      const double au = at_u[r];
+      za = 0.5 * odzp[km - 1] * wk * (c + au);
+      zb1 = -0.5 * odzp[km - 1] * wk * wk * odzt[km - 1] * (au - c) * dts;
+      zb2 = 0.0;
+      zc = -odzp[km - 1] * c * wk;
+    } else {
+      const double au = at_u[r], ad = at_d[r], w1 = ws_d[u];
+      za = 0.5 * odzp[kk] * wk * (c + au) - 0.5 * odzp[kk] * w1 * (c + ad);
+      zb1 = -0.5 * odzp[kk] * wk * wk * odzt[kk] * (au - c) * dts;
+      zb2 = 0.5 * odzp[kk] * w1 * w1 * odzt[kk + 1] * (c - ad) * dts;
+      zc = -odzp[kk] * c * (wk - w1);
+    }
+    const double xx = -(x0v + xy1 + xy2 + cx);
+    const double yy = -(y0v + xy3 + xy4 + cy);
+    const double zz = -(zb1 + zb2 + za + zc);
+    o00[m] = c + (xx + yy + zz) * dts;
+    auto vitk = [&](int kl, int rr) { return (kl < S.kmt[rr]) ? 1.0 : 0.0; };
+    auto mxv = [&](double t, double vt) { return t * vt + (1.0 - vt) * -1.0e10; };
+    auto mnv = [&](double t, double vt) { return t * vt + (1.0 - vt) * 1.0e10; };
+    const double vc = vitk(kk, r), vn_ = vitk(kk, r - SW), vs_ = vitk(kk, r + SW), vw = vitk(kk, r - 1),
+                 ve = vitk(kk, r + 1);
+    double hi_ = mxv(c, vc), lo_ = mnv(c, vc), t;
+    t = mxv(n, vn_); if (hi_ < t) hi_ = t;
+    t = mxv(s, vs_); if (hi_ < t) hi_ = t;
+    t = mxv(w, vw); if (hi_ < t) hi_ = t;
+    t = mxv(e, ve); if (hi_ < t) hi_ = t;
+    t = mnv(n, vn_); if (lo_ > t) lo_ = t;
+    t = mnv(s, vs_); if (lo_ > t) lo_ = t;
+    t = mnv(w, vw); if (lo_ > t) lo_ = t;
+    t = mnv(e, ve); if (lo_ > t) lo_ = t;
+    if (kk > 0) {
+      const double au = at_u[r], vu = vitk(kk - 1, r);
+      t = mxv(au, vu); if (hi_ < t) hi_ = t;
+      t = mnv(au, vu); if (lo_ > t) lo_ = t;
+    }
+    if (kk < km - 1) {
+      const double ad = at_d[r], vd = vitk(kk + 1, r);
+      t = mxv(ad, vd); if (hi_ < t) hi_ = t;
+      t = mnv(ad, vd); if (lo_ > t) lo_ = t;
+    }
+    omx[m] = hi_;
+    omn[m] = lo_;
+  }
+}
+
+__device__ void del4_first_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0) {
+  const double* atb = S.slot[kk % NSX].atb;
+  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
+    const int hj = m / HQX, hi = m % HQX;
+    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+    if (!(gi >= 1 && gi < a.imt - 1 && gj >= 1 && gj < a.jmt - 1)) { S.d2[m] = 0.0; continue; }
+    const int r = r2(hj, hi);
+    const long q = (long)gj * a.imt + gi;
+    double h = 0.0, cc = 0.0;
+    if (kk <= S.kmt[r] - 1) {
+      if (kk <= S.kmt[r - SW] - 1) { const double cf = __ldg(a.dtn + q); h += cf * atb[r - SW]; cc -= cf; }
+      if (kk <= S.kmt[r + SW] - 1) { const double cf = __ldg(a.dts + q); h += cf * atb[r + SW]; cc -= cf; }
+      if (kk <= S.kmt[r + 1] - 1) { const double cf = __ldg(a.dte + q); h += cf * atb[r + 1]; cc -= cf; }
+      if (kk <= S.kmt[r - 1] - 1) { const double cf = __ldg(a.dtw + q); h += cf * atb[r - 1]; cc -= cf; }
+    }
+    S.d2[m] = __ldg(a.ahf + q) * (cc * atb[r] + h);
+  }
+}
+
+struct ExactHw {
+  __device__ double operator()(double a, double b) const { return a * b; }
+};
+
+template <bool DIAG>
+__global__ void __launch_bounds__(TTHREADS, 3)
+    k_tracer_tma64(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
+  extern __shared__ __align__(128) unsigned char smem_tma[];
+  ExSmem& S = *reinterpret_cast<ExSmem*>(smem_tma);
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A, F = a.F, FB = a.FB;
+  const lt_params& p = a.p;
+  const double dts = p.dts;
+  const double aidif = 0.5;
+  const double* __restrict__ odzp = a.odzp;
+  const double* __restrict__ odzt = a.odzt;
+  const int NV = a.nv_scratch;
+  double* scr = a.col_scratch + (long)blockIdx.x * km * NV * TTHREADS;
+  if (tid == 0) {
+    for (int s = 0; s < NSX; ++s) mbar_init(&S.bar[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t par = 0, outstanding = 0;
+
+  for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x) {
+    const long tile = w >> 1;
+    const int n = (int)(w & 1);
+    const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * TY;
+    const int i = x0 + tx, j = y0 + ty;
+    const double* at_in = a.at[a.cur] + n * F;
+    double* at_out = a.at[a.cur ^ 1] + n * F;
+    double* atb_out = a.atb[a.cur ^ 1] + n * FB;
+
+    __syncthreads();  // the previous item is done with every slot
+    auto issue = [&](int L) {
+      if (tid == 0) issue_level(S.slot[L % NSX], &S.bar[L % NSX], maps, a.cur, n, km, L, x0, y0);
+      outstanding |= 1u << (L % NSX);
+    };
+    auto wait = [&](int L) -> bool {
+      const int s = L % NSX;
+      const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u);
+      if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
+      return ok;
+    };
+    const int lowest_pro = km - NSX > 0 ? km - NSX : 0;
+    for (int L = km - 1; L >= lowest_pro; --L) issue(L);
+    for (int m = tid; m < (TY + 4) * SW; m += TTHREADS) {
+      const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
+      S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
+    }
+
+    const bool own = (i < imt && j < jmt);
+    const bool ring = own && i >= 1 && i < imt - 1 && j >= 1 && j < jmt - 1;
+    const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
+    const long qo = own ? (long)j * imt + i : 0;
+    const int kz = own ? a.kmt[qo] : 0;
+    const int hc = (ty + 1) * HQX + (tx + 1);
+    const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1), vc = rv(ty + 1, tx + 1), ac = ty * TX + tx;
+    const double swv = (inner && n == 0) ? a.swv[qo] : 0.0;
+    const double stf = own ? a.stf_n[n * A + qo] : 0.0;
+    const double err_norm2 = a.scalars[0];
+    double e_prev = 0.0, f_prev = 0.0;
+
+    {
+      const bool ok = wait(km - 1) && wait(km - 2);
+      // a wait that ran out anywhere in the CTA sends every thread out together
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
+    }
+    predictor_tma(S, a, km - 1, x0, y0);
+
+    for (int k = km - 1; k >= 0; --k) {
+      const bool ok = (k >= 2) ? wait(k - 2) : true;
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
+      // ---- phase B
+      if (k >= 1) predictor_tma(S, a, k - 1, x0, y0);
+      del4_first_tma(S, a, k, x0, y0);
+      __syncthreads();
+      // ---- phase C
+      if (ring) {
+        const LevelSlot<double>& Lk = S.slot[k % NSX];
+        const double* at_c = Lk.at;
+        const double* at_u = k > 0 ? S.slot[(k - 1) % NSX].at : nullptr;
+        const double* at_d = k < km - 1 ? S.slot[(k + 1) % NSX].at : nullptr;
+        const double* o00 = S.a00[k % 3];
+        const double* omx = S.amx[k % 3];
+        const double* omn = S.amn[k % 3];
+        auto out = [&](const double* a0, const double* mx, const double* mn, int m) {
+          return a0[m] > mx[m] || a0[m] < mn[m];
+        };
+        const double tr = __ldg(a.tarea_r + qo);
+        const double hwe = __ldg(a.htw + qo + 1) * __ldg(a.hun + qo + 1), hww = __ldg(a.htw + qo) * __ldg(a.hun + qo);
+        const double hss = __ldg(a.hts + qo) * __ldg(a.hue + qo);
+        const double hsn = __ldg(a.hts + qo - imt) * __ldg(a.hue + qo - imt);
+        const double c = at_c[rc], e = at_c[rc + 1], w = at_c[rc - 1], s = at_c[rc + SW], nn = at_c[rc - SW];
+        const double ue = Lk.uw[uc + 1], uwc = Lk.uw[uc], vsc = Lk.vs[vc], vn = Lk.vs[vc - SW];
+        const bool self = out(o00, omx, omn, hc);
+        const bool edge_k = (k == 0 || k == km - 1);
+        auto lim = [&](int m, bool guard) {
+          const bool nb = out(o00, omx, omn, m);
+          return edge_k ? (self || (nb && guard)) : ((self || nb) && guard);
+        };
+        double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
+        if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
+        else xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
+        if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
+        else xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
+        if (lim(hc + HQX, j <= jmt - 3)) xy3 = -(s - c) * fabs(vsc) * tr;
+        else xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
+        if (lim(hc - HQX, j >= 2)) xy4 = (c - nn) * fabs(vn) * tr;
+        else xy4 = dts * (c - nn) * 2.0 * tr * vn * vn / hsn;
+        const double wk = Lk.ws[uc];
+        if (k == 0) {
+          const double w1 = S.slot[1 % NSX].ws[uc], ad = at_d[rc];
+          zb1 = 0.0;
+          if (self || (out(S.a00[1 % 3], S.amx[1 % 3], S.amn[1 % 3], hc) && k <= km - 2))
+            zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
+          else
+            zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
+          za = -0.5 * odzp[0] * w1 * (ad + c);
+          zc = odzp[0] * c * w1;
+        } else if (k == km - 1) {
+          const double au = at_u[rc];
+          if (self || out(S.a00[(k - 1) % 3], S.amx[(k - 1) % 3], S.amn[(k - 1) % 3], hc))
+            zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
+          else
+            zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
+          zb2 = 0.0;
+          za = 0.5 * odzp[km - 1] * wk * (c + au);
+          zc = -odzp[km - 1] * c * wk;
+        } else {
+          const double au = at_u[rc], ad = at_d[rc], w1 = S.slot[(k + 1) % NSX].ws[uc];
+          if ((self || out(S.a00[(k - 1) % 3], S.amx[(k - 1) % 3], S.amn[(k - 1) % 3], hc)) && k >= 1)
+            zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
+          else
+            zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
+          if ((self || out(S.a00[(k + 1) % 3], S.amx[(k + 1) % 3], S.amn[(k + 1) % 3], hc)) && k <= km - 2)
+            zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
+          else
+            zb2 = 0.5 * odzp[k] * w1 * w1 * odzt[k + 1] * (c - ad) * dts;
+          za = 0.5 * odzp[k] * wk * (c + au) - 0.5 * odzp[k] * w1 * (c + ad);
+          zc = -odzp[k] * c * (wk - w1);
+        }
+        const double cx = -c * (ue - uwc) * tr * 2.0;
+        const double cy = -c * (vsc - vn) * tr * 2.0;
+        const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
+        const double y0v = ((s + c) * vsc - (c + nn) * vn) * tr;
+        const double xx = -(x0v + xy1 + xy2 + cx);
+        const double yy = -(y0v + xy3 + xy4 + cy);
+        const double zz = -(za + zb1 + zb2 + zc);
+        const double adv = xx + yy + zz;
+        const long cg = (long)k * A + qo;
+        if (DIAG) {
+          a.ax[n * F + cg] = xx;
+          a.ay[n * F + cg] = yy;
+          a.az[n * F + cg] = zz;
+        }
+        if (inner) {
+          const double vit_k = k < kz ? 1.0 : 0.0;
+          const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
+          const double atb_k = Lk.atb[rc];
+          const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSX].atb[rc] : 0.0;
+          const double atb_kp1 = k < km - 1 ? S.slot[(k + 1) % NSX].atb[rc] : 0.0;
+          const double wkc_k = Lk.akt[ac];
+          const double wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSX].akt[ac] : 0.0;
+          double tf = adv * vit_k;
+          {
+            const int r = rc;
+            double h = 0.0, cc = 0.0;
+            if (k <= S.kmt[r] - 1) {
+              if (k <= S.kmt[r - SW] - 1) { const double cf = __ldg(a.dtn + qo); h += cf * S.d2[hc - HQX]; cc -= cf; }
+              if (k <= S.kmt[r + SW] - 1) { const double cf = __ldg(a.dts + qo); h += cf * S.d2[hc + HQX]; cc -= cf; }
+              if (k <= S.kmt[r + 1] - 1) { const double cf = __ldg(a.dte + qo); h += cf * S.d2[hc + 1]; cc -= cf; }
+              if (k <= S.kmt[r - 1] - 1) { const double cf = __ldg(a.dtw + qo); h += cf * S.d2[hc - 1]; cc -= cf; }
+            }
+            tf += p.ah * (cc * S.d2[hc] + h);
+          }
+          if (n == 0) {
+            if (k >= 1 && k < km - 1) {
+              const double w1 = swv * a.pen[k - 1] * vit_k;
+              const double w2 = swv * a.pen[k] * vit_kp1;
+              tf = tf + (w1 - w2) * odzp[k];
+              if (DIAG) a.penetrate[cg] = (w1 - w2) * odzp[k];
+            } else if (k == 0) {
+              const double w1 = swv * a.pen[0] * ((1 < kz) ? 1.0 : 0.0);
+              tf = tf - odzp[0] * w1;
+              if (DIAG) a.penetrate[cg] = -w1 * odzp[0];
+            } else {
+              const double w2 = swv * a.pen[km - 2] * vit_k;
+              tf = tf + odzp[km - 1] * w2;
+              if (DIAG) a.penetrate[cg] = w2 * odzp[km - 1];
+            }
+          }
+          if (k >= 1 && k < km - 1) {
+            const double w1 = wkc_km1 * (atb_km1 - atb_k) * odzt[k] * vit_k;
+            const double w2 = wkc_k * (atb_k - atb_kp1) * odzt[k + 1] * vit_kp1;
+            tf = tf + odzp[k] * (w1 - w2) * 0.5;
+            if (DIAG) a.dzd[n * F + cg] = odzp[k] * (w1 - w2) * 0.5;
+          } else if (k == 0) {
+            const double w1 = wkc_k * (atb_k - atb_kp1) * odzt[1] * vit_kp1;
+            tf = tf - odzp[0] * w1 * 0.5;
+            if (DIAG) a.dzd[n * F + cg] = -odzp[0] * w1 * 0.5;
+          } else {
+            const double w2 = wkc_km1 * (atb_km1 - atb_k) * odzt[km - 1] * vit_k;
+            tf = tf + odzp[km - 1] * w2 * (1.0 - aidif);
+            if (DIAG) a.dzd[n * F + cg] = odzp[km - 1] * w2 * 0.5;
+          }
+          if (k == 0) {
+            if (n == 1) {
+              if (kz > 0) tf = tf + stf * (1.0 - aidif) * odzp[0];
+              tf = tf + err_norm2 * vit_k;
+            } else if (kz > 0) {
+              tf = tf + stf * odzp[0] * 0.5;
+            }
+          }
+          if (p.boundary_restore == 1 && k >= 1) {
+            const double lamda = 1.0 / (15.0 * 86400.0);
+            tf = tf + vit_k * (a.restore[n * F + cg] - atb_k) * lamda;
+          }
+          const double d8 = c + dts * tf;
+          double ev = 0.0, fv = d8;
+          if (k < kz) {
+            double a8, c8, b8;
+            if (k >= 1) a8 = wkc_km1 * odzt[k] * odzp[k] * dts * 0.5;
+            else a8 = odzp[0] * dts * 0.5;
+            if (k == kz - 1) {
+              c8 = odzp[kz - 1] * dts * 0.5;
+              b8 = 1.0 + a8;
+            } else if (k >= 1) {
+              c8 = wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
+              b8 = 1.0 + a8 + c8;
+            } else {
+              c8 = wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
+              b8 = 1.0 + c8;
+            }
+            if (k == kz - 1) { e_prev = 0.0; f_prev = 0.0; }
+            const double g0 = 1.0 / (b8 - c8 * e_prev);
+            ev = a8 * g0;
+            fv = (d8 + c8 * f_prev) * g0;
+            e_prev = ev;
+            f_prev = fv;
+          }
+          double* sl = scr + (long)k * NV * TTHREADS;
+          sl[tid] = ev;
+          sl[TTHREADS + tid] = fv;
+          if (DIAG) sl[2 * TTHREADS + tid] = d8;
+        }
+      }
+      __syncthreads();  // level k+1 is no longer read: its slot takes level k+1-NSX
+      if (k + 1 <= km - 1 && k + 1 - NSX >= 0) issue(k + 1 - NSX);
+    }
+    // ---- substitution, top down
+    if (inner) {
+      double x = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < km; ++k) {
+        const double* sl = scr + (long)k * NV * TTHREADS;
+        const double ev = sl[tid], fv = sl[TTHREADS + tid];
+        const long cg = (long)k * A + qo;
+        double v;
+        if (k < kz) {
+          const double vit_k = 1.0;
+          v = (k == 0) ? (ev * stf + fv) * vit_k : (ev * x + fv) * vit_k;
+          x = v;
+        } else {
+          v = fv;
+        }
+        if (DIAG) {
+          const double d8 = sl[2 * TTHREADS + tid];
+          const double vit_k = k < kz ? 1.0 : 0.0;
+          const double at_old = at_in[cg];
+          a.tend[n * F + cg] = (v - at_old) / dts * vit_k;
+          if (k == 0) a.dt_diff[n * F + cg] = (v - d8) / dts * vit_k - stf * 0.5 * odzp[0];
+          else a.dt_diff[n * F + cg] = (v - d8) / dts * vit_k;
+          if (j == 2 && a.tripole) a.fold_save[((long)(n * km + k)) * imt + i] = d8;
+        }
+        at_out[cg] = v;
+        atb_out[(long)(k + 1) * A + qo] = v;
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------- state halo
 // One block per (level, tracer): ghost cells of the new state take the halo
 // values (pop_haloupdate_tracer2 then tracer_9 for every point); cells the
@@ -694,7 +1186,8 @@ __global__ void k_halo_state(Arena a, int n) {
   double* lvl = a.at[a.cur ^ 1] + n * F + (long)k * A;
   double* lvlb = a.atb[a.cur ^ 1] + n * FB + (long)(k + 1) * A;
   const double* old = a.at[a.cur] + n * F + (long)k * A;
-  const double* vin = a.vtl + (long)k * A;
+  const double* vin = a.vtl ? a.vtl + (long)k * A : nullptr;
+  const float* vin32 = a.vtl32 ? a.vtl32 + (long)k * A : nullptr;
   const double* tnew = a.at[a.cur ^ 1] + (long)k * A;  // temperature after its halo (n == 1 only)
   for (int i = threadIdx.x; i < imt; i += blockDim.x) top[i] = lvl[2L * imt + i];
   __syncthreads();
@@ -707,13 +1200,13 @@ __global__ void k_halo_state(Arena a, int n) {
     const long q = (long)j * imt + i;
     double v;
     const bool filled = halo_cell_value(lvl, top, j, i, imt, jmt, a.ew_cyclic, a.tripole, v);
-    if (!filled) v = vin[q];
+    if (!filled) v = vin ? vin[q] : (double)vin32[q];
     if (DIAG) {
       const double vit = k < a.kmt[q] ? 1.0 : 0.0;
       const bool inner = (i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2);
       double ori;
       if (inner) ori = a.fold_save[((long)(n * a.km + k)) * imt + i];
-      else if (n == 0 || !filled) ori = vin[q];
+      else if (n == 0 || !filled) ori = vin ? vin[q] : (double)vin32[q];
       else ori = tnew[q];
       a.tend[n * F + (long)k * A + q] = (v - old[q]) / dts * vit;
       if (k == 0)
@@ -772,6 +1265,15 @@ int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripo
 }
 
 int launch_continuity_fp64(const Arena& a, cudaStream_t s) {
+  if (a.wka) {
+    dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8, a.km);
+    k_cont_level<<<g, b, 0, s>>>(a);
+    LT_LAUNCHED();
+    dim3 g2((a.imt + 31) / 32, (a.jmt + 7) / 8);
+    k_cont_column<<<g2, b, 0, s>>>(a);
+    LT_LAUNCHED();
+    return LT_OK;
+  }
   dim3 g((a.imt + TX - 1) / TX, (a.jmt + TY - 1) / TY);
   const size_t sm = sizeof(double) * (5 * CY * CX + (size_t)a.km * TTHREADS);
   static bool attr = false;
@@ -806,6 +1308,22 @@ int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots) {
   }
   if (a.diagnostics) k_tracer64<true><<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
   else k_tracer64<false><<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid) {
+  const int ntx = (a.imt + TX - 1) / TX;
+  const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
+  const size_t sm = sizeof(ExSmem);
+  static bool attr = false;
+  if (!attr) {
+    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_tma64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_tma64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
+  if (a.diagnostics) k_tracer_tma64<true><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+  else k_tracer_tma64<false><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
   LT_LAUNCHED();
   return LT_OK;
 }

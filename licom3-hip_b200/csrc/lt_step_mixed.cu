@@ -1,0 +1,632 @@
+// lt_step_mixed.cu - the mixed-precision tracer step.
+//
+// Storage: the prognostic state (at, atb) stays f64; the dynamics inputs, the
+// mixing coefficient and the derived fields (w, face transports, scaled
+// utf/vtf) are f32.  Arithmetic: the flux, stencil and diffusion terms are
+// computed in f32 from f64 differences of the state (predictor, limiter
+// fluxes, Lax-Wendroff and upwind parts, both Laplacians, explicit vertical
+// diffusion, shortwave); the tspas predictor is formed as state + f32
+// increment in f64 and compared with the f64 extrema, so the limiter
+// decisions are those of an f64 run except at exact ties.  f64 remains where
+// the global tracer content needs it: the centred advective product d*u of
+// the final update (both cells of a face add it with the same sign, so its
+// rounding would not cancel), the face-flux sums and their metric weights,
+// the surface fluxes, the explicit update and the tridiagonal sweep.
+//
+// The tspas terms of tracer.cpp:291-921 are regrouped per face.  For a face
+// between cells L (lower index) and R with difference d = a_R - a_L (for the
+// horizontal faces) and transport u, the centred part A = d*u and the
+// Lax-Wendroff part B = 2*dts*u*u*d/(face metric) (horizontal) or
+// B = w*w*odzt*dts*d (vertical, d = a_upper - a_lower) enter
+//    L: -(A - X), R: -(A + X)   horizontally,  upper: -(A + X), lower: -(A - X) vertically,
+// times tarea_r (0.5*odzp vertically), with X = B, or X = |u|*d where the
+// predictor leaves the local bounds at either cell (the upwind fallback).
+// This is the reference's advective form algebraically (the centred and
+// divergence terms x0 + c1 combine to d*u per face); each face is evaluated
+// once for both cells.
+#include <cstdio>
+#include "lt_common.cuh"
+#include "lt_halo.cuh"
+#include "lt_tracer_tma.cuh"
+
+namespace lt {
+namespace {
+
+__global__ void k_f64_to_f32(const double* __restrict__ x, float* __restrict__ y, long n) {
+  for (long m = (long)blockIdx.x * blockDim.x + threadIdx.x; m < n; m += (long)gridDim.x * blockDim.x)
+    y[m] = (float)x[m];
+}
+
+__global__ void k_f32_to_f64(const float* __restrict__ x, double* __restrict__ y, long n) {
+  for (long m = (long)blockIdx.x * blockDim.x + threadIdx.x; m < n; m += (long)gridDim.x * blockDim.x)
+    y[m] = (double)x[m];
+}
+
+// Face transports from the U-point means (u_wface, v_sface of
+// advection_tracer_1_0, tracer.cpp:83-119):
+//   uw(j,i) = (wkd(j-1,i) + wkd(j,i)) * htw(j,i) / 4
+//   vs(j,i) = (wkb(j,i) + wkb(j,i+1)) * hts(j,i) / 4
+// The f64 forms are the one expression the continuity march and the tracer
+// march's centred term both use, so the divergence that builds w and the
+// transports that advect the tracer agree to f64 rounding.  The f32 forms
+// feed the predictor, the Lax-Wendroff and the upwind parts.
+__device__ __forceinline__ double face_x64(float wn, float wc, double htw) {
+  return ((double)wn + (double)wc) * htw * 0.25;
+}
+__device__ __forceinline__ double face_y64(float wc, float we, double hts) {
+  return ((double)wc + (double)we) * hts * 0.25;
+}
+__device__ __forceinline__ float face32(float w1, float w2, float h) { return (w1 + w2) * h * 0.25f; }
+
+
+// ------------------------------------------------------------- continuity
+// As the f64 k_cont_level / k_cont_column (tracer_1, upwell_2..4,
+// operators_div, advection_tracer_1_0) with f32 storage.  The tracer march
+// uses the advective form, whose content change is sum(T * 3-D divergence of
+// the transports it advects with); to keep that divergence zero in exact
+// arithmetic where the flow is non-divergent, both marches form the face
+// transports in f64 from the same stored f32 U-point means (face_x64,
+// face_y64), the free-surface factor enters the divergence as an additive
+// correction that vanishes with the surface height, and w is integrated in
+// f64 and rounded once.  Rounding w to f32 then costs f32 precision of w
+// only, not of the transports.
+//
+// One CTA marches a 32 x 8 column tile down the levels: the 2-D metric and
+// free-surface factors are read once per tile, each level's U-point means
+// (with a one-point halo north and east) pass through shared memory, and the
+// vertical recurrence of upwell_4,
+//   raw(k) = raw(k-1) + dzp(k-1) * (W * ohbt + wka(k-1)),  ws(k) = fac * raw(k),
+// with W = -sum dzp*wka over the wet levels, is evaluated after the march
+// from the partial sums P(k) = sum_{k'<k} dzp*wka as
+//   raw(k) = ws(0) + W * ohbt * Z(k) + P(k),  Z(k) = sum_{k'<k} dzp,
+// with P(k) parked in the ws field between the two passes.
+constexpr int CBX = 32, CBY = 8;
+__global__ void __launch_bounds__(CBX * CBY) k_cont_march32(Arena a) {
+  constexpr int UX = CBX + 1, UY = CBY + 1, UN = UX * UY, NT = CBX * CBY;
+  // wkd/wkb: mean velocities at U points, double-buffered over levels;
+  // fm1: free-surface factor minus one (-1 where the reference's uk/vk are zero)
+  __shared__ float s_wkd[2][UN], s_wkb[2][UN], s_fm1[UN];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CBX + tx;
+  const int x0 = blockIdx.x * CBX, y0 = blockIdx.y * CBY;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A;
+  const float oncc = (float)a.p.oncc;
+  for (int m = tid; m < UN; m += NT) {
+    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+    float fm1 = -1.f;
+    if (uj >= 0 && uj < jmt - 1 && ui >= 1 && ui < imt) {
+      const long q = (long)uj * imt + ui;
+      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
+                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
+      fm1 = (float)(work * a.ohbu[q]);
+    }
+    s_fm1[m] = fm1;
+  }
+  const int i = x0 + tx, j = y0 + ty;
+  const bool own = i < imt && j < jmt;
+  const bool div_here = own && j >= 1 && i < imt - 1;
+  const bool col_here = own && j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1;
+  const long qo = own ? (long)j * imt + i : 0;
+  const int kz = own ? a.kmt[qo] : 0;
+  const double htw_cd = own ? a.htw[qo] : 0.0, hts_cd = own ? a.hts[qo] : 0.0;
+  const double htw_ed = div_here ? a.htw[qo + 1] : 0.0, hts_nd = div_here ? a.hts[qo - imt] : 0.0;
+  const double tr = div_here ? a.tarea_r[qo] : 0.0;
+  const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
+  double P = 0.0;
+  for (int k = 0; k < km; ++k) {
+    const int b = k & 1;
+    const long lvl = (long)k * A;
+    for (int m = tid; m < UN; m += NT) {
+      const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+      float wkd = 0.f, wkb = 0.f;
+      if (uj >= 0 && uj < jmt && ui < imt) {
+        const long c = lvl + (long)uj * imt + ui;
+        wkd = 0.5f * (a.utf32[c] * oncc) + 0.5f * a.utl32[c];
+        wkb = 0.5f * (a.vtf32[c] * oncc) + 0.5f * a.vtl32[c];
+      }
+      s_wkd[b][m] = wkd;
+      s_wkb[b][m] = wkb;
+    }
+    __syncthreads();
+    if (own) {
+      const long c = lvl + qo;
+      const float* wd = s_wkd[b];
+      const float* wb = s_wkb[b];
+      a.utf_out32[c] = a.utf32[c] * oncc;
+      a.vtf_out32[c] = a.vtf32[c] * oncc;
+      a.wkd32[c] = wd[m0];
+      a.wkb32[c] = wb[m0];
+      if (col_here && k < kz) {
+        // the four faces, as the tracer kernel forms them (face_x64/face_y64)
+        const double uw_w = face_x64(wd[mn], wd[m0], htw_cd);
+        const double uw_e = face_x64(wd[mn + 1], wd[m0 + 1], htw_ed);
+        const double vs_s = face_y64(wb[m0], wb[m0 + 1], hts_cd);
+        const double vs_n = face_y64(wb[mn], wb[mn + 1], hts_nd);
+        // (uk_1 + uk_2) * htw = 4 * uw + htw * (fm1_1 * wkd_1 + fm1_2 * wkd_2)
+        auto corr = [&](const float* s, int m1, int m2) {
+          return (double)s_fm1[m1] * (double)s[m1] + (double)s_fm1[m2] * (double)s[m2];
+        };
+        const double east = 4.0 * uw_e + htw_ed * corr(wd, m0 + 1, mn + 1);
+        const double west = 4.0 * uw_w + htw_cd * corr(wd, m0, mn);
+        const double south = 4.0 * vs_s + hts_cd * corr(wb, m0 + 1, m0);
+        const double north = 4.0 * vs_n + hts_nd * corr(wb, mn + 1, mn);
+        const double wka = 0.5 * (east - west + south - north) * tr;
+        if (k >= 1) a.ws32[c] = (float)P;
+        P += a.dzp[k] * wka;
+      }
+    }
+  }
+  if (!col_here) return;
+  const double ohbt = a.ohbt[qo];
+  const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
+  const double W = -P;
+  const double ws0 = a.ws32[qo];
+  double Z = 0.0;
+  for (int k = 1; k < km; ++k) {
+    Z += a.dzp[k - 1];
+    const long c = (long)k * A + qo;
+    a.ws32[c] = (k < kz) ? (float)(fac * (ws0 + W * ohbt * Z + (double)a.ws32[c])) : 0.f;
+  }
+}
+
+}  // namespace
+
+int launch_f64_to_f32(const double* x, float* y, long n, cudaStream_t s) {
+  k_f64_to_f32<<<1184, 256, 0, s>>>(x, y, n);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s) {
+  k_f32_to_f64<<<1184, 256, 0, s>>>(x, y, n);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+namespace {
+
+// ------------------------------------------------------------ column march
+constexpr int NSM = 4;                     // level slots (k+1 .. k-2)
+constexpr int FXN = (TY + 2) * (TX + 3);   // x faces of the 1-halo region
+constexpr int FYN = (TY + 3) * (TX + 2);   // y faces of the 1-halo region
+
+// One level of the column tile, filled by five TMA boxes.  The f32 fields
+// are w and the U-point means wkd, wkb from which the kernel forms the face
+// transports (face32, face_x64, face_y64).
+struct alignas(128) MxSlot {
+  alignas(128) double at[(TY + 4) * SW];   // rows y0-2 .. y0+TY+1
+  alignas(128) double atb[(TY + 4) * SW];  // tracer level L of the previous time level
+  alignas(128) float ws[(TY + 2) * SW];    // rows y0-1 .. y0+TY
+  alignas(128) float wkd[(TY + 3) * SW];   // rows y0-2 .. y0+TY
+  alignas(128) float wkb[(TY + 3) * SW];   // rows y0-2 .. y0+TY
+  alignas(128) float akt[TY * TX];         // the tile itself, columns x0 .. x0+TX-1
+};
+constexpr uint32_t kMxLevelBytes =
+    (uint32_t)(2 * (TY + 4) * SW * sizeof(double) + ((TY + 2) * SW + 2 * (TY + 3) * SW + TY * TX) * sizeof(float));
+
+struct MxSmem {
+  MxSlot slot[NSM];
+  float fxd[2][FXN], fxb[2][FXN];    // per level parity: difference d and Lax-Wendroff part B
+  float fyd[2][FYN], fyb[2][FYN];
+  unsigned char flag[3][HN];          // predictor outside its local bounds
+  float d2[HN];                       // first Laplacian (times ahf)
+  float tr[HN], dtn[HN], dts[HN], dte[HN], dtw[HN], ahf[HN];
+  float cxf[FXN], cyf[FYN];           // 2*dts/(htw*hun), 2*dts/(hts*hue) at the faces
+  float hwx[FXN], hsy[FYN];           // htw, hts at the faces (f32)
+  int kmt[(TY + 4) * SW];
+  uint64_t bar[NSM];
+};
+
+// Issue the five boxes of level L of tracer n into a slot (one thread).
+__device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const TracerMaps& m, int cur, int n, int km,
+                                         int L, int x0, int y0) {
+  mbar_expect_tx(bar, kMxLevelBytes);
+  tma_load_3d(sl.at, &m.at[cur], x0 - 4, y0 - 2, n * km + L, bar);
+  tma_load_3d(sl.atb, &m.atb[cur], x0 - 4, y0 - 2, n * (km + 1) + L + 1, bar);
+  tma_load_3d(sl.ws, &m.ws, x0 - 4, y0 - 1, L, bar);
+  tma_load_3d(sl.wkd, &m.uw, x0 - 4, y0 - 2, L, bar);
+  tma_load_3d(sl.wkb, &m.vs, x0 - 4, y0 - 2, L, bar);
+  tma_load_3d(sl.akt, &m.akt, x0, y0, n * km + L, bar);
+}
+
+// f32 face transports of the 1-halo region from a slot: x face (fj, fi) and
+// y face (fj, fi) as indexed by fx / fy below
+__device__ __forceinline__ float ux32(const MxSlot& L, const MxSmem& S, int fj, int fi, int m) {
+  return face32(L.wkd[fj * SW + fi + 3], L.wkd[(fj + 1) * SW + fi + 3], S.hwx[m]);
+}
+__device__ __forceinline__ float vy32(const MxSlot& L, const MxSmem& S, int fj, int fi, int m) {
+  return face32(L.wkb[fj * SW + fi + 3], L.wkb[fj * SW + fi + 4], S.hsy[m]);
+}
+
+// x face (fj, fi): row y0-1+fj, west side of column x0-1+fi
+// y face (fj, fi): south side of row y0-2+fj, column x0-1+fi
+__device__ __forceinline__ int fx(int fj, int fi) { return fj * (TX + 3) + fi; }
+__device__ __forceinline__ int fy(int fj, int fi) { return fj * (TX + 2) + fi; }
+
+// face differences and Lax-Wendroff parts of level kk for the 1-halo region
+__device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
+  const MxSlot& L = S.slot[kk % NSM];
+  float* dx = S.fxd[kk & 1];
+  float* bx = S.fxb[kk & 1];
+  float* dy = S.fyd[kk & 1];
+  float* by = S.fyb[kk & 1];
+  for (int m = threadIdx.x; m < FXN + FYN; m += TTHREADS) {
+    if (m < FXN) {
+      const int fj = m / (TX + 3), fi = m % (TX + 3);
+      const int r = (fj + 1) * SW + fi + 3;           // cell R in the tracer box
+      const float d = (float)(L.at[r] - L.at[r - 1]);
+      const float u = ux32(L, S, fj, fi, m);
+      dx[m] = d;
+      bx[m] = d * u * u * S.cxf[m];
+    } else {
+      const int mm = m - FXN;
+      const int fj = mm / (TX + 2), fi = mm % (TX + 2);
+      const int r = fj * SW + fi + 3;                 // cell L (north) in the tracer box
+      const float d = (float)(L.at[r + SW] - L.at[r]);
+      const float v = vy32(L, S, fj, fi, mm);
+      dy[mm] = d;
+      by[mm] = d * v * v * S.cyf[mm];
+    }
+  }
+}
+
+// predictor and bound test at level kk on the 1-halo region
+__device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int kk, int x0, int y0) {
+  const int km = a.km, imt = a.imt, jmt = a.jmt;
+  const float dts = (float)a.p.dts;
+  const MxSlot& L = S.slot[kk % NSM];
+  const double* at_c = L.at;
+  const double* at_u = kk > 0 ? S.slot[(kk - 1) % NSM].at : nullptr;
+  const double* at_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].at : nullptr;
+  const float* wsd = kk < km - 1 ? S.slot[(kk + 1) % NSM].ws : nullptr;
+  const float* dx = S.fxd[kk & 1];
+  const float* bx = S.fxb[kk & 1];
+  const float* dy = S.fyd[kk & 1];
+  const float* by = S.fyb[kk & 1];
+  const float hodz = 0.5f * (float)a.odzp[kk];
+  const float odzt_k = (float)a.odzt[kk];
+  const float odzt_k1 = kk < km - 1 ? (float)a.odzt[kk + 1] : 0.f;
+  unsigned char* fl = S.flag[kk % 3];
+  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
+    const int hj = m / HQX, hi = m % HQX;
+    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+    if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) { fl[m] = 0; continue; }
+    const int r = r2(hj, hi), u = ru(hj, hi);
+    // horizontal: east/west x faces, south/north y faces
+    const int fe = fx(hj, hi + 1), fw = fx(hj, hi), fs = fy(hj + 1, hi), fn = fy(hj, hi);
+    const float ue = ux32(L, S, hj, hi + 1, fe), uwv = ux32(L, S, hj, hi, fw);
+    const float vs = vy32(L, S, hj + 1, hi, fs), vn = vy32(L, S, hj, hi, fn);
+    const float sx = (dx[fe] * ue - bx[fe]) + (dx[fw] * uwv + bx[fw]);
+    const float sy = (dy[fs] * vs - by[fs]) + (dy[fn] * vn + by[fn]);
+    // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
+    float sz = 0.f;
+    const double c = at_c[r];
+    if (kk > 0) {
+      const float w = L.ws[u];
+      const float d = (float)(at_u[r] - c);
+      const float A = w * d;
+      sz += A - A * w * odzt_k * dts;
+    }
+    if (kk < km - 1) {
+      const float w = wsd[u];
+      const float d = (float)(c - at_d[r]);
+      const float A = w * d;
+      sz += A + A * w * odzt_k1 * dts;
+    }
+    const float inc = -(S.tr[m] * (sx + sy) + hodz * sz) * dts;
+    const double a00 = c + (double)inc;
+    // masked 7-point extrema in f64 (land: -1e10 for the max, +1e10 for the min)
+    const int* kt = S.kmt;
+    auto hv = [&](double t, int rr, int kl) { return kl < kt[rr] ? t : -1.0e10; };
+    auto lv = [&](double t, int rr, int kl) { return kl < kt[rr] ? t : 1.0e10; };
+    double hi_ = hv(c, r, kk), lo_ = lv(c, r, kk);
+    hi_ = fmax(hi_, hv(at_c[r - SW], r - SW, kk)); lo_ = fmin(lo_, lv(at_c[r - SW], r - SW, kk));
+    hi_ = fmax(hi_, hv(at_c[r + SW], r + SW, kk)); lo_ = fmin(lo_, lv(at_c[r + SW], r + SW, kk));
+    hi_ = fmax(hi_, hv(at_c[r - 1], r - 1, kk));   lo_ = fmin(lo_, lv(at_c[r - 1], r - 1, kk));
+    hi_ = fmax(hi_, hv(at_c[r + 1], r + 1, kk));   lo_ = fmin(lo_, lv(at_c[r + 1], r + 1, kk));
+    if (kk > 0) { hi_ = fmax(hi_, hv(at_u[r], r, kk - 1)); lo_ = fmin(lo_, lv(at_u[r], r, kk - 1)); }
+    if (kk < km - 1) { hi_ = fmax(hi_, hv(at_d[r], r, kk + 1)); lo_ = fmin(lo_, lv(at_d[r], r, kk + 1)); }
+    fl[m] = (a00 > hi_ || a00 < lo_) ? 1 : 0;
+  }
+}
+
+// first Laplacian of atb at level kk (f32 on f64 differences), masked
+__device__ __forceinline__ void del4_first_mixed(MxSmem& S, const Arena& a, int kk, int x0, int y0) {
+  const double* atb = S.slot[kk % NSM].atb;
+  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
+    const int hj = m / HQX, hi = m % HQX;
+    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+    float v = 0.f;
+    if (gi >= 1 && gi < a.imt - 1 && gj >= 1 && gj < a.jmt - 1) {
+      const int r = r2(hj, hi);
+      const double c = atb[r];
+      if (kk <= S.kmt[r] - 1) {
+        float h = 0.f;
+        if (kk <= S.kmt[r - SW] - 1) h += S.dtn[m] * (float)(atb[r - SW] - c);
+        if (kk <= S.kmt[r + SW] - 1) h += S.dts[m] * (float)(atb[r + SW] - c);
+        if (kk <= S.kmt[r + 1] - 1) h += S.dte[m] * (float)(atb[r + 1] - c);
+        if (kk <= S.kmt[r - 1] - 1) h += S.dtw[m] * (float)(atb[r - 1] - c);
+        v = S.ahf[m] * h;
+      }
+    }
+    S.d2[m] = v;
+  }
+}
+
+__global__ void __launch_bounds__(TTHREADS, 4)
+    k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
+  extern __shared__ __align__(128) unsigned char smem_mx[];
+  MxSmem& S = *reinterpret_cast<MxSmem*>(smem_mx);
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A, F = a.F, FB = a.FB;
+  const lt_params& p = a.p;
+  const double dts = p.dts;
+  const float dtsf = (float)dts;
+  const double* __restrict__ odzp = a.odzp;
+  const double* __restrict__ odzt = a.odzt;
+  double* scr = a.col_scratch + (long)blockIdx.x * km * 2 * TTHREADS;
+  if (tid == 0) {
+    for (int s = 0; s < NSM; ++s) mbar_init(&S.bar[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t par = 0, outstanding = 0;
+
+  for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x) {
+    const long tile = w >> 1;
+    const int n = (int)(w & 1);
+    const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * TY;
+    const int i = x0 + tx, j = y0 + ty;
+    double* at_out = a.at[a.cur ^ 1] + n * F;
+    double* atb_out = a.atb[a.cur ^ 1] + n * FB;
+
+    __syncthreads();
+    auto issue = [&](int L) {
+      if (tid == 0) issue_mx(S.slot[L % NSM], &S.bar[L % NSM], maps, a.cur, n, km, L, x0, y0);
+      outstanding |= 1u << (L % NSM);
+    };
+    auto wait = [&](int L) -> bool {
+      const int s = L % NSM;
+      const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u);
+      if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
+      return ok;
+    };
+    for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L);
+    // per-tile 2-D data
+    for (int m = tid; m < (TY + 4) * SW; m += TTHREADS) {
+      const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
+      S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
+    }
+    for (int m = tid; m < HN; m += TTHREADS) {
+      const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
+      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
+      const long q = in ? (long)gj * imt + gi : 0;
+      S.tr[m] = in ? (float)a.tarea_r[q] : 0.f;
+      S.dtn[m] = in ? (float)a.dtn[q] : 0.f;
+      S.dts[m] = in ? (float)a.dts[q] : 0.f;
+      S.dte[m] = in ? (float)a.dte[q] : 0.f;
+      S.dtw[m] = in ? (float)a.dtw[q] : 0.f;
+      S.ahf[m] = in ? (float)a.ahf[q] : 0.f;
+    }
+    for (int m = tid; m < FXN + FYN; m += TTHREADS) {
+      int gj, gi;
+      if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
+      else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
+      float v = 0.f;
+      if (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) {
+        const long q = (long)gj * imt + gi;
+        v = (m < FXN) ? (float)(2.0 * dts / (a.htw[q] * a.hun[q])) : (float)(2.0 * dts / (a.hts[q] * a.hue[q]));
+      }
+      if (m < FXN) S.cxf[m] = v; else S.cyf[m - FXN] = v;
+      const bool inb = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+      if (m < FXN) S.hwx[m] = inb ? (float)a.htw[(long)gj * imt + gi] : 0.f;
+      else S.hsy[m - FXN] = inb ? (float)a.hts[(long)gj * imt + gi] : 0.f;
+    }
+
+    const bool own = (i < imt && j < jmt);
+    const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
+    const long qo = own ? (long)j * imt + i : 0;
+    const int kz = own ? a.kmt[qo] : 0;
+    const int hc = (ty + 1) * HQX + (tx + 1);
+    const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1), ac = ty * TX + tx;
+    const int fe = fx(ty + 1, tx + 2), fwi = fx(ty + 1, tx + 1), fs = fy(ty + 2, tx + 1), fn = fy(ty + 1, tx + 1);
+    const float swv = (inner && n == 0) ? (float)a.swv[qo] : 0.f;
+    const double stf = own ? a.stf_n[n * A + qo] : 0.0;
+    const double err_norm2 = a.scalars[0];
+    const float ah = (float)p.ah;
+    const double trc = inner ? a.tarea_r[qo] : 0.0;
+    const double htw_w64 = inner ? a.htw[qo] : 0.0, htw_e64 = inner ? a.htw[qo + 1] : 0.0;
+    const double hts_s64 = inner ? a.hts[qo] : 0.0, hts_n64 = inner ? a.hts[qo - imt] : 0.0;
+    double e_prev = 0.0, f_prev = 0.0;
+    double carry = 0.0;  // lower face of the level below, as seen by the level above: A + X
+
+    {
+      const bool ok = wait(km - 1) && wait(km - 2);
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
+    }
+    faces_level(S, km - 1);
+    __syncthreads();
+    predictor_mixed(S, a, km - 1, x0, y0);
+
+    for (int k = km - 1; k >= 0; --k) {
+      const bool ok = (k >= 2) ? wait(k - 2) : true;
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
+      // ---- phase B1: faces one level up, first Laplacian here
+      if (k >= 1) faces_level(S, k - 1);
+      del4_first_mixed(S, a, k, x0, y0);
+      __syncthreads();
+      // ---- phase B2: predictor one level up
+      if (k >= 1) predictor_mixed(S, a, k - 1, x0, y0);
+      __syncthreads();
+      // ---- phase C: own column at level k
+      if (inner) {
+        const MxSlot& Lk = S.slot[k % NSM];
+        const unsigned char* fl = S.flag[k % 3];
+        const bool self = fl[hc] != 0;
+        const float* dx = S.fxd[k & 1];
+        const float* bx = S.fxb[k & 1];
+        const float* dy = S.fyd[k & 1];
+        const float* by = S.fyb[k & 1];
+        const float ue = ux32(Lk, S, ty + 1, tx + 2, fe), uwv = ux32(Lk, S, ty + 1, tx + 1, fwi);
+        const float vsv = vy32(Lk, S, ty + 2, tx + 1, fs), vnv = vy32(Lk, S, ty + 1, tx + 1, fn);
+        // the same faces in f64, as the continuity march formed them
+        const int xw = (ty + 1) * SW + tx + 4;   // wkd of U point (j-1, i); (j, i) is one row down
+        const double ue64 = face_x64(Lk.wkd[xw + 1], Lk.wkd[xw + 1 + SW], htw_e64);
+        const double uw64 = face_x64(Lk.wkd[xw], Lk.wkd[xw + SW], htw_w64);
+        const int ys = (ty + 2) * SW + tx + 4;   // wkb of U point (j, i); (j, i+1) is next
+        const double vs64 = face_y64(Lk.wkb[ys], Lk.wkb[ys + 1], hts_s64);
+        const double vn64 = face_y64(Lk.wkb[ys - SW], Lk.wkb[ys - SW + 1], hts_n64);
+        // Content bookkeeping.  Both cells of a face receive its centred part
+        // A = d*u with the same sign (the advective form), so any rounding of
+        // A adds up over the domain instead of cancelling: A is formed in f64
+        // from the exact f64 state difference and the f32 transport.  The
+        // upwind / Lax-Wendroff part X (f32) enters the two cells with
+        // opposite signs and cancels exactly in the f64 face sums.
+        const double c = Lk.at[rc];
+        const double dE = Lk.at[rc + 1] - c, dW = c - Lk.at[rc - 1];
+        const double dS = Lk.at[rc + SW] - c, dN = c - Lk.at[rc - SW];
+        float t;
+        t = dx[fe];                                   // east face: this cell is L
+        const float Xe = (self || fl[hc + 1]) ? fabsf(ue) * t : bx[fe];
+        t = dx[fwi];
+        const float Xw = (self || fl[hc - 1]) ? fabsf(uwv) * t : bx[fwi];
+        t = dy[fs];
+        const float Xs = (self || fl[hc + HQX]) ? fabsf(vsv) * t : by[fs];
+        t = dy[fn];
+        const float Xn = (self || fl[hc - HQX]) ? fabsf(vnv) * t : by[fn];
+        double sh = dE * ue64 + dW * uw64 + dS * vs64 + dN * vn64;
+        sh += ((double)Xw - (double)Xe) + ((double)Xn - (double)Xs);
+        // vertical: face above (k-1|k) computed here, face below carried
+        double sz = carry;
+        if (k > 0) {
+          const float wv = Lk.ws[uc];
+          const double d64 = S.slot[(k - 1) % NSM].at[rc] - c;
+          const float d = (float)d64;
+          const bool up = self || (S.flag[(k - 1) % 3][hc] != 0);
+          const float Xv = up ? fabsf(wv) * d : (wv * d) * wv * (float)odzt[k] * dtsf;
+          const double Av = (double)wv * d64;
+          sz += Av - (double)Xv;
+          carry = Av + (double)Xv;
+        } else {
+          carry = 0.0;
+        }
+        // Face-flux sums are weighted by tarea_r (horizontal) and odzp
+        // (vertical) in f64, so a flux leaves one cell and enters the next
+        // with weights that cancel against the cell volumes to f64 rounding.
+        const float vit_k = k < kz ? 1.f : 0.f;
+        const float vit_kp1 = (k + 1 < kz) ? 1.f : 0.f;
+        sh *= (double)vit_k;                          // horizontal advection, times -tarea_r
+        const double vadv = -0.5 * sz * (double)vit_k;  // vertical advection, times odzp
+        float vz = 0.f;                               // other vertical face-flux differences, times odzp
+        float tf = 0.f;                               // the remaining tendency terms
+        // second Laplacian
+        if (k <= S.kmt[rc] - 1) {
+          const float dc = S.d2[hc];
+          float h = 0.f;
+          if (k <= S.kmt[rc - SW] - 1) h += S.dtn[hc] * (S.d2[hc - HQX] - dc);
+          if (k <= S.kmt[rc + SW] - 1) h += S.dts[hc] * (S.d2[hc + HQX] - dc);
+          if (k <= S.kmt[rc + 1] - 1) h += S.dte[hc] * (S.d2[hc + 1] - dc);
+          if (k <= S.kmt[rc - 1] - 1) h += S.dtw[hc] * (S.d2[hc - 1] - dc);
+          tf += ah * h;
+        }
+        const double atb_k = Lk.atb[rc];
+        const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSM].atb[rc] : 0.0;
+        const double atb_kp1 = k < km - 1 ? S.slot[(k + 1) % NSM].atb[rc] : 0.0;
+        const float wkc_k = Lk.akt[ac];
+        const float wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSM].akt[ac] : 0.f;
+        if (n == 0) {
+          if (k >= 1 && k < km - 1) vz += swv * ((float)a.pen[k - 1] * vit_k - (float)a.pen[k] * vit_kp1);
+          else if (k == 0) vz -= swv * (float)a.pen[0] * vit_kp1;
+          else vz += swv * (float)a.pen[km - 2] * vit_k;
+        }
+        // explicit half of the vertical diffusion: the flux through a face is
+        // the same f32 expression in the cells above and below it
+        const float w1 = k >= 1 ? wkc_km1 * (float)(atb_km1 - atb_k) * (float)odzt[k] * vit_k : 0.f;
+        const float w2 = k < km - 1 ? wkc_k * (float)(atb_k - atb_kp1) * (float)odzt[k + 1] * vit_kp1 : 0.f;
+        vz += (w1 - w2) * 0.5f;
+        // surface flux and the freshwater-norm correction stay f64: the
+        // correction cancels the global salt flux, which f32 would leave at
+        // f32 precision of the flux
+        double sfc = 0.0;
+        if (k == 0) {
+          if (kz > 0) sfc = stf * 0.5 * odzp[0];
+          if (n == 1) sfc += err_norm2 * (double)vit_k;
+        }
+        if (p.boundary_restore == 1 && k >= 1)
+          tf += vit_k * (float)(a.restore[n * F + (long)k * A + qo] - atb_k) * (float)(1.0 / (15.0 * 86400.0));
+        const double d8 = c + dts * ((double)tf - trc * (double)sh + odzp[k] * ((double)vz + vadv) + sfc);
+        double ev = 0.0, fv = d8;
+        if (k < kz) {
+          double a8, c8, b8;
+          if (k >= 1) a8 = (double)wkc_km1 * odzt[k] * odzp[k] * dts * 0.5;
+          else a8 = odzp[0] * dts * 0.5;
+          if (k == kz - 1) {
+            c8 = odzp[kz - 1] * dts * 0.5;
+            b8 = 1.0 + a8;
+          } else if (k >= 1) {
+            c8 = (double)wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
+            b8 = 1.0 + a8 + c8;
+          } else {
+            c8 = (double)wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
+            b8 = 1.0 + c8;
+          }
+          if (k == kz - 1) { e_prev = 0.0; f_prev = 0.0; }
+          const double g0 = 1.0 / (b8 - c8 * e_prev);
+          ev = a8 * g0;
+          fv = (d8 + c8 * f_prev) * g0;
+          e_prev = ev;
+          f_prev = fv;
+        }
+        double* sl = scr + (long)k * 2 * TTHREADS;
+        sl[tid] = ev;
+        sl[TTHREADS + tid] = fv;
+      }
+      __syncthreads();
+      if (k + 1 <= km - 1 && k + 1 - NSM >= 0) issue(k + 1 - NSM);
+    }
+    if (inner) {
+      double x = 0.0;
+#pragma unroll 4
+      for (int k = 0; k < km; ++k) {
+        const double* sl = scr + (long)k * 2 * TTHREADS;
+        const double ev = sl[tid], fv = sl[TTHREADS + tid];
+        double v;
+        if (k < kz) {
+          v = (k == 0) ? ev * stf + fv : ev * x + fv;
+          x = v;
+        } else {
+          v = fv;
+        }
+        const long cg = (long)k * A + qo;
+        at_out[cg] = v;
+        atb_out[(long)(k + 1) * A + qo] = v;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid) {
+  const int ntx = (a.imt + TX - 1) / TX;
+  const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
+  const size_t sm = sizeof(MxSmem);
+  static bool attr = false;
+  if (!attr) {
+    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    attr = true;
+  }
+  k_tracer_mixed<<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_continuity_mixed(const Arena& a, cudaStream_t s) {
+  dim3 b(CBX, CBY), g((a.imt + CBX - 1) / CBX, (a.jmt + CBY - 1) / CBY);
+  k_cont_march32<<<g, b, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+}  // namespace lt
