@@ -211,11 +211,14 @@ struct MxSmem {
   unsigned char flag[3][HN];          // predictor outside its local bounds
   float d2[HN];                       // first Laplacian (times ahf)
   float tr[HN], dtn[HN], dts[HN], dte[HN], dtw[HN], ahf[HN];
+  float kx[HN], ky[HN];               // del4 face weights tarea*dte (east face), tarea*dts (south face)
   float cxf[FXN], cyf[FYN];           // 2*dts/(htw*hun), 2*dts/(hts*hue) at the faces
   float hwx[FXN], hsy[FYN];           // htw, hts at the faces (f32)
   int kmt[(TY + 4) * SW];
   uint64_t bar[NSM];
 };
+// four CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
+static_assert(4 * (sizeof(MxSmem) + 1024) <= 228 * 1024, "mixed tracer tile no longer fits 4 CTAs per SM");
 
 // Issue the five boxes of level L of tracer n into a slot (one thread).
 __device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const TracerMaps& m, int cur, int n, int km,
@@ -408,6 +411,8 @@ __global__ void __launch_bounds__(TTHREADS, 4)
       S.dte[m] = in ? (float)a.dte[q] : 0.f;
       S.dtw[m] = in ? (float)a.dtw[q] : 0.f;
       S.ahf[m] = in ? (float)a.ahf[q] : 0.f;
+      S.kx[m] = in ? (float)(a.tarea[q] * a.dte[q]) : 0.f;
+      S.ky[m] = in ? (float)(a.tarea[q] * a.dts[q]) : 0.f;
     }
     for (int m = tid; m < FXN + FYN; m += TTHREADS) {
       int gj, gi;
@@ -434,7 +439,7 @@ __global__ void __launch_bounds__(TTHREADS, 4)
     const float swv = (inner && n == 0) ? (float)a.swv[qo] : 0.f;
     const double stf = own ? a.stf_n[n * A + qo] : 0.0;
     const double err_norm2 = a.scalars[0];
-    const float ah = (float)p.ah;
+    const double ah64 = p.ah;
     const double trc = inner ? a.tarea_r[qo] : 0.0;
     const double htw_w64 = inner ? a.htw[qo] : 0.0, htw_e64 = inner ? a.htw[qo + 1] : 0.0;
     const double hts_s64 = inner ? a.hts[qo] : 0.0, hts_n64 = inner ? a.hts[qo - imt] : 0.0;
@@ -518,33 +523,35 @@ __global__ void __launch_bounds__(TTHREADS, 4)
         const float vit_kp1 = (k + 1 < kz) ? 1.f : 0.f;
         sh *= (double)vit_k;                          // horizontal advection, times -tarea_r
         const double vadv = -0.5 * sz * (double)vit_k;  // vertical advection, times odzp
-        float vz = 0.f;                               // other vertical face-flux differences, times odzp
+        double vz = 0.0;                              // other vertical face-flux differences, times odzp
         float tf = 0.f;                               // the remaining tendency terms
-        // second Laplacian
+        // second Laplacian as face fluxes K*(d2_R - d2_L), K = tarea*dte
+        // (x) or tarea*dts (y): one f32 value per face, the same in both of
+        // its cells, summed in f64 (dtn/dts/dte/dtw are K*tarea_r of the
+        // cell, hmix_del4.F90:368-385)
+        double hd = 0.0;
         if (k <= S.kmt[rc] - 1) {
           const float dc = S.d2[hc];
-          float h = 0.f;
-          if (k <= S.kmt[rc - SW] - 1) h += S.dtn[hc] * (S.d2[hc - HQX] - dc);
-          if (k <= S.kmt[rc + SW] - 1) h += S.dts[hc] * (S.d2[hc + HQX] - dc);
-          if (k <= S.kmt[rc + 1] - 1) h += S.dte[hc] * (S.d2[hc + 1] - dc);
-          if (k <= S.kmt[rc - 1] - 1) h += S.dtw[hc] * (S.d2[hc - 1] - dc);
-          tf += ah * h;
+          if (k <= S.kmt[rc + 1] - 1) hd += (double)(S.kx[hc] * (S.d2[hc + 1] - dc));
+          if (k <= S.kmt[rc - 1] - 1) hd -= (double)(S.kx[hc - 1] * (dc - S.d2[hc - 1]));
+          if (k <= S.kmt[rc + SW] - 1) hd += (double)(S.ky[hc] * (S.d2[hc + HQX] - dc));
+          if (k <= S.kmt[rc - SW] - 1) hd -= (double)(S.ky[hc - HQX] * (dc - S.d2[hc - HQX]));
         }
         const double atb_k = Lk.atb[rc];
         const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSM].atb[rc] : 0.0;
         const double atb_kp1 = k < km - 1 ? S.slot[(k + 1) % NSM].atb[rc] : 0.0;
         const float wkc_k = Lk.akt[ac];
         const float wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSM].akt[ac] : 0.f;
+        // shortwave through the faces above and below (tracer.cpp:1430-1474)
+        // and the explicit half of the vertical diffusion: each face flux is
+        // the same f32 expression in the cells above and below it, summed in f64
         if (n == 0) {
-          if (k >= 1 && k < km - 1) vz += swv * ((float)a.pen[k - 1] * vit_k - (float)a.pen[k] * vit_kp1);
-          else if (k == 0) vz -= swv * (float)a.pen[0] * vit_kp1;
-          else vz += swv * (float)a.pen[km - 2] * vit_k;
+          if (k >= 1) vz += (double)(swv * (float)a.pen[k - 1] * vit_k);
+          if (k < km - 1) vz -= (double)(swv * (float)a.pen[k] * vit_kp1);
         }
-        // explicit half of the vertical diffusion: the flux through a face is
-        // the same f32 expression in the cells above and below it
         const float w1 = k >= 1 ? wkc_km1 * (float)(atb_km1 - atb_k) * (float)odzt[k] * vit_k : 0.f;
         const float w2 = k < km - 1 ? wkc_k * (float)(atb_k - atb_kp1) * (float)odzt[k + 1] * vit_kp1 : 0.f;
-        vz += (w1 - w2) * 0.5f;
+        vz += 0.5 * ((double)w1 - (double)w2);
         // surface flux and the freshwater-norm correction stay f64: the
         // correction cancels the global salt flux, which f32 would leave at
         // f32 precision of the flux
@@ -555,7 +562,7 @@ __global__ void __launch_bounds__(TTHREADS, 4)
         }
         if (p.boundary_restore == 1 && k >= 1)
           tf += vit_k * (float)(a.restore[n * F + (long)k * A + qo] - atb_k) * (float)(1.0 / (15.0 * 86400.0));
-        const double d8 = c + dts * ((double)tf - trc * (double)sh + odzp[k] * ((double)vz + vadv) + sfc);
+        const double d8 = c + dts * ((double)tf - trc * sh + odzp[k] * (vz + vadv) + sfc + ah64 * trc * hd);
         double ev = 0.0, fv = d8;
         if (k < kz) {
           double a8, c8, b8;
