@@ -31,9 +31,15 @@ PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
 # algorithmic bytes per cell-step (compulsory traffic of the whole step, both
-# tracers; 2-D/1-D coefficients not counted) and of the fused column kernel
+# tracers; 2-D/1-D coefficients not counted) and of the fused column kernel:
+# at, atb read and written (64), w (8 | 4), face transports uw, vs (16) or the
+# U-point means wkd, wkb (8), akt (16 | 8)
 STEP_BYTES = {"fp64": 136.0, "mixed": 100.0}
-TRACER_KERNEL_BYTES = {"fp64": 104.0, "mixed": 80.0}
+TRACER_KERNEL_BYTES = {"fp64": 104.0, "mixed": 84.0}
+# DRAM bytes per cell (read + write) of the column kernel, from one ncu
+# --set full capture of a 720x460x55 launch; traffic grows with the cells, so
+# it scales to the bench's launch
+TRACER_KERNEL_TRAFFIC = {"fp64": 3.061e9 / (720 * 460 * 55), "mixed": 2.444e9 / (720 * 460 * 55)}
 
 
 def load_package():
@@ -191,19 +197,29 @@ def dist_setup(args):
 
 
 def reduce_max(pg, value, local):
+    """Max of a per-rank value over all ranks (NCCL on the GPUs; gloo on CPU)."""
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda:%d" % local)
+    dev = "cpu" if pg.get_backend() == "gloo" else "cuda:%d" % local
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
 
 def barrier(pg, local):
     if pg is not None:
-        import torch
         pg.barrier()
-        torch.cuda.synchronize(local)
+        if pg.get_backend() != "gloo":
+            import torch
+            torch.cuda.synchronize(local)
+
+
+def whole_job_rate(cells_per_rank, steps, world, max_ms):
+    """cell-steps/s of the whole job: every rank advanced its own replica of
+    cells_per_rank cells for `steps` steps, and the job lasted as long as the
+    slowest rank's device time max_ms."""
+    return cells_per_rank * steps * world / (max_ms * 1e-3)
 
 
 def run_reference(args):
@@ -251,7 +267,7 @@ def run_ours(args):
     ms = reduce_max(pg, dom.last_step_ms(), local)
     nprof, phases = dom.phase_ms()
     dom.profile(False)
-    value = cells * args.steps * world / (ms * 1e-3)
+    value = whole_job_rate(cells, args.steps, world, ms)
 
     # ---- roofline of the dominant kernel (the fused tracer column kernel)
     hbm, hbm_kind = peaks()
@@ -260,7 +276,10 @@ def run_ours(args):
     achieved = kbytes / (t_tracer * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": "tracer column kernel", "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
-                "algorithmic_bytes_per_launch": kbytes, "traffic": None,
+                "algorithmic_bytes_per_launch": kbytes,
+                "traffic": TRACER_KERNEL_TRAFFIC[args.precision] * cells,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 720x460x55 launch, "
+                                  "scaled by cells",
                 "step_frac": STEP_BYTES[args.precision] * cells / (ms / args.steps * 1e-3) / 1e9 / hbm,
                 "phase_ms_per_step": {k: v / max(nprof, 1) for k, v in phases.items()}}
 
@@ -286,7 +305,7 @@ def run_ours(args):
     dom.sync()
     barrier(pg, local)
     ms_e2e = reduce_max(pg, dom.last_step_ms(), local)
-    e2e = {"value": cells * e2e_steps * world / (ms_e2e * 1e-3), "unit": "cell-steps/s",
+    e2e = {"value": whole_job_rate(cells, e2e_steps, world, ms_e2e), "unit": "cell-steps/s",
            "h2d_bytes_per_step": 6 * A * 8, "d2h_bytes_per_step": 8,
            "api": "lt_step_host (C ABI), pinned host forcing"}
 

@@ -160,6 +160,12 @@ int lt_phase_ms(lt_domain* dom, float* ms, int nphase);
 /* Select the tracer column kernel: 1 = TMA-fed pipeline (default where the
  * row pitch allows 16-byte strides), 0 = plain-load variant. */
 int lt_use_tma(lt_domain* dom, int on);
+/* Failure-detection hook.  Each level wait of the TMA-fed column kernels polls
+ * its mbarrier at most `polls` times (default 2^24) before the CTA records a
+ * timeout, drains the boxes it has in flight and returns; lt_sync and
+ * lt_step_host then return LT_E_TIMEOUT.  0 makes every wait give up at once,
+ * which exercises that path without any fault. */
+int lt_set_wait_limit(lt_domain* dom, unsigned polls);
 /* Kernels this library has launched in this process (all domains). */
 long long lt_launch_count(void);
 

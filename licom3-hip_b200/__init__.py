@@ -65,6 +65,7 @@ _SIGS = {
     "lt_profile": ([_vp, _i], _i),
     "lt_mark": ([_vp, _i], _i),
     "lt_use_tma": ([_vp, _i], _i),
+    "lt_set_wait_limit": ([_vp, C.c_uint], _i),
     "lt_phase_ms": ([_vp, C.POINTER(C.c_float), _i], _i),
     "lt_launch_count": ([], C.c_longlong),
     "lt_set_device": ([_i], _i),
@@ -221,6 +222,9 @@ class TracerDomain:
 
     def use_tma(self, on=True):
         _check(lib.lt_use_tma(self.h, int(on)), "lt_use_tma")
+
+    def set_wait_limit(self, polls):
+        _check(lib.lt_set_wait_limit(self.h, int(polls)), "lt_set_wait_limit")
 
     def mark(self, which):
         _check(lib.lt_mark(self.h, int(which)), "lt_mark")

@@ -205,6 +205,7 @@ void init_arena_dims(Arena& a, const lt_grid* g, const lt_params* p) {
   a.diagnostics = g->diagnostics; a.precision = g->precision;
   if (p) a.p = *p;
   a.nv_scratch = a.diagnostics ? 3 : 2;
+  a.wait_limit = 1u << 24;
 }
 
 long slots_for(const Arena& a, int sms) {
@@ -523,6 +524,17 @@ int lt_step(lt_domain* d, int nsteps) {
   return LT_OK;
 }
 
+// After the stream has drained: a column kernel whose bounded wait for its
+// TMA boxes ran out set status[1] and returned early; report it once.
+static int timeout_status(lt_domain* d) {
+  int h = 0;
+  LT_CUDA_OK(cudaMemcpy(&h, d->a.status + 1, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!h) return LT_OK;
+  LT_CUDA_OK(cudaMemset(d->a.status + 1, 0, sizeof(int)));
+  set_error("a tracer column kernel gave up waiting for its level data; the state of that step is not valid");
+  return LT_E_TIMEOUT;
+}
+
 int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2_out, double* content2_out) {
   if (!d) return LT_E_INVALID;
   Arena& a = d->a;
@@ -539,7 +551,7 @@ int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2
   }
   if (fw_norm2_out) LT_CUDA_OK(cudaMemcpyAsync(fw_norm2_out, a.scalars, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
   LT_CUDA_OK(cudaStreamSynchronize(d->stream));
-  return LT_OK;
+  return timeout_status(d);
 }
 
 int lt_convadj(lt_domain* d) {
@@ -568,7 +580,7 @@ int lt_fw_norm2(lt_domain* d, double* out) {
 int lt_sync(lt_domain* d) {
   if (!d) return LT_E_INVALID;
   LT_CUDA_OK(cudaStreamSynchronize(d->stream));
-  return LT_OK;
+  return timeout_status(d);
 }
 
 int lt_check_numeric(lt_domain* d, long long* bad) {
@@ -606,6 +618,12 @@ int lt_use_tma(lt_domain* d, int on) {
   return LT_OK;
 }
 
+int lt_set_wait_limit(lt_domain* d, unsigned polls) {
+  if (!d) return LT_E_INVALID;
+  d->a.wait_limit = polls;
+  return LT_OK;
+}
+
 int lt_shim_bind(lt_domain* d) {
   g_shim = d;
   return LT_OK;
@@ -615,6 +633,7 @@ int lt_shim_bind(lt_domain* d) {
 // bound domain: utf/vtf/h0f scaled in place, vtl left holding S.
 void tracer_(int ii) {
   (void)ii;
+  set_error("%s", "");   // the shim has no status: an empty lt_last_error() means success
   lt_domain* d = g_shim;
   if (!d) { set_error("tracer_: no domain bound (lt_shim_bind)"); return; }
   Arena& a = d->a;
@@ -631,15 +650,19 @@ void tracer_(int ii) {
     launch_vtl_clobber(a, d->stream);
   }
   cudaMemcpyAsync(a.h0f, a.h0f_out, sizeof(double) * a.A, cudaMemcpyDeviceToDevice, d->stream);
-  cudaStreamSynchronize(d->stream);
+  cudaError_t e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) cuda_fail(e, "tracer_");
+  else timeout_status(d);
 }
 
 // convadj.cpp:290
 void convadj_(void) {
+  set_error("%s", "");
   lt_domain* d = g_shim;
   if (!d) { set_error("convadj_: no domain bound (lt_shim_bind)"); return; }
-  launch_convadj(d->a, d->stream);
-  cudaStreamSynchronize(d->stream);
+  if (launch_convadj(d->a, d->stream)) return;
+  cudaError_t e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) cuda_fail(e, "convadj_");
 }
 
 }  // extern "C"

@@ -57,6 +57,7 @@ struct Arena {
   int *status;                // [4] device status words
   long col_scratch_slots;
   int nv_scratch;             // values per level per column in col_scratch
+  unsigned wait_limit;        // polls of each level wait in the column kernels before giving up
 };
 
 #define LT_CUDA_OK(call)                                   \

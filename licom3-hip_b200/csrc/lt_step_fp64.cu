@@ -927,7 +927,7 @@ __global__ void __launch_bounds__(TTHREADS, 3)
     };
     auto wait = [&](int L) -> bool {
       const int s = L % NSX;
-      const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u);
+      const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u, a.wait_limit);
       if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
       return ok;
     };
