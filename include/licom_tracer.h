@@ -141,6 +141,21 @@ int lt_convadj(lt_domain* dom);
 /* Global tracer integrals sum(tarea*dzp*vit*tracer) over the interior, f64,
  * fixed-order pairwise tree (deterministic). out2[0] = T, out2[1] = S. */
 int lt_tracer_content(lt_domain* dom, double* out2);
+/* No counterpart in the reference.  The same integrals as lt_tracer_content,
+ * bit-identical, for callers that cannot let a library allocate device memory
+ * (a host model that owns all of HBM through its own pool or data regions).
+ * Every argument is a device pointer the caller owns, in the layouts of
+ * lt_set_field: at = AT [2][km][ny+4][nx+4], tarea = TAREA and kmt = KMT
+ * [ny+4][nx+4], dzp = DZP [km]; out2[0..1] receives T and S.  stream is a
+ * cudaStream_t (NULL = legacy default stream); the call only enqueues work.
+ * Partial sums live in a fixed 2 MiB device array inside the library (held on
+ * every GPU that loads it until exit), which caps nx*ny*km at about 5.3e8
+ * cells; larger sizes return LT_E_INVALID.  All calls share that array, so
+ * calls that overlap on the GPU race.  The first call on each device looks up
+ * the array's address and should come before any stream capture.  Allocates
+ * nothing. */
+int lt_tracer_content_noalloc(const double* at, const double* tarea, const double* dzp, const int* kmt,
+                              int nx, int ny, int km, double* out2, void* stream);
 /* fw_norm2 of the last step (tracer.cpp:1862-1865). */
 int lt_fw_norm2(lt_domain* dom, double* out);
 int lt_sync(lt_domain* dom);

@@ -27,6 +27,7 @@ CU_UNITS = {
     "lt_step_fp64.cu": ["-fmad=false"],
     "lt_step_mixed.cu": [],
     "lt_misc.cu": ["-fmad=false"],
+    "lt_noalloc.cu": ["-fmad=false"],
 }
 CPP_UNITS = ["lt_synth_api.cpp"]
 
