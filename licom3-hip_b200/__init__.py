@@ -49,6 +49,10 @@ class SynthConfig(C.Structure):
                 ("tpert", C.c_double), ("ah_bihar", C.c_double)]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("column_ctas_per_sm", C.c_int), ("continuity_tile_y", C.c_int), ("use_graph", C.c_int)]
+
+
 _vp, _sz, _i = C.c_void_p, C.c_size_t, C.c_int
 _SIGS = {
     "lt_create": ([C.POINTER(Grid), C.POINTER(Params), C.POINTER(_vp)], _i),
@@ -92,6 +96,16 @@ _SIGS = {
     "lt_synth_field": ([_vp, _i, _vp, _sz], _i),
     "lt_synth_field_count": ([_vp, _i], C.c_long),
     "lt_synth_upload": ([_vp, _vp], _i),
+    "lt_tracer_content_noalloc": ([_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp], _i),
+    "lt_batch_create": ([C.POINTER(_vp), _i, C.POINTER(_vp)], _i),
+    "lt_batch_destroy": ([_vp], _i),
+    "lt_batch_size": ([_vp, C.POINTER(_i)], _i),
+    "lt_batch_get_config": ([_vp, C.POINTER(BatchConfig)], _i),
+    "lt_batch_set_config": ([_vp, C.POINTER(BatchConfig)], _i),
+    "lt_batch_step": ([_vp, _i], _i),
+    "lt_batch_sync": ([_vp], _i),
+    "lt_batch_last_ms": ([_vp, C.POINTER(C.c_float)], _i),
+    "lt_batch_autotune": ([_vp, _i, C.POINTER(BatchConfig)], _i),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(lib, _name)
@@ -337,3 +351,61 @@ class Synth:
             for n, a in self.inputs().items():
                 dom.set(n, a)
         return dom
+
+
+class Batch:
+    """Several domains stepped together (include/licom_batch.h): ensemble
+    members of one grid or regional domains of different sizes, all of one
+    precision, on the current device.  Mixed-precision members share one
+    continuity launch and one persistent column launch per step; the steps
+    replay captured CUDA graphs."""
+
+    def __init__(self, domains):
+        self.domains = list(domains)          # the batch holds the domains' arenas
+        arr = (_vp * len(self.domains))(*[d.h for d in self.domains])
+        h = _vp()
+        _check(lib.lt_batch_create(arr, len(self.domains), C.byref(h)), "lt_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.lt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, nsteps=1):
+        _check(lib.lt_batch_step(self.h, int(nsteps)), "lt_batch_step")
+
+    def sync(self):
+        _check(lib.lt_batch_sync(self.h), "lt_batch_sync")
+
+    def last_ms(self):
+        ms = C.c_float()
+        _check(lib.lt_batch_last_ms(self.h, C.byref(ms)), "lt_batch_last_ms")
+        return ms.value
+
+    def config(self):
+        c = BatchConfig()
+        _check(lib.lt_batch_get_config(self.h, C.byref(c)), "lt_batch_get_config")
+        return {"column_ctas_per_sm": c.column_ctas_per_sm, "continuity_tile_y": c.continuity_tile_y,
+                "use_graph": c.use_graph}
+
+    def set_config(self, column_ctas_per_sm=None, continuity_tile_y=None, use_graph=None):
+        cur = self.config()
+        for k, v in (("column_ctas_per_sm", column_ctas_per_sm), ("continuity_tile_y", continuity_tile_y),
+                     ("use_graph", use_graph)):
+            if v is not None:
+                cur[k] = int(v)
+        c = BatchConfig(cur["column_ctas_per_sm"], cur["continuity_tile_y"], cur["use_graph"])
+        _check(lib.lt_batch_set_config(self.h, C.byref(c)), "lt_batch_set_config")
+
+    def autotune(self, trial_steps=2):
+        c = BatchConfig()
+        _check(lib.lt_batch_autotune(self.h, int(trial_steps), C.byref(c)), "lt_batch_autotune")
+        return {"column_ctas_per_sm": c.column_ctas_per_sm, "continuity_tile_y": c.continuity_tile_y,
+                "use_graph": c.use_graph}

@@ -28,6 +28,7 @@ CU_UNITS = {
     "lt_step_mixed.cu": [],
     "lt_misc.cu": ["-fmad=false"],
     "lt_noalloc.cu": ["-fmad=false"],
+    "lt_batch.cu": [],
 }
 CPP_UNITS = ["lt_synth_api.cpp"]
 

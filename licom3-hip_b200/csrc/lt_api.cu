@@ -13,25 +13,7 @@
 #include "lt_tracer_tma.cuh"
 #include <cudaTypedefs.h>
 
-constexpr int LT_NPHASE = 6;       // surface, sss sum, net halo, continuity, tracer, state halo
-constexpr int LT_PROF_STEPS = 512;  // steps whose phase events are kept
-
-struct lt_domain {
-  lt::Arena a;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int profile = 0;
-  int prof_steps = 0;
-  std::vector<cudaEvent_t> prof_ev;   // [LT_PROF_STEPS][LT_NPHASE + 1]
-  std::vector<void*> allocations;
-  int slots = 0;
-  int steps_done = 0;
-  bool have_state = false;
-  bool owns_stream = false;
-  bool use_tma = false;       // tracer kernel fed by TMA boxes (needs 16-byte row pitch)
-  int tma_grid = 0;           // persistent CTAs of the TMA tracer kernel
-  lt::TracerMaps maps;
-};
+#include "lt_domain.h"
 
 namespace lt {
 
@@ -256,8 +238,6 @@ bool build_tracer_maps(const Arena& a, TracerMaps* m) {
   return ok;
 }
 
-namespace {
-
 int run_step(lt_domain* d) {
   Arena& a = d->a;
   cudaStream_t s = d->stream;
@@ -296,7 +276,17 @@ int run_step(lt_domain* d) {
   return LT_OK;
 }
 
-}  // namespace
+// After the stream has drained: a column kernel whose bounded wait for its
+// TMA boxes ran out set status[1] and returned early; report it once.
+int timeout_status(lt_domain* d) {
+  int h = 0;
+  LT_CUDA_OK(cudaMemcpy(&h, d->a.status + 1, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!h) return LT_OK;
+  LT_CUDA_OK(cudaMemset(d->a.status + 1, 0, sizeof(int)));
+  set_error("a tracer column kernel gave up waiting for its level data; the state of that step is not valid");
+  return LT_E_TIMEOUT;
+}
+
 }  // namespace lt
 
 using namespace lt;
@@ -522,17 +512,6 @@ int lt_step(lt_domain* d, int nsteps) {
   }
   LT_CUDA_OK(cudaEventRecord(d->ev1, d->stream));
   return LT_OK;
-}
-
-// After the stream has drained: a column kernel whose bounded wait for its
-// TMA boxes ran out set status[1] and returned early; report it once.
-static int timeout_status(lt_domain* d) {
-  int h = 0;
-  LT_CUDA_OK(cudaMemcpy(&h, d->a.status + 1, sizeof(int), cudaMemcpyDeviceToHost));
-  if (!h) return LT_OK;
-  LT_CUDA_OK(cudaMemset(d->a.status + 1, 0, sizeof(int)));
-  set_error("a tracer column kernel gave up waiting for its level data; the state of that step is not valid");
-  return LT_E_TIMEOUT;
 }
 
 int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2_out, double* content2_out) {

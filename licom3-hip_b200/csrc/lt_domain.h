@@ -1,0 +1,34 @@
+// lt_domain.h - the per-domain state behind the C ABI handle (private to the
+// library: lt_api.cu and lt_batch.cu).
+#pragma once
+#include <vector>
+#include "lt_common.cuh"
+#include "lt_tracer_tma.cuh"
+
+constexpr int LT_NPHASE = 6;       // surface, sss sum, net halo, continuity, tracer, state halo
+constexpr int LT_PROF_STEPS = 512;  // steps whose phase events are kept
+
+struct lt_domain {
+  lt::Arena a;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int profile = 0;
+  int prof_steps = 0;
+  std::vector<cudaEvent_t> prof_ev;   // [LT_PROF_STEPS][LT_NPHASE + 1]
+  std::vector<void*> allocations;
+  int slots = 0;
+  int steps_done = 0;
+  bool have_state = false;
+  bool owns_stream = false;
+  bool use_tma = false;       // tracer kernel fed by TMA boxes (needs 16-byte row pitch)
+  int tma_grid = 0;           // persistent CTAs of the TMA tracer kernel
+  lt::TracerMaps maps;
+};
+
+namespace lt {
+// one tracer step of a domain on its own stream (the tracer_ body)
+int run_step(lt_domain* d);
+// after the stream has drained: LT_E_TIMEOUT once if a column kernel's
+// bounded wait ran out since the last check
+int timeout_status(lt_domain* d);
+}  // namespace lt

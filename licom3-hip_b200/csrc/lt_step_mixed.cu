@@ -80,14 +80,15 @@ __device__ __forceinline__ float face32(float w1, float w2, float h) { return (w
 // from the partial sums P(k) = sum_{k'<k} dzp*wka as
 //   raw(k) = ws(0) + W * ohbt * Z(k) + P(k),  Z(k) = sum_{k'<k} dzp,
 // with P(k) parked in the ws field between the two passes.
-constexpr int CBX = 32, CBY = 8;
-__global__ void __launch_bounds__(CBX * CBY) k_cont_march32(Arena a) {
+constexpr int CBX = 32;
+template <int CBY>
+__device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
   constexpr int UX = CBX + 1, UY = CBY + 1, UN = UX * UY, NT = CBX * CBY;
   // wkd/wkb: mean velocities at U points, double-buffered over levels;
   // fm1: free-surface factor minus one (-1 where the reference's uk/vk are zero)
   __shared__ float s_wkd[2][UN], s_wkb[2][UN], s_fm1[UN];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CBX + tx;
-  const int x0 = blockIdx.x * CBX, y0 = blockIdx.y * CBY;
+  const int x0 = bx * CBX, y0 = by * CBY;
   const int imt = a.imt, jmt = a.jmt, km = a.km;
   const long A = a.A;
   const float oncc = (float)a.p.oncc;
@@ -167,6 +168,21 @@ __global__ void __launch_bounds__(CBX * CBY) k_cont_march32(Arena a) {
     const long c = (long)k * A + qo;
     a.ws32[c] = (k < kz) ? (float)(fac * (ws0 + W * ohbt * Z + (double)a.ws32[c])) : 0.f;
   }
+}
+
+constexpr int kContTileY = 8;   // tile height of the single-domain continuity march
+
+__global__ void __launch_bounds__(CBX * kContTileY) k_cont_march32(Arena a) {
+  cont_tile<kContTileY>(a, blockIdx.x, blockIdx.y);
+}
+
+// every member's tiles in one launch: blockIdx.z is the member; tiles beyond
+// a smaller member's grid leave at once
+template <int CBY>
+__global__ void __launch_bounds__(CBX * CBY) k_cont_batch(const MemberDesc* __restrict__ mem) {
+  const Arena& a = mem[blockIdx.z].a;
+  if ((int)blockIdx.x * CBX >= a.imt || (int)blockIdx.y * CBY >= a.jmt) return;
+  cont_tile<CBY>(a, blockIdx.x, blockIdx.y);
 }
 
 }  // namespace
@@ -356,10 +372,11 @@ __device__ __forceinline__ void del4_first_mixed(MxSmem& S, const Arena& a, int 
   }
 }
 
-__global__ void __launch_bounds__(TTHREADS, 4)
-    k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
-  extern __shared__ __align__(128) unsigned char smem_mx[];
-  MxSmem& S = *reinterpret_cast<MxSmem*>(smem_mx);
+// One work item (tile, tracer) of the mixed column march.  Returns false if
+// a level wait gave up: the CTA has then recorded the timeout and drained
+// its boxes, and must return.
+__device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const TracerMaps& maps, double* scr, int ntx,
+                                           long tile, int n, uint32_t& par, uint32_t& outstanding) {
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int imt = a.imt, jmt = a.jmt, km = a.km;
   const long A = a.A, F = a.F, FB = a.FB;
@@ -368,17 +385,7 @@ __global__ void __launch_bounds__(TTHREADS, 4)
   const float dtsf = (float)dts;
   const double* __restrict__ odzp = a.odzp;
   const double* __restrict__ odzt = a.odzt;
-  double* scr = a.col_scratch + (long)blockIdx.x * km * 2 * TTHREADS;
-  if (tid == 0) {
-    for (int s = 0; s < NSM; ++s) mbar_init(&S.bar[s], 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  uint32_t par = 0, outstanding = 0;
-
-  for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x) {
-    const long tile = w >> 1;
-    const int n = (int)(w & 1);
+  {
     const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * TY;
     const int i = x0 + tx, j = y0 + ty;
     double* at_out = a.at[a.cur ^ 1] + n * F;
@@ -448,7 +455,7 @@ __global__ void __launch_bounds__(TTHREADS, 4)
 
     {
       const bool ok = wait(km - 1) && wait(km - 2);
-      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
     }
     faces_level(S, km - 1);
     __syncthreads();
@@ -456,7 +463,7 @@ __global__ void __launch_bounds__(TTHREADS, 4)
 
     for (int k = km - 1; k >= 0; --k) {
       const bool ok = (k >= 2) ? wait(k - 2) : true;
-      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
       // ---- phase B1: faces one level up, first Laplacian here
       if (k >= 1) faces_level(S, k - 1);
       del4_first_mixed(S, a, k, x0, y0);
@@ -611,6 +618,46 @@ __global__ void __launch_bounds__(TTHREADS, 4)
       }
     }
   }
+  return true;
+}
+
+__device__ __forceinline__ MxSmem& mixed_smem_init() {
+  extern __shared__ __align__(128) unsigned char smem_mx[];
+  MxSmem& S = *reinterpret_cast<MxSmem*>(smem_mx);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSM; ++s) mbar_init(&S.bar[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  return S;
+}
+
+__global__ void __launch_bounds__(TTHREADS, 4)
+    k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
+  MxSmem& S = mixed_smem_init();
+  uint32_t par = 0, outstanding = 0;
+  double* scr = a.col_scratch + (long)blockIdx.x * a.km * 2 * TTHREADS;
+  for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x)
+    if (!mixed_item(S, a, maps, scr, ntx, w >> 1, (int)(w & 1), par, outstanding)) return;
+}
+
+// Several domains (ensemble members, serving requests; any sizes) in one
+// persistent launch: the work list is the concatenation of every member's
+// (tile, tracer) items, member after member, so neighbouring CTAs work on
+// neighbouring tiles of the same member.  Each CTA's items ascend, so its
+// member index only moves forward.
+__global__ void __launch_bounds__(TTHREADS, 4)
+    k_tracer_mixed_batch(const MemberDesc* __restrict__ mem, int nmem, long total, double* scratch, int km_max) {
+  MxSmem& S = mixed_smem_init();
+  uint32_t par = 0, outstanding = 0;
+  double* scr = scratch + (long)blockIdx.x * km_max * 2 * TTHREADS;
+  int m = 0;
+  for (long w = blockIdx.x; w < total; w += gridDim.x) {
+    while (m + 1 < nmem && mem[m + 1].item0 <= w) ++m;
+    const MemberDesc& d = mem[m];
+    const long local = w - d.item0;
+    if (!mixed_item(S, d.a, d.maps, scr, d.ntx, local >> 1, (int)(local & 1), par, outstanding)) return;
+  }
 }
 
 }  // namespace
@@ -629,8 +676,38 @@ int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t
   return LT_OK;
 }
 
+size_t mixed_tracer_smem_bytes() { return sizeof(MxSmem); }
+
+int prepare_tracer_mixed_batch() {
+  LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sizeof(MxSmem)));
+  return LT_OK;
+}
+
+// prepare_tracer_mixed_batch() must have run on this device (it cannot run
+// inside a stream capture)
+int launch_tracer_mixed_batch(const MemberDesc* mem, int nmem, long total, double* scratch, int km_max, int grid,
+                              cudaStream_t s) {
+  k_tracer_mixed_batch<<<grid, TTHREADS, sizeof(MxSmem), s>>>(mem, nmem, total, scratch, km_max);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_continuity_mixed_batch(const MemberDesc* mem, int nmem, int max_imt, int max_jmt, int cby,
+                                  cudaStream_t s) {
+  const unsigned gx = (max_imt + CBX - 1) / CBX;
+  switch (cby) {
+    case 4: k_cont_batch<4><<<dim3(gx, (max_jmt + 3) / 4, nmem), dim3(CBX, 4), 0, s>>>(mem); break;
+    case 8: k_cont_batch<8><<<dim3(gx, (max_jmt + 7) / 8, nmem), dim3(CBX, 8), 0, s>>>(mem); break;
+    case 16: k_cont_batch<16><<<dim3(gx, (max_jmt + 15) / 16, nmem), dim3(CBX, 16), 0, s>>>(mem); break;
+    default: set_error("continuity tile height %d not built (4, 8, 16)", cby); return LT_E_INVALID;
+  }
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
 int launch_continuity_mixed(const Arena& a, cudaStream_t s) {
-  dim3 b(CBX, CBY), g((a.imt + CBX - 1) / CBX, (a.jmt + CBY - 1) / CBY);
+  dim3 b(CBX, kContTileY), g((a.imt + CBX - 1) / CBX, (a.jmt + kContTileY - 1) / kContTileY);
   k_cont_march32<<<g, b, 0, s>>>(a);
   LT_LAUNCHED();
   return LT_OK;

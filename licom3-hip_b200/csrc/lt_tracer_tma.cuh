@@ -115,7 +115,27 @@ __device__ __forceinline__ void load_tile_statics(SM& S, const Arena& a, int x0,
   }
 }
 
+// One member of a batched launch, in device memory.  The tensor maps come
+// first: a map read from global memory must be 64-byte aligned.
+struct alignas(64) MemberDesc {
+  TracerMaps maps;
+  Arena a;
+  long item0;    // first (tile, tracer) work item of this member in the batch list
+  long ntiles;   // column tiles of this member
+  int ntx;       // tiles along i
+};
+
 int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
+// Batched forms (mixed precision): nmem members, total work items, one
+// persistent column launch of `grid` CTAs with per-CTA scratch of km_max
+// levels; continuity over every member's tiles with tiles of 32 x cby columns.
+int launch_tracer_mixed_batch(const MemberDesc* mem, int nmem, long total, double* scratch, int km_max, int grid,
+                              cudaStream_t s);
+int launch_continuity_mixed_batch(const MemberDesc* mem, int nmem, int max_imt, int max_jmt, int cby,
+                                  cudaStream_t s);
+size_t mixed_tracer_smem_bytes();
+// sets the batched column kernel's shared-memory size on the current device
+int prepare_tracer_mixed_batch();
 int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
 // Build the tensor maps of a domain; false if the layout does not allow TMA
 // (row pitch not a multiple of 16 bytes for some field).
