@@ -17,6 +17,7 @@ sample of the same workload.
 """
 import argparse
 import ctypes as C
+from math import exp as math_exp, log as math_log
 import importlib.util
 import json
 import os
@@ -63,6 +64,12 @@ def parse():
     ap.add_argument("--grid", type=int, nargs=3, default=[3600, 2302, 55])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
+    ap.add_argument("--workload", default="tracer", choices=["tracer", "ensemble", "serving"],
+                    help="tracer: the 0.1-degree step (default); ensemble: 64 perturbed members of the 1-degree "
+                         "grid in one batch; serving: Poisson-arriving regional requests")
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: mean arrivals per second")
     return ap.parse_args()
 
 
@@ -332,9 +339,105 @@ def run_ours(args):
         pg.destroy_process_group()
 
 
+def run_ensemble(args):
+    """Configuration 3: members of the 1-degree 360x218x30 grid, T perturbed
+    by seeded N(0, 0.01 K) per member, advanced --steps steps as ONE batch
+    (one continuity and one persistent column launch per step, replayed from
+    a CUDA graph, launch shape from the autotuner), mixed precision; every
+    member is then checked against its own FP64 run."""
+    import numpy as np
+    lt = load_package()
+    lt.set_device(0)
+    nx, ny, km, nmem, steps = 360, 218, 30, args.members, args.steps
+    syns = [lt.Synth(nx, ny, km, member=m + 1, tpert=0.01, forced=1, cap_north=0) for m in range(nmem)]
+    doms = [s.domain(precision=lt.PREC_MIXED) for s in syns]
+    batch = lt.Batch(doms)
+    cfg = batch.autotune(trial_steps=2)
+    batch.step(args.warmup)
+    batch.sync()
+    n0 = lt.launch_count()
+    with ClockSampler(0) as clk:
+        batch.step(steps)
+        batch.sync()
+    launches = lt.launch_count() - n0
+    ms = batch.last_ms()
+    cells = nx * ny * km
+    value = whole_job_rate(cells * nmem, steps, 1, ms)
+    # accuracy of every member against its FP64 run over the same steps
+    worst_t = worst_s = 0.0
+    for s, d in zip(syns, doms):
+        ref = s.domain(precision=lt.PREC_FP64)
+        ref.step(args.warmup + steps)
+        ref.sync()
+        kmt = s.field("KMT")
+        wet = (np.arange(km)[:, None, None] < kmt[None])[:, 2:-2, 2:-2]
+        a, g = ref.get("AT")[:, :, 2:-2, 2:-2], d.get("AT")[:, :, 2:-2, 2:-2]
+        worst_t = max(worst_t, float(np.abs(a[0] - g[0])[wet].max()))
+        worst_s = max(worst_s, float(np.abs(a[1] - g[1])[wet].max()) * 1e3)
+        del ref
+    hbm, hbm_kind = peaks()
+    line = {"metric": "ensemble tracer cell-steps/s (%d x 1deg %dx%dx%d, MIXED, one batch)" % (nmem, nx, ny, km),
+            "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 arithmetic, f64 state", "data": "synthetic (seeded generators, perturbed members)",
+            "config": {"workload": "ensemble %d x %dx%dx%d" % (nmem, nx, ny, km), "members": nmem,
+                       "launch_shape": cfg, "l2": "%.1f GB resident, far larger than L2" % (
+                           nmem * 66.8e9 / 4.56e8 * cells / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": value * STEP_BYTES["mixed"] / 1e9, "peak": hbm,
+                         "unit": "GB/s", "frac": value * STEP_BYTES["mixed"] / 1e9 / hbm, "peak_kind": hbm_kind,
+                         "basis": "whole step, 100 B per cell-step"},
+            "accuracy": {"max_abs_dT_K": worst_t, "max_abs_dS_psu": worst_s, "steps": args.warmup + steps,
+                         "against": "FP64 run of each member"},
+            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": None, "e2e": None}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Configuration 4: Poisson-arriving requests (mean --rate per second) for
+    closed regional domains, horizontal area log-uniform from 128x128 to
+    1200x900 (4:3, km 30 below the geometric middle of the range, 55 above),
+    10..200 steps each, mixed precision, through the request server
+    (admission by free HBM, resident state, continuous batching)."""
+    import random
+    lt = load_package()
+    lt.set_device(0)
+    rng = random.Random(2024)
+    srv = lt.Server(precision=lt.PREC_MIXED, chunk_steps=10)
+    a_lo, a_hi = 128 * 128, 1200 * 900
+    t, t0 = 0.0, srv.clock()
+    for r in range(args.requests):
+        t += rng.expovariate(args.rate)
+        area = math_exp(rng.uniform(math_log(a_lo), math_log(a_hi)))
+        nx = max(64, int(round((area * 4.0 / 3.0) ** 0.5 / 4.0)) * 4)
+        ny = max(48, int(round(area / nx)))
+        km = 30 if area < (a_lo * a_hi) ** 0.5 else 55
+        srv.submit(nx, ny, km, rng.randint(10, 200), arrival=t0 + t, seed=1000 + r,
+                   ew_cyclic=0, tripole=0, forced=1)
+    n0 = lt.launch_count()
+    with ClockSampler(0) as clk:
+        srv.drain()
+    st = srv.stats()
+    value = st["cell_steps"] / st["wall_s"]
+    line = {"metric": "serving tracer cell-steps/s and latency (Poisson %.0f/s, regional 128x128..1200x900)" % args.rate,
+            "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": None, "warmup": 0,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 arithmetic, f64 state", "data": "synthetic (seeded generators, seeded arrivals)",
+            "config": {"workload": "serving %d requests" % args.requests, "rate_per_s": args.rate,
+                       "chunk_steps": 10},
+            "latency_s": {"p50": st["latency_p50"], "p99": st["latency_p99"], "max": st["latency_max"]},
+            "device_busy_cell_steps_per_s": st["cell_steps"] / st["busy_s"] if st["busy_s"] else None,
+            "server": st, "gpu_launches": lt.launch_count() - n0, "clocks": clk.summary(),
+            "cpu_baseline": None, "e2e": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "ensemble":
+        run_ensemble(args)
+    elif args.workload == "serving":
+        run_serving(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

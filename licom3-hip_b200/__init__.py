@@ -53,6 +53,28 @@ class BatchConfig(C.Structure):
     _fields_ = [("column_ctas_per_sm", C.c_int), ("continuity_tile_y", C.c_int), ("use_graph", C.c_int)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_active", C.c_int), ("chunk_steps", C.c_int),
+                ("precision", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("domain", SynthConfig), ("steps", C.c_int), ("arrival", C.c_double), ("keep_state", C.c_int)]
+
+
+class RequestStatus(C.Structure):
+    _fields_ = [("state", C.c_int), ("steps_done", C.c_int), ("arrival", C.c_double), ("admitted", C.c_double),
+                ("finished", C.c_double), ("content", C.c_double * 2), ("cells", C.c_longlong),
+                ("bytes", C.c_size_t)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_longlong), ("requests_refused", C.c_longlong), ("iterations", C.c_longlong),
+                ("cell_steps", C.c_double), ("busy_s", C.c_double), ("wall_s", C.c_double),
+                ("latency_p50", C.c_double), ("latency_p99", C.c_double), ("latency_max", C.c_double),
+                ("max_resident", C.c_int), ("peak_bytes", C.c_size_t)]
+
+
 _vp, _sz, _i = C.c_void_p, C.c_size_t, C.c_int
 _SIGS = {
     "lt_create": ([C.POINTER(Grid), C.POINTER(Params), C.POINTER(_vp)], _i),
@@ -106,6 +128,15 @@ _SIGS = {
     "lt_batch_sync": ([_vp], _i),
     "lt_batch_last_ms": ([_vp, C.POINTER(C.c_float)], _i),
     "lt_batch_autotune": ([_vp, _i, C.POINTER(BatchConfig)], _i),
+    "lt_server_create": ([C.POINTER(ServerConfig), C.POINTER(_vp)], _i),
+    "lt_server_destroy": ([_vp], _i),
+    "lt_server_clock": ([_vp], C.c_double),
+    "lt_server_submit": ([_vp, C.POINTER(Request), C.POINTER(_i)], _i),
+    "lt_server_run_once": ([_vp, C.POINTER(_i)], _i),
+    "lt_server_drain": ([_vp], _i),
+    "lt_server_status": ([_vp, _i, C.POINTER(RequestStatus)], _i),
+    "lt_server_state": ([_vp, _i, _vp, _sz], _i),
+    "lt_server_stats_get": ([_vp, C.POINTER(ServerStats)], _i),
 }
 for _name, (_args, _res) in _SIGS.items():
     _fn = getattr(lib, _name)
@@ -409,3 +440,71 @@ class Batch:
         _check(lib.lt_batch_autotune(self.h, int(trial_steps), C.byref(c)), "lt_batch_autotune")
         return {"column_ctas_per_sm": c.column_ctas_per_sm, "continuity_tile_y": c.continuity_tile_y,
                 "use_graph": c.use_graph}
+
+
+REQ_STATES = {0: "pending", 1: "queued", 2: "resident", 3: "done", -1: "refused"}
+
+
+class Server:
+    """Request server (include/licom_serve.h): admission by free HBM,
+    resident state, continuous batching of every resident request."""
+
+    def __init__(self, precision=PREC_MIXED, hbm_budget=0, max_active=0, chunk_steps=0):
+        c = ServerConfig(int(hbm_budget), int(max_active), int(chunk_steps), int(precision))
+        h = _vp()
+        _check(lib.lt_server_create(C.byref(c), C.byref(h)), "lt_server_create")
+        self.h = h
+        self.precision = precision
+        self._shapes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.lt_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def clock(self):
+        return lib.lt_server_clock(self.h)
+
+    def submit(self, nx, ny, km, steps, arrival=None, keep_state=False, **synth):
+        cfg = SynthConfig()
+        lib.lt_synth_defaults(C.byref(cfg))
+        cfg.nx, cfg.ny, cfg.km = nx, ny, km
+        for k, v in synth.items():
+            setattr(cfg, k, v)
+        r = Request(cfg, int(steps), self.clock() if arrival is None else float(arrival), int(keep_state))
+        rid = C.c_int()
+        _check(lib.lt_server_submit(self.h, C.byref(r), C.byref(rid)), "lt_server_submit")
+        self._shapes[rid.value] = (nx, ny, km)
+        return rid.value
+
+    def run_once(self):
+        busy = C.c_int()
+        _check(lib.lt_server_run_once(self.h, C.byref(busy)), "lt_server_run_once")
+        return bool(busy.value)
+
+    def drain(self):
+        _check(lib.lt_server_drain(self.h), "lt_server_drain")
+
+    def status(self, rid):
+        st = RequestStatus()
+        _check(lib.lt_server_status(self.h, int(rid), C.byref(st)), "lt_server_status")
+        return {"state": REQ_STATES.get(st.state, st.state), "steps_done": st.steps_done, "arrival": st.arrival,
+                "admitted": st.admitted, "finished": st.finished, "content": tuple(st.content), "cells": st.cells,
+                "bytes": st.bytes}
+
+    def state(self, rid):
+        nx, ny, km = self._shapes[rid]
+        a = np.empty((2, km, ny + 4, nx + 4))
+        _check(lib.lt_server_state(self.h, int(rid), a.ctypes.data, a.nbytes), "lt_server_state")
+        return a
+
+    def stats(self):
+        st = ServerStats()
+        _check(lib.lt_server_stats_get(self.h, C.byref(st)), "lt_server_stats_get")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}

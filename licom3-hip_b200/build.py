@@ -29,6 +29,7 @@ CU_UNITS = {
     "lt_misc.cu": ["-fmad=false"],
     "lt_noalloc.cu": ["-fmad=false"],
     "lt_batch.cu": [],
+    "lt_serve.cu": [],
 }
 CPP_UNITS = ["lt_synth_api.cpp"]
 

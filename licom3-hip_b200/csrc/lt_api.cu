@@ -401,13 +401,15 @@ int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
     *it.first = base + off;
     off += (it.second + 255) / 256 * 256;
   }
-  cudaMemset(base, 0, pl.off);
   if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
     cudaFree(base);
     delete d;
     return LT_E_CUDA;
   }
   d->owns_stream = true;
+  // cleared on the domain's own stream, so every later use on that stream is
+  // ordered after it without stalling other streams of the device
+  cudaMemsetAsync(base, 0, pl.off, d->stream);
   cudaEventCreate(&d->ev0);
   cudaEventCreate(&d->ev1);
   // TMA-fed tracer kernel where the row pitch is a multiple of 16 bytes
@@ -416,7 +418,10 @@ int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
   // mixed kernel 4 (its __launch_bounds__ and shared-memory footprint)
   const long per_sm = d->a.precision == LT_PREC_MIXED ? 4 : 3;
   d->tma_grid = (int)std::min<long>(d->a.col_scratch_slots, (long)sms * per_sm);
-  cudaDeviceSynchronize();
+  if (cudaStreamSynchronize(d->stream) != cudaSuccess) {
+    lt_destroy(d);
+    return LT_E_CUDA;
+  }
   *out = d;
   return LT_OK;
 }
