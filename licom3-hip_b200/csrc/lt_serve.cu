@@ -4,10 +4,12 @@
 // One scheduling iteration:
 //   1. step every resident request through one batch by k steps, k the
 //      smallest remaining step count capped at chunk_steps (enqueued, async);
-//   2. meanwhile on the host: queue the requests that have arrived and admit
-//      from the head of the queue while their arenas fit the HBM budget
-//      (inputs built from the generators, uploaded on the new domain's own
-//      stream); they join the batch at the next iteration;
+//   2. meanwhile on the host: queue the requests that have arrived, start
+//      building their inputs from the generators on worker threads (at most
+//      one per host core in flight), and admit from the head of the queue
+//      while their arenas fit the HBM budget (arena allocated, inputs
+//      uploaded on the new domain's own stream); they join the batch at the
+//      next iteration;
 //   3. wait for the step, retire the requests that reached their step count
 //      (content sums, optional host copy of the state), free their arenas.
 // The queue is first come, first served; a request larger than the whole
@@ -16,6 +18,7 @@
 #include <chrono>
 #include <cmath>
 #include <deque>
+#include <future>
 #include <new>
 #include <thread>
 #include <vector>
@@ -34,7 +37,15 @@ struct Req {
   lt_domain* dom = nullptr;
   int remaining = 0;
   std::vector<double> final_at;
+  std::future<std::pair<int, lt_synth*>> inputs;   // generator build on a worker thread
+  bool building = false;
 };
+
+std::pair<int, lt_synth*> build_inputs(lt_synth_config cfg) {
+  lt_synth* syn = nullptr;
+  const int rc = lt_synth_build(&cfg, &syn);
+  return {rc, syn};
+}
 
 }  // namespace
 
@@ -50,6 +61,7 @@ struct lt_server {
   lt_batch* batch = nullptr;
   std::vector<int> batch_ids;   // membership of `batch`
   lt_server_stats stats{};
+  int builders = 4;             // input builds in flight at most
 };
 
 namespace {
@@ -72,6 +84,17 @@ int admit(lt_server* s) {
     s->reqs[id].st.state = LT_REQ_QUEUED;
     s->queue.push_back(id);
   }
+  // start input builds for the head of the queue
+  int in_flight = 0;
+  for (int id : s->queue) in_flight += s->reqs[id].building;
+  for (int id : s->queue) {
+    if (in_flight >= s->builders) break;
+    Req& q = s->reqs[id];
+    if (q.building || q.st.bytes > s->cfg.hbm_budget) continue;
+    q.inputs = std::async(std::launch::async, build_inputs, q.r.domain);
+    q.building = true;
+    ++in_flight;
+  }
   while (!s->queue.empty() && (int)s->active.size() < s->cfg.max_active) {
     Req& q = s->reqs[s->queue.front()];
     if (q.st.bytes > s->cfg.hbm_budget) {
@@ -81,9 +104,15 @@ int admit(lt_server* s) {
       continue;
     }
     if (s->used + q.st.bytes > s->cfg.hbm_budget) break;
-    lt_synth* syn = nullptr;
+    if (!q.building) {
+      q.inputs = std::async(std::launch::async, build_inputs, q.r.domain);
+      q.building = true;
+    }
+    auto built = q.inputs.get();
+    q.building = false;
+    lt_synth* syn = built.second;
     lt_params prm;
-    int rc = lt_synth_build(&q.r.domain, &syn);
+    int rc = built.first;
     if (!rc) rc = lt_synth_params(syn, &prm);
     if (!rc) rc = lt_create(&q.grid, &prm, &q.dom);
     if (!rc) rc = lt_synth_upload(syn, q.dom);
@@ -138,6 +167,7 @@ int lt_server_create(const lt_server_config* cfg, lt_server** out) {
   s->cfg = *cfg;
   if (s->cfg.max_active <= 0) s->cfg.max_active = 512;
   if (s->cfg.chunk_steps <= 0) s->cfg.chunk_steps = 10;
+  s->builders = std::max(4, (int)std::thread::hardware_concurrency());
   if (s->cfg.hbm_budget == 0) {
     size_t free_b = 0, total_b = 0;
     LT_CUDA_OK(cudaMemGetInfo(&free_b, &total_b));
@@ -152,8 +182,13 @@ int lt_server_create(const lt_server_config* cfg, lt_server** out) {
 int lt_server_destroy(lt_server* s) {
   if (!s) return LT_E_INVALID;
   drop_batch(s);
-  for (Req& q : s->reqs)
+  for (Req& q : s->reqs) {
+    if (q.building) {
+      auto built = q.inputs.get();
+      if (built.second) lt_synth_free(built.second);
+    }
     if (q.dom) lt_destroy(q.dom);
+  }
   delete s;
   return LT_OK;
 }
