@@ -13,10 +13,12 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblicom_tracer.so")
+# LICOM_TRACER_LIB selects another build of the same library (e.g. one
+# compiled with different flags); the default is the in-tree build
+LIB_PATH = os.environ.get("LICOM_TRACER_LIB") or os.path.join(_HERE, "liblicom_tracer.so")
 
 if not os.path.exists(LIB_PATH):
-    raise ImportError("liblicom_tracer.so is not built; run python licom3-hip_b200/build.py")
+    raise ImportError("%s is not built; run python licom3-hip_b200/build.py" % LIB_PATH)
 
 lib = C.CDLL(LIB_PATH)
 

@@ -452,6 +452,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     const double hts_s64 = inner ? a.hts[qo] : 0.0, hts_n64 = inner ? a.hts[qo - imt] : 0.0;
     double e_prev = 0.0, f_prev = 0.0;
     double carry = 0.0;  // lower face of the level below, as seen by the level above: A + X
+    float w_below = 0.f;  // explicit diffusion flux through the bottom face, from the level below
 
     {
       const bool ok = wait(km - 1) && wait(km - 2);
@@ -461,13 +462,14 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     __syncthreads();
     predictor_mixed(S, a, km - 1, x0, y0);
 
+    // Level slots: after step k the slot of level k+1 takes level k+1-NSM.
     for (int k = km - 1; k >= 0; --k) {
-      const bool ok = (k >= 2) ? wait(k - 2) : true;
-      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
-      // ---- phase B1: faces one level up, first Laplacian here
+      // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
+      // arrived in earlier steps; the previous step ended with a barrier)
       if (k >= 1) faces_level(S, k - 1);
       del4_first_mixed(S, a, k, x0, y0);
-      __syncthreads();
+      const bool ok = (k >= 2) ? wait(k - 2) : true;
+      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
       // ---- phase B2: predictor one level up
       if (k >= 1) predictor_mixed(S, a, k - 1, x0, y0);
       __syncthreads();
@@ -546,7 +548,6 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         }
         const double atb_k = Lk.atb[rc];
         const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSM].atb[rc] : 0.0;
-        const double atb_kp1 = k < km - 1 ? S.slot[(k + 1) % NSM].atb[rc] : 0.0;
         const float wkc_k = Lk.akt[ac];
         const float wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSM].akt[ac] : 0.f;
         // shortwave through the faces above and below (tracer.cpp:1430-1474)
@@ -557,7 +558,8 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
           if (k < km - 1) vz -= (double)(swv * (float)a.pen[k] * vit_kp1);
         }
         const float w1 = k >= 1 ? wkc_km1 * (float)(atb_km1 - atb_k) * (float)odzt[k] * vit_k : 0.f;
-        const float w2 = k < km - 1 ? wkc_k * (float)(atb_k - atb_kp1) * (float)odzt[k + 1] * vit_kp1 : 0.f;
+        const float w2 = w_below;   // = wkc_k * (atb_k - atb_kp1) * odzt[k+1] * vit_kp1, as formed at level k+1
+        w_below = w1;
         vz += 0.5 * ((double)w1 - (double)w2);
         // surface flux and the freshwater-norm correction stay f64: the
         // correction cancels the global salt flux, which f32 would leave at
