@@ -5,9 +5,10 @@
 // utf/vtf) are f32.  Arithmetic: the flux, stencil and diffusion terms are
 // computed in f32 from f64 differences of the state (predictor, limiter
 // fluxes, Lax-Wendroff and upwind parts, both Laplacians, explicit vertical
-// diffusion, shortwave); the tspas predictor is formed as state + f32
-// increment in f64 and compared with the f64 extrema, so the limiter
-// decisions are those of an f64 run except at exact ties.  f64 remains where
+// diffusion, shortwave); the tspas bound test compares the f32 predictor
+// increment with the f32 differences between the cell and its six
+// neighbours, so the limiter decisions are those of an f64 run except at
+// near-ties.  f64 remains where
 // the global tracer content needs it: the centred advective product d*u of
 // the final update (both cells of a face add it with the same sign, so its
 // rounding would not cancel), the face-flux sums and their metric weights,
@@ -318,34 +319,40 @@ __device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int k
     const float sx = (dx[fe] * ue - bx[fe]) + (dx[fw] * uwv + bx[fw]);
     const float sy = (dy[fs] * vs - by[fs]) + (dy[fn] * vn + by[fn]);
     // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
-    float sz = 0.f;
+    float sz = 0.f, dup = 0.f, ddn = 0.f;   // dup, ddn: a_above - c, a_below - c
     const double c = at_c[r];
     if (kk > 0) {
       const float w = L.ws[u];
-      const float d = (float)(at_u[r] - c);
-      const float A = w * d;
+      dup = (float)(at_u[r] - c);
+      const float A = w * dup;
       sz += A - A * w * odzt_k * dts;
     }
     if (kk < km - 1) {
       const float w = wsd[u];
       const float d = (float)(c - at_d[r]);
+      ddn = -d;
       const float A = w * d;
       sz += A + A * w * odzt_k1 * dts;
     }
     const float inc = -(S.tr[m] * (sx + sy) + hodz * sz) * dts;
-    const double a00 = c + (double)inc;
-    // masked 7-point extrema in f64 (land: -1e10 for the max, +1e10 for the min)
+    // Bound test of the predictor c + inc against the masked 7-point extrema
+    // (land excluded: -1e10 for the max, +1e10 for the min), done on
+    // differences from c: c + inc > max_p a_p  <=>  inc > max_p (a_p - c).
+    // The horizontal differences are the face differences already formed;
+    // with no wet point the reference's extrema flag the cell, as -inf does.
     const int* kt = S.kmt;
-    auto hv = [&](double t, int rr, int kl) { return kl < kt[rr] ? t : -1.0e10; };
-    auto lv = [&](double t, int rr, int kl) { return kl < kt[rr] ? t : 1.0e10; };
-    double hi_ = hv(c, r, kk), lo_ = lv(c, r, kk);
-    hi_ = fmax(hi_, hv(at_c[r - SW], r - SW, kk)); lo_ = fmin(lo_, lv(at_c[r - SW], r - SW, kk));
-    hi_ = fmax(hi_, hv(at_c[r + SW], r + SW, kk)); lo_ = fmin(lo_, lv(at_c[r + SW], r + SW, kk));
-    hi_ = fmax(hi_, hv(at_c[r - 1], r - 1, kk));   lo_ = fmin(lo_, lv(at_c[r - 1], r - 1, kk));
-    hi_ = fmax(hi_, hv(at_c[r + 1], r + 1, kk));   lo_ = fmin(lo_, lv(at_c[r + 1], r + 1, kk));
-    if (kk > 0) { hi_ = fmax(hi_, hv(at_u[r], r, kk - 1)); lo_ = fmin(lo_, lv(at_u[r], r, kk - 1)); }
-    if (kk < km - 1) { hi_ = fmax(hi_, hv(at_d[r], r, kk + 1)); lo_ = fmin(lo_, lv(at_d[r], r, kk + 1)); }
-    fl[m] = (a00 > hi_ || a00 < lo_) ? 1 : 0;
+    float dmax = -INFINITY, dmin = INFINITY;
+    auto acc = [&](bool wet, float d) {
+      if (wet) { dmax = fmaxf(dmax, d); dmin = fminf(dmin, d); }
+    };
+    acc(kk < kt[r], 0.f);
+    acc(kk < kt[r + 1], dx[fe]);
+    acc(kk < kt[r - 1], -dx[fw]);
+    acc(kk < kt[r + SW], dy[fs]);
+    acc(kk < kt[r - SW], -dy[fn]);
+    if (kk > 0) acc(kk - 1 < kt[r], dup);
+    if (kk < km - 1) acc(kk + 1 < kt[r], ddn);
+    fl[m] = (inc > dmax || inc < dmin) ? 1 : 0;
   }
 }
 
