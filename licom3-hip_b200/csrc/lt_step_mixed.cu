@@ -207,7 +207,8 @@ constexpr int NSM = 4;                     // level slots (k+1 .. k-2)
 constexpr int FXN = (TY + 2) * (TX + 3);   // x faces of the 1-halo region
 constexpr int FYN = (TY + 3) * (TX + 2);   // y faces of the 1-halo region
 
-// One level of the column tile, filled by five TMA boxes.  The f32 fields
+// One level of the column tile, filled by five TMA boxes (the mixing
+// coefficient of the own column comes by plain loads, a step ahead).  The f32 fields
 // are w and the U-point means wkd, wkb from which the kernel forms the face
 // transports (face32, face_x64, face_y64).
 struct alignas(128) MxSlot {
@@ -216,10 +217,9 @@ struct alignas(128) MxSlot {
   alignas(128) float ws[(TY + 2) * SW];    // rows y0-1 .. y0+TY
   alignas(128) float wkd[(TY + 3) * SW];   // rows y0-2 .. y0+TY
   alignas(128) float wkb[(TY + 3) * SW];   // rows y0-2 .. y0+TY
-  alignas(128) float akt[TY * TX];         // the tile itself, columns x0 .. x0+TX-1
 };
 constexpr uint32_t kMxLevelBytes =
-    (uint32_t)(2 * (TY + 4) * SW * sizeof(double) + ((TY + 2) * SW + 2 * (TY + 3) * SW + TY * TX) * sizeof(float));
+    (uint32_t)(2 * (TY + 4) * SW * sizeof(double) + ((TY + 2) * SW + 2 * (TY + 3) * SW) * sizeof(float));
 
 struct MxSmem {
   MxSlot slot[NSM];
@@ -230,14 +230,15 @@ struct MxSmem {
   float tr[HN], dtn[HN], dts[HN], dte[HN], dtw[HN], ahf[HN];
   float kx[HN], ky[HN];               // del4 face weights tarea*dte (east face), tarea*dts (south face)
   float cxf[FXN], cyf[FYN];           // 2*dts/(htw*hun), 2*dts/(hts*hue) at the faces
+  float fxu[2][FXN], fyv[2][FYN];    // per level parity: f32 face transports uw, vs
   float hwx[FXN], hsy[FYN];           // htw, hts at the faces (f32)
-  int kmt[(TY + 4) * SW];
+  uint16_t kmt[(TY + 4) * SW];        // bottom level of the tile's columns and their 2-cell halo
   uint64_t bar[NSM];
 };
 // four CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
 static_assert(4 * (sizeof(MxSmem) + 1024) <= 228 * 1024, "mixed tracer tile no longer fits 4 CTAs per SM");
 
-// Issue the five boxes of level L of tracer n into a slot (one thread).
+// Issue the boxes of level L of tracer n into a slot (one thread).
 __device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const TracerMaps& m, int cur, int n, int km,
                                          int L, int x0, int y0) {
   mbar_expect_tx(bar, kMxLevelBytes);
@@ -246,36 +247,33 @@ __device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const Tracer
   tma_load_3d(sl.ws, &m.ws, x0 - 4, y0 - 1, L, bar);
   tma_load_3d(sl.wkd, &m.uw, x0 - 4, y0 - 2, L, bar);
   tma_load_3d(sl.wkb, &m.vs, x0 - 4, y0 - 2, L, bar);
-  tma_load_3d(sl.akt, &m.akt, x0, y0, n * km + L, bar);
 }
 
-// f32 face transports of the 1-halo region from a slot: x face (fj, fi) and
-// y face (fj, fi) as indexed by fx / fy below
-__device__ __forceinline__ float ux32(const MxSlot& L, const MxSmem& S, int fj, int fi, int m) {
-  return face32(L.wkd[fj * SW + fi + 3], L.wkd[(fj + 1) * SW + fi + 3], S.hwx[m]);
-}
-__device__ __forceinline__ float vy32(const MxSlot& L, const MxSmem& S, int fj, int fi, int m) {
-  return face32(L.wkb[fj * SW + fi + 3], L.wkb[fj * SW + fi + 4], S.hsy[m]);
-}
 
 // x face (fj, fi): row y0-1+fj, west side of column x0-1+fi
 // y face (fj, fi): south side of row y0-2+fj, column x0-1+fi
 __device__ __forceinline__ int fx(int fj, int fi) { return fj * (TX + 3) + fi; }
 __device__ __forceinline__ int fy(int fj, int fi) { return fj * (TX + 2) + fi; }
 
-// face differences and Lax-Wendroff parts of level kk for the 1-halo region
+// Face quantities of level kk for the 1-halo region, once per face: the f32
+// transport (face32 on the U-point means), the difference d and the
+// Lax-Wendroff part B.  Every later use reads these, so both cells of a face
+// see the same f32 values.
 __device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
   const MxSlot& L = S.slot[kk % NSM];
   float* dx = S.fxd[kk & 1];
   float* bx = S.fxb[kk & 1];
+  float* ux = S.fxu[kk & 1];
   float* dy = S.fyd[kk & 1];
   float* by = S.fyb[kk & 1];
+  float* vy = S.fyv[kk & 1];
   for (int m = threadIdx.x; m < FXN + FYN; m += TTHREADS) {
     if (m < FXN) {
       const int fj = m / (TX + 3), fi = m % (TX + 3);
       const int r = (fj + 1) * SW + fi + 3;           // cell R in the tracer box
       const float d = (float)(L.at[r] - L.at[r - 1]);
-      const float u = ux32(L, S, fj, fi, m);
+      const float u = face32(L.wkd[fj * SW + fi + 3], L.wkd[(fj + 1) * SW + fi + 3], S.hwx[m]);
+      ux[m] = u;
       dx[m] = d;
       bx[m] = d * u * u * S.cxf[m];
     } else {
@@ -283,7 +281,8 @@ __device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
       const int fj = mm / (TX + 2), fi = mm % (TX + 2);
       const int r = fj * SW + fi + 3;                 // cell L (north) in the tracer box
       const float d = (float)(L.at[r + SW] - L.at[r]);
-      const float v = vy32(L, S, fj, fi, mm);
+      const float v = face32(L.wkb[fj * SW + fi + 3], L.wkb[fj * SW + fi + 4], S.hsy[mm]);
+      vy[mm] = v;
       dy[mm] = d;
       by[mm] = d * v * v * S.cyf[mm];
     }
@@ -314,8 +313,8 @@ __device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int k
     const int r = r2(hj, hi), u = ru(hj, hi);
     // horizontal: east/west x faces, south/north y faces
     const int fe = fx(hj, hi + 1), fw = fx(hj, hi), fs = fy(hj + 1, hi), fn = fy(hj, hi);
-    const float ue = ux32(L, S, hj, hi + 1, fe), uwv = ux32(L, S, hj, hi, fw);
-    const float vs = vy32(L, S, hj + 1, hi, fs), vn = vy32(L, S, hj, hi, fn);
+    const float ue = S.fxu[kk & 1][fe], uwv = S.fxu[kk & 1][fw];
+    const float vs = S.fyv[kk & 1][fs], vn = S.fyv[kk & 1][fn];
     const float sx = (dx[fe] * ue - bx[fe]) + (dx[fw] * uwv + bx[fw]);
     const float sy = (dy[fs] * vs - by[fs]) + (dy[fn] * vn + by[fn]);
     // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
@@ -340,7 +339,7 @@ __device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int k
     // differences from c: c + inc > max_p a_p  <=>  inc > max_p (a_p - c).
     // The horizontal differences are the face differences already formed;
     // with no wet point the reference's extrema flag the cell, as -inf does.
-    const int* kt = S.kmt;
+    const uint16_t* kt = S.kmt;
     float dmax = -INFINITY, dmin = INFINITY;
     auto acc = [&](bool wet, float d) {
       if (wet) { dmax = fmaxf(dmax, d); dmin = fminf(dmin, d); }
@@ -448,7 +447,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     const long qo = own ? (long)j * imt + i : 0;
     const int kz = own ? a.kmt[qo] : 0;
     const int hc = (ty + 1) * HQX + (tx + 1);
-    const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1), ac = ty * TX + tx;
+    const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1);
     const int fe = fx(ty + 1, tx + 2), fwi = fx(ty + 1, tx + 1), fs = fy(ty + 2, tx + 1), fn = fy(ty + 1, tx + 1);
     const float swv = (inner && n == 0) ? (float)a.swv[qo] : 0.f;
     const double stf = own ? a.stf_n[n * A + qo] : 0.0;
@@ -460,6 +459,9 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     double e_prev = 0.0, f_prev = 0.0;
     double carry = 0.0;  // lower face of the level below, as seen by the level above: A + X
     float w_below = 0.f;  // explicit diffusion flux through the bottom face, from the level below
+    // own column's mixing coefficient: level k in akt_here, level k-1 loaded a step ahead
+    const float* akt_col = a.akt32 + n * F + qo;
+    float akt_here = inner ? __ldg(akt_col + (long)(km - 1) * A) : 0.f;
 
     {
       const bool ok = wait(km - 1) && wait(km - 2);
@@ -471,6 +473,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
 
     // Level slots: after step k the slot of level k+1 takes level k+1-NSM.
     for (int k = km - 1; k >= 0; --k) {
+      const float akt_above = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
       // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
       // arrived in earlier steps; the previous step ended with a barrier)
       if (k >= 1) faces_level(S, k - 1);
@@ -489,8 +492,8 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         const float* bx = S.fxb[k & 1];
         const float* dy = S.fyd[k & 1];
         const float* by = S.fyb[k & 1];
-        const float ue = ux32(Lk, S, ty + 1, tx + 2, fe), uwv = ux32(Lk, S, ty + 1, tx + 1, fwi);
-        const float vsv = vy32(Lk, S, ty + 2, tx + 1, fs), vnv = vy32(Lk, S, ty + 1, tx + 1, fn);
+        const float ue = S.fxu[k & 1][fe], uwv = S.fxu[k & 1][fwi];
+        const float vsv = S.fyv[k & 1][fs], vnv = S.fyv[k & 1][fn];
         // the same faces in f64, as the continuity march formed them
         const int xw = (ty + 1) * SW + tx + 4;   // wkd of U point (j-1, i); (j, i) is one row down
         const double ue64 = face_x64(Lk.wkd[xw + 1], Lk.wkd[xw + 1 + SW], htw_e64);
@@ -555,8 +558,8 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         }
         const double atb_k = Lk.atb[rc];
         const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSM].atb[rc] : 0.0;
-        const float wkc_k = Lk.akt[ac];
-        const float wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSM].akt[ac] : 0.f;
+        const float wkc_k = akt_here;
+        const float wkc_km1 = akt_above;
         // shortwave through the faces above and below (tracer.cpp:1430-1474)
         // and the explicit half of the vertical diffusion: each face flux is
         // the same f32 expression in the cells above and below it, summed in f64
@@ -605,6 +608,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         sl[tid] = ev;
         sl[TTHREADS + tid] = fv;
       }
+      akt_here = akt_above;
       __syncthreads();
       if (k + 1 <= km - 1 && k + 1 - NSM >= 0) issue(k + 1 - NSM);
     }
