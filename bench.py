@@ -4,7 +4,7 @@ Metric: tracer cell-steps/s (nx*ny*km physical cells, land included, halo
 excluded, both T and S advanced per step) on the 0.1-degree grid
 3600 x 2302 x 55, seeded synthetic inputs of that shape (no NetCDF here).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed|both]
                     [--impl ours|reference] [--grid NX NY KM]
 
 One JSON line on rank 0.  Under torchrun each rank advances an independent
@@ -40,7 +40,7 @@ TRACER_KERNEL_BYTES = {"fp64": 104.0, "mixed": 84.0}
 # DRAM bytes per cell (read + write) of the column kernel, from one ncu
 # --set full capture of a 720x460x55 launch; traffic grows with the cells, so
 # it scales to the bench's launch
-TRACER_KERNEL_TRAFFIC = {"fp64": 3.061e9 / (720 * 460 * 55), "mixed": 2.444e9 / (720 * 460 * 55)}
+TRACER_KERNEL_TRAFFIC = {"fp64": 3.061e9 / (720 * 460 * 55), "mixed": 2.563e9 / (720 * 460 * 55)}
 
 
 def load_package():
@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                    help="both: the mixed step as the headline, with the FP64 drop-in measured beside it")
     ap.add_argument("--grid", type=int, nargs=3, default=[3600, 2302, 55])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
@@ -235,7 +236,7 @@ def run_reference(args):
     if rank == 0:
         rate, cb = cpu_reference_rate(lt, args, args.steps, args.warmup, budget_s=120.0)
         nx, ny, km = args.grid
-        line = {"impl": "reference", "metric": "tracer cell-steps/s (0.1deg 3600x2302x55, FP64)", "value": rate,
+        line = {"impl": "reference", "metric": "tracer cell-steps/s (0.1deg 3600x2302x55)", "value": rate,
                 "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": nx * ny * km / rate * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators, configuration shapes)",
@@ -249,13 +250,13 @@ def run_reference(args):
         pg.destroy_process_group()
 
 
-def run_ours(args):
-    world, rank, local, pg = dist_setup(args)
-    lt = load_package()
-    lt.set_device(local)
+def measure(lt, args, pg, world, local, precision, keep_state):
+    """One precision on the bench grid: device-resident throughput, the
+    column kernel's roofline, end-to-end rate through the C ABI, and the
+    final state (host copy) when asked.  The domain is freed on return."""
     nx, ny, km = args.grid
     w = workload(args)
-    prec = lt.PREC_MIXED if args.precision == "mixed" else lt.PREC_FP64
+    prec = lt.PREC_MIXED if precision == "mixed" else lt.PREC_FP64
     syn = lt.Synth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
     dom = syn.domain(precision=prec)
     cells = nx * ny * km
@@ -279,15 +280,15 @@ def run_ours(args):
     # ---- roofline of the dominant kernel (the fused tracer column kernel)
     hbm, hbm_kind = peaks()
     t_tracer = phases["tracer"] / max(nprof, 1)            # ms per launch
-    kbytes = TRACER_KERNEL_BYTES[args.precision] * cells   # algorithmic bytes per launch
+    kbytes = TRACER_KERNEL_BYTES[precision] * cells        # algorithmic bytes per launch
     achieved = kbytes / (t_tracer * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": "tracer column kernel", "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "peak_kind": hbm_kind,
                 "algorithmic_bytes_per_launch": kbytes,
-                "traffic": TRACER_KERNEL_TRAFFIC[args.precision] * cells,
+                "traffic": TRACER_KERNEL_TRAFFIC[precision] * cells,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 720x460x55 launch, "
                                   "scaled by cells",
-                "step_frac": STEP_BYTES[args.precision] * cells / (ms / args.steps * 1e-3) / 1e9 / hbm,
+                "step_frac": STEP_BYTES[precision] * cells / (ms / args.steps * 1e-3) / 1e9 / hbm,
                 "phase_ms_per_step": {k: v / max(nprof, 1) for k, v in phases.items()}}
 
     # ---- end to end through the C ABI with host buffers: every step copies
@@ -315,25 +316,55 @@ def run_ours(args):
     e2e = {"value": whole_job_rate(cells, e2e_steps, world, ms_e2e), "unit": "cell-steps/s",
            "h2d_bytes_per_step": 6 * A * 8, "d2h_bytes_per_step": 8,
            "api": "lt_step_host (C ABI), pinned host forcing"}
+    state = dom.get("AT") if keep_state else None
+    kmt = syn.field("KMT") if keep_state else None
+    dom.close()
+    return {"value": value, "ms_per_step": ms / args.steps, "roofline": roofline, "e2e": e2e,
+            "gpu_launches": launches, "clocks": clk.summary(), "fw_norm2": fw.value, "state": state, "kmt": kmt,
+            "steps_total": args.warmup + args.steps + 1 + e2e_steps}
+
+
+def run_ours(args):
+    world, rank, local, pg = dist_setup(args)
+    lt = load_package()
+    lt.set_device(local)
+    nx, ny, km = args.grid
+    cells = nx * ny * km
+    both = args.precision == "both"
+    precs = ["fp64", "mixed"] if both else [args.precision]
+    res = {p: measure(lt, args, pg, world, local, p, keep_state=both and rank == 0) for p in precs}
+    main = "mixed" if both else args.precision
+    r = res[main]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         _, cpu = cpu_reference_rate(lt, args, 2, 0)
 
     if rank == 0:
-        line = {"metric": "tracer cell-steps/s (0.1deg 3600x2302x55, %s)" % args.precision.upper(),
-                "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        line = {"metric": "tracer cell-steps/s (0.1deg 3600x2302x55)",
+                "value": r["value"], "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "f32 arithmetic, f64 state",
+                "dtype": "f64" if main == "fp64" else "f32 arithmetic, f64 state",
                 "data": "synthetic (seeded generators with the configuration's shapes and distributions)",
                 "config": {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
-                           "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
+                           "precision": main, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary(), "fw_norm2": fw.value}
+                "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"],
+                "clocks": r["clocks"], "fw_norm2": r["fw_norm2"]}
+        if both:
+            import numpy as np
+            f = res["fp64"]
+            wet = (np.arange(km)[:, None, None] < f["kmt"][None])[:, 2:-2, 2:-2]
+            a, g = f["state"][:, :, 2:-2, 2:-2], r["state"][:, :, 2:-2, 2:-2]
+            line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "e2e": f["e2e"]["value"],
+                            "roofline_frac": f["roofline"]["frac"], "step_frac": f["roofline"]["step_frac"],
+                            "phase_ms_per_step": f["roofline"]["phase_ms_per_step"], "clocks": f["clocks"]}
+            line["mixed_over_fp64"] = r["value"] / f["value"]
+            line["accuracy"] = {"max_abs_dT_K": float(np.abs(a[0] - g[0])[wet].max()),
+                                "max_abs_dS_psu": float(np.abs(a[1] - g[1])[wet].max()) * 1e3,
+                                "steps": r["steps_total"], "against": "the FP64 drop-in on the same inputs"}
         print(json.dumps(line), flush=True)
-    dom.close()
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
