@@ -43,6 +43,13 @@ TRACER_KERNEL_BYTES = {"fp64": 104.0, "mixed": 84.0}
 TRACER_KERNEL_TRAFFIC = {"fp64": 3.061e9 / (720 * 460 * 55), "mixed": 2.563e9 / (720 * 460 * 55)}
 
 
+def ICESNOW_BYTES_PER_POINT(km):
+    """Sea-ice adjustment, per point of the domain (halo included): T read at
+    every level, KMT read, QICE written; S and T are written only where water
+    froze."""
+    return 8.0 * km + 4.0 + 8.0
+
+
 def load_package():
     if "licom3_hip_b200" in sys.modules:
         return sys.modules["licom3_hip_b200"]
@@ -318,10 +325,28 @@ def measure(lt, args, pg, world, local, precision, keep_state):
            "api": "lt_step_host (C ABI), pinned host forcing"}
     state = dom.get("AT") if keep_state else None
     kmt = syn.field("KMT") if keep_state else None
+
+    # ---- the sea-ice adjustment that follows each tracer step in the model
+    # (icesnow.cpp): its own HBM-bound kernel, timed over repeated launches
+    ice = lt.IcesnowParams()
+    for _ in range(3):
+        dom.icesnow(ice)
+    n_ice = 20
+    dom.mark(0)
+    for _ in range(n_ice):
+        dom.icesnow(ice)
+    dom.mark(1)
+    dom.sync()
+    ms_ice = dom.last_step_ms() / n_ice
+    ice_bytes = ICESNOW_BYTES_PER_POINT(km) * (nx + 4) * (ny + 4)
+    icesnow = {"ms_per_launch": ms_ice, "algorithmic_bytes_per_launch": ice_bytes,
+               "achieved_gbs": ice_bytes / (ms_ice * 1e-3) / 1e9,
+               "frac": ice_bytes / (ms_ice * 1e-3) / 1e9 / hbm, "peak_kind": hbm_kind,
+               "share_of_step": ms_ice / (ms / args.steps)}
     dom.close()
     return {"value": value, "ms_per_step": ms / args.steps, "roofline": roofline, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(), "fw_norm2": fw.value, "state": state, "kmt": kmt,
-            "steps_total": args.warmup + args.steps + 1 + e2e_steps}
+            "steps_total": args.warmup + args.steps + 1 + e2e_steps, "icesnow": icesnow}
 
 
 def run_ours(args):
@@ -351,7 +376,7 @@ def run_ours(args):
                            "precision": main, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"],
-                "clocks": r["clocks"], "fw_norm2": r["fw_norm2"]}
+                "clocks": r["clocks"], "fw_norm2": r["fw_norm2"], "icesnow": r["icesnow"]}
         if both:
             import numpy as np
             f = res["fp64"]

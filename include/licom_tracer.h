@@ -4,6 +4,7 @@
  * Drop-in for the tracer path of LICOM3-HIP:
  *   tracer_(int ii)   replaces  tracer.cpp:1701-1903   (extern "C" void tracer_(int))
  *   convadj_(void)    replaces  convadj.cpp:290-298    (extern "C" void convadj_())
+ *   icesnow_(void)    replaces  icesnow.cpp:70-85      (extern "C" void icesnow_())
  * and the device state those read, which the reference keeps in global d_*
  * pointers (cuda_data.h:35-345, allocated by cudainit in cuda_init.cpp:372-707).
  * Here the state lives in a per-domain arena created by lt_create; the two
@@ -71,6 +72,8 @@ typedef enum {
   /* diagnostics, f64 (written when the domain was created with diagnostics) */
   LT_F_AX, LT_F_AY, LT_F_AZ, LT_F_DZ, LT_F_TEND, LT_F_DT_DIFF, LT_F_DT_CONV,  /* [2][km][jmt][imt] */
   LT_F_PENETRATE,                   /* [km][jmt][imt] */
+  /* sea-ice bookkeeping of icesnow, f64 */
+  LT_F_QICE,                        /* [jmt][imt] ice formed, tracer_mod licomqice (d_licomqice) */
   LT_F_COUNT
 } lt_field;
 
@@ -138,6 +141,26 @@ int lt_step(lt_domain* dom, int nsteps);
 int lt_step_host(lt_domain* dom, const double* const forcing6[6], double* fw_norm2_out, double* content2_out);
 /* Convective adjustment of the current state (convadj.cpp:29-288). */
 int lt_convadj(lt_domain* dom);
+
+/* Parameters of the sea-ice adjustment (icesnow.cpp:15-85). */
+typedef struct {
+  double tbice;          /* freezing point of sea water, degC: pconst_mod tbice (constant_mod.F90:168, -1.8) */
+  double cp;             /* heat capacity of sea water: pconst_mod cp (constant_mod.F90:164, 3996.0) */
+  double latice;         /* latent heat of fusion, J/kg: SHR_CONST_LATICE (shr_const_mod.h:51, 3.337e5) */
+  int reset_qice;        /* 1: QICE set to zero first, as the FRC_CORE build does (icesnow.cpp:76-78);
+                            0: QICE carries over between calls */
+} lt_icesnow_params;
+/* The reference's values: tbice -1.8, cp 3996.0, latice 3.337e5, reset_qice 1
+ * (its def-undef.h defines FRC_CORE). */
+void lt_icesnow_defaults(lt_icesnow_params* p);
+/* Sea-ice adjustment of the current state over every point of the domain,
+ * halo included (icesnow_cu, icesnow.cpp:15-68): where the surface T of an
+ * ocean column is below tbice, the deficit goes to QICE, S(level 0) gains
+ * the brine term and T is set to tbice; where QICE is positive and the
+ * surface T is above tbice, ice melts back (T and S lowered, QICE reduced);
+ * finally T at every level is raised to tbice where below.  p NULL means
+ * lt_icesnow_defaults.  Asynchronous on the domain's stream. */
+int lt_icesnow(lt_domain* dom, const lt_icesnow_params* p);
 /* Global tracer integrals sum(tarea*dzp*vit*tracer) over the interior, f64,
  * fixed-order pairwise tree (deterministic). out2[0] = T, out2[1] = S. */
 int lt_tracer_content(lt_domain* dom, double* out2);
@@ -192,6 +215,9 @@ int lt_shim_bind(lt_domain* dom);
 void tracer_(int ii);
 /* convadj.cpp:290: convective adjustment of the bound domain. */
 void convadj_(void);
+/* icesnow.cpp:70 (called after tracer_ in stepon.cpp:71): sea-ice adjustment
+ * of the bound domain with the reference's parameters (lt_icesnow_defaults). */
+void icesnow_(void);
 
 /* --- field metadata ------------------------------------------------------ */
 /* Upper-case name of a field id without the LT_F_ prefix ("AT", "ATB", ...). */

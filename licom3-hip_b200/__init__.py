@@ -43,6 +43,15 @@ class Params(C.Structure):
         ("nss", C.c_int), ("boundary_restore", C.c_int)]
 
 
+class IcesnowParams(C.Structure):
+    """lt_icesnow_params; defaults are the reference's (tbice -1.8, cp 3996.0,
+    latice 3.337e5, QICE reset before each call as in its FRC_CORE build)."""
+    _fields_ = [("tbice", C.c_double), ("cp", C.c_double), ("latice", C.c_double), ("reset_qice", C.c_int)]
+
+    def __init__(self, tbice=-1.8, cp=3996.0, latice=3.337e5, reset_qice=1):
+        super().__init__(tbice, cp, latice, reset_qice)
+
+
 class SynthConfig(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("km", C.c_int), ("lat_s", C.c_double), ("lat_n", C.c_double),
                 ("dz_top", C.c_double), ("dz_bot", C.c_double), ("depth", C.c_double), ("umax", C.c_double),
@@ -98,6 +107,8 @@ _SIGS = {
     "lt_launch_count": ([], C.c_longlong),
     "lt_set_device": ([_i], _i),
     "lt_convadj": ([_vp], _i),
+    "lt_icesnow": ([_vp, C.POINTER(IcesnowParams)], _i),
+    "lt_icesnow_defaults": ([C.POINTER(IcesnowParams)], None),
     "lt_tracer_content": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_fw_norm2": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_sync": ([_vp], _i),
@@ -106,6 +117,7 @@ _SIGS = {
     "lt_shim_bind": ([_vp], _i),
     "tracer_": ([_i], None),
     "convadj_": ([], None),
+    "icesnow_": ([], None),
     "lt_last_error": ([], C.c_char_p),
     "lt_device_count": ([C.POINTER(_i)], _i),
     "lt_version": ([], C.c_char_p),
@@ -156,7 +168,8 @@ while True:
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 INT_FIELDS = {n for n in FIELDS if lib.lt_field_is_int(FIELD_ID[n])}
 # inputs a caller supplies (everything except step outputs and diagnostics)
-# (WS and NET are model state the step reads and rewrites; they start at zero)
+# (WS, NET and QICE are model state the step or icesnow reads and rewrites;
+# they start at zero)
 INPUT_FIELDS = [n for n in FIELDS if n not in (
     "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE")]
 
@@ -291,6 +304,11 @@ class TracerDomain:
     def convadj(self):
         _check(lib.lt_convadj(self.h), "lt_convadj")
 
+    def icesnow(self, params=None):
+        """Sea-ice adjustment of the current state (icesnow.cpp:15-85);
+        params an IcesnowParams, None for the reference's values."""
+        _check(lib.lt_icesnow(self.h, C.byref(params) if params is not None else None), "lt_icesnow")
+
     def tracer_content(self):
         out = (C.c_double * 2)()
         _check(lib.lt_tracer_content(self.h, out), "lt_tracer_content")
@@ -330,6 +348,14 @@ def tracer_(ii=0):
 def convadj_():
     """convadj.cpp:290 - convective adjustment of the bound domain."""
     lib.convadj_()
+
+
+def icesnow_():
+    """icesnow.cpp:70 - sea-ice adjustment of the bound domain with the
+    reference's parameters."""
+    lib.icesnow_()
+    err = lib.lt_last_error()
+    return err.decode() if err else ""
 
 
 class Synth:

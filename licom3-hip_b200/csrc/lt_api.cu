@@ -121,6 +121,7 @@ void* field_ptr(lt_domain* d, int f, int which_state) {
     case LT_F_DT_DIFF: return a.dt_diff;
     case LT_F_DT_CONV: return a.dt_conv;
     case LT_F_PENETRATE: return a.penetrate;
+    case LT_F_QICE: return a.qice;
   }
   return nullptr;
 }
@@ -160,6 +161,7 @@ void plan_arena(Arena& a, Plan& pl) {
                       &a.ohbt, &a.ohbu, &a.au0, &a.aus, &a.auw, &a.ausw, &a.stf_ssh};
   for (auto p : two_d) D(p, A);
   D(&a.stf_n, 2 * A);
+  D(&a.qice, A);
   int** masks[] = {&a.kmt, &a.kmu, &a.kmtn, &a.kmts, &a.kmte, &a.kmtw};
   for (auto p : masks) I(p, A);
   D(&a.dzp, km); D(&a.odzp, km); D(&a.odzt, km); D(&a.pen, km); D(&a.to, km); D(&a.so, km); D(&a.cc, 9 * km);
@@ -300,7 +302,7 @@ static const char* const k_field_names[LT_F_COUNT] = {
     "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE", "DXU", "DYU",
     "AHF", "DTN", "DTS", "DTE", "DTW", "OHBT", "OHBU", "AU0", "AUS", "AUW", "AUSW", "KMT", "KMU", "KMTN", "KMTS",
     "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND",
-    "DT_DIFF", "DT_CONV", "PENETRATE"};
+    "DT_DIFF", "DT_CONV", "PENETRATE", "QICE"};
 
 const char* lt_field_name(int f) { return (f >= 0 && f < LT_F_COUNT) ? k_field_names[f] : nullptr; }
 long lt_field_count(int f, int nx, int ny, int km) {
@@ -545,6 +547,21 @@ int lt_convadj(lt_domain* d) {
   return LT_OK;
 }
 
+void lt_icesnow_defaults(lt_icesnow_params* p) {
+  if (!p) return;
+  p->tbice = -1.8;       // constant_mod.F90:168
+  p->cp = 3996.0;        // constant_mod.F90:164
+  p->latice = 3.337e5;   // shr_const_mod.h:51
+  p->reset_qice = 1;     // def-undef.h defines FRC_CORE
+}
+
+int lt_icesnow(lt_domain* d, const lt_icesnow_params* p) {
+  if (!d) return LT_E_INVALID;
+  lt_icesnow_params def;
+  lt_icesnow_defaults(&def);
+  return launch_icesnow(d->a, p ? *p : def, d->stream);
+}
+
 int lt_tracer_content(lt_domain* d, double* out2) {
   if (!d || !out2) return LT_E_INVALID;
   int rc = launch_tracer_content(d->a, d->stream);
@@ -647,6 +664,18 @@ void convadj_(void) {
   if (launch_convadj(d->a, d->stream)) return;
   cudaError_t e = cudaStreamSynchronize(d->stream);
   if (e != cudaSuccess) cuda_fail(e, "convadj_");
+}
+
+// icesnow.cpp:70
+void icesnow_(void) {
+  set_error("%s", "");
+  lt_domain* d = g_shim;
+  if (!d) { set_error("icesnow_: no domain bound (lt_shim_bind)"); return; }
+  lt_icesnow_params p;
+  lt_icesnow_defaults(&p);
+  if (launch_icesnow(d->a, p, d->stream)) return;
+  cudaError_t e = cudaStreamSynchronize(d->stream);
+  if (e != cudaSuccess) cuda_fail(e, "icesnow_");
 }
 
 }  // extern "C"

@@ -37,6 +37,7 @@ struct Arena {
   double *au0, *aus, *auw, *ausw;
   int *kmt, *kmu, *kmtn, *kmts, *kmte, *kmtw;
   double *dzp, *odzp, *odzt, *pen, *to, *so, *cc, *restore;
+  double *qice;               // [jmt][imt] ice formed by icesnow (tracer_mod licomqice)
   // diagnostics (null when off)
   double *ax, *ay, *az, *dzd, *tend, *dt_diff, *dt_conv, *penetrate;
 
@@ -89,6 +90,7 @@ int launch_tree_sum(const double* x, long n, double* part, double* out, cudaStre
 int launch_interior_sum_sss(const Arena& a, cudaStream_t s);
 int launch_tracer_content(const Arena& a, cudaStream_t s);
 int launch_convadj(const Arena& a, cudaStream_t s);
+int launch_icesnow(const Arena& a, const lt_icesnow_params& p, cudaStream_t s);
 int launch_check_numeric(const Arena& a, cudaStream_t s);
 int launch_derive_masks(const Arena& a, cudaStream_t s);
 int launch_vtl_clobber(const Arena& a, cudaStream_t s);

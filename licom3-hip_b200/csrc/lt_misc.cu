@@ -1,6 +1,6 @@
-// lt_misc.cu - convective adjustment, mask derivation, global sums, numeric
-// scan and the device side of the synthetic-domain upload.  Compiled with
-// -fmad=false (operation order kept as written).
+// lt_misc.cu - convective adjustment, sea-ice adjustment, mask derivation,
+// global sums, numeric scan and the device side of the synthetic-domain
+// upload.  Compiled with -fmad=false (operation order kept as written).
 #include <cstring>
 #include <vector>
 #include "lt_common.cuh"
@@ -123,6 +123,53 @@ __global__ void k_convadj(Arena a) {
       a.tend[c] += d;
       atb[n * FB + (long)(k + 1) * A + q] = at[c];
     }
+}
+
+// ---------------------------------------------------------------- icesnow
+// icesnow_cu (icesnow.cpp:15-68): one thread per point of the domain, halo
+// included, i fastest across a warp.  Surface freezing of ocean columns into
+// QICE with the brine term on S, melting of QICE where the surface is above
+// the freezing point, then T raised to tbice at every level (land included).
+// Operation order is the reference's, so the results are bit-identical; the
+// FRC_CORE reset of QICE is folded in (0 + x == x exactly).  HBM-bound: T is
+// read at every level and written only where it changes.
+__global__ void k_icesnow(Arena a, double tbice, double cp, double latice, int reset) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.imt || j >= a.jmt) return;
+  const long q = (long)j * a.imt + i;
+  const long A = a.A;
+  double* T = a.at[a.cur] + q;
+  double* S = T + a.F;
+  const double sal_ocn = 34.7e0, sal_ice = 4.0e0;
+  double qi = reset ? 0.0 : a.qice[q];
+  double t0 = T[0];
+  if (t0 < tbice && a.kmt[q] > 0) {
+    const double tdiff = tbice - t0;
+    qi += tdiff * a.dzp[0] / a.dzp[0];
+    S[0] += tdiff * (sal_ocn - sal_ice) * cp / latice * 0.001e0;
+    t0 = tbice;
+    T[0] = t0;
+  }
+  if (qi > 0.0 && t0 > tbice) {
+    const double tdiff = fmin(t0 - tbice, qi);
+    qi -= tdiff;
+    t0 -= tdiff;
+    T[0] = t0;
+    S[0] -= tdiff * (sal_ocn - sal_ice) * cp / latice * 0.001e0;
+  }
+  if (t0 < tbice) T[0] = tbice;
+  a.qice[q] = qi;
+  // the levels below in groups of 8: all loads of a group issued before any
+  // store, so that a warp keeps 8 rows in flight
+  for (int k0 = 1; k0 < a.km; k0 += 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = (k0 + u < a.km) ? T[(k0 + u) * A] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u < a.km && v[u] < tbice) T[(k0 + u) * A] = tbice;
+  }
 }
 
 // ---------------------------------------------------------------- masks
@@ -248,6 +295,13 @@ int launch_convadj(const Arena& a, cudaStream_t s) {
   if (a.km > KMAX_CONV) { set_error("convadj: km > %d", KMAX_CONV); return LT_E_INVALID; }
   dim3 b(8, 16), g((a.imt + 7) / 8, (a.jmt + 15) / 16);
   k_convadj<<<g, b, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_icesnow(const Arena& a, const lt_icesnow_params& p, cudaStream_t s) {
+  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
+  k_icesnow<<<g, b, 0, s>>>(a, p.tbice, p.cp, p.latice, p.reset_qice != 0);
   LT_LAUNCHED();
   return LT_OK;
 }

@@ -14,6 +14,7 @@
 //   halo and tripole fold           POP_HaloMod.F90:2716-3139, 5602-5680,
 //                                   POP_BlocksMod.F90:284-375
 //   convective adjustment           convadj.cpp:29-288
+//   sea-ice adjustment              icesnow.cpp:15-85
 //
 // Arithmetic keeps the reference's operation order term by term (so that a
 // build with -ffp-contract=off reproduces the reference's own code compiled
@@ -739,6 +740,35 @@ void convadj_call(Oracle& o) {
   }
 }
 
+// icesnow_cu over every point of the domain, halo included, with the
+// FRC_CORE reset of licomqice first when reset is set (icesnow.cpp:15-85)
+void icesnow_call(Oracle& o, const lt_icesnow_params& p) {
+  double* at = o.fd[LT_F_AT].data();
+  double* qice = o.fd[LT_F_QICE].data();
+  const int* kmt = o.fi[LT_F_KMT].data();
+  const double* dzp = o.fd[LT_F_DZP].data();
+  const double sal_ocn = 34.7e0, sal_ice = 4.0e0;
+  if (p.reset_qice) std::fill(o.fd[LT_F_QICE].begin(), o.fd[LT_F_QICE].end(), 0.0);
+  for (long c = 0; c < o.A; ++c) {
+    double& t = at[c];
+    double& s = at[o.F + c];
+    if (t < p.tbice && kmt[c] > 0) {
+      const double tdiff = p.tbice - t;
+      qice[c] += tdiff * dzp[0] / dzp[0];
+      s += tdiff * (sal_ocn - sal_ice) * p.cp / p.latice * 0.001e0;
+      t = p.tbice;
+    }
+    if (qice[c] > 0 && t > p.tbice) {
+      const double tdiff = std::fmin(t - p.tbice, qice[c]);
+      qice[c] -= tdiff;
+      t -= tdiff;
+      s -= tdiff * (sal_ocn - sal_ice) * p.cp / p.latice * 0.001e0;
+    }
+    for (int k = 0; k < o.km; ++k)
+      if (at[(long)k * o.A + c] < p.tbice) at[(long)k * o.A + c] = p.tbice;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -804,6 +834,11 @@ int or_step(void* h, int nsteps) {
 }
 int or_convadj(void* h) {
   convadj_call(*static_cast<Oracle*>(h));
+  return 0;
+}
+int or_icesnow(void* h, const lt_icesnow_params* p) {
+  if (!p) return LT_E_INVALID;
+  icesnow_call(*static_cast<Oracle*>(h), *p);
   return 0;
 }
 double or_fw_norm2(void* h) { return static_cast<Oracle*>(h)->fw_norm2; }

@@ -2,9 +2,9 @@
 
 ``Oracle`` wraps liblicom_oracle.so (the FP64 restatement in licom_oracle.cpp);
 ``Reference`` wraps oracle/_ref/libref_tracer.so, the reference's own
-tracer.cpp and convadj.cpp compiled for the CPU (present only where the
-reference tree was available at build time).  Field ids are those of
-include/licom_tracer.h.
+tracer.cpp, convadj.cpp and icesnow.cpp compiled for the CPU (present only
+where the reference tree was available at build time).  Field ids are those
+of include/licom_tracer.h.
 """
 import ctypes as C
 import os
@@ -19,7 +19,7 @@ FIELDS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "N
           "H0F_OUT", "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE",
           "DXU", "DYU", "AHF", "DTN", "DTS", "DTE", "DTW", "OHBT", "OHBU", "AU0", "AUS", "AUW", "AUSW", "KMT", "KMU",
           "KMTN", "KMTS", "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ",
-          "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE"]
+          "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE", "QICE"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 INT = {"KMT", "KMU", "KMTN", "KMTS", "KMTE", "KMTW"}
 
@@ -64,6 +64,7 @@ class Oracle:
         lib.or_halo.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         lib.or_set_threads.argtypes = [C.c_int]
         lib.or_set_sum_order.argtypes = [C.c_void_p, C.c_int]
+        lib.or_icesnow.argtypes = [C.c_void_p, C.c_void_p]
         self.nx, self.ny, self.km = nx, ny, km
         self.h = C.c_void_p(lib.or_create(nx, ny, km))
         if not self.h:
@@ -104,6 +105,11 @@ class Oracle:
     def convadj(self):
         self.lib.or_convadj(self.h)
 
+    def icesnow(self, params):
+        """params: an object with the lt_icesnow_params layout (IcesnowParams)."""
+        if self.lib.or_icesnow(self.h, C.byref(params)):
+            raise ValueError("oracle icesnow")
+
     def fw_norm2(self):
         return self.lib.or_fw_norm2(self.h)
 
@@ -138,6 +144,7 @@ class Reference:
         lib.ref_get_field.argtypes = [C.c_int, C.c_void_p, C.c_size_t]
         lib.ref_set_params.argtypes = [C.c_void_p, C.c_int, C.c_int]
         lib.ref_tracer_call.argtypes = [C.c_int]
+        lib.ref_icesnow_call.argtypes = [C.c_double, C.c_double, C.c_int]
         lib.ref_fw_norm2.restype = C.c_double
         imt, jmt, km = C.c_int(), C.c_int(), C.c_int()
         lib.ref_dims(C.byref(imt), C.byref(jmt), C.byref(km))
@@ -165,6 +172,11 @@ class Reference:
 
     def convadj(self):
         self.lib.ref_convadj_call()
+
+    def icesnow(self, tbice=-1.8, cp=3996.0, frc_core=1):
+        """icesnow_ as the reference is configured (frc_core 1: licomqice
+        zeroed first) or its build without FRC_CORE (0)."""
+        self.lib.ref_icesnow_call(float(tbice), float(cp), int(frc_core))
 
     def fw_norm2(self):
         return self.lib.ref_fw_norm2()

@@ -1,6 +1,9 @@
 // ref_harness.cpp - host-side harness that runs the reference's own
-// tracer.cpp / convadj.cpp (compiled from their place in the reference tree
-// with the CPU HIP stand-in in oracle/ref_harness/hip) on one block.
+// tracer.cpp / convadj.cpp / icesnow.cpp (compiled from their place in the
+// reference tree with the CPU HIP stand-in in oracle/ref_harness/hip) on one
+// block.  icesnow.cpp is compiled twice: as configured (def-undef.h defines
+// FRC_CORE: licomqice is zeroed before each call) and, renamed
+// icesnow_nofrc_, with that one define removed (licomqice carries over).
 // TEST INFRASTRUCTURE ONLY: builds oracle/_ref/libref_tracer.so, used by tests
 // to pin the oracle against the reference's own code.
 //
@@ -28,6 +31,8 @@ thread_local dim3 threadIdx, blockIdx, blockDim, gridDim;
 
 extern "C" void tracer_(int ii);
 extern "C" void convadj_();
+extern "C" void icesnow_();
+extern "C" void icesnow_nofrc_();
 
 // ---- device pointers (cuda_data.h) used by tracer.cpp / convadj.cpp
 double *d_at00, *d_atmax, *d_atmin, *d_adv_tt, *d_ori, *d_temp11, *d_uk, *d_vk, *d_u_wface, *d_v_sface;
@@ -38,6 +43,7 @@ double *d_ws, *d_at, *d_atb, *d_ax, *d_ay, *d_az, *d_tf, *d_akt, *d_d2tk, *d_ahf
 double *d_dtn, *d_dts, *d_dte, *d_dtw, *d_swv, *d_pen, *d_penetrate, *d_dz, *d_ssf, *d_sss, *d_ifrac, *d_net;
 double *d_dt_restore, *d_fresh, *d_seaice, *d_tsf, *d_nswv, *d_sst, *d_dqdt, *d_restore, *d_restore_at;
 double *d_tend, *d_dt_diff, *d_dt_conv, *d_icmon;
+double *d_licomqice;
 int *d_kmt, *d_kmtn, *d_kmts, *d_kmte, *d_kmtw;
 size_t dataSize2d, dataSize3d, dataSize33d, dataSize4d, dataSize44d;
 
@@ -47,6 +53,7 @@ double pconst_mod_mp_onbc_, pconst_mod_mp_oncc_, pconst_mod_mp_dts_, pconst_mod_
 double pconst_mod_mp_gamma_, pconst_mod_mp_od0_, pconst_mod_mp_od0cp_;
 int pconst_mod_mp_nss_, pconst_mod_mp_ist_, pconst_mod_mp_boundary_restore_;
 double hmix_del4_mp_ah_, grid_mp_area_t_, tracer_mod_mp_fw_norm2_;
+double pconst_mod_mp_tbice_ = -1.8, pconst_mod_mp_cp_ = 3996.0;   // constant_mod.F90:164,168
 int param_mod_mp_mytid_ = 0;
 double (*tracer_mod_mp_net_)[2][R_JMT][R_IMT];
 double (*dyn_mod_mp_vtl_)[R_KM][R_JMT][R_IMT];
@@ -117,6 +124,7 @@ void setup() {
   d_ax = store[LT_F_AX].data(); d_ay = store[LT_F_AY].data(); d_az = store[LT_F_AZ].data();
   d_dz = store[LT_F_DZ].data(); d_tend = store[LT_F_TEND].data(); d_dt_diff = store[LT_F_DT_DIFF].data();
   d_dt_conv = store[LT_F_DT_CONV].data(); d_penetrate = store[LT_F_PENETRATE].data();
+  d_licomqice = store[LT_F_QICE].data();
   // scratch arrays of the reference (sizes from cuda_init.cpp)
   d_at00 = fresh_scratch(F); d_atmax = fresh_scratch(F); d_atmin = fresh_scratch(F);
   d_adv_tt = fresh_scratch(F); d_ori = fresh_scratch(F); d_temp11 = fresh_scratch(A);
@@ -206,6 +214,16 @@ int ref_convadj_call(void) {
   setup();
   refresh_vit();
   return in_big_stack(run_convadj, nullptr);
+}
+// icesnow_ with the given tbice and cp (SHR_CONST_LATICE is compiled in);
+// frc_core 1 runs the file as configured, 0 the build without FRC_CORE
+int ref_icesnow_call(double tbice, double cp, int frc_core) {
+  setup();
+  pconst_mod_mp_tbice_ = tbice;
+  pconst_mod_mp_cp_ = cp;
+  if (frc_core) icesnow_();
+  else icesnow_nofrc_();
+  return 0;
 }
 double ref_fw_norm2(void) { return tracer_mod_mp_fw_norm2_; }
 

@@ -1,9 +1,10 @@
 """Generate tests/golden/reference_digests.json from the reference's own code.
 
-Runs LICOM3-HIP's tracer.cpp and convadj.cpp, compiled for the CPU by
-oracle/Makefile (target ``ref``) from the reference tree, on seeded synthetic
-inputs at the reference's built-in block size (36 x 40 physical, 55 levels)
-and records SHA-256 digests of every output field plus fw_norm2.
+Runs LICOM3-HIP's tracer.cpp, convadj.cpp and icesnow.cpp, compiled for the
+CPU by oracle/Makefile (target ``ref``) from the reference tree, on seeded
+synthetic inputs at the reference's built-in block size (36 x 40 physical, 55
+levels) and records SHA-256 digests of every output field plus fw_norm2.  The
+icesnow cases start from the cold states of tests/icesnow_state.py.
 
     make -C oracle ref && python tests/golden/make_golden.py
 """
@@ -20,10 +21,14 @@ sys.path.insert(0, os.path.join(REPO, "oracle"))
 import numpy as np  # noqa: E402
 from conftest import load_package  # noqa: E402
 import pyoracle  # noqa: E402
+from icesnow_state import ICE_CASES, cold_state  # noqa: E402
 
 CASES = [(1, 5, 20240611), (0, 3, 7), (1, 2, 99)]
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
               "DT_DIFF", "DT_CONV", "PENETRATE"]
+
+
+ICE_OUT = ["AT", "ATB", "QICE", "TEND", "DT_CONV", "WS", "NET"]
 
 
 def digest(a):
@@ -47,6 +52,24 @@ def main():
             "outputs": {n: digest(ref.get(n)) for n in OUT_FIELDS},
             "fw_norm2": ref.fw_norm2(),
             "surface_T_sample": ref.get("AT")[0, 0, 20, 5:15].tolist(),
+        }
+    for frc_core, nsteps, seed in ICE_CASES:
+        syn = lt.Synth(36, 40, 55, forced=1, cap_north=0, cap_south=3, dz_top=5.0, dz_bot=300.0, seed=seed)
+        inp = syn.all_fields()
+        inp["AT"], inp["QICE"] = cold_state(inp, seed)
+        ref = pyoracle.Reference(syn.params)
+        ref.load(inp)
+        if nsteps == 0:
+            ref.icesnow(frc_core=frc_core)
+        for s in range(nsteps):
+            ref.tracer_call(s)
+            ref.icesnow(frc_core=frc_core)
+            if s == 0:
+                ref.convadj()
+        key = "icesnow_frc%d_steps%d_seed%d" % (frc_core, nsteps, seed)
+        out[key] = {
+            "inputs": {"AT": digest(inp["AT"]), "QICE": digest(inp["QICE"])},
+            "outputs": {n: digest(ref.get(n)) for n in ICE_OUT},
         }
     with open(os.path.join(HERE, "reference_digests.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
