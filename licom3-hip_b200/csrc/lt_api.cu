@@ -194,7 +194,7 @@ void init_arena_dims(Arena& a, const lt_grid* g, const lt_params* p) {
 
 long slots_for(const Arena& a, int sms) {
   const long ntiles = (long)((a.imt + TX - 1) / TX) * ((a.jmt + TY - 1) / TY);
-  long s = (long)sms * 4;
+  long s = (long)sms * kMixedCtasPerSm;
   if (s > 2 * ntiles) s = 2 * ntiles;
   return s;
 }
@@ -416,9 +416,9 @@ int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
   cudaEventCreate(&d->ev1);
   // TMA-fed tracer kernel where the row pitch is a multiple of 16 bytes
   d->use_tma = build_tracer_maps(d->a, &d->maps);
-  // one persistent CTA per resident slot: the f64 kernel fits 3 per SM, the
-  // mixed kernel 4 (its __launch_bounds__ and shared-memory footprint)
-  const long per_sm = d->a.precision == LT_PREC_MIXED ? 4 : 3;
+  // one persistent CTA per resident slot (kFp64CtasPerSm, kMixedCtasPerSm
+  // per SM: the kernels' __launch_bounds__ and shared-memory footprints)
+  const long per_sm = d->a.precision == LT_PREC_MIXED ? kMixedCtasPerSm : kFp64CtasPerSm;
   d->tma_grid = (int)std::min<long>(d->a.col_scratch_slots, (long)sms * per_sm);
   if (cudaStreamSynchronize(d->stream) != cudaSuccess) {
     lt_destroy(d);

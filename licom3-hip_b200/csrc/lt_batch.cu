@@ -28,9 +28,9 @@ struct lt_batch {
   bool mixed = false;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evx = nullptr;
-  lt_batch_config cfg{4, 8, 1};
+  lt_batch_config cfg{kMixedCtasPerSm, 8, 1};
   MemberDesc* d_desc[2] = {nullptr, nullptr};   // per parity
-  double* scratch = nullptr;                     // column scratch, 4 CTAs per SM
+  double* scratch = nullptr;                     // column scratch, kMixedCtasPerSm CTAs per SM
   int km_max = 0, max_imt = 0, max_jmt = 0;
   long total_items = 0;
   int parity = 0;
@@ -169,7 +169,7 @@ int capture_graphs(lt_batch* b) {
 bool config_ok(const lt_batch* b, const lt_batch_config& c) {
   if (c.use_graph != 0 && c.use_graph != 1) return false;
   if (!b->mixed) return true;
-  return c.column_ctas_per_sm >= 1 && c.column_ctas_per_sm <= 4 &&
+  return c.column_ctas_per_sm >= 1 && c.column_ctas_per_sm <= kMixedCtasPerSm &&
          (c.continuity_tile_y == 4 || c.continuity_tile_y == 8 || c.continuity_tile_y == 16);
 }
 
@@ -245,7 +245,7 @@ int lt_batch_create(lt_domain* const* members, int n, lt_batch** out) {
     return fail(LT_E_CUDA);
   if ((rc = build_descriptors(b))) return fail(rc);
   if (b->mixed) {
-    const size_t bytes = sizeof(double) * (size_t)b->sms * 4 * b->km_max * 2 * TTHREADS;
+    const size_t bytes = sizeof(double) * (size_t)b->sms * kMixedCtasPerSm * b->km_max * 2 * TTHREADS;
     if (cudaMalloc(&b->scratch, bytes) != cudaSuccess) {
       set_error("lt_batch_create: cudaMalloc(%zu) for the column scratch failed", bytes);
       return fail(LT_E_OOM);
@@ -344,7 +344,7 @@ int lt_batch_autotune(lt_batch* b, int trial_steps, lt_batch_config* chosen) {
   }
   std::vector<lt_batch_config> cands;
   if (b->mixed) {
-    for (int ctas : {2, 3, 4})
+    for (int ctas : {3, 4, 5})
       for (int ty : {4, 8, 16}) cands.push_back({ctas, ty, 1});
   } else {
     cands.push_back({b->cfg.column_ctas_per_sm, b->cfg.continuity_tile_y, 1});

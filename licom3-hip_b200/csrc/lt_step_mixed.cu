@@ -58,6 +58,9 @@ __device__ __forceinline__ double face_y64(float wc, float we, double hts) {
   return ((double)wc + (double)we) * hts * 0.25;
 }
 __device__ __forceinline__ float face32(float w1, float w2, float h) { return (w1 + w2) * h * 0.25f; }
+// Lax-Wendroff part of a face flux, d*u*u*(2 dts / (h_t h_u)): one expression
+// wherever a face is used, so both cells of the face get the same value
+__device__ __forceinline__ float lw_part(float d, float u, float c) { return d * u * u * c; }
 
 
 // ------------------------------------------------------------- continuity
@@ -203,7 +206,10 @@ int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s) {
 namespace {
 
 // ------------------------------------------------------------ column march
-constexpr int NSM = 4;                     // level slots (k+1 .. k-2)
+// Level slots.  Step k (the march runs downward) reads levels k-2, k-1 and
+// k only, so at the end of step k the slot of level k takes level k-3: three
+// slots keep one step of lead time for every box.
+constexpr int NSM = 3;
 constexpr int FXN = (TY + 2) * (TX + 3);   // x faces of the 1-halo region
 constexpr int FYN = (TY + 3) * (TX + 2);   // y faces of the 1-halo region
 
@@ -223,8 +229,8 @@ constexpr uint32_t kMxLevelBytes =
 
 struct MxSmem {
   MxSlot slot[NSM];
-  float fxd[2][FXN], fxb[2][FXN];    // per level parity: difference d and Lax-Wendroff part B
-  float fyd[2][FYN], fyb[2][FYN];
+  float fxd[2][FXN];                  // per level parity: face difference d
+  float fyd[2][FYN];
   unsigned char flag[3][HN];          // predictor outside its local bounds
   float d2[HN];                       // first Laplacian (times ahf)
   float tr[HN], dtn[HN], dts[HN], dte[HN], dtw[HN], ahf[HN];
@@ -236,7 +242,9 @@ struct MxSmem {
   uint64_t bar[NSM];
 };
 // four CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
-static_assert(4 * (sizeof(MxSmem) + 1024) <= 228 * 1024, "mixed tracer tile no longer fits 4 CTAs per SM");
+// five CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
+static_assert(kMixedCtasPerSm * (sizeof(MxSmem) + 1024) <= 228 * 1024,
+              "mixed tracer tile no longer fits kMixedCtasPerSm CTAs per SM");
 
 // Issue the boxes of level L of tracer n into a slot (one thread).
 __device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const TracerMaps& m, int cur, int n, int km,
@@ -262,10 +270,8 @@ __device__ __forceinline__ int fy(int fj, int fi) { return fj * (TX + 2) + fi; }
 __device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
   const MxSlot& L = S.slot[kk % NSM];
   float* dx = S.fxd[kk & 1];
-  float* bx = S.fxb[kk & 1];
   float* ux = S.fxu[kk & 1];
   float* dy = S.fyd[kk & 1];
-  float* by = S.fyb[kk & 1];
   float* vy = S.fyv[kk & 1];
   for (int m = threadIdx.x; m < FXN + FYN; m += TTHREADS) {
     if (m < FXN) {
@@ -275,7 +281,6 @@ __device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
       const float u = face32(L.wkd[fj * SW + fi + 3], L.wkd[(fj + 1) * SW + fi + 3], S.hwx[m]);
       ux[m] = u;
       dx[m] = d;
-      bx[m] = d * u * u * S.cxf[m];
     } else {
       const int mm = m - FXN;
       const int fj = mm / (TX + 2), fi = mm % (TX + 2);
@@ -284,7 +289,6 @@ __device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
       const float v = face32(L.wkb[fj * SW + fi + 3], L.wkb[fj * SW + fi + 4], S.hsy[mm]);
       vy[mm] = v;
       dy[mm] = d;
-      by[mm] = d * v * v * S.cyf[mm];
     }
   }
 }
@@ -299,9 +303,7 @@ __device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int k
   const double* at_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].at : nullptr;
   const float* wsd = kk < km - 1 ? S.slot[(kk + 1) % NSM].ws : nullptr;
   const float* dx = S.fxd[kk & 1];
-  const float* bx = S.fxb[kk & 1];
   const float* dy = S.fyd[kk & 1];
-  const float* by = S.fyb[kk & 1];
   const float hodz = 0.5f * (float)a.odzp[kk];
   const float odzt_k = (float)a.odzt[kk];
   const float odzt_k1 = kk < km - 1 ? (float)a.odzt[kk + 1] : 0.f;
@@ -315,8 +317,8 @@ __device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int k
     const int fe = fx(hj, hi + 1), fw = fx(hj, hi), fs = fy(hj + 1, hi), fn = fy(hj, hi);
     const float ue = S.fxu[kk & 1][fe], uwv = S.fxu[kk & 1][fw];
     const float vs = S.fyv[kk & 1][fs], vn = S.fyv[kk & 1][fn];
-    const float sx = (dx[fe] * ue - bx[fe]) + (dx[fw] * uwv + bx[fw]);
-    const float sy = (dy[fs] * vs - by[fs]) + (dy[fn] * vn + by[fn]);
+    const float sx = (dx[fe] * ue - lw_part(dx[fe], ue, S.cxf[fe])) + (dx[fw] * uwv + lw_part(dx[fw], uwv, S.cxf[fw]));
+    const float sy = (dy[fs] * vs - lw_part(dy[fs], vs, S.cyf[fs])) + (dy[fn] * vn + lw_part(dy[fn], vn, S.cyf[fn]));
     // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
     float sz = 0.f, dup = 0.f, ddn = 0.f;   // dup, ddn: a_above - c, a_below - c
     const double c = at_c[r];
@@ -471,7 +473,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     __syncthreads();
     predictor_mixed(S, a, km - 1, x0, y0);
 
-    // Level slots: after step k the slot of level k+1 takes level k+1-NSM.
+    // Level slots: after step k the slot of level k takes level k-NSM.
     for (int k = km - 1; k >= 0; --k) {
       const float akt_above = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
       // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
@@ -489,9 +491,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         const unsigned char* fl = S.flag[k % 3];
         const bool self = fl[hc] != 0;
         const float* dx = S.fxd[k & 1];
-        const float* bx = S.fxb[k & 1];
         const float* dy = S.fyd[k & 1];
-        const float* by = S.fyb[k & 1];
         const float ue = S.fxu[k & 1][fe], uwv = S.fxu[k & 1][fwi];
         const float vsv = S.fyv[k & 1][fs], vnv = S.fyv[k & 1][fn];
         // the same faces in f64, as the continuity march formed them
@@ -512,13 +512,13 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         const double dS = Lk.at[rc + SW] - c, dN = c - Lk.at[rc - SW];
         float t;
         t = dx[fe];                                   // east face: this cell is L
-        const float Xe = (self || fl[hc + 1]) ? fabsf(ue) * t : bx[fe];
+        const float Xe = (self || fl[hc + 1]) ? fabsf(ue) * t : lw_part(t, ue, S.cxf[fe]);
         t = dx[fwi];
-        const float Xw = (self || fl[hc - 1]) ? fabsf(uwv) * t : bx[fwi];
+        const float Xw = (self || fl[hc - 1]) ? fabsf(uwv) * t : lw_part(t, uwv, S.cxf[fwi]);
         t = dy[fs];
-        const float Xs = (self || fl[hc + HQX]) ? fabsf(vsv) * t : by[fs];
+        const float Xs = (self || fl[hc + HQX]) ? fabsf(vsv) * t : lw_part(t, vsv, S.cyf[fs]);
         t = dy[fn];
-        const float Xn = (self || fl[hc - HQX]) ? fabsf(vnv) * t : by[fn];
+        const float Xn = (self || fl[hc - HQX]) ? fabsf(vnv) * t : lw_part(t, vnv, S.cyf[fn]);
         double sh = dE * ue64 + dW * uw64 + dS * vs64 + dN * vn64;
         sh += ((double)Xw - (double)Xe) + ((double)Xn - (double)Xs);
         // vertical: face above (k-1|k) computed here, face below carried
@@ -610,7 +610,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       }
       akt_here = akt_above;
       __syncthreads();
-      if (k + 1 <= km - 1 && k + 1 - NSM >= 0) issue(k + 1 - NSM);
+      if (k - NSM >= 0) issue(k - NSM);
     }
     if (inner) {
       double x = 0.0;
@@ -645,7 +645,7 @@ __device__ __forceinline__ MxSmem& mixed_smem_init() {
   return S;
 }
 
-__global__ void __launch_bounds__(TTHREADS, 4)
+__global__ void __launch_bounds__(TTHREADS, kMixedCtasPerSm)
     k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
   MxSmem& S = mixed_smem_init();
   uint32_t par = 0, outstanding = 0;
@@ -659,7 +659,7 @@ __global__ void __launch_bounds__(TTHREADS, 4)
 // (tile, tracer) items, member after member, so neighbouring CTAs work on
 // neighbouring tiles of the same member.  Each CTA's items ascend, so its
 // member index only moves forward.
-__global__ void __launch_bounds__(TTHREADS, 4)
+__global__ void __launch_bounds__(TTHREADS, kMixedCtasPerSm)
     k_tracer_mixed_batch(const MemberDesc* __restrict__ mem, int nmem, long total, double* scratch, int km_max) {
   MxSmem& S = mixed_smem_init();
   uint32_t par = 0, outstanding = 0;
