@@ -14,8 +14,8 @@ constexpr int TX = 32;
 constexpr int TY = 4;
 constexpr int TTHREADS = TX * TY;
 // Persistent CTAs per SM of the column kernels (their shared-memory footprint
-// decides): FP64 3, mixed 5.
-constexpr int kFp64CtasPerSm = 3;
+// decides): FP64 4, mixed 5.
+constexpr int kFp64CtasPerSm = 4;
 constexpr int kMixedCtasPerSm = 5;
 
 // Everything the step kernels touch, as raw device pointers (dense

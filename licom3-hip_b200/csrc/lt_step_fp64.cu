@@ -760,11 +760,13 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
 
 // -------------------------------------------- tracer march, TMA pipeline
 // Same arithmetic as k_tracer64 (term for term), data staged by TMA boxes.
-// Four level slots (k+1 .. k-2 in use; the slot freed after step k receives
-// level k-3), predictor ring and first Laplacian in shared memory; the 2-D
-// metric terms are read through L1 (the same 2-D values serve every level), so
-// three CTAs fit on an SM.
-constexpr int NSX = 4;
+// Three level slots: step k reads levels k-2 .. k from shared memory; the
+// own cell's at, ws and atb of level k+1 that the column phase also needs are
+// carried in registers from step k+1, so the slot of level k takes level k-3
+// at the end of step k.  Predictor ring and first Laplacian in shared memory;
+// the 2-D metric terms are read through L1 (the same 2-D values serve every
+// level), so kFp64CtasPerSm CTAs fit on an SM.
+constexpr int NSX = 3;
 struct ExSmem {
   LevelSlot<double> slot[NSX];
   double a00[3][HN], amx[3][HN], amn[3][HN];
@@ -889,8 +891,12 @@ struct ExactHw {
   __device__ double operator()(double a, double b) const { return a * b; }
 };
 
+// kFp64CtasPerSm CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA
+static_assert(kFp64CtasPerSm * (sizeof(ExSmem) + 1024) <= 228 * 1024,
+              "FP64 tracer tile no longer fits kFp64CtasPerSm CTAs per SM");
+
 template <bool DIAG>
-__global__ void __launch_bounds__(TTHREADS, 3)
+__global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     k_tracer_tma64(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
   extern __shared__ __align__(128) unsigned char smem_tma[];
   ExSmem& S = *reinterpret_cast<ExSmem*>(smem_tma);
@@ -949,6 +955,8 @@ __global__ void __launch_bounds__(TTHREADS, 3)
     const double stf = own ? a.stf_n[n * A + qo] : 0.0;
     const double err_norm2 = a.scalars[0];
     double e_prev = 0.0, f_prev = 0.0;
+    // own cell's at, ws and atb of level k+1, kept from step k+1
+    double at_dn = 0.0, ws_dn = 0.0, atb_dn = 0.0;
 
     {
       const bool ok = wait(km - 1) && wait(km - 2);
@@ -969,7 +977,6 @@ __global__ void __launch_bounds__(TTHREADS, 3)
         const LevelSlot<double>& Lk = S.slot[k % NSX];
         const double* at_c = Lk.at;
         const double* at_u = k > 0 ? S.slot[(k - 1) % NSX].at : nullptr;
-        const double* at_d = k < km - 1 ? S.slot[(k + 1) % NSX].at : nullptr;
         const double* o00 = S.a00[k % 3];
         const double* omx = S.amx[k % 3];
         const double* omn = S.amn[k % 3];
@@ -999,7 +1006,7 @@ __global__ void __launch_bounds__(TTHREADS, 3)
         else xy4 = dts * (c - nn) * 2.0 * tr * vn * vn / hsn;
         const double wk = Lk.ws[uc];
         if (k == 0) {
-          const double w1 = S.slot[1 % NSX].ws[uc], ad = at_d[rc];
+          const double w1 = ws_dn, ad = at_dn;
           zb1 = 0.0;
           if (self || (out(S.a00[1 % 3], S.amx[1 % 3], S.amn[1 % 3], hc) && k <= km - 2))
             zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
@@ -1017,7 +1024,7 @@ __global__ void __launch_bounds__(TTHREADS, 3)
           za = 0.5 * odzp[km - 1] * wk * (c + au);
           zc = -odzp[km - 1] * c * wk;
         } else {
-          const double au = at_u[rc], ad = at_d[rc], w1 = S.slot[(k + 1) % NSX].ws[uc];
+          const double au = at_u[rc], ad = at_dn, w1 = ws_dn;
           if ((self || out(S.a00[(k - 1) % 3], S.amx[(k - 1) % 3], S.amn[(k - 1) % 3], hc)) && k >= 1)
             zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
           else
@@ -1048,7 +1055,7 @@ __global__ void __launch_bounds__(TTHREADS, 3)
           const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
           const double atb_k = Lk.atb[rc];
           const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSX].atb[rc] : 0.0;
-          const double atb_kp1 = k < km - 1 ? S.slot[(k + 1) % NSX].atb[rc] : 0.0;
+          const double atb_kp1 = k < km - 1 ? atb_dn : 0.0;
           const double wkc_k = Lk.akt[ac];
           const double wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSX].akt[ac] : 0.0;
           double tf = adv * vit_k;
@@ -1132,10 +1139,13 @@ __global__ void __launch_bounds__(TTHREADS, 3)
           sl[tid] = ev;
           sl[TTHREADS + tid] = fv;
           if (DIAG) sl[2 * TTHREADS + tid] = d8;
+          atb_dn = atb_k;
         }
+        at_dn = c;
+        ws_dn = wk;
       }
-      __syncthreads();  // level k+1 is no longer read: its slot takes level k+1-NSX
-      if (k + 1 <= km - 1 && k + 1 - NSX >= 0) issue(k + 1 - NSX);
+      __syncthreads();  // level k is no longer read: its slot takes level k-NSX
+      if (k - NSX >= 0) issue(k - NSX);
     }
     // ---- substitution, top down
     if (inner) {
