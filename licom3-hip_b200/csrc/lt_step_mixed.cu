@@ -293,91 +293,151 @@ __device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
   }
 }
 
-// predictor and bound test at level kk on the 1-halo region
-__device__ __forceinline__ void predictor_mixed(MxSmem& S, const Arena& a, int kk, int x0, int y0) {
-  const int km = a.km, imt = a.imt, jmt = a.jmt;
-  const float dts = (float)a.p.dts;
-  const MxSlot& L = S.slot[kk % NSM];
-  const double* at_c = L.at;
-  const double* at_u = kk > 0 ? S.slot[(kk - 1) % NSM].at : nullptr;
-  const double* at_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].at : nullptr;
-  const float* wsd = kk < km - 1 ? S.slot[(kk + 1) % NSM].ws : nullptr;
-  const float* dx = S.fxd[kk & 1];
-  const float* dy = S.fyd[kk & 1];
-  const float hodz = 0.5f * (float)a.odzp[kk];
-  const float odzt_k = (float)a.odzt[kk];
-  const float odzt_k1 = kk < km - 1 ? (float)a.odzt[kk + 1] : 0.f;
-  unsigned char* fl = S.flag[kk % 3];
-  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
-    const int hj = m / HQX, hi = m % HQX;
-    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
-    if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) { fl[m] = 0; continue; }
-    const int r = r2(hj, hi), u = ru(hj, hi);
-    // horizontal: east/west x faces, south/north y faces
-    const int fe = fx(hj, hi + 1), fw = fx(hj, hi), fs = fy(hj + 1, hi), fn = fy(hj, hi);
-    const float ue = S.fxu[kk & 1][fe], uwv = S.fxu[kk & 1][fw];
-    const float vs = S.fyv[kk & 1][fs], vn = S.fyv[kk & 1][fn];
-    const float sx = (dx[fe] * ue - lw_part(dx[fe], ue, S.cxf[fe])) + (dx[fw] * uwv + lw_part(dx[fw], uwv, S.cxf[fw]));
-    const float sy = (dy[fs] * vs - lw_part(dy[fs], vs, S.cyf[fs])) + (dy[fn] * vn + lw_part(dy[fn], vn, S.cyf[fn]));
-    // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
-    float sz = 0.f, dup = 0.f, ddn = 0.f;   // dup, ddn: a_above - c, a_below - c
-    const double c = at_c[r];
-    if (kk > 0) {
-      const float w = L.ws[u];
-      dup = (float)(at_u[r] - c);
-      const float A = w * dup;
-      sz += A - A * w * odzt_k * dts;
-    }
-    if (kk < km - 1) {
-      const float w = wsd[u];
-      const float d = (float)(c - at_d[r]);
-      ddn = -d;
-      const float A = w * d;
-      sz += A + A * w * odzt_k1 * dts;
-    }
-    const float inc = -(S.tr[m] * (sx + sy) + hodz * sz) * dts;
-    // Bound test of the predictor c + inc against the masked 7-point extrema
-    // (land excluded: -1e10 for the max, +1e10 for the min), done on
-    // differences from c: c + inc > max_p a_p  <=>  inc > max_p (a_p - c).
-    // The horizontal differences are the face differences already formed;
-    // with no wet point the reference's extrema flag the cell, as -inf does.
-    const uint16_t* kt = S.kmt;
-    float dmax = -INFINITY, dmin = INFINITY;
-    auto acc = [&](bool wet, float d) {
-      if (wet) { dmax = fmaxf(dmax, d); dmin = fminf(dmin, d); }
-    };
-    acc(kk < kt[r], 0.f);
-    acc(kk < kt[r + 1], dx[fe]);
-    acc(kk < kt[r - 1], -dx[fw]);
-    acc(kk < kt[r + SW], dy[fs]);
-    acc(kk < kt[r - SW], -dy[fn]);
-    if (kk > 0) acc(kk - 1 < kt[r], dup);
-    if (kk < km - 1) acc(kk + 1 < kt[r], ddn);
-    fl[m] = (inc > dmax || inc < dmin) ? 1 : 0;
+// A cell of the 1-halo region as one thread handles it: its index m in the
+// region, box index r (at, atb, kmt boxes), u (ws box), its west x face fw and
+// north y face fn (the east and south faces are fw + 1 and fn + HQX); valid:
+// inside the rows and columns the reference computes (1 .. imt-2, 1 .. jmt-2).
+// Every thread owns the interior cell above its column; the 76 ring cells of
+// the region go to threads 0 .. 75, one each.
+struct HCell {
+  int m, r, u, fw, fn;
+  bool valid;
+};
+constexpr int RING = HN - TX * TY;
+
+__device__ __forceinline__ HCell hcell(int hj, int hi, int x0, int y0, int imt, int jmt) {
+  HCell c;
+  c.m = hj * HQX + hi;
+  c.r = r2(hj, hi);
+  c.u = ru(hj, hi);
+  c.fw = fx(hj, hi);
+  c.fn = fy(hj, hi);
+  const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
+  c.valid = gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1;
+  return c;
+}
+
+// ring cell q (0 .. RING-1): top row, bottom row, west column, east column
+__device__ __forceinline__ HCell ring_hcell(int q, int x0, int y0, int imt, int jmt) {
+  int hj, hi;
+  if (q < HQX) { hj = 0; hi = q; }
+  else if (q < 2 * HQX) { hj = HQY - 1; hi = q - HQX; }
+  else if (q < 2 * HQX + TY) { hj = q - 2 * HQX + 1; hi = 0; }
+  else { hj = q - 2 * HQX - TY + 1; hi = HQX - 1; }
+  return hcell(hj, hi, x0, y0, imt, jmt);
+}
+
+// Per-level constants of the predictor at level kk.
+struct PredLevel {
+  const double *at_c, *at_u, *at_d;
+  const float *ws_c, *ws_d, *dx, *dy, *ux, *vy;
+  float hodz, odzt_k, odzt_k1, dts;
+  int kk, km;
+};
+
+__device__ __forceinline__ PredLevel pred_level(const MxSmem& S, const Arena& a, int kk) {
+  PredLevel P;
+  const int km = a.km;
+  P.kk = kk;
+  P.km = km;
+  P.at_c = S.slot[kk % NSM].at;
+  P.at_u = kk > 0 ? S.slot[(kk - 1) % NSM].at : nullptr;
+  P.at_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].at : nullptr;
+  P.ws_c = S.slot[kk % NSM].ws;
+  P.ws_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].ws : nullptr;
+  P.dx = S.fxd[kk & 1];
+  P.dy = S.fyd[kk & 1];
+  P.ux = S.fxu[kk & 1];
+  P.vy = S.fyv[kk & 1];
+  P.hodz = 0.5f * (float)a.odzp[kk];
+  P.odzt_k = (float)a.odzt[kk];
+  P.odzt_k1 = kk < km - 1 ? (float)a.odzt[kk + 1] : 0.f;
+  P.dts = (float)a.p.dts;
+  return P;
+}
+
+// Predictor and bound test of one cell: true if the predictor leaves the
+// local bounds (the reference's a00 > amax or a00 < amin).
+__device__ __forceinline__ bool pred_cell(const MxSmem& S, const PredLevel& P, const HCell& h) {
+  if (!h.valid) return false;
+  const int kk = P.kk, km = P.km, r = h.r, u = h.u;
+  const int fw = h.fw, fe = fw + 1, fn = h.fn, fs = fn + HQX;
+  const float* dx = P.dx;
+  const float* dy = P.dy;
+  const float dts = P.dts;
+  // horizontal: east/west x faces, south/north y faces
+  const float ue = P.ux[fe], uwv = P.ux[fw];
+  const float vs = P.vy[fs], vn = P.vy[fn];
+  const float sx = (dx[fe] * ue - lw_part(dx[fe], ue, S.cxf[fe])) + (dx[fw] * uwv + lw_part(dx[fw], uwv, S.cxf[fw]));
+  const float sy = (dy[fs] * vs - lw_part(dy[fs], vs, S.cyf[fs])) + (dy[fn] * vn + lw_part(dy[fn], vn, S.cyf[fn]));
+  // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
+  float sz = 0.f, dup = 0.f, ddn = 0.f;   // dup, ddn: a_above - c, a_below - c
+  const double c = P.at_c[r];
+  if (kk > 0) {
+    const float w = P.ws_c[u];
+    dup = (float)(P.at_u[r] - c);
+    const float A = w * dup;
+    sz += A - A * w * P.odzt_k * dts;
   }
+  if (kk < km - 1) {
+    const float w = P.ws_d[u];
+    const float d = (float)(c - P.at_d[r]);
+    ddn = -d;
+    const float A = w * d;
+    sz += A + A * w * P.odzt_k1 * dts;
+  }
+  const float inc = -(S.tr[h.m] * (sx + sy) + P.hodz * sz) * dts;
+  // Bound test of the predictor c + inc against the masked 7-point extrema
+  // (land excluded: -1e10 for the max, +1e10 for the min), done on
+  // differences from c: c + inc > max_p a_p  <=>  inc > max_p (a_p - c).
+  // The horizontal differences are the face differences already formed;
+  // with no wet point the reference's extrema flag the cell, as -inf does.
+  const uint16_t* kt = S.kmt;
+  float dmax = -INFINITY, dmin = INFINITY;
+  auto acc = [&](bool wet, float d) {
+    if (wet) { dmax = fmaxf(dmax, d); dmin = fminf(dmin, d); }
+  };
+  acc(kk < kt[r], 0.f);
+  acc(kk < kt[r + 1], dx[fe]);
+  acc(kk < kt[r - 1], -dx[fw]);
+  acc(kk < kt[r + SW], dy[fs]);
+  acc(kk < kt[r - SW], -dy[fn]);
+  if (kk > 0) acc(kk - 1 < kt[r], dup);
+  if (kk < km - 1) acc(kk + 1 < kt[r], ddn);
+  return inc > dmax || inc < dmin;
+}
+
+// Predictor flags of level kk for the thread's own cell and ring cell;
+// returns the own cell's flag.
+__device__ __forceinline__ bool predictor_mixed(MxSmem& S, const Arena& a, int kk, const HCell& own,
+                                                const HCell& ring, bool has_ring) {
+  const PredLevel P = pred_level(S, a, kk);
+  unsigned char* fl = S.flag[kk % 3];
+  const bool f = pred_cell(S, P, own);
+  fl[own.m] = f ? 1 : 0;
+  if (has_ring) fl[ring.m] = pred_cell(S, P, ring) ? 1 : 0;
+  return f;
 }
 
 // first Laplacian of atb at level kk (f32 on f64 differences), masked
-__device__ __forceinline__ void del4_first_mixed(MxSmem& S, const Arena& a, int kk, int x0, int y0) {
+__device__ __forceinline__ float d2_cell(const MxSmem& S, const double* atb, int kk, const HCell& h) {
+  if (!h.valid) return 0.f;
+  const int r = h.r, m = h.m;
+  const double c = atb[r];
+  if (kk > S.kmt[r] - 1) return 0.f;
+  float v = 0.f;
+  if (kk <= S.kmt[r - SW] - 1) v += S.dtn[m] * (float)(atb[r - SW] - c);
+  if (kk <= S.kmt[r + SW] - 1) v += S.dts[m] * (float)(atb[r + SW] - c);
+  if (kk <= S.kmt[r + 1] - 1) v += S.dte[m] * (float)(atb[r + 1] - c);
+  if (kk <= S.kmt[r - 1] - 1) v += S.dtw[m] * (float)(atb[r - 1] - c);
+  return S.ahf[m] * v;
+}
+
+__device__ __forceinline__ void del4_first_mixed(MxSmem& S, int kk, const HCell& own, const HCell& ring,
+                                                 bool has_ring) {
   const double* atb = S.slot[kk % NSM].atb;
-  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
-    const int hj = m / HQX, hi = m % HQX;
-    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
-    float v = 0.f;
-    if (gi >= 1 && gi < a.imt - 1 && gj >= 1 && gj < a.jmt - 1) {
-      const int r = r2(hj, hi);
-      const double c = atb[r];
-      if (kk <= S.kmt[r] - 1) {
-        float h = 0.f;
-        if (kk <= S.kmt[r - SW] - 1) h += S.dtn[m] * (float)(atb[r - SW] - c);
-        if (kk <= S.kmt[r + SW] - 1) h += S.dts[m] * (float)(atb[r + SW] - c);
-        if (kk <= S.kmt[r + 1] - 1) h += S.dte[m] * (float)(atb[r + 1] - c);
-        if (kk <= S.kmt[r - 1] - 1) h += S.dtw[m] * (float)(atb[r - 1] - c);
-        v = S.ahf[m] * h;
-      }
-    }
-    S.d2[m] = v;
-  }
+  S.d2[own.m] = d2_cell(S, atb, kk, own);
+  if (has_ring) S.d2[ring.m] = d2_cell(S, atb, kk, ring);
 }
 
 // One work item (tile, tracer) of the mixed column march.  Returns false if
@@ -450,6 +510,9 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     const int kz = own ? a.kmt[qo] : 0;
     const int hc = (ty + 1) * HQX + (tx + 1);
     const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1);
+    const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
+    const bool has_ring = tid < RING;
+    const HCell ring_cell = ring_hcell(has_ring ? tid : 0, x0, y0, imt, jmt);
     const int fe = fx(ty + 1, tx + 2), fwi = fx(ty + 1, tx + 1), fs = fy(ty + 2, tx + 1), fn = fy(ty + 1, tx + 1);
     const float swv = (inner && n == 0) ? (float)a.swv[qo] : 0.f;
     const double stf = own ? a.stf_n[n * A + qo] : 0.0;
@@ -471,7 +534,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     }
     faces_level(S, km - 1);
     __syncthreads();
-    predictor_mixed(S, a, km - 1, x0, y0);
+    predictor_mixed(S, a, km - 1, own_cell, ring_cell, has_ring);
 
     // Level slots: after step k the slot of level k takes level k-NSM.
     for (int k = km - 1; k >= 0; --k) {
@@ -479,12 +542,14 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
       // arrived in earlier steps; the previous step ended with a barrier)
       if (k >= 1) faces_level(S, k - 1);
-      del4_first_mixed(S, a, k, x0, y0);
+      del4_first_mixed(S, k, own_cell, ring_cell, has_ring);
       const bool ok = (k >= 2) ? wait(k - 2) : true;
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
-      // ---- phase B2: predictor one level up
-      if (k >= 1) predictor_mixed(S, a, k - 1, x0, y0);
-      __syncthreads();
+      // ---- phase B2: predictor one level up.  The column phase below reads
+      // the flags of level k (written in the previous step) and, of level
+      // k-1, only its own cell's flag, which this thread computes: no barrier
+      // between the two phases.
+      const bool flag_up = (k >= 1) ? predictor_mixed(S, a, k - 1, own_cell, ring_cell, has_ring) : false;
       // ---- phase C: own column at level k
       if (inner) {
         const MxSlot& Lk = S.slot[k % NSM];
@@ -527,7 +592,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
           const float wv = Lk.ws[uc];
           const double d64 = S.slot[(k - 1) % NSM].at[rc] - c;
           const float d = (float)d64;
-          const bool up = self || (S.flag[(k - 1) % 3][hc] != 0);
+          const bool up = self || flag_up;
           const float Xv = up ? fabsf(wv) * d : (wv * d) * wv * (float)odzt[k] * dtsf;
           const double Av = (double)wv * d64;
           sz += Av - (double)Xv;
