@@ -264,34 +264,91 @@ __device__ __forceinline__ int fx(int fj, int fi) { return fj * (TX + 3) + fi; }
 __device__ __forceinline__ int fy(int fj, int fi) { return fj * (TX + 2) + fi; }
 
 // Face quantities of level kk for the 1-halo region, once per face: the f32
-// transport (face32 on the U-point means), the difference d and the
-// Lax-Wendroff part B.  Every later use reads these, so both cells of a face
-// see the same f32 values.
-__device__ __forceinline__ void faces_level(MxSmem& S, int kk) {
-  const MxSlot& L = S.slot[kk % NSM];
-  float* dx = S.fxd[kk & 1];
-  float* ux = S.fxu[kk & 1];
-  float* dy = S.fyd[kk & 1];
-  float* vy = S.fyv[kk & 1];
-  for (int m = threadIdx.x; m < FXN + FYN; m += TTHREADS) {
-    if (m < FXN) {
-      const int fj = m / (TX + 3), fi = m % (TX + 3);
-      const int r = (fj + 1) * SW + fi + 3;           // cell R in the tracer box
-      const float d = (float)(L.at[r] - L.at[r - 1]);
-      const float u = face32(L.wkd[fj * SW + fi + 3], L.wkd[(fj + 1) * SW + fi + 3], S.hwx[m]);
-      ux[m] = u;
-      dx[m] = d;
-    } else {
-      const int mm = m - FXN;
-      const int fj = mm / (TX + 2), fi = mm % (TX + 2);
-      const int r = fj * SW + fi + 3;                 // cell L (north) in the tracer box
-      const float d = (float)(L.at[r + SW] - L.at[r]);
-      const float v = face32(L.wkb[fj * SW + fi + 3], L.wkb[fj * SW + fi + 4], S.hsy[mm]);
-      vy[mm] = v;
-      dy[mm] = d;
-    }
+// transport (face32 on the U-point means) and the difference d.  Every later
+// use reads these, so both cells of a face see the same f32 values.
+//
+// A face is described by (kind, index in its array, box index r): an x face
+// by its east cell R = r, a y face by its north cell r.  Each thread forms the
+// west x face and the north y face of its own cell, and up to two of the 192
+// faces on the region's border (FaceSet).
+__device__ __forceinline__ void face_one(MxSmem& S, const MxSlot& L, int kk, bool is_x, int m, int r) {
+  if (is_x) {
+    S.fxd[kk & 1][m] = (float)(L.at[r] - L.at[r - 1]);
+    S.fxu[kk & 1][m] = face32(L.wkd[r - SW], L.wkd[r], S.hwx[m]);
+  } else {
+    S.fyd[kk & 1][m] = (float)(L.at[r + SW] - L.at[r]);
+    S.fyv[kk & 1][m] = face32(L.wkb[r], L.wkb[r + 1], S.hsy[m]);
   }
 }
+
+constexpr int FX_OWN = TX * TY, FX_EXTRA = FXN - FX_OWN, FY_EXTRA = FYN - TX * TY;
+constexpr int F_EXTRA = FX_EXTRA + FY_EXTRA;   // border faces of the region
+
+struct FaceSet {
+  int own_x, own_y, own_r;   // own cell's west x face, north y face, box index of the cell
+  uint32_t e[2];             // border faces: bit 31 = y face, bits 16..30 index, bits 0..15 box index
+  int ne;
+};
+
+__device__ __forceinline__ uint32_t face_desc(bool is_y, int m, int r) {
+  return (is_y ? 0x80000000u : 0u) | ((uint32_t)m << 16) | (uint32_t)r;
+}
+
+// border face q (0 .. F_EXTRA-1): x faces of the top and bottom rows, x faces
+// of the west column and the two east columns, y faces of rows 0, TY+1, TY+2,
+// y faces of the west and east columns
+__device__ __forceinline__ uint32_t border_face(int q) {
+  int fj, fi;
+  if (q < 2 * (TX + 3)) {
+    fj = q < TX + 3 ? 0 : TY + 1;
+    fi = q % (TX + 3);
+    return face_desc(false, fx(fj, fi), (fj + 1) * SW + fi + 3);
+  }
+  q -= 2 * (TX + 3);
+  if (q < 3 * TY) {
+    const int c = q % 3;
+    fj = 1 + q / 3;
+    fi = c == 0 ? 0 : TX + c;
+    return face_desc(false, fx(fj, fi), (fj + 1) * SW + fi + 3);
+  }
+  q -= 3 * TY;
+  if (q < 3 * (TX + 2)) {
+    const int row = q / (TX + 2);
+    fj = row == 0 ? 0 : TY + row;
+    fi = q % (TX + 2);
+    return face_desc(true, fy(fj, fi), fj * SW + fi + 3);
+  }
+  q -= 3 * (TX + 2);
+  fj = 1 + q / 2;
+  fi = (q % 2) ? TX + 1 : 0;
+  return face_desc(true, fy(fj, fi), fj * SW + fi + 3);
+}
+
+__device__ __forceinline__ FaceSet face_set(int tid) {
+  const int tx = tid % TX, ty = tid / TX;
+  FaceSet f;
+  f.own_x = fx(ty + 1, tx + 1);
+  f.own_y = fy(ty + 1, tx + 1);
+  f.own_r = (ty + 2) * SW + tx + 4;
+  f.ne = 0;
+  for (int q = tid; q < F_EXTRA && f.ne < 2; q += TTHREADS) f.e[f.ne++] = border_face(q);
+  if (f.ne < 2) f.e[1] = 0;
+  if (f.ne < 1) f.e[0] = 0;
+  return f;
+}
+
+__device__ __forceinline__ void faces_level(MxSmem& S, int kk, const FaceSet& f) {
+  const MxSlot& L = S.slot[kk % NSM];
+  face_one(S, L, kk, true, f.own_x, f.own_r);
+  face_one(S, L, kk, false, f.own_y, f.own_r - SW);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+    if (i < f.ne) {
+      const uint32_t d = f.e[i];
+      face_one(S, L, kk, !(d >> 31), (int)((d >> 16) & 0x7fffu), (int)(d & 0xffffu));
+    }
+}
+static_assert(F_EXTRA <= 2 * TTHREADS, "border faces: at most two per thread");
 
 // A cell of the 1-halo region as one thread handles it: its index m in the
 // region, box index r (at, atb, kmt boxes), u (ws box), its west x face fw and
@@ -513,6 +570,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
     const bool has_ring = tid < RING;
     const HCell ring_cell = ring_hcell(has_ring ? tid : 0, x0, y0, imt, jmt);
+    const FaceSet fset = face_set(tid);
     const int fe = fx(ty + 1, tx + 2), fwi = fx(ty + 1, tx + 1), fs = fy(ty + 2, tx + 1), fn = fy(ty + 1, tx + 1);
     const float swv = (inner && n == 0) ? (float)a.swv[qo] : 0.f;
     const double stf = own ? a.stf_n[n * A + qo] : 0.0;
@@ -532,7 +590,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       const bool ok = wait(km - 1) && wait(km - 2);
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
     }
-    faces_level(S, km - 1);
+    faces_level(S, km - 1, fset);
     __syncthreads();
     predictor_mixed(S, a, km - 1, own_cell, ring_cell, has_ring);
 
@@ -541,7 +599,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       const float akt_above = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
       // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
       // arrived in earlier steps; the previous step ended with a barrier)
-      if (k >= 1) faces_level(S, k - 1);
+      if (k >= 1) faces_level(S, k - 1, fset);
       del4_first_mixed(S, k, own_cell, ring_cell, has_ring);
       const bool ok = (k >= 2) ? wait(k - 2) : true;
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
