@@ -118,21 +118,50 @@ __device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
   const double tr = div_here ? a.tarea_r[qo] : 0.0;
   const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
   double P = 0.0;
+  // U-point means of the region at one level: each thread loads the raw f32
+  // velocities of up to two region points into registers one level ahead, so
+  // the loads of level k+1 are in flight while level k is computed
+  constexpr int NPT = (UN + NT - 1) / NT;
+  static_assert(NPT <= 2, "region points per thread");
+  float ruf[NPT], rul[NPT], rvf[NPT], rvl[NPT];
+  long rc[NPT];
+  bool rin[NPT];
+#pragma unroll
+  for (int p = 0; p < NPT; ++p) {
+    const int m = tid + p * NT;
+    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+    rin[p] = m < UN && uj >= 0 && uj < jmt && ui < imt;
+    rc[p] = rin[p] ? (long)uj * imt + ui : 0;
+  }
+  auto fetch = [&](int k) {
+    const long lvl = (long)k * A;
+#pragma unroll
+    for (int p = 0; p < NPT; ++p) {
+      ruf[p] = rul[p] = rvf[p] = rvl[p] = 0.f;
+      if (rin[p]) {
+        const long c = lvl + rc[p];
+        ruf[p] = a.utf32[c]; rul[p] = a.utl32[c];
+        rvf[p] = a.vtf32[c]; rvl[p] = a.vtl32[c];
+      }
+    }
+  };
+  auto park = [&](int b) {
+#pragma unroll
+    for (int p = 0; p < NPT; ++p) {
+      const int m = tid + p * NT;
+      if (m < UN) {
+        s_wkd[b][m] = rin[p] ? 0.5f * (ruf[p] * oncc) + 0.5f * rul[p] : 0.f;
+        s_wkb[b][m] = rin[p] ? 0.5f * (rvf[p] * oncc) + 0.5f * rvl[p] : 0.f;
+      }
+    }
+  };
+  fetch(0);
+  park(0);
   for (int k = 0; k < km; ++k) {
     const int b = k & 1;
     const long lvl = (long)k * A;
-    for (int m = tid; m < UN; m += NT) {
-      const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
-      float wkd = 0.f, wkb = 0.f;
-      if (uj >= 0 && uj < jmt && ui < imt) {
-        const long c = lvl + (long)uj * imt + ui;
-        wkd = 0.5f * (a.utf32[c] * oncc) + 0.5f * a.utl32[c];
-        wkb = 0.5f * (a.vtf32[c] * oncc) + 0.5f * a.vtl32[c];
-      }
-      s_wkd[b][m] = wkd;
-      s_wkb[b][m] = wkb;
-    }
     __syncthreads();
+    if (k + 1 < km) fetch(k + 1);
     if (own) {
       const long c = lvl + qo;
       const float* wd = s_wkd[b];
@@ -160,6 +189,8 @@ __device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
         P += a.dzp[k] * wka;
       }
     }
+    // buffer b^1 was last read in step k-1, before this step's barrier
+    if (k + 1 < km) park(b ^ 1);
   }
   if (!col_here) return;
   const double ohbt = a.ohbt[qo];
