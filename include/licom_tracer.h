@@ -74,6 +74,20 @@ typedef enum {
   LT_F_PENETRATE,                   /* [km][jmt][imt] */
   /* sea-ice bookkeeping of icesnow, f64 */
   LT_F_QICE,                        /* [jmt][imt] ice formed, tracer_mod licomqice (d_licomqice) */
+  /* Canuto turbulence closure (lt_turb), f64; allocated on first use */
+  LT_F_RIT, LT_F_RICDTTMS,          /* [km-1][jmt][imt] Richardson numbers Ri = Ri_T + Ri_C, Ri_d = Ri_T - Ri_C */
+  LT_F_S2T,                         /* [km-1][jmt][imt] shear squared at T points (readyc1_2) */
+  LT_F_RICT,                        /* [km-1][jmt][imt] buoyancy frequency squared N^2 */
+  LT_F_PDENSITY,                    /* [km+1][jmt][imt] potential density (levels 0..km-1 used) */
+  LT_F_FZ_TIDE,                     /* [km][jmt][imt] vertical structure of tidal dissipation */
+  LT_F_BUOYTUR, LT_F_BUOYSOL,       /* [jmt][imt] turbulent and solar surface buoyancy flux */
+  LT_F_FCORT,                       /* [jmt][imt] Coriolis parameter at T points */
+  LT_F_WAVE_DIS,                    /* [jmt][imt] tidal wave dissipation */
+  LT_F_ZKP,                         /* [km+1] depths of the level interfaces (negative, m) */
+  LT_F_AKMT,                        /* [km][jmt][imt] viscosity at T points (output) */
+  LT_F_AK_TIDE,                     /* [km][jmt][imt] tidal mixing (output) */
+  LT_F_AMLD,                        /* [jmt][imt] mixed-layer depth (output, m) */
+  LT_F_RICHARDSON, LT_F_FZTIDAL, LT_F_WP3_TIDAL,  /* [km][jmt][imt] tidal diagnostics (output) */
   LT_F_COUNT
 } lt_field;
 
@@ -161,6 +175,63 @@ void lt_icesnow_defaults(lt_icesnow_params* p);
  * finally T at every level is raised to tbice where below.  p NULL means
  * lt_icesnow_defaults.  Asynchronous on the domain's stream. */
 int lt_icesnow(lt_domain* dom, const lt_icesnow_params* p);
+
+/* --- Canuto turbulence closure (turb_cu, readyc.cpp:1456-1612) ------------ */
+/* Table sizes of the reference's canuto_mod.h (mt, mt0, n_theta_r_oct). */
+#define LT_TURB_MT 1462
+#define LT_TURB_MT0 400
+#define LT_TURB_NTHETA 75
+#define LT_TURB_N1 (2 * LT_TURB_MT + 1)       /* entries of the Ri-type tables */
+#define LT_TURB_NB (4 * LT_TURB_NTHETA + 1)   /* entries of the background tables */
+/* The closure's tables, as canuto_ini_2002.F90 leaves them in canuto_mod and
+ * turbinit (turb_init.cpp:37-88) copies them to the device.  Host pointers. */
+typedef struct {
+  const double* rib;        /* [N1] Richardson-number grid, linear |i| <= MT0, geometric beyond */
+  const int* irimax;        /* [N1] last realizable Ri index for each Ri_d index (-MT .. MT) */
+  const double* slq2b;      /* [N1][N1] (S l/q)^2, row = Ri_d index, column = Ri index */
+  const double* smb;        /* [N1][N1] S_M */
+  const double* shb;        /* [N1][N1] S_H */
+  const double* ssb;        /* [N1][N1] S_S */
+  const double* and2on2a1;  /* [N1] zero-shear table grid of N_d^2/N^2 */
+  const double* amtaun2a1;  /* [N1] -(tau N)^2 of the zero-shear table */
+  const double* sma1;       /* [N1] zero-shear S_M, S_H, S_S */
+  const double* sha1;
+  const double* ssa1;
+  const double* back_ra_r;  /* [NB] background radius in the (Ri_T, Ri_C) plane vs angle */
+  const double* sm_r1;      /* [NB] background S_M, S_H, S_S, (S l/q)^2 vs angle */
+  const double* sh_r1;
+  const double* ss_r1;
+  const double* slq2_r1;
+  double rri;               /* ratio of adjacent Ri in the geometric part (canuto_mod rri) */
+  double rnd2on2;           /* the same for the zero-shear table */
+  double dri;               /* Ri step of the linear part */
+  double deltheta_r;        /* angle step of the background tables */
+  double b1;                /* B_1 */
+  double theta_rcrp;        /* critical angles */
+  double theta_rcrn;
+  double dand2on2;          /* N_d^2/N^2 step of the zero-shear table */
+} lt_turb_tables;
+typedef struct lt_turb_tab lt_turb_tab;
+/* Copy the tables to the current device once; a table set serves any number
+ * of domains on that device. */
+int lt_turb_tables_create(const lt_turb_tables* host, lt_turb_tab** out);
+int lt_turb_tables_destroy(lt_turb_tab* tab);
+typedef struct {
+  int ncc;                  /* pconst_mod ncc (akt is divided by it) */
+  double dfricmx;           /* pconst_mod dfricmx: upper bound of the diffusivities (m^2/s) */
+} lt_turb_params;
+/* The closure over the current state, every column with i in 1..imt-2,
+ * j in 1..jmt-2 and kmt >= 1 (turb_cu with TIDEMIX, the reference's
+ * configuration): writes AKT (levels 0..km-2; the tracer step's mixing, as f32
+ * in a mixed-precision domain), AKMT, AK_TIDE, AMLD and the tidal
+ * diagnostics; reads T of AT, DZP, KMT, dwndmix of the domain's parameters and
+ * the turbulence inputs (RIT .. ZKP).  AKMT, AK_TIDE and AMLD are zero where
+ * no column is computed, as after the reference's memsets (readyc.cpp:1642,
+ * 1647, 1668).  Asynchronous on the domain's stream.  The reference leaves two
+ * locals unset on some paths (the buoyancy frequency when N^2 < 0 at the top
+ * level, the background S l/q where Ri <= 0 before any Ri > 0); they start at
+ * zero here. */
+int lt_turb(lt_domain* dom, const lt_turb_tab* tab, const lt_turb_params* p);
 /* Global tracer integrals sum(tarea*dzp*vit*tracer) over the interior, f64,
  * fixed-order pairwise tree (deterministic). out2[0] = T, out2[1] = S. */
 int lt_tracer_content(lt_domain* dom, double* out2);
@@ -226,6 +297,9 @@ const char* lt_field_name(int field);
 long lt_field_count(int field, int nx, int ny, int km);
 /* 1 for the int32 mask fields, 0 for f64 fields. */
 int lt_field_is_int(int field);
+/* 1 for the turbulence closure's fields (LT_F_RIT .. LT_F_WP3_TIDAL), which a
+ * domain allocates on first use. */
+int lt_field_is_turb(int field);
 
 /* --- errors, device ------------------------------------------------------ */
 const char* lt_last_error(void);

@@ -52,6 +52,34 @@ class IcesnowParams(C.Structure):
         super().__init__(tbice, cp, latice, reset_qice)
 
 
+TURB_TABLE_ARRAYS = ("rib", "irimax", "slq2b", "smb", "shb", "ssb", "and2on2a1", "amtaun2a1", "sma1", "sha1", "ssa1",
+                     "back_ra_r", "sm_r1", "sh_r1", "ss_r1", "slq2_r1")
+TURB_TABLE_SCALARS = ("rri", "rnd2on2", "dri", "deltheta_r", "b1", "theta_rcrp", "theta_rcrn", "dand2on2")
+
+
+class TurbTablesStruct(C.Structure):
+    """lt_turb_tables: host pointers to the closure's tables and its scalars."""
+    _fields_ = [(n, C.c_void_p) for n in TURB_TABLE_ARRAYS] + [(n, C.c_double) for n in TURB_TABLE_SCALARS]
+
+
+def turb_tables_struct(t):
+    """lt_turb_tables over a dict of arrays and scalars (turb_synth.tables()
+    layout); the arrays must stay alive while the struct is used."""
+    st = TurbTablesStruct()
+    for n in TURB_TABLE_ARRAYS:
+        a = t[n]
+        want = np.int32 if n == "irimax" else np.float64
+        assert a.dtype == want and a.flags["C_CONTIGUOUS"], n
+        setattr(st, n, a.ctypes.data)
+    for n in TURB_TABLE_SCALARS:
+        setattr(st, n, float(t[n]))
+    return st
+
+
+class TurbParams(C.Structure):
+    _fields_ = [("ncc", C.c_int), ("dfricmx", C.c_double)]
+
+
 class SynthConfig(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("km", C.c_int), ("lat_s", C.c_double), ("lat_n", C.c_double),
                 ("dz_top", C.c_double), ("dz_bot", C.c_double), ("depth", C.c_double), ("umax", C.c_double),
@@ -109,6 +137,9 @@ _SIGS = {
     "lt_convadj": ([_vp], _i),
     "lt_icesnow": ([_vp, C.POINTER(IcesnowParams)], _i),
     "lt_icesnow_defaults": ([C.POINTER(IcesnowParams)], None),
+    "lt_turb_tables_create": ([C.POINTER(TurbTablesStruct), C.POINTER(_vp)], _i),
+    "lt_turb_tables_destroy": ([_vp], _i),
+    "lt_turb": ([_vp, _vp, C.POINTER(TurbParams)], _i),
     "lt_tracer_content": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_fw_norm2": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_sync": ([_vp], _i),
@@ -124,6 +155,7 @@ _SIGS = {
     "lt_field_name": ([_i], C.c_char_p),
     "lt_field_count": ([_i, _i, _i, _i], C.c_long),
     "lt_field_is_int": ([_i], _i),
+    "lt_field_is_turb": ([_i], _i),
     "lt_synth_defaults": ([C.POINTER(SynthConfig)], None),
     "lt_synth_build": ([C.POINTER(SynthConfig), C.POINTER(_vp)], _i),
     "lt_synth_free": ([_vp], _i),
@@ -171,7 +203,10 @@ INT_FIELDS = {n for n in FIELDS if lib.lt_field_is_int(FIELD_ID[n])}
 # (WS, NET and QICE are model state the step or icesnow reads and rewrites;
 # they start at zero)
 INPUT_FIELDS = [n for n in FIELDS if n not in (
-    "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE")]
+    "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE")
+    and not lib.lt_field_is_turb(FIELD_ID[n])]
+# the turbulence closure's fields (allocated by a domain on first use)
+TURB_FIELDS = [n for n in FIELDS if lib.lt_field_is_turb(FIELD_ID[n])]
 
 
 def _check(rc, where):
@@ -184,7 +219,8 @@ def field_shape(name, nx, ny, km):
     n = lib.lt_field_count(FIELD_ID[name], nx, ny, km)
     shapes = {2 * km * jmt * imt: (2, km, jmt, imt), 2 * (km + 1) * jmt * imt: (2, km + 1, jmt, imt),
               km * jmt * imt: (km, jmt, imt), (km + 1) * jmt * imt: (km + 1, jmt, imt),
-              jmt * imt: (jmt, imt), 2 * jmt * imt: (2, jmt, imt), km: (km,), 9 * km: (9, km)}
+              jmt * imt: (jmt, imt), 2 * jmt * imt: (2, jmt, imt), km: (km,), 9 * km: (9, km),
+              (km - 1) * jmt * imt: (km - 1, jmt, imt), km + 1: (km + 1,)}
     return shapes[n]
 
 
@@ -304,6 +340,13 @@ class TracerDomain:
     def convadj(self):
         _check(lib.lt_convadj(self.h), "lt_convadj")
 
+    def turb(self, tab, ncc=1, dfricmx=0.1):
+        """Canuto turbulence closure (turb_cu, readyc.cpp:1456-1612) with the
+        tables of ``tab`` (a TurbTab on this device): writes AKT, AKMT,
+        AK_TIDE, AMLD and the tidal diagnostics."""
+        prm = TurbParams(int(ncc), float(dfricmx))
+        _check(lib.lt_turb(self.h, tab.h, C.byref(prm)), "lt_turb")
+
     def icesnow(self, params=None):
         """Sea-ice adjustment of the current state (icesnow.cpp:15-85);
         params an IcesnowParams, None for the reference's values."""
@@ -336,6 +379,28 @@ class TracerDomain:
 
     def bind_shim(self):
         _check(lib.lt_shim_bind(self.h), "lt_shim_bind")
+
+
+class TurbTab:
+    """The closure's tables copied to the current device (lt_turb_tables_create);
+    ``tables`` is a dict in the turb_synth.tables() layout."""
+
+    def __init__(self, tables):
+        st = turb_tables_struct(tables)
+        h = _vp()
+        _check(lib.lt_turb_tables_create(C.byref(st), C.byref(h)), "lt_turb_tables_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.lt_turb_tables_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def tracer_(ii=0):

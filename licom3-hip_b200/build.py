@@ -30,6 +30,7 @@ CU_UNITS = {
     "lt_noalloc.cu": ["-fmad=false"],
     "lt_batch.cu": [],
     "lt_serve.cu": [],
+    "lt_turb.cu": ["-fmad=false"],
 }
 CPP_UNITS = ["lt_synth_api.cpp"]
 

@@ -122,6 +122,23 @@ void* field_ptr(lt_domain* d, int f, int which_state) {
     case LT_F_DT_CONV: return a.dt_conv;
     case LT_F_PENETRATE: return a.penetrate;
     case LT_F_QICE: return a.qice;
+    case LT_F_RIT: return a.rit;
+    case LT_F_RICDTTMS: return a.ricdttms;
+    case LT_F_S2T: return a.s2t;
+    case LT_F_RICT: return a.rict;
+    case LT_F_PDENSITY: return a.pdensity;
+    case LT_F_FZ_TIDE: return a.fz_tide;
+    case LT_F_BUOYTUR: return a.buoytur;
+    case LT_F_BUOYSOL: return a.buoysol;
+    case LT_F_FCORT: return a.fcort;
+    case LT_F_WAVE_DIS: return a.wave_dis;
+    case LT_F_ZKP: return a.zkp;
+    case LT_F_AKMT: return a.akmt;
+    case LT_F_AK_TIDE: return a.ak_tide;
+    case LT_F_AMLD: return a.amld;
+    case LT_F_RICHARDSON: return a.richardson;
+    case LT_F_FZTIDAL: return a.fztidal;
+    case LT_F_WP3_TIDAL: return a.wp3_tidal;
   }
   return nullptr;
 }
@@ -291,6 +308,39 @@ int timeout_status(lt_domain* d) {
 
 }  // namespace lt
 
+namespace lt {
+// The turbulence closure's fields: one zeroed allocation, taken the first time
+// the domain uses any of them (a domain that only steps tracers never pays
+// for them).
+int ensure_turb(lt_domain* d) {
+  Arena& a = d->a;
+  if (a.rit) return LT_OK;
+  double** f3m1[] = {&a.rit, &a.ricdttms, &a.s2t, &a.rict};
+  double** f3[] = {&a.fz_tide, &a.akmt, &a.ak_tide, &a.richardson, &a.fztidal, &a.wp3_tidal};
+  double** f2[] = {&a.buoytur, &a.buoysol, &a.fcort, &a.wave_dis, &a.amld};
+  Plan pl;
+  for (auto p : f3m1) pl.add(reinterpret_cast<void**>(p), sizeof(double) * a.A * (a.km - 1));
+  for (auto p : f3) pl.add(reinterpret_cast<void**>(p), sizeof(double) * a.F);
+  for (auto p : f2) pl.add(reinterpret_cast<void**>(p), sizeof(double) * a.A);
+  pl.add(reinterpret_cast<void**>(&a.pdensity), sizeof(double) * a.FB);
+  pl.add(reinterpret_cast<void**>(&a.zkp), sizeof(double) * (a.km + 1));
+  char* base = nullptr;
+  cudaError_t e = cudaMalloc(&base, pl.off);
+  if (e != cudaSuccess) {
+    set_error("turbulence fields: cudaMalloc(%zu) failed: %s", pl.off, cudaGetErrorString(e));
+    return LT_E_OOM;
+  }
+  d->allocations.push_back(base);
+  size_t off = 0;
+  for (auto& it : pl.items) {
+    *it.first = base + off;
+    off += (it.second + 255) / 256 * 256;
+  }
+  LT_CUDA_OK(cudaMemsetAsync(base, 0, pl.off, d->stream));
+  return LT_OK;
+}
+}  // namespace lt
+
 using namespace lt;
 
 extern "C" {
@@ -302,7 +352,9 @@ static const char* const k_field_names[LT_F_COUNT] = {
     "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE", "DXU", "DYU",
     "AHF", "DTN", "DTS", "DTE", "DTW", "OHBT", "OHBU", "AU0", "AUS", "AUW", "AUSW", "KMT", "KMU", "KMTN", "KMTS",
     "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND",
-    "DT_DIFF", "DT_CONV", "PENETRATE", "QICE"};
+    "DT_DIFF", "DT_CONV", "PENETRATE", "QICE", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY", "FZ_TIDE",
+    "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "ZKP", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON", "FZTIDAL",
+    "WP3_TIDAL"};
 
 const char* lt_field_name(int f) { return (f >= 0 && f < LT_F_COUNT) ? k_field_names[f] : nullptr; }
 long lt_field_count(int f, int nx, int ny, int km) {
@@ -310,6 +362,7 @@ long lt_field_count(int f, int nx, int ny, int km) {
   return lt::field_count(f, nx + 4, ny + 4, km);
 }
 int lt_field_is_int(int f) { return (f >= 0 && f < LT_F_COUNT) ? (int)lt::field_is_int(f) : 0; }
+int lt_field_is_turb(int f) { return (f >= 0 && f < LT_F_COUNT) ? (int)lt::field_is_turb(f) : 0; }
 
 const char* lt_version(void) { return "licom3-hip_b200 tracer 0.1 (sm_100a)"; }
 
@@ -451,8 +504,13 @@ int lt_set_params(lt_domain* d, const lt_params* p) {
   return LT_OK;
 }
 
+
 static int xfer(lt_domain* d, int f, void* ptr, size_t nbytes, cudaMemcpyKind kind, bool set) {
   if (!d || !ptr || f < 0 || f >= LT_F_COUNT) { set_error("bad field transfer"); return LT_E_INVALID; }
+  if (lt::field_is_turb(f)) {
+    const int rc = lt::ensure_turb(d);
+    if (rc) return rc;
+  }
   const size_t need = lt::field_bytes(f, d->a.imt, d->a.jmt, d->a.km);
   if (nbytes != need) {
     set_error("field %d: %zu bytes given, %zu expected", f, nbytes, need);

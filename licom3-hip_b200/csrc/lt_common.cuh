@@ -42,6 +42,10 @@ struct Arena {
   int *kmt, *kmu, *kmtn, *kmts, *kmte, *kmtw;
   double *dzp, *odzp, *odzt, *pen, *to, *so, *cc, *restore;
   double *qice;               // [jmt][imt] ice formed by icesnow (tracer_mod licomqice)
+  // turbulence closure (lt_turb): inputs and outputs, null until the domain
+  // first uses one of them
+  double *rit, *ricdttms, *s2t, *rict, *pdensity, *fz_tide, *buoytur, *buoysol, *fcort, *wave_dis, *zkp;
+  double *akmt, *ak_tide, *amld, *richardson, *fztidal, *wp3_tidal;
   // diagnostics (null when off)
   double *ax, *ay, *az, *dzd, *tend, *dt_diff, *dt_conv, *penetrate;
 
@@ -63,6 +67,15 @@ struct Arena {
   long col_scratch_slots;
   int nv_scratch;             // values per level per column in col_scratch
   unsigned wait_limit;        // polls of each level wait in the column kernels before giving up
+};
+
+// The turbulence closure's tables on the device (lt_turb_tables, copied by
+// lt_turb_tables_create).
+struct TurbTabDev {
+  const double *rib, *slq2b, *smb, *shb, *ssb, *and2on2a1, *amtaun2a1, *sma1, *sha1, *ssa1;
+  const double *back_ra_r, *sm_r1, *sh_r1, *ss_r1, *slq2_r1;
+  const int* irimax;
+  double rri, rnd2on2, dri, deltheta_r, b1, theta_rcrp, theta_rcrn, dand2on2;
 };
 
 #define LT_CUDA_OK(call)                                   \
@@ -95,6 +108,7 @@ int launch_interior_sum_sss(const Arena& a, cudaStream_t s);
 int launch_tracer_content(const Arena& a, cudaStream_t s);
 int launch_convadj(const Arena& a, cudaStream_t s);
 int launch_icesnow(const Arena& a, const lt_icesnow_params& p, cudaStream_t s);
+int launch_turb(const Arena& a, const TurbTabDev& T, int ncc, double dfricmx, cudaStream_t s);
 int launch_check_numeric(const Arena& a, cudaStream_t s);
 int launch_derive_masks(const Arena& a, cudaStream_t s);
 int launch_vtl_clobber(const Arena& a, cudaStream_t s);

@@ -13,7 +13,9 @@ enum FieldShape {
   SH_SURF2N,        // [2][jmt][imt]
   SH_MASK2,         // [jmt][imt] int32
   SH_COL1,          // [km]
-  SH_COEF9          // [9][km]
+  SH_COEF9,         // [9][km]
+  SH_LEVEL3M1,      // [km-1][jmt][imt]
+  SH_COL1P          // [km+1]
 };
 
 inline int field_shape(int f) {
@@ -23,9 +25,12 @@ inline int field_shape(int f) {
       return SH_TRACER3;
     case LT_F_ATB: return SH_TRACERB;
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
-    case LT_F_PENETRATE:
+    case LT_F_PENETRATE: case LT_F_FZ_TIDE: case LT_F_AKMT: case LT_F_AK_TIDE: case LT_F_RICHARDSON:
+    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL:
       return SH_LEVEL3;
-    case LT_F_WS: return SH_W3;
+    case LT_F_RIT: case LT_F_RICDTTMS: case LT_F_S2T: case LT_F_RICT: return SH_LEVEL3M1;
+    case LT_F_ZKP: return SH_COL1P;
+    case LT_F_WS: case LT_F_PDENSITY: return SH_W3;
     case LT_F_NET: return SH_SURF2N;
     case LT_F_KMT: case LT_F_KMU: case LT_F_KMTN: case LT_F_KMTS: case LT_F_KMTE: case LT_F_KMTW:
       return SH_MASK2;
@@ -38,6 +43,9 @@ inline int field_shape(int f) {
 
 inline bool field_is_int(int f) { return field_shape(f) == SH_MASK2; }
 
+// fields of the turbulence closure, allocated with the domain's first use of any of them
+inline bool field_is_turb(int f) { return f >= LT_F_RIT && f <= LT_F_WP3_TIDAL; }
+
 inline long field_count(int f, int imt, int jmt, int km) {
   const long A = (long)imt * jmt;
   switch (field_shape(f)) {
@@ -49,6 +57,8 @@ inline long field_count(int f, int imt, int jmt, int km) {
     case SH_SURF2N: return 2 * A;
     case SH_COL1: return km;
     case SH_COEF9: return 9L * km;
+    case SH_LEVEL3M1: return A * (km - 1);
+    case SH_COL1P: return km + 1;
   }
   return 0;
 }

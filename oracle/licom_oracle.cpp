@@ -15,6 +15,9 @@
 //                                   POP_BlocksMod.F90:284-375
 //   convective adjustment           convadj.cpp:29-288
 //   sea-ice adjustment              icesnow.cpp:15-85
+//   Canuto turbulence closure       readyc.cpp:880-1612 (turb_cu, turb_device,
+//                                   interp1d_expabs, interp2d_expabs, formld,
+//                                   eplatidepend_fun), TIDEMIX configuration
 //
 // Arithmetic keeps the reference's operation order term by term (so that a
 // build with -ffp-contract=off reproduces the reference's own code compiled
@@ -35,7 +38,7 @@
 
 namespace {
 
-enum Kind { K3N = 0, KB3N, K3, KW, K2, K2N, K2I, K1, K1C };
+enum Kind { K3N = 0, KB3N, K3, KW, K2, K2N, K2I, K1, K1C, K3M1, K1P };
 
 struct FieldInfo { int kind; bool is_int; };
 
@@ -46,9 +49,12 @@ FieldInfo field_info(int f) {
       return {K3N, false};
     case LT_F_ATB: return {KB3N, false};
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
-    case LT_F_PENETRATE:
+    case LT_F_PENETRATE: case LT_F_FZ_TIDE: case LT_F_AKMT: case LT_F_AK_TIDE: case LT_F_RICHARDSON:
+    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL:
       return {K3, false};
-    case LT_F_WS: return {KW, false};
+    case LT_F_RIT: case LT_F_RICDTTMS: case LT_F_S2T: case LT_F_RICT: return {K3M1, false};
+    case LT_F_ZKP: return {K1P, false};
+    case LT_F_WS: case LT_F_PDENSITY: return {KW, false};
     case LT_F_NET: return {K2N, false};
     case LT_F_KMT: case LT_F_KMU: case LT_F_KMTN: case LT_F_KMTS: case LT_F_KMTE: case LT_F_KMTW:
       return {K2I, true};
@@ -83,6 +89,8 @@ struct Oracle {
       case K2: case K2I: return A;
       case K1: return km;
       case K1C: return 9L * km;
+      case K3M1: return A * (km - 1);
+      case K1P: return km + 1;
     }
     return 0;
   }
@@ -769,6 +777,390 @@ void icesnow_call(Oracle& o, const lt_icesnow_params& p) {
   }
 }
 
+
+// ---- Canuto turbulence closure (readyc.cpp:880-1612), TIDEMIX configuration.
+// Table sizes of canuto_mod.h; constants of pconst_mod.h:242-247.
+namespace turb {
+constexpr int mt = LT_TURB_MT, mt0 = LT_TURB_MT0, nth = LT_TURB_NTHETA;
+constexpr double back_tidalmixing = 1.0e-6, max_tidalmixing = 1.0e-2, mixing_ef = 0.20,
+                 local_mixing_fraction = 0.33;
+constexpr double epson2__ = 0.288e0, eplatidependmin = 7.0e-2, s2min = 1.0e-14;
+
+inline double sgn(double x, double y) { return y >= 0.0e0 ? std::fabs(x) : -std::fabs(x); }
+inline int sgn_i(int x, int y) { return y >= 0 ? std::abs(x) : -std::abs(x); }
+
+// eplatidepend_fun with wavelat (readyc.cpp:880-896)
+double eplat(double f, double an) {
+  const double an0 = 5.24e-3;
+  const double f_30 = 4.0e0 * std::atan(1.0e0) / 43082.0e0;
+  const double den = f_30 * std::acosh(an0 / f_30);
+  const double anum = f * std::acosh(an / f);
+  return anum / den;
+}
+
+// formld (readyc.cpp:902-913)
+void formld(int n, const double* z, const double* t, double* amld) {
+  for (int k = 0; k < n; k++) {
+    if (std::fabs(t[k] - t[0]) > 0.1) {
+      const double tm = t[0] - sgn(0.1e0, t[0] - t[k]);
+      *amld = z[k] + (z[k - 1] - z[k]) * (tm - t[k]) / (t[k - 1] - t[k] + 1.0e-20);
+      return;
+    }
+  }
+  *amld = z[n - 1];
+}
+
+// interp1d_expabs (readyc.cpp:915-973)
+void interp1d(double x, const double* x_1, const double* slq2_1, const double* sm_1, const double* sh_1,
+              const double* ss_1, double* slq2, double* sm, double* sh, double* ss, double delta, double rat) {
+  int lx0, lx1;
+  if (x > x_1[2 * mt]) x = x_1[2 * mt];
+  else if (x < x_1[0]) x = x_1[0];
+  if (std::fabs(x) >= x_1[mt + mt0] && std::fabs(x) >= x_1[2 * mt]) {
+    lx0 = (int)sgn((double)mt, x);
+    lx1 = lx0;
+  } else {
+    if (std::fabs(x) < x_1[mt + mt0]) {
+      lx1 = (int)(x / delta) + (int)sgn(1.0, x);
+    } else {
+      const double tabindx = sgn((double)mt0 + ((std::log(std::fabs(x)) - std::log(x_1[mt + mt0])) / std::log(rat)), x);
+      lx1 = (int)tabindx + (int)sgn(1.0, x);
+    }
+    lx1 = std::max(-mt, std::min(mt, lx1));   // the reference reads past its table here
+    if (std::fabs(x_1[mt + lx1]) < std::fabs(x)) lx1 += sgn_i(1, lx1);
+    else if (std::fabs(x_1[mt + lx1 - sgn_i(1, lx1)]) > std::fabs(x)) lx1 += -sgn_i(1, lx1);
+    lx0 = lx1 - (int)sgn(1.0, x);
+    if (std::fabs(x) <= 0.0e0) lx1 = 1;
+  }
+  if ((x > 0.0e0 && (x < x_1[mt + lx0] || x > x_1[mt + lx1])) ||
+      (x < 0.0e0 && (x > x_1[mt + lx0] || x < x_1[mt + lx1])))
+    return;
+  const double deltaxta = x_1[mt + lx1] - x_1[mt + lx0];
+  const double deltax = x - x_1[mt + lx0];
+  double dslq2_x, dsm_x, dsh_x, dss_x;
+  if (lx1 == lx0) {
+    dslq2_x = dsm_x = dsh_x = dss_x = 0.0e0;
+  } else {
+    dslq2_x = (slq2_1[mt + lx1] - slq2_1[mt + lx0]) / deltaxta;
+    dsm_x = (sm_1[mt + lx1] - sm_1[mt + lx0]) / deltaxta;
+    dsh_x = (sh_1[mt + lx1] - sh_1[mt + lx0]) / deltaxta;
+    dss_x = (ss_1[mt + lx1] - ss_1[mt + lx0]) / deltaxta;
+  }
+  *slq2 = slq2_1[mt + lx0] + dslq2_x * deltax;
+  *sm = sm_1[mt + lx0] + dsm_x * deltax;
+  *sh = sh_1[mt + lx0] + dsh_x * deltax;
+  *ss = ss_1[mt + lx0] + dss_x * deltax;
+}
+
+// index search of interp2d_expabs for one coordinate; false if x is not
+// bracketed (the reference returns)
+bool index2d(double x, const lt_turb_tables& T, int* l0, int* l1) {
+  const double* rib = T.rib;
+  const double tmp = rib[mt + mt0], tmp1 = rib[2 * mt];
+  if (std::fabs(x) >= tmp && std::fabs(x) >= tmp1) {
+    *l0 = (int)sgn((double)mt, x);
+    *l1 = *l0;
+  } else {
+    if (std::fabs(x) < tmp) {
+      *l1 = (int)(x / T.dri) + (int)sgn(1.0, x);
+    } else {
+      const double ti = sgn((double)mt0 + ((std::log(std::fabs(x)) - std::log(tmp)) / std::log(T.rri)), x);
+      *l1 = (int)ti + (int)sgn(1.0, x);
+    }
+    *l1 = std::max(-mt, std::min(mt, *l1));   // the reference reads past its table here
+    if (std::fabs(rib[mt + *l1]) < std::fabs(x)) *l1 += sgn_i(1, *l1);
+    else if (std::fabs(rib[mt + *l1 - sgn_i(1, *l1)]) > std::fabs(x)) *l1 += -sgn_i(1, *l1);
+    *l0 = *l1 - (int)sgn(1.0, x);
+    if (x == 0.0e0) *l1 = 1;
+  }
+  return !((x > 0.0e0 && (x < rib[mt + *l0] || x > rib[mt + *l1])) ||
+           (x < 0.0e0 && (x > rib[mt + *l0] || x < rib[mt + *l1])));
+}
+
+// interp2d_expabs (readyc.cpp:975-1114)
+void interp2d(double* ri, double* rid, double* slq2, double* sm, double* sh, double* ss, const lt_turb_tables& T) {
+  const double* rib = T.rib;
+  if (*ri > rib[2 * mt]) {
+    if (std::fabs(*rid) <= *ri) { *rid = rib[2 * mt] * (*rid / *ri); *ri = rib[2 * mt]; }
+    else if (*rid > *ri) { *ri = rib[2 * mt] * (*ri / *rid); *rid = rib[2 * mt]; }
+    else if (*rid < -*ri) { *ri = rib[0] * (*ri / *rid); *rid = rib[0]; }
+  } else if (*ri < rib[0]) {
+    if (std::fabs(*rid) <= -*ri) { *rid = rib[0] * (*rid / *ri); *ri = rib[0]; }
+    else if (*rid > -*ri) { *ri = rib[2 * mt] * (*ri / *rid); *rid = rib[2 * mt]; }
+    else if (*rid < *ri) { *ri = rib[0] * (*ri / *rid); *rid = rib[0]; }
+  } else if (*rid > rib[2 * mt]) {
+    *ri = rib[2 * mt] * (*ri / *rid);
+    *rid = rib[2 * mt];
+  } else if (*rid < rib[0]) {
+    *ri = rib[0] * (*ri / *rid);
+    *rid = rib[0];
+  }
+  const double ri_tmp = *ri, rid_tmp = *rid;
+  int lrid0, lrid1, lri0, lri1;
+  if (!index2d(rid_tmp, T, &lrid0, &lrid1)) return;
+  if (ri_tmp > std::fmin(rib[mt + T.irimax[mt + lrid0]], rib[mt + T.irimax[mt + lrid1]])) {
+    *slq2 = 0.0e0; *sm = 0.0e0; *sh = 0.0e0; *ss = 0.0e0;
+    return;
+  }
+  if (!index2d(ri_tmp, T, &lri0, &lri1)) return;
+  const long w = 2 * mt + 1;
+  const long c00 = w * (lrid0 + mt) + lri0 + mt, c10 = w * (lrid1 + mt) + lri0 + mt, c01 = w * (lrid0 + mt) + lri1 + mt;
+  const double deltaridta = rib[mt + lrid1] - rib[mt + lrid0];
+  const double deltarita = rib[mt + lri1] - rib[mt + lri0];
+  const double deltarid = rid_tmp - rib[mt + lrid0];
+  const double deltari = ri_tmp - rib[mt + lri0];
+  const double* tb[4] = {T.slq2b, T.smb, T.shb, T.ssb};
+  double* out[4] = {slq2, sm, sh, ss};
+  for (int m = 0; m < 4; ++m) {
+    double d_rid = 0.0e0, d_ri = 0.0e0;
+    if (lrid1 != lrid0) {
+      d_rid = (tb[m][c10] - tb[m][c00]) / deltaridta;
+      d_ri = (tb[m][c01] - tb[m][c00]) / deltarita;
+    }
+    *out[m] = tb[m][c00] + d_ri * deltari + d_rid * deltarid;
+  }
+}
+
+// turb_device (readyc.cpp:1116-1455) on one column's work arrays; the two
+// locals the reference can read unset start at zero
+void turb_device(const double* z, const double* t, const double* rh, const double* ri, const double* rid, double* s2,
+                 double fricmx, double wndmix, const double* an2, double buoytur, double buoysol, double coriol,
+                 double* amld, double* akm, double* akh, double* aks, int n, int nmax, const lt_turb_tables& T) {
+  const double b1 = T.b1;
+  double v_back, t_back, s_back;
+  double al2, tmp = 0.0, slq2 = 0.0, sm = 0.0, ss = 0.0, sh = 0.0;
+  double amtaun2 = 0.0;
+  double back_ri1 = 0.0e0;
+  double sh_back = 0.0, slq2_back = 0.0, sm_back = 0.0, ss_back = 0.0;
+  double epson2;
+  const int nb = n > 0 ? n : 0;
+  const double buoytot = buoytur + buoysol;
+  if (n > 0) formld(n, z, t, amld);
+  else if (n == 0) *amld = z[0];
+  else *amld = 0.0e0;
+  const double al0 = 0.17 * *amld;
+  double ifbelow = 0;
+  double an = 0.0;
+  for (int k = 0; k < n; k++) {
+    double ifnofsmall = 0;
+    if (an2[k] >= 0.0e0) an = std::sqrt(an2[k]);
+    if (an < std::fabs(coriol)) ifnofsmall = 1;
+    double ri1 = ri[k];
+    double rid1 = rid[k];
+    const double and2 = rid[k] / (ri[k] + 1.0e-25) * an2[k];
+    const double and2on2 = and2 / (an2[k] + 1.0e-25);
+    const int ifpureshear = (an2[k] < T.rib[0] * s2[k]) ? 1 : 0;
+    if (ifpureshear == 1) {
+      interp1d(and2on2, T.and2on2a1, T.amtaun2a1, T.sma1, T.sha1, T.ssa1, &amtaun2, &sm, &sh, &ss, T.dand2on2,
+               T.rnd2on2);
+      slq2 = (-amtaun2) / ((b1 * b1) * ri[k] + 1.0e-25);
+    } else {
+      interp2d(&ri1, &rid1, &slq2, &sm, &sh, &ss, T);
+      if (slq2 < 0.0e0) return;
+      if (slq2 == 0.0e0) ifbelow = 1;
+    }
+    const bool lifupper = ((ifbelow == 0 || ifnofsmall == 1 || ((ri1 < 0.0e0) && (k <= 1))) && (slq2 > 0.0e0));
+    double epsy = 0.0e0;
+    bool lifepsy = false;
+    if (n > 0) {
+      if (slq2 == 0.0e0) epsy = 0.0e0;
+      else epsy = -buoytot / ((1.0e0 / ((b1 * b1) * (slq2))) - 0.5e0 * sm);
+      lifepsy = ((epsy >= 0.0e0) && lifupper);
+    }
+    const double akz = 0.4 * z[k];
+    const double al = akz * al0 / (al0 + akz);
+    al2 = al * al;
+    if (ifbelow != 1 && !lifepsy) {
+      if (ri1 > 0.0e0) {
+        const double anlq2 = slq2 * ri1;
+        if (anlq2 > 0.281e0) {
+          al2 *= 0.281e0 / anlq2;
+          slq2 = 0.281e0 / (ri1 + 1.0e-20);
+        }
+      }
+    }
+    if (an2[k] < 0.0e0) {
+      epson2 = epson2__;
+    } else {
+      double eplatidepend = (ifnofsmall == 1) ? 0.0e0 : eplat(std::fabs(coriol), an);
+      eplatidepend = std::fmax(eplatidepend, eplatidependmin);
+      epson2 = epson2__ * eplatidepend;
+    }
+    if (ri[k] > 0.0e0) {
+      const double rit = (ri[k] + rid[k]) / 2.0e0;
+      const double ric = (ri[k] - rid[k]) / 2.0e0;
+      const double ra_r = std::sqrt((rit * rit) + (ric * ric));
+      double theta_r;
+      if (std::fabs(rit) <= 0.0e0) theta_r = (std::fabs(ric) <= 0.0e0) ? std::atan(1.0e0) : 2.0e0 * std::atan(1.0e0);
+      else theta_r = std::atan(ric / rit);
+      if (std::fabs(theta_r) > 2.0e0 * std::atan(1.0e0)) return;
+      if (theta_r < -std::atan(1.0e0)) theta_r += 4.0e0 * std::atan(1.0e0);
+      const int jtheta_r0 = (int)((theta_r + std::atan(1.0e0)) / T.deltheta_r);
+      int itheta_r0 = jtheta_r0 - nth;
+      int itheta_r1 = itheta_r0 + 1;
+      double theta_r0 = itheta_r0 * T.deltheta_r;
+      double theta_r1 = itheta_r1 * T.deltheta_r;
+      if ((theta_r0 <= T.theta_rcrp) && (theta_r > T.theta_rcrp)) {
+        theta_r = theta_r1; theta_r0 = theta_r1; itheta_r0 = itheta_r1; ++itheta_r1; theta_r1 += T.deltheta_r;
+      } else if ((theta_r1 >= T.theta_rcrn) && (theta_r < T.theta_rcrn)) {
+        theta_r = theta_r0; theta_r1 = theta_r0; itheta_r1 = itheta_r0; --itheta_r0; theta_r0 += -T.deltheta_r;
+      }
+      if ((itheta_r1 > 3 * nth) || (itheta_r0 < -nth)) return;
+      double deltheta_r_1 = theta_r - theta_r0;
+      const double delback_ra_r = T.back_ra_r[nth + itheta_r1] - T.back_ra_r[nth + itheta_r0];
+      const double dback_ra_r_o_dtheta = delback_ra_r / T.deltheta_r;
+      double back_ra_r1 = T.back_ra_r[nth + itheta_r0] + deltheta_r_1 * dback_ra_r_o_dtheta;
+      int ifrafglt = 0;
+      if ((theta_r <= T.theta_rcrp) || (theta_r >= T.theta_rcrn)) {
+        if (back_ra_r1 > ra_r) { ifrafglt = 1; back_ra_r1 = ra_r; }
+      }
+      if (back_ra_r1 < 0.0e0) return;
+      const double back_rit1 = std::cos(theta_r) * back_ra_r1;
+      const double back_ric1 = std::sin(theta_r) * back_ra_r1;
+      back_ri1 = back_rit1 + back_ric1;
+      double back_rid1 = back_rit1 - back_ric1;
+      if (ifrafglt == 1) {
+        interp2d(&back_ri1, &back_rid1, &slq2_back, &sm_back, &sh_back, &ss_back, T);
+      } else {
+        deltheta_r_1 = theta_r - itheta_r0 * T.deltheta_r;
+        sm_back = T.sm_r1[nth + itheta_r0] + deltheta_r_1 * ((T.sm_r1[nth + itheta_r1] - T.sm_r1[nth + itheta_r0]) / T.deltheta_r);
+        sh_back = T.sh_r1[nth + itheta_r0] + deltheta_r_1 * ((T.sh_r1[nth + itheta_r1] - T.sh_r1[nth + itheta_r0]) / T.deltheta_r);
+        ss_back = T.ss_r1[nth + itheta_r0] + deltheta_r_1 * ((T.ss_r1[nth + itheta_r1] - T.ss_r1[nth + itheta_r0]) / T.deltheta_r);
+        slq2_back = T.slq2_r1[nth + itheta_r0] +
+                    deltheta_r_1 * ((T.slq2_r1[nth + itheta_r1] - T.slq2_r1[nth + itheta_r0]) / T.deltheta_r);
+      }
+      if (slq2_back < 0.0e0) return;
+    }
+    if (ri[k] <= 0.0e0) back_ri1 = 0.0e0;
+    if (ri1 <= 0.0e0) { sm_back = 0.0e0; sh_back = 0.0e0; ss_back = 0.0e0; }
+    if ((sm_back < 0.0e0) || (sh_back < 0.0e0) || (ss_back < 0.0e0)) return;
+    const double tmp_back = 0.5e0 * b1 * b1 * back_ri1 * slq2_back * epson2;
+    v_back = tmp_back * sm_back;
+    t_back = tmp_back * sh_back;
+    s_back = tmp_back * ss_back;
+    if ((v_back < 0.0e0) || (t_back < 0.0e0) || (s_back < 0.0e0)) return;
+    if ((ri[k] > 0.0e0) && ((std::fabs(v_back) <= 0.0e0) || (std::fabs(t_back) <= 0.0e0) || (std::fabs(s_back) < 0.0e0)))
+      return;
+    if (ifbelow == 1) {
+      if (ri1 >= 0.0e0) {
+        tmp = 0.5e0 * b1 * b1 * ri1 * slq2 * epson2;
+      } else if (k >= 2) {
+        double delz, delrh, del2rh;
+        if (k == n - 1) {
+          delz = z[k] - z[k - 1]; delrh = rh[k] - rh[k - 1]; del2rh = rh[k] - 2.0e0 * rh[k - 1] + rh[k - 2];
+        } else {
+          delz = z[k + 1] - z[k - 1]; delrh = rh[k + 1] - rh[k - 1]; del2rh = rh[k + 1] - 2.0e0 * rh[k] + rh[k - 1];
+        }
+        const double dzrh = delrh / delz;
+        const double d2zrh = 4.0e0 * del2rh / (delz * delz);
+        const double rdzlndzrh = dzrh / d2zrh;
+        const double al0deep = 0.17e0 * std::fabs(rdzlndzrh);
+        const double akz2 = 0.4e0 * z[k];
+        const double aldeep = akz2 * al0deep / (al0deep + akz2);
+        al2 = aldeep * aldeep;
+        if (ifpureshear != 1) {
+          s2[k] = std::fmax(s2[k], s2min);
+          tmp = 0.5e0 * b1 * al2 * std::sqrt(s2[k] / (slq2 + 1.0e-40));
+        }
+      } else if (ifpureshear != 1) {
+        s2[k] = std::fmax(s2[k], s2min);
+        if (lifepsy) tmp = 0.5e0 * epsy / (s2[k] + 1.0e-40);
+        else tmp = 0.5e0 * b1 * al2 * std::sqrt(s2[k] / (slq2 + 1.0e-40));
+      }
+    } else if (ifpureshear != 1) {
+      s2[k] = std::fmax(s2[k], s2min);
+      if (lifepsy) tmp = 0.5e0 * epsy / (s2[k] + 1.0e-40);
+      else tmp = 0.5e0 * b1 * al2 * std::sqrt(s2[k] / (slq2 + 1.0e-40));
+    }
+    if (ifpureshear == 1) tmp = 0.5e0 * (b1 * b1) * al2 * std::sqrt(-an2[k] / amtaun2);
+    akm[k] = std::fmin(tmp * sm + v_back, fricmx);
+    akh[k] = std::fmin(tmp * sh + t_back, fricmx);
+    aks[k] = std::fmin(tmp * ss + s_back, fricmx);
+  }
+  for (int k = nb; k < nmax; k++) { akm[k] = 0.0e0; akh[k] = 0.0e0; aks[k] = 0.0e0; }
+  if (n > 0) {
+    if (akm[0] < wndmix) akm[0] = wndmix;
+    if (akh[0] < wndmix) akh[0] = wndmix;
+    if (aks[0] < wndmix) aks[0] = wndmix;
+  }
+}
+}  // namespace turb
+
+// turb_cu (readyc.cpp:1456-1612) with the memsets of readyc_ before it
+// (readyc.cpp:1642, 1647, 1668-1671): every column of the interior ring
+// (1 .. imt-2, 1 .. jmt-2) that has a wet top level
+void turb_call(Oracle& o, const lt_turb_tables& T, int ncc, double dfricmx) {
+  const int km = o.km, imt = o.imt, jmt = o.jmt;
+  const long A = o.A, F = o.F;
+  double* akmt = o.fd[LT_F_AKMT].data();
+  double* akt = o.fd[LT_F_AKT].data();
+  double* ak_tide = o.fd[LT_F_AK_TIDE].data();
+  double* amld = o.fd[LT_F_AMLD].data();
+  std::fill(o.fd[LT_F_AKMT].begin(), o.fd[LT_F_AKMT].end(), 0.0);
+  std::fill(o.fd[LT_F_AK_TIDE].begin(), o.fd[LT_F_AK_TIDE].end(), 0.0);
+  std::fill(o.fd[LT_F_AMLD].begin(), o.fd[LT_F_AMLD].end(), 0.0);
+  const double* at = o.fd[LT_F_AT].data();
+  const double* dzp = o.fd[LT_F_DZP].data();
+  const double* zkp = o.fd[LT_F_ZKP].data();
+  const double* pdensity = o.fd[LT_F_PDENSITY].data();
+  const double* rit = o.fd[LT_F_RIT].data();
+  const double* ricdttms = o.fd[LT_F_RICDTTMS].data();
+  const double* s2t = o.fd[LT_F_S2T].data();
+  const double* rict = o.fd[LT_F_RICT].data();
+  const double* fz_tide = o.fd[LT_F_FZ_TIDE].data();
+  const int* kmt = o.fi[LT_F_KMT].data();
+  const int d_ncc = ncc;
+  const double dwndmix = o.p.dwndmix;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int j = 1; j < jmt - 1; ++j) {
+    std::vector<double> wp1(km), wp3(km), wp7(km), wp8(km), wp4(km), wp5(km), wp6(km), wk1(km), wk2(km), wk3(km);
+    for (int i = 1; i < imt - 1; ++i) {
+      const long tid = (long)j * imt + i;
+      auto vit = [&](int k) { return k < kmt[tid] ? 1.0 : 0.0; };
+      if (!(vit(0) > 0.5)) continue;
+      const int iwk = kmt[tid] - 1;
+      for (int k = 0; k < km; k++) {
+        wp1[k] = wp3[k] = wp7[k] = wp8[k] = 0.0e0;
+        wp4[k] = wp5[k] = wp6[k] = 0.0e0;
+        wk1[k] = wk2[k] = wk3[k] = 0.0e0;
+      }
+      for (int k = 0; k < iwk; k++) {
+        wp8[k] = -vit(k + 1) * zkp[k + 1] * 1.0e+2;
+        wp1[k] = vit(k + 1) * (at[k * A + tid] - (at[k * A + tid] - at[(k + 1) * A + tid]) * dzp[k] / (dzp[k] + dzp[k + 1]));
+      }
+      for (int k = 0; k < iwk; k++) {
+        wp4[k] = vit(k + 1) * rit[k * A + tid];
+        wp5[k] = vit(k + 1) * ricdttms[k * A + tid];
+        wp6[k] = vit(k + 1) * s2t[k * A + tid];
+        wp7[k] = vit(k + 1) * rict[k * A + tid];
+        wp3[k] = vit(k + 1) * (pdensity[k * A + tid] + (pdensity[(k + 1) * A + tid] - pdensity[k * A + tid]) * dzp[k] /
+                                                          (dzp[k] + dzp[k + 1])) * 1.0e-3;
+      }
+      const double wp10 = vit(0) * o.fd[LT_F_BUOYTUR][tid] * 1.0e+4;
+      const double wp11 = vit(0) * o.fd[LT_F_BUOYSOL][tid] * 1.0e+4;
+      double mldtmp = 0.0;
+      turb::turb_device(wp8.data(), wp1.data(), wp3.data(), wp4.data(), wp5.data(), wp6.data(), dfricmx * 1.0e+4,
+                        dwndmix * 1.0e+4, wp7.data(), wp10, wp11, o.fd[LT_F_FCORT][tid], &mldtmp, wk1.data(),
+                        wk2.data(), wk3.data(), iwk, km - 1, T);
+      amld[tid] = mldtmp * 1.0e-2;
+      for (int k = 0; k < iwk; k++) {
+        ak_tide[k * A + tid] = turb::back_tidalmixing + turb::mixing_ef * turb::local_mixing_fraction *
+                                                            o.fd[LT_F_WAVE_DIS][tid] * fz_tide[k * A + tid] /
+                                                            (std::fmax(rict[k * A + tid], 1.0e-8) * (wp3[k] * 1000.0));
+        if (ak_tide[k * A + tid] > turb::max_tidalmixing) ak_tide[k * A + tid] = turb::max_tidalmixing;
+        o.fd[LT_F_RICHARDSON][k * A + tid] = rict[k * A + tid];
+        o.fd[LT_F_FZTIDAL][k * A + tid] = fz_tide[k * A + tid];
+        o.fd[LT_F_WP3_TIDAL][k * A + tid] = wp3[k];
+      }
+      for (int k = iwk - 2; k >= 0; k--) ak_tide[k * A + tid] = std::fmin(ak_tide[k * A + tid], ak_tide[(k + 1) * A + tid]);
+      for (int k = 0; k < km - 1; k++) {
+        akmt[k * A + tid] = wk1[k] * 1.0e-4 + ak_tide[k * A + tid] * 5.0;
+        akt[k * A + tid] = (wk2[k] * 1.0e-4 + ak_tide[k * A + tid]) / (float)d_ncc;
+        akt[F + k * A + tid] = (wk3[k] * 1.0e-4 + ak_tide[k * A + tid]) / (float)d_ncc;
+      }
+    }
+  }
+}
 }  // namespace
 
 extern "C" {
@@ -834,6 +1226,11 @@ int or_step(void* h, int nsteps) {
 }
 int or_convadj(void* h) {
   convadj_call(*static_cast<Oracle*>(h));
+  return 0;
+}
+int or_turb(void* h, const lt_turb_tables* t, int ncc, double dfricmx) {
+  if (!t || ncc < 1) return LT_E_INVALID;
+  turb_call(*static_cast<Oracle*>(h), *t, ncc, dfricmx);
   return 0;
 }
 int or_icesnow(void* h, const lt_icesnow_params* p) {

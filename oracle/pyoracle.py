@@ -14,12 +14,15 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liblicom_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_tracer.so")
+REF_TURB_LIB = os.path.join(HERE, "_ref", "libref_turb.so")
 
 FIELDS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "NET", "UTF_OUT", "VTF_OUT",
           "H0F_OUT", "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE",
           "DXU", "DYU", "AHF", "DTN", "DTS", "DTE", "DTW", "OHBT", "OHBU", "AU0", "AUS", "AUW", "AUSW", "KMT", "KMU",
           "KMTN", "KMTS", "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ",
-          "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE", "QICE"]
+          "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE", "QICE", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY",
+          "FZ_TIDE", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "ZKP", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON",
+          "FZTIDAL", "WP3_TIDAL"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 INT = {"KMT", "KMU", "KMTN", "KMTS", "KMTE", "KMTW"}
 
@@ -30,9 +33,14 @@ def shape_of(name, nx, ny, km):
         return (2, km, jmt, imt)
     if name == "ATB":
         return (2, km + 1, jmt, imt)
-    if name in ("UTF", "VTF", "UTL", "VTL", "UTF_OUT", "VTF_OUT", "PENETRATE"):
+    if name in ("UTF", "VTF", "UTL", "VTL", "UTF_OUT", "VTF_OUT", "PENETRATE", "FZ_TIDE", "AKMT", "AK_TIDE",
+                "RICHARDSON", "FZTIDAL", "WP3_TIDAL"):
         return (km, jmt, imt)
-    if name == "WS":
+    if name in ("RIT", "RICDTTMS", "S2T", "RICT"):
+        return (km - 1, jmt, imt)
+    if name == "ZKP":
+        return (km + 1,)
+    if name in ("WS", "PDENSITY"):
         return (km + 1, jmt, imt)
     if name == "NET":
         return (2, jmt, imt)
@@ -65,6 +73,7 @@ class Oracle:
         lib.or_set_threads.argtypes = [C.c_int]
         lib.or_set_sum_order.argtypes = [C.c_void_p, C.c_int]
         lib.or_icesnow.argtypes = [C.c_void_p, C.c_void_p]
+        lib.or_turb.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
         self.nx, self.ny, self.km = nx, ny, km
         self.h = C.c_void_p(lib.or_create(nx, ny, km))
         if not self.h:
@@ -104,6 +113,11 @@ class Oracle:
 
     def convadj(self):
         self.lib.or_convadj(self.h)
+
+    def turb(self, tables, ncc, dfricmx):
+        """tables: an lt_turb_tables structure (TurbTablesStruct)."""
+        if self.lib.or_turb(self.h, C.byref(tables), int(ncc), float(dfricmx)):
+            raise ValueError("oracle turb")
 
     def icesnow(self, params):
         """params: an object with the lt_icesnow_params layout (IcesnowParams)."""
@@ -180,3 +194,48 @@ class Reference:
 
     def fw_norm2(self):
         return self.lib.ref_fw_norm2()
+
+
+def reference_turb_available():
+    return os.path.exists(REF_TURB_LIB)
+
+
+class ReferenceTurb:
+    """The reference's own turb_cu (readyc.cpp) compiled for the CPU at its
+    built-in block size (imt=40, jmt=44, km=55)."""
+
+    NAMES = ("AT", "AKT", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY", "FZ_TIDE", "AKMT", "AK_TIDE", "RICHARDSON",
+             "FZTIDAL", "WP3_TIDAL", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "AMLD", "DZP", "ZKP", "KMT")
+
+    def __init__(self):
+        self.lib = lib = C.CDLL(REF_TURB_LIB)
+        lib.ref_turb_set.argtypes = [C.c_char_p, C.c_void_p, C.c_size_t]
+        lib.ref_turb_get.argtypes = [C.c_char_p, C.c_void_p, C.c_size_t]
+        lib.ref_turb_set_tables.argtypes = [C.c_void_p]
+        lib.ref_turb_call.argtypes = [C.c_int, C.c_double, C.c_double]
+        imt, jmt, km = C.c_int(), C.c_int(), C.c_int()
+        lib.ref_turb_dims(C.byref(imt), C.byref(jmt), C.byref(km))
+        self.nx, self.ny, self.km = imt.value - 4, jmt.value - 4, km.value
+
+    def set(self, name, a):
+        a = np.ascontiguousarray(a, dtype=_dtype(name))
+        if self.lib.ref_turb_set(name.encode(), a.ctypes.data, a.nbytes):
+            raise ValueError("reference turb set " + name)
+
+    def get(self, name):
+        a = np.empty(shape_of(name, self.nx, self.ny, self.km), dtype=_dtype(name))
+        if self.lib.ref_turb_get(name.encode(), a.ctypes.data, a.nbytes):
+            raise ValueError("reference turb get " + name)
+        return a
+
+    def load(self, inputs):
+        for n in self.NAMES:
+            if n in inputs:
+                self.set(n, inputs[n])
+
+    def set_tables(self, tables):
+        self._tables = tables          # the reference reads them where they lie
+        self.lib.ref_turb_set_tables(C.byref(tables))
+
+    def call(self, ncc, dfricmx, dwndmix):
+        self.lib.ref_turb_call(int(ncc), float(dfricmx), float(dwndmix))

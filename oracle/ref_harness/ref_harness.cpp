@@ -83,8 +83,11 @@ long field_count(int f) {
     case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV: return 2 * F;
     case LT_F_ATB: return 2 * FB;
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
-    case LT_F_PENETRATE: return F;
-    case LT_F_WS: return FB;
+    case LT_F_PENETRATE: case LT_F_FZ_TIDE: case LT_F_AKMT: case LT_F_AK_TIDE: case LT_F_RICHARDSON:
+    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL: return F;
+    case LT_F_RIT: case LT_F_RICDTTMS: case LT_F_S2T: case LT_F_RICT: return A * (R_KM - 1);
+    case LT_F_ZKP: return R_KM + 1;
+    case LT_F_WS: case LT_F_PDENSITY: return FB;
     case LT_F_NET: return 2 * A;
     case LT_F_DZP: case LT_F_ODZP: case LT_F_ODZT: case LT_F_PEN: case LT_F_TO: case LT_F_SO: return R_KM;
     case LT_F_C: return 9L * R_KM;

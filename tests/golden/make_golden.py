@@ -1,10 +1,13 @@
 """Generate tests/golden/reference_digests.json from the reference's own code.
 
-Runs LICOM3-HIP's tracer.cpp, convadj.cpp and icesnow.cpp, compiled for the
-CPU by oracle/Makefile (target ``ref``) from the reference tree, on seeded
+Runs LICOM3-HIP's tracer.cpp, convadj.cpp, icesnow.cpp and readyc.cpp
+(turb_cu), compiled for the CPU by oracle/Makefile (target ``ref``) from the
+reference tree, on seeded
 synthetic inputs at the reference's built-in block size (36 x 40 physical, 55
 levels) and records SHA-256 digests of every output field plus fw_norm2.  The
-icesnow cases start from the cold states of tests/icesnow_state.py.
+icesnow cases start from the cold states of tests/icesnow_state.py; the
+turbulence cases use the closure inputs and stand-in tables of
+tests/turb_case.py.
 
     make -C oracle ref && python tests/golden/make_golden.py
 """
@@ -22,6 +25,7 @@ import numpy as np  # noqa: E402
 from conftest import load_package  # noqa: E402
 import pyoracle  # noqa: E402
 from icesnow_state import ICE_CASES, cold_state  # noqa: E402
+from turb_case import DFRICMX, NCC, TURB_CASES, case, tables  # noqa: E402
 
 CASES = [(1, 5, 20240611), (0, 3, 7), (1, 2, 99)]
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
@@ -29,6 +33,7 @@ OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX",
 
 
 ICE_OUT = ["AT", "ATB", "QICE", "TEND", "DT_CONV", "WS", "NET"]
+TURB_OUT = ["AKT", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON", "FZTIDAL", "WP3_TIDAL"]
 
 
 def digest(a):
@@ -71,6 +76,17 @@ def main():
             "inputs": {"AT": digest(inp["AT"]), "QICE": digest(inp["QICE"])},
             "outputs": {n: digest(ref.get(n)) for n in ICE_OUT},
         }
+    if pyoracle.reference_turb_available():
+        for seed, forced in TURB_CASES:
+            syn, f = case(lt, seed, forced)
+            ref = pyoracle.ReferenceTurb()
+            ref.load(f)
+            ref.set_tables(lt.turb_tables_struct(tables(lt)))
+            ref.call(NCC, DFRICMX, syn.params.dwndmix)
+            out["turb_seed%d_forced%d" % (seed, forced)] = {
+                "inputs": {n: digest(f[n]) for n in ("RIT", "PDENSITY", "AT")},
+                "outputs": {n: digest(ref.get(n)) for n in TURB_OUT},
+            }
     with open(os.path.join(HERE, "reference_digests.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     print("wrote", len(out), "cases")
