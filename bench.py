@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-turb", action="store_true", help="skip the turbulence closure's timing")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: the mixed step as the headline, with the FP64 drop-in measured beside it")
     ap.add_argument("--grid", type=int, nargs=3, default=[3600, 2302, 55])
@@ -349,6 +350,42 @@ def measure(lt, args, pg, world, local, precision, keep_state):
             "steps_total": args.warmup + args.steps + 1 + e2e_steps, "icesnow": icesnow}
 
 
+def measure_turb(lt, args, precision):
+    """The Canuto closure (lt_turb) that produces the step's mixing, on a
+    720x460x55 patch of the bench configuration (its inputs are built on the
+    host; 1/25 of the 0.1-degree columns) with the stand-in closure tables:
+    device time per launch over 10 launches after 3 untimed ones."""
+    sys.path.insert(0, PKG_DIR)
+    import turb_synth
+    nx, ny, km = 720, 460, 55
+    w = workload(args)
+    syn = lt.Synth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+    f = {n: syn.field(n) for n in ("AT", "KMT", "DZP")}
+    inp = turb_synth.inputs(f["AT"], f["KMT"], f["DZP"], seed=3)
+    tab = lt.TurbTab(turb_synth.tables())
+    dom = syn.domain(precision=lt.PREC_MIXED if precision == "mixed" else lt.PREC_FP64)
+    for n, a in inp.items():
+        dom.set(n, a)
+    for _ in range(3):
+        dom.turb(tab, ncc=4, dfricmx=0.1)
+    dom.sync()
+    reps = 10
+    dom.mark(0)
+    for _ in range(reps):
+        dom.turb(tab, ncc=4, dfricmx=0.1)
+    dom.mark(1)
+    dom.sync()
+    ms = dom.last_step_ms() / reps
+    dom.close()
+    tab.close()
+    cells = nx * ny * km
+    full = args.grid[0] * args.grid[1] * args.grid[2]
+    return {"grid": "%dx%dx%d patch of the bench grid" % (nx, ny, km), "ms_per_launch": ms,
+            "cells_per_s": cells / (ms * 1e-3), "ms_scaled_to_bench_grid": ms * full / cells,
+            "bound": "fp64 arithmetic (table-index logarithms, atan, sin, cos, acosh, divisions)",
+            "tables": "stand-ins on the reference's table grids"}
+
+
 def run_ours(args):
     world, rank, local, pg = dist_setup(args)
     lt = load_package()
@@ -377,6 +414,8 @@ def run_ours(args):
                            "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"],
                 "clocks": r["clocks"], "fw_norm2": r["fw_norm2"], "icesnow": r["icesnow"]}
+        if not args.no_turb and world == 1:
+            line["turb"] = measure_turb(lt, args, main)
         if both:
             import numpy as np
             f = res["fp64"]

@@ -221,7 +221,7 @@ struct Iface {
   __device__ double z(int k) const { return -zkp[k + 1] * 1.0e+2; }
 };
 
-__global__ void __launch_bounds__(128) k_turb(Arena a, TurbTabDev T, double ncc_f, double fricmx, double wndmix) {
+__global__ void __launch_bounds__(128, 5) k_turb(Arena a, TurbTabDev T, double ncc_f, double fricmx, double wndmix) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= a.imt || j >= a.jmt) return;
