@@ -67,7 +67,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-turb", action="store_true", help="skip the turbulence closure's timing")
+    ap.add_argument("--no-turb", action="store_true",
+                    help="skip the timing of the turbulence closure and the momentum friction")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: the mixed step as the headline, with the FP64 drop-in measured beside it")
     ap.add_argument("--grid", type=int, nargs=3, default=[3600, 2302, 55])
@@ -350,11 +351,13 @@ def measure(lt, args, pg, world, local, precision, keep_state):
             "steps_total": args.warmup + args.steps + 1 + e2e_steps, "icesnow": icesnow}
 
 
-def measure_turb(lt, args, precision):
-    """The Canuto closure (lt_turb) that produces the step's mixing, on a
-    720x460x55 patch of the bench configuration (its inputs are built on the
-    host; 1/25 of the 0.1-degree columns) with the stand-in closure tables:
-    device time per launch over 10 launches after 3 untimed ones."""
+def measure_readyc(lt, args, precision):
+    """The kernels of the next rows on a 720x460x55 patch of the bench
+    configuration (their inputs are built on the host; 1/25 of the 0.1-degree
+    columns): the Canuto closure (lt_turb) that produces the step's mixing,
+    with the stand-in closure tables, and the momentum biharmonic friction
+    (lt_hdiffu_del4).  Device time per launch over 10 launches after 3
+    untimed ones."""
     sys.path.insert(0, PKG_DIR)
     import turb_synth
     nx, ny, km = 720, 460, 55
@@ -376,14 +379,40 @@ def measure_turb(lt, args, precision):
     dom.mark(1)
     dom.sync()
     ms = dom.last_step_ms() / reps
+    # the momentum biharmonic friction on the same patch (readyc.cpp:1754-1775)
+    import del4u_synth
+    fm = {n: syn.field(n) for n in ("HUN", "HUE", "HTW", "HTS", "DXU", "DYU", "TAREA_R", "KMU")}
+    mom = del4u_synth.coefficients(fm)
+    mom.update(del4u_synth.velocities(fm["KMU"], km, seed=3))
+    for n, a in mom.items():
+        dom.set(n, a)
+    am = 4.0 * syn.params.ah
+    for _ in range(3):
+        dom.hdiffu_del4(am, 2.6e-3)
+    dom.sync()
+    dom.mark(0)
+    for _ in range(reps):
+        dom.hdiffu_del4(am, 2.6e-3)
+    dom.mark(1)
+    dom.sync()
+    ms_d = dom.last_step_ms() / reps
     dom.close()
     tab.close()
     cells = nx * ny * km
     full = args.grid[0] * args.grid[1] * args.grid[2]
-    return {"grid": "%dx%dx%d patch of the bench grid" % (nx, ny, km), "ms_per_launch": ms,
+    hbm, hbm_kind = peaks()
+    # per cell: up, vp read (16), dlu, dlv read and written (32), the drag
+    # speed written (8); the 2-D coefficients are shared by the levels
+    d_bytes = 56.0 * cells
+    turb = {"grid": "%dx%dx%d patch of the bench grid" % (nx, ny, km), "ms_per_launch": ms,
             "cells_per_s": cells / (ms * 1e-3), "ms_scaled_to_bench_grid": ms * full / cells,
             "bound": "fp64 arithmetic (table-index logarithms, atan, sin, cos, acosh, divisions)",
             "tables": "stand-ins on the reference's table grids"}
+    del4u = {"grid": turb["grid"], "ms_per_launch": ms_d, "cells_per_s": cells / (ms_d * 1e-3),
+             "ms_scaled_to_bench_grid": ms_d * full / cells, "algorithmic_bytes_per_launch": d_bytes,
+             "achieved_gbs": d_bytes / (ms_d * 1e-3) / 1e9, "frac": d_bytes / (ms_d * 1e-3) / 1e9 / hbm,
+             "peak_kind": hbm_kind}
+    return turb, del4u
 
 
 def run_ours(args):
@@ -415,7 +444,7 @@ def run_ours(args):
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"],
                 "clocks": r["clocks"], "fw_norm2": r["fw_norm2"], "icesnow": r["icesnow"]}
         if not args.no_turb and world == 1:
-            line["turb"] = measure_turb(lt, args, main)
+            line["turb"], line["hdiffu_del4"] = measure_readyc(lt, args, main)
         if both:
             import numpy as np
             f = res["fp64"]

@@ -88,6 +88,14 @@ typedef enum {
   LT_F_AK_TIDE,                     /* [km][jmt][imt] tidal mixing (output) */
   LT_F_AMLD,                        /* [jmt][imt] mixed-layer depth (output, m) */
   LT_F_RICHARDSON, LT_F_FZTIDAL, LT_F_WP3_TIDAL,  /* [km][jmt][imt] tidal diagnostics (output) */
+  /* momentum biharmonic friction (lt_hdiffu_del4), f64; allocated on first use */
+  LT_F_UP, LT_F_VP,                 /* [km][jmt][imt] velocities at U points (dyn_mod up, vp) */
+  LT_F_DLU, LT_F_DLV,               /* [km][jmt][imt] momentum tendencies, accumulated into */
+  LT_F_WKA_DRAG,                    /* [km][jmt][imt] c0f*|u| left in the reference's wka (output) */
+  LT_F_DUC, LT_F_DUM, LT_F_DUN, LT_F_DUS, LT_F_DUE, LT_F_DUW,  /* [jmt][imt] del4 stencil (init_del4u) */
+  LT_F_DMC, LT_F_DMN, LT_F_DMS, LT_F_DME, LT_F_DMW,
+  LT_F_AMF,                         /* [jmt][imt] resolution factor of the viscosity */
+  LT_F_UAREA_R, LT_F_DXUR, LT_F_DYUR,  /* [jmt][imt] U-cell metrics */
   LT_F_COUNT
 } lt_field;
 
@@ -232,6 +240,22 @@ typedef struct {
  * level, the background S l/q where Ri <= 0 before any Ri > 0); they start at
  * zero here. */
 int lt_turb(lt_domain* dom, const lt_turb_tab* tab, const lt_turb_params* p);
+
+/* --- momentum biharmonic friction (readyc.cpp:343-577) -------------------- */
+typedef struct {
+  double am;             /* hmix_del4 am (AM_BIHAR) */
+  double c0f;            /* pconst_mod c0f (bottom drag coefficient) */
+} lt_del4u_params;
+/* The biharmonic friction of UP, VP with the flow-dependent factor (readyc_'s
+ * BIHAR sequence, readyc.cpp:1754-1775: hdel4_div, hdel4_grad, hdel4_zcurl,
+ * hdel4_grad, hdiffu_del4_0, hdiffu_del4_1) for a domain that is one block
+ * (ib = jb = 3, ie = imt-2, je = jmt-2 in the reference's 1-based block
+ * bounds): DLU and DLV are increased by it over i in 1..imt-2, j in 1..jmt-2
+ * and WKA_DRAG = c0f*sqrt(up^2 + vp^2) everywhere.  Reads DXU, DYU, HTW, HTS,
+ * TAREA_R, KMT, KMU of the domain and the momentum fields above.  One fused
+ * kernel per 32x8 tile and level; FP64 with the reference's operation order,
+ * bit-identical to it.  Asynchronous on the domain's stream. */
+int lt_hdiffu_del4(lt_domain* dom, const lt_del4u_params* p);
 /* Global tracer integrals sum(tarea*dzp*vit*tracer) over the interior, f64,
  * fixed-order pairwise tree (deterministic). out2[0] = T, out2[1] = S. */
 int lt_tracer_content(lt_domain* dom, double* out2);
@@ -297,9 +321,10 @@ const char* lt_field_name(int field);
 long lt_field_count(int field, int nx, int ny, int km);
 /* 1 for the int32 mask fields, 0 for f64 fields. */
 int lt_field_is_int(int field);
-/* 1 for the turbulence closure's fields (LT_F_RIT .. LT_F_WP3_TIDAL), which a
- * domain allocates on first use. */
-int lt_field_is_turb(int field);
+/* 1 for the turbulence closure's fields (LT_F_RIT .. LT_F_WP3_TIDAL) and the
+ * momentum friction's fields (LT_F_UP .. LT_F_DYUR), which a domain allocates
+ * on the first use of a field of each group. */
+int lt_field_on_demand(int field);
 
 /* --- errors, device ------------------------------------------------------ */
 const char* lt_last_error(void);

@@ -76,6 +76,10 @@ def turb_tables_struct(t):
     return st
 
 
+class Del4uParams(C.Structure):
+    _fields_ = [("am", C.c_double), ("c0f", C.c_double)]
+
+
 class TurbParams(C.Structure):
     _fields_ = [("ncc", C.c_int), ("dfricmx", C.c_double)]
 
@@ -140,6 +144,7 @@ _SIGS = {
     "lt_turb_tables_create": ([C.POINTER(TurbTablesStruct), C.POINTER(_vp)], _i),
     "lt_turb_tables_destroy": ([_vp], _i),
     "lt_turb": ([_vp, _vp, C.POINTER(TurbParams)], _i),
+    "lt_hdiffu_del4": ([_vp, C.POINTER(Del4uParams)], _i),
     "lt_tracer_content": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_fw_norm2": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_sync": ([_vp], _i),
@@ -155,7 +160,7 @@ _SIGS = {
     "lt_field_name": ([_i], C.c_char_p),
     "lt_field_count": ([_i, _i, _i, _i], C.c_long),
     "lt_field_is_int": ([_i], _i),
-    "lt_field_is_turb": ([_i], _i),
+    "lt_field_on_demand": ([_i], _i),
     "lt_synth_defaults": ([C.POINTER(SynthConfig)], None),
     "lt_synth_build": ([C.POINTER(SynthConfig), C.POINTER(_vp)], _i),
     "lt_synth_free": ([_vp], _i),
@@ -204,9 +209,11 @@ INT_FIELDS = {n for n in FIELDS if lib.lt_field_is_int(FIELD_ID[n])}
 # they start at zero)
 INPUT_FIELDS = [n for n in FIELDS if n not in (
     "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE")
-    and not lib.lt_field_is_turb(FIELD_ID[n])]
-# the turbulence closure's fields (allocated by a domain on first use)
-TURB_FIELDS = [n for n in FIELDS if lib.lt_field_is_turb(FIELD_ID[n])]
+    and not lib.lt_field_on_demand(FIELD_ID[n])]
+# fields a domain allocates on first use: the turbulence closure's and the
+# momentum friction's
+TURB_FIELDS = FIELDS[FIELD_ID["RIT"]:FIELD_ID["WP3_TIDAL"] + 1]
+MOM_FIELDS = FIELDS[FIELD_ID["UP"]:FIELD_ID["DYUR"] + 1]
 
 
 def _check(rc, where):
@@ -346,6 +353,12 @@ class TracerDomain:
         AK_TIDE, AMLD and the tidal diagnostics."""
         prm = TurbParams(int(ncc), float(dfricmx))
         _check(lib.lt_turb(self.h, tab.h, C.byref(prm)), "lt_turb")
+
+    def hdiffu_del4(self, am, c0f):
+        """Momentum biharmonic friction (readyc.cpp:343-577): DLU, DLV += the
+        friction of UP, VP; WKA_DRAG = c0f*|u|."""
+        prm = Del4uParams(float(am), float(c0f))
+        _check(lib.lt_hdiffu_del4(self.h, C.byref(prm)), "lt_hdiffu_del4")
 
     def icesnow(self, params=None):
         """Sea-ice adjustment of the current state (icesnow.cpp:15-85);

@@ -31,6 +31,7 @@ CU_UNITS = {
     "lt_batch.cu": [],
     "lt_serve.cu": [],
     "lt_turb.cu": ["-fmad=false"],
+    "lt_del4u.cu": ["-fmad=false"],
 }
 CPP_UNITS = ["lt_synth_api.cpp"]
 

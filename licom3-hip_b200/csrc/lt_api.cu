@@ -139,6 +139,26 @@ void* field_ptr(lt_domain* d, int f, int which_state) {
     case LT_F_RICHARDSON: return a.richardson;
     case LT_F_FZTIDAL: return a.fztidal;
     case LT_F_WP3_TIDAL: return a.wp3_tidal;
+    case LT_F_UP: return a.up;
+    case LT_F_VP: return a.vp;
+    case LT_F_DLU: return a.dlu;
+    case LT_F_DLV: return a.dlv;
+    case LT_F_WKA_DRAG: return a.wka_drag;
+    case LT_F_DUC: return a.duc;
+    case LT_F_DUM: return a.dum;
+    case LT_F_DUN: return a.dun;
+    case LT_F_DUS: return a.dus;
+    case LT_F_DUE: return a.due;
+    case LT_F_DUW: return a.duw;
+    case LT_F_DMC: return a.dmc;
+    case LT_F_DMN: return a.dmn;
+    case LT_F_DMS: return a.dms;
+    case LT_F_DME: return a.dme;
+    case LT_F_DMW: return a.dmw;
+    case LT_F_AMF: return a.amf;
+    case LT_F_UAREA_R: return a.uarea_r;
+    case LT_F_DXUR: return a.dxur;
+    case LT_F_DYUR: return a.dyur;
   }
   return nullptr;
 }
@@ -339,6 +359,31 @@ int ensure_turb(lt_domain* d) {
   LT_CUDA_OK(cudaMemsetAsync(base, 0, pl.off, d->stream));
   return LT_OK;
 }
+// The momentum friction's fields: one zeroed allocation on first use.
+int ensure_mom(lt_domain* d) {
+  Arena& a = d->a;
+  if (a.up) return LT_OK;
+  double** f3[] = {&a.up, &a.vp, &a.dlu, &a.dlv, &a.wka_drag};
+  double** f2[] = {&a.duc, &a.dum, &a.dun, &a.dus, &a.due, &a.duw, &a.dmc, &a.dmn,
+                   &a.dms, &a.dme, &a.dmw, &a.amf, &a.uarea_r, &a.dxur, &a.dyur};
+  Plan pl;
+  for (auto p : f3) pl.add(reinterpret_cast<void**>(p), sizeof(double) * a.F);
+  for (auto p : f2) pl.add(reinterpret_cast<void**>(p), sizeof(double) * a.A);
+  char* base = nullptr;
+  cudaError_t e = cudaMalloc(&base, pl.off);
+  if (e != cudaSuccess) {
+    set_error("momentum fields: cudaMalloc(%zu) failed: %s", pl.off, cudaGetErrorString(e));
+    return LT_E_OOM;
+  }
+  d->allocations.push_back(base);
+  size_t off = 0;
+  for (auto& it : pl.items) {
+    *it.first = base + off;
+    off += (it.second + 255) / 256 * 256;
+  }
+  LT_CUDA_OK(cudaMemsetAsync(base, 0, pl.off, d->stream));
+  return LT_OK;
+}
 }  // namespace lt
 
 using namespace lt;
@@ -354,7 +399,8 @@ static const char* const k_field_names[LT_F_COUNT] = {
     "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND",
     "DT_DIFF", "DT_CONV", "PENETRATE", "QICE", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY", "FZ_TIDE",
     "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "ZKP", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON", "FZTIDAL",
-    "WP3_TIDAL"};
+    "WP3_TIDAL", "UP", "VP", "DLU", "DLV", "WKA_DRAG", "DUC", "DUM", "DUN", "DUS", "DUE", "DUW", "DMC", "DMN",
+    "DMS", "DME", "DMW", "AMF", "UAREA_R", "DXUR", "DYUR"};
 
 const char* lt_field_name(int f) { return (f >= 0 && f < LT_F_COUNT) ? k_field_names[f] : nullptr; }
 long lt_field_count(int f, int nx, int ny, int km) {
@@ -362,7 +408,9 @@ long lt_field_count(int f, int nx, int ny, int km) {
   return lt::field_count(f, nx + 4, ny + 4, km);
 }
 int lt_field_is_int(int f) { return (f >= 0 && f < LT_F_COUNT) ? (int)lt::field_is_int(f) : 0; }
-int lt_field_is_turb(int f) { return (f >= 0 && f < LT_F_COUNT) ? (int)lt::field_is_turb(f) : 0; }
+int lt_field_on_demand(int f) {
+  return (f >= 0 && f < LT_F_COUNT) ? (int)(lt::field_is_turb(f) || lt::field_is_mom(f)) : 0;
+}
 
 const char* lt_version(void) { return "licom3-hip_b200 tracer 0.1 (sm_100a)"; }
 
@@ -507,8 +555,8 @@ int lt_set_params(lt_domain* d, const lt_params* p) {
 
 static int xfer(lt_domain* d, int f, void* ptr, size_t nbytes, cudaMemcpyKind kind, bool set) {
   if (!d || !ptr || f < 0 || f >= LT_F_COUNT) { set_error("bad field transfer"); return LT_E_INVALID; }
-  if (lt::field_is_turb(f)) {
-    const int rc = lt::ensure_turb(d);
+  if (lt::field_is_turb(f) || lt::field_is_mom(f)) {
+    const int rc = lt::field_is_turb(f) ? lt::ensure_turb(d) : lt::ensure_mom(d);
     if (rc) return rc;
   }
   const size_t need = lt::field_bytes(f, d->a.imt, d->a.jmt, d->a.km);

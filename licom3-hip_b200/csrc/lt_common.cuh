@@ -46,6 +46,9 @@ struct Arena {
   // first uses one of them
   double *rit, *ricdttms, *s2t, *rict, *pdensity, *fz_tide, *buoytur, *buoysol, *fcort, *wave_dis, *zkp;
   double *akmt, *ak_tide, *amld, *richardson, *fztidal, *wp3_tidal;
+  // momentum biharmonic friction (lt_hdiffu_del4), null until first used
+  double *up, *vp, *dlu, *dlv, *wka_drag;
+  double *duc, *dum, *dun, *dus, *due, *duw, *dmc, *dmn, *dms, *dme, *dmw, *amf, *uarea_r, *dxur, *dyur;
   // diagnostics (null when off)
   double *ax, *ay, *az, *dzd, *tend, *dt_diff, *dt_conv, *penetrate;
 
@@ -109,6 +112,7 @@ int launch_tracer_content(const Arena& a, cudaStream_t s);
 int launch_convadj(const Arena& a, cudaStream_t s);
 int launch_icesnow(const Arena& a, const lt_icesnow_params& p, cudaStream_t s);
 int launch_turb(const Arena& a, const TurbTabDev& T, int ncc, double dfricmx, cudaStream_t s);
+int launch_del4u(const Arena& a, double am, double c0f, cudaStream_t s);
 int launch_check_numeric(const Arena& a, cudaStream_t s);
 int launch_derive_masks(const Arena& a, cudaStream_t s);
 int launch_vtl_clobber(const Arena& a, cudaStream_t s);

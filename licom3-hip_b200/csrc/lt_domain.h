@@ -31,6 +31,8 @@ int run_step(lt_domain* d);
 // after the stream has drained: LT_E_TIMEOUT once if a column kernel's
 // bounded wait ran out since the last check
 int timeout_status(lt_domain* d);
-// allocate the turbulence closure's fields of a domain if not yet done
+// allocate the turbulence closure's / momentum friction's fields of a domain
+// if not yet done
 int ensure_turb(lt_domain* d);
+int ensure_mom(lt_domain* d);
 }  // namespace lt

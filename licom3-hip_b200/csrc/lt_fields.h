@@ -26,7 +26,8 @@ inline int field_shape(int f) {
     case LT_F_ATB: return SH_TRACERB;
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
     case LT_F_PENETRATE: case LT_F_FZ_TIDE: case LT_F_AKMT: case LT_F_AK_TIDE: case LT_F_RICHARDSON:
-    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL:
+    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL: case LT_F_UP: case LT_F_VP: case LT_F_DLU: case LT_F_DLV:
+    case LT_F_WKA_DRAG:
       return SH_LEVEL3;
     case LT_F_RIT: case LT_F_RICDTTMS: case LT_F_S2T: case LT_F_RICT: return SH_LEVEL3M1;
     case LT_F_ZKP: return SH_COL1P;
@@ -43,8 +44,10 @@ inline int field_shape(int f) {
 
 inline bool field_is_int(int f) { return field_shape(f) == SH_MASK2; }
 
-// fields of the turbulence closure, allocated with the domain's first use of any of them
+// fields of the turbulence closure and of the momentum friction, each group
+// allocated with the domain's first use of any of its fields
 inline bool field_is_turb(int f) { return f >= LT_F_RIT && f <= LT_F_WP3_TIDAL; }
+inline bool field_is_mom(int f) { return f >= LT_F_UP && f <= LT_F_DYUR; }
 
 inline long field_count(int f, int imt, int jmt, int km) {
   const long A = (long)imt * jmt;

@@ -15,6 +15,8 @@
 //                                   POP_BlocksMod.F90:284-375
 //   convective adjustment           convadj.cpp:29-288
 //   sea-ice adjustment              icesnow.cpp:15-85
+//   momentum biharmonic friction    readyc.cpp:343-577, 1754-1775 (hdel4_div,
+//                                   hdel4_grad, hdel4_zcurl, hdiffu_del4_0/1)
 //   Canuto turbulence closure       readyc.cpp:880-1612 (turb_cu, turb_device,
 //                                   interp1d_expabs, interp2d_expabs, formld,
 //                                   eplatidepend_fun), TIDEMIX configuration
@@ -50,7 +52,8 @@ FieldInfo field_info(int f) {
     case LT_F_ATB: return {KB3N, false};
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
     case LT_F_PENETRATE: case LT_F_FZ_TIDE: case LT_F_AKMT: case LT_F_AK_TIDE: case LT_F_RICHARDSON:
-    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL:
+    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL: case LT_F_UP: case LT_F_VP: case LT_F_DLU: case LT_F_DLV:
+    case LT_F_WKA_DRAG:
       return {K3, false};
     case LT_F_RIT: case LT_F_RICDTTMS: case LT_F_S2T: case LT_F_RICT: return {K3M1, false};
     case LT_F_ZKP: return {K1P, false};
@@ -1161,6 +1164,120 @@ void turb_call(Oracle& o, const lt_turb_tables& T, int ncc, double dfricmx) {
     }
   }
 }
+
+// readyc_'s BIHAR sequence (readyc.cpp:1754-1775) kernel by kernel over the
+// whole domain, one block (ib = jb = 3, ie = imt-2, je = jmt-2)
+void del4u_call(Oracle& o, double am, double c0f) {
+  const int km = o.km, imt = o.imt, jmt = o.jmt;
+  const long A = o.A, F = o.F;
+  const int ib = 3, jb = 3, ie = imt - 2, je = jmt - 2;
+  const double p5 = 0.5;
+  const double* up = o.fd[LT_F_UP].data();
+  const double* vp = o.fd[LT_F_VP].data();
+  double* dlu = o.fd[LT_F_DLU].data();
+  double* dlv = o.fd[LT_F_DLV].data();
+  double* wkad = o.fd[LT_F_WKA_DRAG].data();
+  const int* kmt = o.fi[LT_F_KMT].data();
+  const int* kmu = o.fi[LT_F_KMU].data();
+  const double *htw = o.fd[LT_F_HTW].data(), *hts = o.fd[LT_F_HTS].data(), *tarea_r = o.fd[LT_F_TAREA_R].data();
+  const double *dxu = o.fd[LT_F_DXU].data(), *dyu = o.fd[LT_F_DYU].data();
+  const double *dxur = o.fd[LT_F_DXUR].data(), *dyur = o.fd[LT_F_DYUR].data(), *uarea_r = o.fd[LT_F_UAREA_R].data();
+  const double *duc = o.fd[LT_F_DUC].data(), *dum = o.fd[LT_F_DUM].data(), *dun = o.fd[LT_F_DUN].data();
+  const double *dus = o.fd[LT_F_DUS].data(), *due = o.fd[LT_F_DUE].data(), *duw = o.fd[LT_F_DUW].data();
+  const double *dmc = o.fd[LT_F_DMC].data(), *dmn = o.fd[LT_F_DMN].data(), *dms = o.fd[LT_F_DMS].data();
+  const double *dme = o.fd[LT_F_DME].data(), *dmw = o.fd[LT_F_DMW].data(), *amf = o.fd[LT_F_AMF].data();
+  std::vector<double> wka(F), am_factor(F, 0.0), hduk2(F), hdvk2(F), d2uk(F), d2vk(F);
+  auto grad = [&]() {   // hdel4_grad (readyc.cpp:405-442)
+    for (int k = 0; k < km; ++k)
+      for (int j = 0; j < jmt; ++j)
+        for (int i = 0; i < imt; ++i) {
+          double gradx = 0.0, grady = 0.0;
+          const long c = k * A + (long)j * imt + i;
+          if ((1 <= i) && (j < jmt - 1) && k <= kmu[j * imt + i] - 1) {
+            gradx = dxur[j * imt + i] * p5 * (wka[c + imt] - wka[c - 1] - wka[c + imt - 1] + wka[c]);
+            grady = dyur[j * imt + i] * p5 * (wka[c + imt] - wka[c - 1] + wka[c + imt - 1] - wka[c]);
+          }
+          am_factor[c] += gradx * gradx + grady * grady;
+        }
+  };
+  // hdel4_div (readyc.cpp:372-403)
+  for (int k = 0; k < km; ++k)
+    for (int j = 0; j < jmt; ++j)
+      for (int i = 0; i < imt; ++i) {
+        const long t = (long)j * imt + i, c = k * A + t;
+        wka[c] = 0.0e0;
+        if (i < imt - 1 && j >= 1 && k <= kmt[t] - 1)
+          wka[c] = 0.5 * ((up[c + 1] + up[c - imt + 1]) * htw[t + 1] - (up[c] + up[c - imt]) * htw[t] +
+                          (vp[c + 1] + vp[c]) * hts[t] - (vp[c - imt + 1] + vp[c - imt]) * hts[t - imt]) *
+                   tarea_r[t];
+      }
+  grad();
+  // hdel4_zcurl (readyc.cpp:343-370)
+  for (int k = 0; k < km; ++k)
+    for (int j = 0; j < jmt; ++j)
+      for (int i = 0; i < imt; ++i) {
+        const long t = (long)j * imt + i, c = k * A + t;
+        wka[c] = 0.0e0;
+        if (i >= 1 && j >= 1 && k <= kmt[t] - 1)
+          wka[c] = 0.5 * ((vp[c] * dyu[t] + vp[c - imt] * dyu[t - imt] - vp[c - 1] * dyu[t - 1] -
+                           vp[c - imt - 1] * dyu[t - imt - 1] - up[c] * dxu[t] - up[c - 1] * dxu[t - 1] +
+                           up[c - imt] * dxu[t - imt] + up[c - imt - 1] * dxu[t - imt - 1]));
+      }
+  grad();
+  // hdiffu_del4_0 (readyc.cpp:444-507)
+  for (int k = 0; k < km; ++k)
+    for (int j = 0; j < jmt; ++j)
+      for (int i = 0; i < imt; ++i) {
+        const long t = (long)j * imt + i, c = k * A + t;
+        double am_f = 1.0e0;
+        hduk2[c] = 0.0;
+        hdvk2[c] = 0.0;
+        if (j >= jb - 2 && j <= je && i >= ib - 2 && i <= ie && k <= kmu[t] - 1) {
+          const double t_area = std::sqrt(1.0e0 / uarea_r[t]);
+          const double dxdy = t_area * t_area * t_area * t_area * t_area * 45.0e0;
+          am_f = std::sqrt(am_factor[c]) * dxdy / std::fabs(am * amf[t]);
+          am_f = std::fmin(40.0e0, am_f);
+          am_f = std::fmax(1.0e0, am_f);
+          hduk2[c] = (((duc[t] + dum[t]) * up[c] + dun[t] * up[c - imt] + dus[t] * up[c + imt] + due[t] * up[c + 1] +
+                       duw[t] * up[c - 1]) +
+                      (dmc[t] * vp[c] + dmn[t] * vp[c - imt] + dms[t] * vp[c + imt] + dme[t] * vp[c + 1] +
+                       dmw[t] * vp[c - 1]));
+          hdvk2[c] = (((duc[t] + dum[t]) * vp[c] + dun[t] * vp[c - imt] + dus[t] * vp[c + imt] + due[t] * vp[c + 1] +
+                       duw[t] * vp[c - 1]) -
+                      (dmc[t] * up[c] + dmn[t] * up[c - imt] + dms[t] * up[c + imt] + dme[t] * up[c + 1] +
+                       dmw[t] * up[c - 1]));
+        }
+        d2uk[c] = am_f * amf[t] * hduk2[c];
+        d2vk[c] = am_f * amf[t] * hdvk2[c];
+      }
+  // hdiffu_del4_1 (readyc.cpp:509-577)
+  for (int k = 0; k < km; ++k)
+    for (int j = 0; j < jmt; ++j)
+      for (int i = 0; i < imt; ++i) {
+        const long t = (long)j * imt + i, c = k * A + t;
+        hduk2[c] = 0.0;
+        hdvk2[c] = 0.0;
+        if (j >= jb - 1 && j < je && i >= ib - 1 && i < ie) {
+          hduk2[c] = am * (((duc[t] + dum[t]) * d2uk[c] + dun[t] * d2uk[c - imt] + dus[t] * d2uk[c + imt] +
+                            due[t] * d2uk[c + 1] + duw[t] * d2uk[c - 1]) +
+                           (dmc[t] * d2vk[c] + dmn[t] * d2vk[c - imt] + dms[t] * d2vk[c + imt] + dme[t] * d2vk[c + 1] +
+                            dmw[t] * d2vk[c - 1]));
+          hdvk2[c] = am * (((duc[t] + dum[t]) * d2vk[c] + dun[t] * d2vk[c - imt] + dus[t] * d2vk[c + imt] +
+                            due[t] * d2vk[c + 1] + duw[t] * d2vk[c - 1]) -
+                           (dmc[t] * d2uk[c] + dmn[t] * d2uk[c - imt] + dms[t] * d2uk[c + imt] + dme[t] * d2uk[c + 1] +
+                            dmw[t] * d2uk[c - 1]));
+        }
+        if (k > kmu[t] - 1) {
+          hduk2[c] = 0.0;
+          hdvk2[c] = 0.0;
+        }
+        if (1 <= j && j < jmt - 1 && 1 <= i && i < imt - 1) {
+          dlv[c] = dlv[c] + hdvk2[c];
+          dlu[c] = dlu[c] + hduk2[c];
+        }
+        wkad[c] = c0f * std::sqrt(up[c] * up[c] + vp[c] * vp[c]);
+      }
+}
 }  // namespace
 
 extern "C" {
@@ -1231,6 +1348,10 @@ int or_convadj(void* h) {
 int or_turb(void* h, const lt_turb_tables* t, int ncc, double dfricmx) {
   if (!t || ncc < 1) return LT_E_INVALID;
   turb_call(*static_cast<Oracle*>(h), *t, ncc, dfricmx);
+  return 0;
+}
+int or_hdiffu_del4(void* h, double am, double c0f) {
+  del4u_call(*static_cast<Oracle*>(h), am, c0f);
   return 0;
 }
 int or_icesnow(void* h, const lt_icesnow_params* p) {

@@ -14,7 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liblicom_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_tracer.so")
-REF_TURB_LIB = os.path.join(HERE, "_ref", "libref_turb.so")
+REF_READYC_LIB = os.path.join(HERE, "_ref", "libref_readyc.so")
 
 FIELDS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "NET", "UTF_OUT", "VTF_OUT",
           "H0F_OUT", "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE",
@@ -22,7 +22,8 @@ FIELDS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "N
           "KMTN", "KMTS", "KMTE", "KMTW", "DZP", "ODZP", "ODZT", "PEN", "TO", "SO", "C", "RESTORE", "AX", "AY", "AZ",
           "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE", "QICE", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY",
           "FZ_TIDE", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "ZKP", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON",
-          "FZTIDAL", "WP3_TIDAL"]
+          "FZTIDAL", "WP3_TIDAL", "UP", "VP", "DLU", "DLV", "WKA_DRAG", "DUC", "DUM", "DUN", "DUS", "DUE", "DUW",
+          "DMC", "DMN", "DMS", "DME", "DMW", "AMF", "UAREA_R", "DXUR", "DYUR"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 INT = {"KMT", "KMU", "KMTN", "KMTS", "KMTE", "KMTW"}
 
@@ -34,7 +35,7 @@ def shape_of(name, nx, ny, km):
     if name == "ATB":
         return (2, km + 1, jmt, imt)
     if name in ("UTF", "VTF", "UTL", "VTL", "UTF_OUT", "VTF_OUT", "PENETRATE", "FZ_TIDE", "AKMT", "AK_TIDE",
-                "RICHARDSON", "FZTIDAL", "WP3_TIDAL"):
+                "RICHARDSON", "FZTIDAL", "WP3_TIDAL", "UP", "VP", "DLU", "DLV", "WKA_DRAG"):
         return (km, jmt, imt)
     if name in ("RIT", "RICDTTMS", "S2T", "RICT"):
         return (km - 1, jmt, imt)
@@ -74,6 +75,7 @@ class Oracle:
         lib.or_set_sum_order.argtypes = [C.c_void_p, C.c_int]
         lib.or_icesnow.argtypes = [C.c_void_p, C.c_void_p]
         lib.or_turb.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
+        lib.or_hdiffu_del4.argtypes = [C.c_void_p, C.c_double, C.c_double]
         self.nx, self.ny, self.km = nx, ny, km
         self.h = C.c_void_p(lib.or_create(nx, ny, km))
         if not self.h:
@@ -118,6 +120,10 @@ class Oracle:
         """tables: an lt_turb_tables structure (TurbTablesStruct)."""
         if self.lib.or_turb(self.h, C.byref(tables), int(ncc), float(dfricmx)):
             raise ValueError("oracle turb")
+
+    def hdiffu_del4(self, am, c0f):
+        if self.lib.or_hdiffu_del4(self.h, float(am), float(c0f)):
+            raise ValueError("oracle hdiffu_del4")
 
     def icesnow(self, params):
         """params: an object with the lt_icesnow_params layout (IcesnowParams)."""
@@ -196,23 +202,27 @@ class Reference:
         return self.lib.ref_fw_norm2()
 
 
-def reference_turb_available():
-    return os.path.exists(REF_TURB_LIB)
+def reference_readyc_available():
+    return os.path.exists(REF_READYC_LIB)
 
 
-class ReferenceTurb:
-    """The reference's own turb_cu (readyc.cpp) compiled for the CPU at its
-    built-in block size (imt=40, jmt=44, km=55)."""
+class ReferenceReadyc:
+    """Kernels of the reference's own readyc.cpp (turb_cu and the momentum
+    biharmonic friction) compiled for the CPU at its built-in block size
+    (imt=40, jmt=44, km=55)."""
 
     NAMES = ("AT", "AKT", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY", "FZ_TIDE", "AKMT", "AK_TIDE", "RICHARDSON",
-             "FZTIDAL", "WP3_TIDAL", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "AMLD", "DZP", "ZKP", "KMT")
+             "FZTIDAL", "WP3_TIDAL", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "AMLD", "DZP", "ZKP", "KMT", "KMU",
+             "UP", "VP", "DLU", "DLV", "WKA_DRAG", "HTW", "HTS", "TAREA_R", "DXU", "DYU", "DXUR", "DYUR", "UAREA_R",
+             "DUC", "DUM", "DUN", "DUS", "DUE", "DUW", "DMC", "DMN", "DMS", "DME", "DMW", "AMF")
 
     def __init__(self):
-        self.lib = lib = C.CDLL(REF_TURB_LIB)
+        self.lib = lib = C.CDLL(REF_READYC_LIB)
         lib.ref_turb_set.argtypes = [C.c_char_p, C.c_void_p, C.c_size_t]
         lib.ref_turb_get.argtypes = [C.c_char_p, C.c_void_p, C.c_size_t]
         lib.ref_turb_set_tables.argtypes = [C.c_void_p]
         lib.ref_turb_call.argtypes = [C.c_int, C.c_double, C.c_double]
+        lib.ref_del4u_call.argtypes = [C.c_double, C.c_double]
         imt, jmt, km = C.c_int(), C.c_int(), C.c_int()
         lib.ref_turb_dims(C.byref(imt), C.byref(jmt), C.byref(km))
         self.nx, self.ny, self.km = imt.value - 4, jmt.value - 4, km.value
@@ -238,4 +248,9 @@ class ReferenceTurb:
         self.lib.ref_turb_set_tables(C.byref(tables))
 
     def call(self, ncc, dfricmx, dwndmix):
+        """turb_cu with readyc_'s memsets before it."""
         self.lib.ref_turb_call(int(ncc), float(dfricmx), float(dwndmix))
+
+    def del4u(self, am, c0f):
+        """readyc_'s momentum biharmonic friction sequence."""
+        self.lib.ref_del4u_call(float(am), float(c0f))

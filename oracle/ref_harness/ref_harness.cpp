@@ -84,7 +84,8 @@ long field_count(int f) {
     case LT_F_ATB: return 2 * FB;
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
     case LT_F_PENETRATE: case LT_F_FZ_TIDE: case LT_F_AKMT: case LT_F_AK_TIDE: case LT_F_RICHARDSON:
-    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL: return F;
+    case LT_F_FZTIDAL: case LT_F_WP3_TIDAL: case LT_F_UP: case LT_F_VP: case LT_F_DLU: case LT_F_DLV:
+    case LT_F_WKA_DRAG: return F;
     case LT_F_RIT: case LT_F_RICDTTMS: case LT_F_S2T: case LT_F_RICT: return A * (R_KM - 1);
     case LT_F_ZKP: return R_KM + 1;
     case LT_F_WS: case LT_F_PDENSITY: return FB;

@@ -1,15 +1,17 @@
-// ref_turb.cpp - host-side harness that runs the reference's own turb_cu
-// (readyc.cpp, compiled from its place in the reference tree with the CPU HIP
+// ref_readyc.cpp - host-side harness that runs kernels of the reference's own
+// readyc.cpp (compiled from its place in the reference tree with the CPU HIP
 // stand-in in oracle/ref_harness/hip) on one block of the reference's built-in
-// size (imt = 40, jmt = 44, km = 55).  TEST INFRASTRUCTURE ONLY: builds
-// oracle/_ref/libref_turb.so, used by tests to pin the oracle's restatement of
-// the turbulence closure against the reference's own code.
+// size (imt = 40, jmt = 44, km = 55): the turbulence closure turb_cu and the
+// momentum biharmonic friction (hdel4_div, hdel4_grad, hdel4_zcurl,
+// hdiffu_del4_0, hdiffu_del4_1).  TEST INFRASTRUCTURE ONLY: builds
+// oracle/_ref/libref_readyc.so, used by tests to pin the oracle's
+// restatements against the reference's own code.
 //
 // readyc.cpp refers to many device pointers and module variables of the
-// model; this file defines every one of them (those turb_cu does not read stay
-// null), fills the ones turb_cu reads from host arrays, does the memsets
-// readyc_ does before it (readyc.cpp:1642, 1647, 1668-1671) and launches
-// turb_cu with the reference's grid.
+// model; this file defines every one of them (those the two sequences do not
+// read stay null), fills the ones they read from host arrays, does the
+// memsets readyc_ does before them (readyc.cpp:1642, 1647, 1668-1671, 1757)
+// and launches the kernels with the reference's grids.
 #include <cstring>
 #include <string>
 #include <vector>
@@ -48,12 +50,25 @@ void turb_cu(double* d_akmt, double* d_akt, double* d_ak_tide, double* d_amld, d
              double* d_sm_r1, double* d_ssa1, double* d_ssb, double* d_ss_r1, double* d_turb_param, double* d_vit,
              double* d_wave_dis, double* d_wp3_tidal, double* d_zkp, int* d_irimax, int* d_kmt, double* d_diff_back,
              double* d_wk1, double* d_wk2, double* d_wk3, double* d_wp1, double* d_wp3, double* d_wp7, double* d_wp8);
+void hdel4_div(double* d_hts, double* d_htw, double* d_tarea_r, double* d_up, double* d_vp, double* d_wka, int* d_kmt);
+void hdel4_grad(double* d_wka, double* d_dxur, double* d_dyur, int* d_kmu, double* d_am_factor);
+void hdel4_zcurl(double* d_dxu, double* d_dyu, double* d_up, double* d_vp, double* d_wka, int* d_kmt);
+void hdiffu_del4_0(double* d_hduk2, double* d_hdvk2, int d_jb, int d_je, int d_ib, int d_ie, double* d_uarea_r,
+                   double d_c0f, double* d_up, double* d_vp, double* d_duc, double* d_dum, double* d_dun, double* d_dus,
+                   double* d_due, double* d_duw, double* d_dmc, double* d_dmn, double* d_dms, double* d_dme,
+                   double* d_dmw, double d_am, double* d_dlu, double* d_dlv, double* d_viv, int* d_kmu,
+                   double* d_amf, double* d_am_factor, double* d_d2uk, double* d_d2vk);
+void hdiffu_del4_1(double* d_hduk2, double* d_hdvk2, int d_jb, int d_je, int d_ib, int d_ie, double* d_wka,
+                   double d_c0f, double* d_up, double* d_vp, double* d_duc, double* d_dum, double* d_dun, double* d_dus,
+                   double* d_due, double* d_duw, double* d_dmc, double* d_dmn, double* d_dms, double* d_dme,
+                   double* d_dmw, double d_am, double* d_dlu, double* d_dlv, double* d_viv, int* d_kmu,
+                   double* d_amf, double* d_am_factor, double* d_d2uk, double* d_d2vk);
 
 namespace {
 const long A = (long)R_IMT * R_JMT, F = A * R_KM;
 struct Arr { double** p; long n; };
 std::vector<std::vector<double>> keep;
-std::vector<int> kmt_store;
+std::vector<int> kmt_store, kmu_store;
 std::vector<int> irimax_store;
 double turb_param[11];
 bool ready = false;
@@ -67,6 +82,11 @@ long count_of(const std::string& n) {
   if (n == "BUOYTUR" || n == "BUOYSOL" || n == "FCORT" || n == "WAVE_DIS" || n == "AMLD") return A;
   if (n == "DZP") return R_KM;
   if (n == "ZKP") return R_KM + 1;
+  if (n == "UP" || n == "VP" || n == "DLU" || n == "DLV" || n == "WKA_DRAG") return F;
+  if (n == "HTW" || n == "HTS" || n == "TAREA_R" || n == "DXU" || n == "DYU" || n == "DXUR" || n == "DYUR" ||
+      n == "UAREA_R" || n == "DUC" || n == "DUM" || n == "DUN" || n == "DUS" || n == "DUE" || n == "DUW" ||
+      n == "DMC" || n == "DMN" || n == "DMS" || n == "DME" || n == "DMW" || n == "AMF")
+    return A;
   return -1;
 }
 double** slot_of(const std::string& n) {
@@ -90,6 +110,31 @@ double** slot_of(const std::string& n) {
   if (n == "AMLD") return &d_amld;
   if (n == "DZP") return &d_dzp;
   if (n == "ZKP") return &d_zkp;
+  if (n == "UP") return &d_up;
+  if (n == "VP") return &d_vp;
+  if (n == "DLU") return &d_dlu;
+  if (n == "DLV") return &d_dlv;
+  if (n == "WKA_DRAG") return &d_wka;
+  if (n == "HTW") return &d_htw;
+  if (n == "HTS") return &d_hts;
+  if (n == "TAREA_R") return &d_tarea_r;
+  if (n == "DXU") return &d_dxu;
+  if (n == "DYU") return &d_dyu;
+  if (n == "DXUR") return &d_dxur;
+  if (n == "DYUR") return &d_dyur;
+  if (n == "UAREA_R") return &d_uarea_r;
+  if (n == "DUC") return &d_duc;
+  if (n == "DUM") return &d_dum;
+  if (n == "DUN") return &d_dun;
+  if (n == "DUS") return &d_dus;
+  if (n == "DUE") return &d_due;
+  if (n == "DUW") return &d_duw;
+  if (n == "DMC") return &d_dmc;
+  if (n == "DMN") return &d_dmn;
+  if (n == "DMS") return &d_dms;
+  if (n == "DME") return &d_dme;
+  if (n == "DMW") return &d_dmw;
+  if (n == "AMF") return &d_amf;
   return nullptr;
 }
 double* fresh(long n) { keep.emplace_back(n, 0.0); return keep.back().data(); }
@@ -97,10 +142,15 @@ void setup() {
   if (ready) return;
   const char* names[] = {"AT", "AKT", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY", "FZ_TIDE", "AKMT", "AK_TIDE",
                          "RICHARDSON", "FZTIDAL", "WP3_TIDAL", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "AMLD",
-                         "DZP", "ZKP"};
+                         "DZP", "ZKP", "UP", "VP", "DLU", "DLV", "WKA_DRAG", "HTW", "HTS", "TAREA_R", "DXU",
+                         "DYU", "DXUR", "DYUR", "UAREA_R", "DUC", "DUM", "DUN", "DUS", "DUE", "DUW", "DMC", "DMN",
+                         "DMS", "DME", "DMW", "AMF"};
   for (const char* n : names) *slot_of(n) = fresh(count_of(n));
   kmt_store.assign(A, 0);
   d_kmt = kmt_store.data();
+  kmu_store.assign(A, 0);
+  d_kmu = kmu_store.data();
+  d_am_factor = fresh(F); d_d2uk = fresh(F); d_d2vk = fresh(F); d_hduk2 = fresh(F); d_hdvk2 = fresh(F);
   d_vit = fresh(F);
   d_wk1 = fresh(F); d_wk2 = fresh(F); d_wk3 = fresh(F);
   d_wp1 = fresh(F); d_wp3 = fresh(F); d_wp7 = fresh(F); d_wp8 = fresh(F);
@@ -121,9 +171,9 @@ int ref_turb_dims(int* imt, int* jmt, int* km) {
 int ref_turb_set(const char* name, const void* src, size_t nbytes) {
   setup();
   const std::string n(name);
-  if (n == "KMT") {
+  if (n == "KMT" || n == "KMU") {
     if (nbytes != sizeof(int) * A) return LT_E_INVALID;
-    std::memcpy(kmt_store.data(), src, nbytes);
+    std::memcpy(n == "KMT" ? kmt_store.data() : kmu_store.data(), src, nbytes);
     return 0;
   }
   const long c = count_of(n);
@@ -175,6 +225,26 @@ int ref_turb_call(int ncc, double dfricmx, double dwndmix) {
                      d_ricdttms, d_richardson, d_rict, d_rit, d_s2t, d_sha1, d_shb, d_sh_r1, d_slq2b, d_slq2_r1,
                      d_sma1, d_smb, d_sm_r1, d_ssa1, d_ssb, d_ss_r1, d_turb_param, d_vit, d_wave_dis, d_wp3_tidal,
                      d_zkp, d_irimax, d_kmt, d_diff_back, d_wk1, d_wk2, d_wk3, d_wp1, d_wp3, d_wp7, d_wp8);
+  return 0;
+}
+
+// readyc_'s BIHAR sequence (readyc.cpp:1754-1775) for one block covering the
+// domain (Fortran block bounds ib = jb = 3, ie = imt-2, je = jmt-2)
+int ref_del4u_call(double am, double c0f) {
+  setup();
+  const int jb = 3, je = R_JMT - 2, ib = 3, ie = R_IMT - 2;
+  dim3 block(8, 16, 4), grid((R_IMT + 7) / 8, (R_JMT + 15) / 16, (R_KM + 3) / 4);
+  hipLaunchKernelGGL(hdel4_div, grid, block, 0, 0, d_hts, d_htw, d_tarea_r, d_up, d_vp, d_wka, d_kmt);
+  hipMemset(d_am_factor, 0, dataSize3d);
+  hipLaunchKernelGGL(hdel4_grad, grid, block, 0, 0, d_wka, d_dxur, d_dyur, d_kmu, d_am_factor);
+  hipLaunchKernelGGL(hdel4_zcurl, grid, block, 0, 0, d_dxu, d_dyu, d_up, d_vp, d_wka, d_kmt);
+  hipLaunchKernelGGL(hdel4_grad, grid, block, 0, 0, d_wka, d_dxur, d_dyur, d_kmu, d_am_factor);
+  hipLaunchKernelGGL(hdiffu_del4_0, grid, block, 0, 0, d_hduk2, d_hdvk2, jb, je, ib, ie, d_uarea_r, c0f, d_up, d_vp,
+                     d_duc, d_dum, d_dun, d_dus, d_due, d_duw, d_dmc, d_dmn, d_dms, d_dme, d_dmw, am, d_dlu, d_dlv,
+                     d_viv, d_kmu, d_amf, d_am_factor, d_d2uk, d_d2vk);
+  hipLaunchKernelGGL(hdiffu_del4_1, grid, block, 0, 0, d_hduk2, d_hdvk2, jb, je, ib, ie, d_wka, c0f, d_up, d_vp,
+                     d_duc, d_dum, d_dun, d_dus, d_due, d_duw, d_dmc, d_dmn, d_dms, d_dme, d_dmw, am, d_dlu, d_dlv,
+                     d_viv, d_kmu, d_amf, d_am_factor, d_d2uk, d_d2vk);
   return 0;
 }
 

@@ -1,7 +1,7 @@
 """Generate tests/golden/reference_digests.json from the reference's own code.
 
 Runs LICOM3-HIP's tracer.cpp, convadj.cpp, icesnow.cpp and readyc.cpp
-(turb_cu), compiled for the CPU by oracle/Makefile (target ``ref``) from the
+(turb_cu and the momentum biharmonic friction), compiled for the CPU by oracle/Makefile (target ``ref``) from the
 reference tree, on seeded
 synthetic inputs at the reference's built-in block size (36 x 40 physical, 55
 levels) and records SHA-256 digests of every output field plus fw_norm2.  The
@@ -26,6 +26,7 @@ from conftest import load_package  # noqa: E402
 import pyoracle  # noqa: E402
 from icesnow_state import ICE_CASES, cold_state  # noqa: E402
 from turb_case import DFRICMX, NCC, TURB_CASES, case, tables  # noqa: E402
+import del4u_case  # noqa: E402
 
 CASES = [(1, 5, 20240611), (0, 3, 7), (1, 2, 99)]
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
@@ -76,16 +77,26 @@ def main():
             "inputs": {"AT": digest(inp["AT"]), "QICE": digest(inp["QICE"])},
             "outputs": {n: digest(ref.get(n)) for n in ICE_OUT},
         }
-    if pyoracle.reference_turb_available():
+    if pyoracle.reference_readyc_available():
         for seed, forced in TURB_CASES:
             syn, f = case(lt, seed, forced)
-            ref = pyoracle.ReferenceTurb()
+            ref = pyoracle.ReferenceReadyc()
             ref.load(f)
             ref.set_tables(lt.turb_tables_struct(tables(lt)))
             ref.call(NCC, DFRICMX, syn.params.dwndmix)
             out["turb_seed%d_forced%d" % (seed, forced)] = {
                 "inputs": {n: digest(f[n]) for n in ("RIT", "PDENSITY", "AT")},
                 "outputs": {n: digest(ref.get(n)) for n in TURB_OUT},
+            }
+    if pyoracle.reference_readyc_available():
+        for seed, cap in del4u_case.DEL4U_CASES:
+            syn, f, am = del4u_case.case(lt, seed, cap)
+            ref = pyoracle.ReferenceReadyc()
+            ref.load(f)
+            ref.del4u(am, del4u_case.C0F)
+            out["del4u_seed%d_cap%d" % (seed, cap)] = {
+                "inputs": {n: digest(f[n]) for n in ("UP", "DUC", "DMS")},
+                "outputs": {n: digest(ref.get(n)) for n in ("DLU", "DLV", "WKA_DRAG")},
             }
     with open(os.path.join(HERE, "reference_digests.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)

@@ -38,11 +38,11 @@ def run_oracle(lt, syn, f):
     return o
 
 
-@pytest.mark.skipif(not pyoracle.reference_turb_available(), reason="reference tree not built here")
+@pytest.mark.skipif(not pyoracle.reference_readyc_available(), reason="reference tree not built here")
 @pytest.mark.parametrize("seed,forced", TURB_CASES)
 def test_turb_oracle_bitexact_vs_reference(lt, seed, forced):
     syn, f = case(lt, seed, forced)
-    ref = pyoracle.ReferenceTurb()
+    ref = pyoracle.ReferenceReadyc()
     ref.load(f)
     ref.set_tables(lt.turb_tables_struct(tables(lt)))
     ref.call(NCC, DFRICMX, syn.params.dwndmix)
