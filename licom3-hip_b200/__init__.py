@@ -80,6 +80,48 @@ class Del4uParams(C.Structure):
     _fields_ = [("am", C.c_double), ("c0f", C.c_double)]
 
 
+class RestartStruct(C.Structure):
+    """lt_restart: host pointers to the restart file's fields."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("km", C.c_int)] + [
+        (n, C.c_void_p) for n in ("h0", "u", "v", "t", "s", "ws", "su", "sv", "swv", "sshf", "lthf", "fresh")] + [
+        ("number_month", C.c_int), ("number_day", C.c_int)]
+
+
+RESTART_2D = ("h0", "su", "sv", "swv", "sshf", "lthf", "fresh")
+RESTART_3D = ("u", "v", "t", "s", "ws")
+
+
+def _restart_struct(nx, ny, km, arrays, month=0, day=0):
+    st = RestartStruct()
+    st.nx, st.ny, st.km = nx, ny, km
+    keep = []
+    for n in RESTART_2D + RESTART_3D:
+        a = arrays.get(n)
+        if a is not None:
+            shape = (ny, nx) if n in RESTART_2D else (km, ny, nx)
+            assert a.shape == shape and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"], n
+            setattr(st, n, a.ctypes.data)
+            keep.append(a)
+    st.number_month, st.number_day = month, day
+    return st, keep
+
+
+def restart_write(path, nx, ny, km, arrays, month=0, day=0):
+    """Write the reference's restart file (include/licom_restart.h) from a
+    dict of host arrays; missing fields are written as zeros."""
+    st, _keep = _restart_struct(nx, ny, km, arrays, month, day)
+    _check(lib.lt_restart_write(os.fsencode(path), C.byref(st)), "lt_restart_write")
+
+
+def restart_read(path, nx, ny, km):
+    """Read a restart file: (dict of arrays, number_month, number_day)."""
+    arrays = {n: np.empty((ny, nx)) for n in RESTART_2D}
+    arrays.update({n: np.empty((km, ny, nx)) for n in RESTART_3D})
+    st, _keep = _restart_struct(nx, ny, km, arrays)
+    _check(lib.lt_restart_read(os.fsencode(path), C.byref(st)), "lt_restart_read")
+    return arrays, st.number_month, st.number_day
+
+
 class TurbParams(C.Structure):
     _fields_ = [("ncc", C.c_int), ("dfricmx", C.c_double)]
 
@@ -145,6 +187,10 @@ _SIGS = {
     "lt_turb_tables_destroy": ([_vp], _i),
     "lt_turb": ([_vp, _vp, C.POINTER(TurbParams)], _i),
     "lt_hdiffu_del4": ([_vp, C.POINTER(Del4uParams)], _i),
+    "lt_restart_write": ([C.c_char_p, C.POINTER(RestartStruct)], _i),
+    "lt_restart_read": ([C.c_char_p, C.POINTER(RestartStruct)], _i),
+    "lt_domain_save_restart": ([_vp, C.c_char_p, C.POINTER(RestartStruct)], _i),
+    "lt_domain_load_restart": ([_vp, C.c_char_p, C.POINTER(RestartStruct)], _i),
     "lt_tracer_content": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_fw_norm2": ([_vp, C.POINTER(C.c_double)], _i),
     "lt_sync": ([_vp], _i),
@@ -359,6 +405,21 @@ class TracerDomain:
         friction of UP, VP; WKA_DRAG = c0f*|u|."""
         prm = Del4uParams(float(am), float(c0f))
         _check(lib.lt_hdiffu_del4(self.h, C.byref(prm)), "lt_hdiffu_del4")
+
+    def save_restart(self, path, extra=None, month=0, day=0):
+        """Write the domain's state as the reference's restart file; extra:
+        dict of host arrays for u, v, su, sv, sshf, lthf (missing: zeros)."""
+        st, _keep = _restart_struct(self.nx, self.ny, self.km, extra or {}, month, day)
+        _check(lib.lt_domain_save_restart(self.h, os.fsencode(path), C.byref(st)), "lt_domain_save_restart")
+
+    def load_restart(self, path):
+        """Set AT (and ATB, H0F as NEXTSTEP does) from a restart file; returns
+        (u, v, number_month, number_day)."""
+        u = np.empty((self.km, self.ny, self.nx))
+        v = np.empty((self.km, self.ny, self.nx))
+        st, _keep = _restart_struct(self.nx, self.ny, self.km, {"u": u, "v": v})
+        _check(lib.lt_domain_load_restart(self.h, os.fsencode(path), C.byref(st)), "lt_domain_load_restart")
+        return u, v, st.number_month, st.number_day
 
     def icesnow(self, params=None):
         """Sea-ice adjustment of the current state (icesnow.cpp:15-85);

@@ -32,6 +32,7 @@ CU_UNITS = {
     "lt_serve.cu": [],
     "lt_turb.cu": ["-fmad=false"],
     "lt_del4u.cu": ["-fmad=false"],
+    "lt_restart.cu": [],
 }
 CPP_UNITS = ["lt_synth_api.cpp"]
 

@@ -13,7 +13,7 @@ import pyoracle
 
 def declared_functions():
     names = set()
-    for h in ("licom_tracer.h", "licom_synth.h"):
+    for h in sorted(f for f in os.listdir(os.path.join(REPO, "include")) if f.endswith(".h")):
         text = open(os.path.join(REPO, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_]*\s*\*?\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(", text,
