@@ -1,9 +1,12 @@
 """A domain's state through the reference's restart file: saved from one
-domain and loaded into another, the state (T and S with the domain's halo
-and fold, ATB = AT as NEXTSTEP sets it, h0) comes back bit for bit, and the
-fields the reference masks over land are zero there."""
+domain and loaded into another, T and S come back bit for bit with the
+domain's halo and fold, ATB = AT as NEXTSTEP sets it, h0 as the reference's
+reader leaves it (the file's interior after its halo update), and the fields
+the reference's writer masks over land are zero there."""
 import numpy as np
 import pytest
+
+import pyoracle
 
 pytestmark = pytest.mark.gpu
 
@@ -30,10 +33,18 @@ def test_save_load_round_trip(lt, tmp_path, precision):
     assert np.array_equal(dst.get("AT"), at)
     atb = dst.get("ATB")
     assert np.array_equal(atb[:, 1:], at)
-    h0 = src.get("H0F")[2:-2, 2:-2]
-    assert np.array_equal(dst.get("H0F")[2:-2, 2:-2], h0)
-    # what the file holds: the masks of the reference's writer
+    # h0: the file holds the interior; loading applies the halo update the
+    # reference applies after reading (POP_HaloUpdate, fill 0), which on a
+    # tripole grid also averages the top row with its mirror
     arr, _, _ = lt.restart_read(p, nx, ny, km)
+    h0 = src.get("H0F")
+    assert np.array_equal(arr["h0"], h0[2:-2, 2:-2])
+    want = np.zeros_like(h0)
+    want[2:-2, 2:-2] = arr["h0"]
+    o = pyoracle.Oracle(nx, ny, km, syn.params)
+    want = o.halo(want, ew_cyclic=syn.cfg.ew_cyclic, tripole=syn.cfg.tripole)
+    assert np.array_equal(dst.get("H0F"), want)
+    # what the file holds: the masks of the reference's writer
     kmu = syn.field("KMU")[2:-2, 2:-2]
     kmt = syn.field("KMT")[2:-2, 2:-2]
     assert not arr["su"][kmu < 1].any() and np.array_equal(arr["su"][kmu >= 1], su[kmu >= 1])
