@@ -27,7 +27,7 @@ typedef struct lt_batch lt_batch;
 
 /* Launch shape of a batch step (what the autotuner chooses). */
 typedef struct {
-  int column_ctas_per_sm;   /* persistent CTAs of the column kernel per SM: 1..5 (mixed) */
+  int column_ctas_per_sm;   /* persistent CTAs of the column kernel per SM: 1..3 (mixed) */
   int continuity_tile_y;    /* rows of a continuity tile (32 x 4, 8 or 16 columns) */
   int use_graph;            /* 1: replay captured CUDA graphs, 0: launch directly */
 } lt_batch_config;

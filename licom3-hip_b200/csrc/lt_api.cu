@@ -214,7 +214,9 @@ void plan_arena(Arena& a, Plan& pl) {
     D(&a.dt_conv, 2 * F);  // convadj writes it
     D(&a.tend, 2 * F);     // convadj accumulates into it
   }
-  D(&a.col_scratch, (size_t)a.col_scratch_slots * km * a.nv_scratch * TTHREADS);
+  // the Thomas sweep's per-level coefficients of each resident CTA
+  const size_t cta_threads = a.precision == LT_PREC_MIXED ? kMixedThreads : TTHREADS;
+  D(&a.col_scratch, (size_t)a.col_scratch_slots * km * a.nv_scratch * cta_threads);
 }
 
 void init_arena_dims(Arena& a, const lt_grid* g, const lt_params* p) {
@@ -230,8 +232,9 @@ void init_arena_dims(Arena& a, const lt_grid* g, const lt_params* p) {
 }
 
 long slots_for(const Arena& a, int sms) {
-  const long ntiles = (long)((a.imt + TX - 1) / TX) * ((a.jmt + TY - 1) / TY);
-  long s = (long)sms * kMixedCtasPerSm;
+  const int ty = a.precision == LT_PREC_MIXED ? kMixedTileY : TY;
+  const long ntiles = (long)((a.imt + TX - 1) / TX) * ((a.jmt + ty - 1) / ty);
+  long s = (long)sms * (a.precision == LT_PREC_MIXED ? kMixedCtasPerSm : kFp64CtasPerSm);
   if (s > 2 * ntiles) s = 2 * ntiles;
   return s;
 }
@@ -261,19 +264,20 @@ bool make_tensor_map_3d(CUtensorMap* map, const void* base, int esize, long nx, 
 
 bool build_tracer_maps(const Arena& a, TracerMaps* m) {
   const long imt = a.imt, jmt = a.jmt, km = a.km;
+  const bool mx = a.precision == LT_PREC_MIXED;
+  const int ty = mx ? kMixedTileY : TY;   // tile rows of the column kernel
   bool ok = true;
   for (int b = 0; b < 2; ++b) {
-    ok = ok && make_tensor_map_3d(&m->at[b], a.at[b], 8, imt, jmt, 2 * km, SW, TY + 4);
-    ok = ok && make_tensor_map_3d(&m->atb[b], a.atb[b], 8, imt, jmt, 2 * (km + 1), SW, TY + 4);
+    ok = ok && make_tensor_map_3d(&m->at[b], a.at[b], 8, imt, jmt, 2 * km, SW, ty + 4);
+    ok = ok && make_tensor_map_3d(&m->atb[b], a.atb[b], 8, imt, jmt, 2 * (km + 1), SW, ty + 4);
   }
-  const bool mx = a.precision == LT_PREC_MIXED;
   const int es = mx ? 4 : 8;
-  ok = ok && make_tensor_map_3d(&m->ws, mx ? (const void*)a.ws32 : a.ws, es, imt, jmt, km + 1, SW, TY + 2);
+  ok = ok && make_tensor_map_3d(&m->ws, mx ? (const void*)a.ws32 : a.ws, es, imt, jmt, km + 1, SW, ty + 2);
   // f64: face transports u_wface (rows y0-1..) and v_sface (rows y0-2..);
   // mixed: the U-point means wkd, wkb (rows y0-2..), faces formed in the kernel
-  ok = ok && make_tensor_map_3d(&m->uw, mx ? (const void*)a.wkd32 : a.uwf, es, imt, jmt, km, SW, mx ? TY + 3 : TY + 2);
-  ok = ok && make_tensor_map_3d(&m->vs, mx ? (const void*)a.wkb32 : a.vsf, es, imt, jmt, km, SW, TY + 3);
-  ok = ok && make_tensor_map_3d(&m->akt, mx ? (const void*)a.akt32 : a.akt, es, imt, jmt, 2 * km, TX, TY);
+  ok = ok && make_tensor_map_3d(&m->uw, mx ? (const void*)a.wkd32 : a.uwf, es, imt, jmt, km, SW, mx ? ty + 3 : ty + 2);
+  ok = ok && make_tensor_map_3d(&m->vs, mx ? (const void*)a.wkb32 : a.vsf, es, imt, jmt, km, SW, ty + 3);
+  ok = ok && make_tensor_map_3d(&m->akt, mx ? (const void*)a.akt32 : a.akt, es, imt, jmt, 2 * km, TX, ty);
   return ok;
 }
 

@@ -73,7 +73,7 @@ int build_descriptors(lt_batch* b) {
     lt_domain* d = b->m[i];
     const Arena& a = d->a;
     const int ntx = (a.imt + TX - 1) / TX;
-    const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
+    const long ntiles = (long)ntx * ((a.jmt + kMixedTileY - 1) / kMixedTileY);
     b->base_cur[i] = a.cur;
     for (int p = 0; p < 2; ++p) {
       MemberDesc& e = h[p][i];
@@ -245,7 +245,7 @@ int lt_batch_create(lt_domain* const* members, int n, lt_batch** out) {
     return fail(LT_E_CUDA);
   if ((rc = build_descriptors(b))) return fail(rc);
   if (b->mixed) {
-    const size_t bytes = sizeof(double) * (size_t)b->sms * kMixedCtasPerSm * b->km_max * 2 * TTHREADS;
+    const size_t bytes = sizeof(double) * (size_t)b->sms * kMixedCtasPerSm * b->km_max * 2 * kMixedThreads;
     if (cudaMalloc(&b->scratch, bytes) != cudaSuccess) {
       set_error("lt_batch_create: cudaMalloc(%zu) for the column scratch failed", bytes);
       return fail(LT_E_OOM);
@@ -344,7 +344,7 @@ int lt_batch_autotune(lt_batch* b, int trial_steps, lt_batch_config* chosen) {
   }
   std::vector<lt_batch_config> cands;
   if (b->mixed) {
-    for (int ctas : {3, 4, 5})
+    for (int ctas : {1, 2, 3})
       for (int ty : {4, 8, 16}) cands.push_back({ctas, ty, 1});
   } else {
     cands.push_back({b->cfg.column_ctas_per_sm, b->cfg.continuity_tile_y, 1});

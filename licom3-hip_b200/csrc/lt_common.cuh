@@ -14,9 +14,12 @@ constexpr int TX = 32;
 constexpr int TY = 4;
 constexpr int TTHREADS = TX * TY;
 // Persistent CTAs per SM of the column kernels (their shared-memory footprint
-// decides): FP64 4, mixed 5.
+// decides): FP64 4 of 128 threads, mixed 3 of 256.
 constexpr int kFp64CtasPerSm = 4;
-constexpr int kMixedCtasPerSm = 5;
+constexpr int kMixedCtasPerSm = 3;
+// The mixed column kernel's tile: TX x kMixedTileY columns, one thread each.
+constexpr int kMixedTileY = 8;
+constexpr int kMixedThreads = TX * kMixedTileY;
 
 // Everything the step kernels touch, as raw device pointers (dense
 // [n][k][j][i] layout of the reference, i fastest).

@@ -237,43 +237,50 @@ int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s) {
 namespace {
 
 // ------------------------------------------------------------ column march
+// Tile of the mixed march: TX x MY columns, one thread per column.  Taller
+// than the FP64 kernel's 32 x 4 tile: the 1-cell halo the predictor, the first
+// Laplacian and the faces are computed on grows less than the tile.
+constexpr int MY = kMixedTileY;
+constexpr int MTH = kMixedThreads;
+constexpr int MHQY = MY + 2;          // tile plus 1-cell halo, rows
+constexpr int MHN = HQX * MHQY;
 // Level slots.  Step k (the march runs downward) reads levels k-2, k-1 and
 // k only, so at the end of step k the slot of level k takes level k-3: three
 // slots keep one step of lead time for every box.
 constexpr int NSM = 3;
-constexpr int FXN = (TY + 2) * (TX + 3);   // x faces of the 1-halo region
-constexpr int FYN = (TY + 3) * (TX + 2);   // y faces of the 1-halo region
+constexpr int FXN = (MY + 2) * (TX + 3);   // x faces of the 1-halo region
+constexpr int FYN = (MY + 3) * (TX + 2);   // y faces of the 1-halo region
 
 // One level of the column tile, filled by five TMA boxes (the mixing
 // coefficient of the own column comes by plain loads, a step ahead).  The f32 fields
 // are w and the U-point means wkd, wkb from which the kernel forms the face
 // transports (face32, face_x64, face_y64).
 struct alignas(128) MxSlot {
-  alignas(128) double at[(TY + 4) * SW];   // rows y0-2 .. y0+TY+1
-  alignas(128) double atb[(TY + 4) * SW];  // tracer level L of the previous time level
-  alignas(128) float ws[(TY + 2) * SW];    // rows y0-1 .. y0+TY
-  alignas(128) float wkd[(TY + 3) * SW];   // rows y0-2 .. y0+TY
-  alignas(128) float wkb[(TY + 3) * SW];   // rows y0-2 .. y0+TY
+  alignas(128) double at[(MY + 4) * SW];   // rows y0-2 .. y0+MY+1
+  alignas(128) double atb[(MY + 4) * SW];  // tracer level L of the previous time level
+  alignas(128) float ws[(MY + 2) * SW];    // rows y0-1 .. y0+MY
+  alignas(128) float wkd[(MY + 3) * SW];   // rows y0-2 .. y0+MY
+  alignas(128) float wkb[(MY + 3) * SW];   // rows y0-2 .. y0+MY
 };
 constexpr uint32_t kMxLevelBytes =
-    (uint32_t)(2 * (TY + 4) * SW * sizeof(double) + ((TY + 2) * SW + 2 * (TY + 3) * SW) * sizeof(float));
+    (uint32_t)(2 * (MY + 4) * SW * sizeof(double) + ((MY + 2) * SW + 2 * (MY + 3) * SW) * sizeof(float));
 
 struct MxSmem {
   MxSlot slot[NSM];
   float fxd[2][FXN];                  // per level parity: face difference d
   float fyd[2][FYN];
-  unsigned char flag[3][HN];          // predictor outside its local bounds
-  float d2[HN];                       // first Laplacian (times ahf)
-  float tr[HN], dtn[HN], dts[HN], dte[HN], dtw[HN], ahf[HN];
-  float kx[HN], ky[HN];               // del4 face weights tarea*dte (east face), tarea*dts (south face)
+  unsigned char flag[3][MHN];          // predictor outside its local bounds
+  float d2[MHN];                       // first Laplacian (times ahf)
+  float tr[MHN], dtn[MHN], dts[MHN], dte[MHN], dtw[MHN], ahf[MHN];
+  float kx[MHN], ky[MHN];               // del4 face weights tarea*dte (east face), tarea*dts (south face)
   float cxf[FXN], cyf[FYN];           // 2*dts/(htw*hun), 2*dts/(hts*hue) at the faces
   float fxu[2][FXN], fyv[2][FYN];    // per level parity: f32 face transports uw, vs
   float hwx[FXN], hsy[FYN];           // htw, hts at the faces (f32)
-  uint16_t kmt[(TY + 4) * SW];        // bottom level of the tile's columns and their 2-cell halo
+  uint16_t kmt[(MY + 4) * SW];        // bottom level of the tile's columns and their 2-cell halo
   uint64_t bar[NSM];
 };
 // four CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
-// five CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
+// kMixedCtasPerSm CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
 static_assert(kMixedCtasPerSm * (sizeof(MxSmem) + 1024) <= 228 * 1024,
               "mixed tracer tile no longer fits kMixedCtasPerSm CTAs per SM");
 
@@ -312,7 +319,7 @@ __device__ __forceinline__ void face_one(MxSmem& S, const MxSlot& L, int kk, boo
   }
 }
 
-constexpr int FX_OWN = TX * TY, FX_EXTRA = FXN - FX_OWN, FY_EXTRA = FYN - TX * TY;
+constexpr int FX_OWN = TX * MY, FX_EXTRA = FXN - FX_OWN, FY_EXTRA = FYN - TX * MY;
 constexpr int F_EXTRA = FX_EXTRA + FY_EXTRA;   // border faces of the region
 
 struct FaceSet {
@@ -326,26 +333,26 @@ __device__ __forceinline__ uint32_t face_desc(bool is_y, int m, int r) {
 }
 
 // border face q (0 .. F_EXTRA-1): x faces of the top and bottom rows, x faces
-// of the west column and the two east columns, y faces of rows 0, TY+1, TY+2,
+// of the west column and the two east columns, y faces of rows 0, MY+1, MY+2,
 // y faces of the west and east columns
 __device__ __forceinline__ uint32_t border_face(int q) {
   int fj, fi;
   if (q < 2 * (TX + 3)) {
-    fj = q < TX + 3 ? 0 : TY + 1;
+    fj = q < TX + 3 ? 0 : MY + 1;
     fi = q % (TX + 3);
     return face_desc(false, fx(fj, fi), (fj + 1) * SW + fi + 3);
   }
   q -= 2 * (TX + 3);
-  if (q < 3 * TY) {
+  if (q < 3 * MY) {
     const int c = q % 3;
     fj = 1 + q / 3;
     fi = c == 0 ? 0 : TX + c;
     return face_desc(false, fx(fj, fi), (fj + 1) * SW + fi + 3);
   }
-  q -= 3 * TY;
+  q -= 3 * MY;
   if (q < 3 * (TX + 2)) {
     const int row = q / (TX + 2);
-    fj = row == 0 ? 0 : TY + row;
+    fj = row == 0 ? 0 : MY + row;
     fi = q % (TX + 2);
     return face_desc(true, fy(fj, fi), fj * SW + fi + 3);
   }
@@ -362,7 +369,7 @@ __device__ __forceinline__ FaceSet face_set(int tid) {
   f.own_y = fy(ty + 1, tx + 1);
   f.own_r = (ty + 2) * SW + tx + 4;
   f.ne = 0;
-  for (int q = tid; q < F_EXTRA && f.ne < 2; q += TTHREADS) f.e[f.ne++] = border_face(q);
+  for (int q = tid; q < F_EXTRA && f.ne < 2; q += MTH) f.e[f.ne++] = border_face(q);
   if (f.ne < 2) f.e[1] = 0;
   if (f.ne < 1) f.e[0] = 0;
   return f;
@@ -379,7 +386,7 @@ __device__ __forceinline__ void faces_level(MxSmem& S, int kk, const FaceSet& f)
       face_one(S, L, kk, !(d >> 31), (int)((d >> 16) & 0x7fffu), (int)(d & 0xffffu));
     }
 }
-static_assert(F_EXTRA <= 2 * TTHREADS, "border faces: at most two per thread");
+static_assert(F_EXTRA <= 2 * MTH, "border faces: at most two per thread");
 
 // A cell of the 1-halo region as one thread handles it: its index m in the
 // region, box index r (at, atb, kmt boxes), u (ws box), its west x face fw and
@@ -391,7 +398,7 @@ struct HCell {
   int m, r, u, fw, fn;
   bool valid;
 };
-constexpr int RING = HN - TX * TY;
+constexpr int RING = MHN - TX * MY;
 
 __device__ __forceinline__ HCell hcell(int hj, int hi, int x0, int y0, int imt, int jmt) {
   HCell c;
@@ -409,9 +416,9 @@ __device__ __forceinline__ HCell hcell(int hj, int hi, int x0, int y0, int imt, 
 __device__ __forceinline__ HCell ring_hcell(int q, int x0, int y0, int imt, int jmt) {
   int hj, hi;
   if (q < HQX) { hj = 0; hi = q; }
-  else if (q < 2 * HQX) { hj = HQY - 1; hi = q - HQX; }
-  else if (q < 2 * HQX + TY) { hj = q - 2 * HQX + 1; hi = 0; }
-  else { hj = q - 2 * HQX - TY + 1; hi = HQX - 1; }
+  else if (q < 2 * HQX) { hj = MHQY - 1; hi = q - HQX; }
+  else if (q < 2 * HQX + MY) { hj = q - 2 * HQX + 1; hi = 0; }
+  else { hj = q - 2 * HQX - MY + 1; hi = HQX - 1; }
   return hcell(hj, hi, x0, y0, imt, jmt);
 }
 
@@ -542,7 +549,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
   const double* __restrict__ odzp = a.odzp;
   const double* __restrict__ odzt = a.odzt;
   {
-    const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * TY;
+    const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * MY;
     const int i = x0 + tx, j = y0 + ty;
     double* at_out = a.at[a.cur ^ 1] + n * F;
     double* atb_out = a.atb[a.cur ^ 1] + n * FB;
@@ -560,11 +567,11 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     };
     for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L);
     // per-tile 2-D data
-    for (int m = tid; m < (TY + 4) * SW; m += TTHREADS) {
+    for (int m = tid; m < (MY + 4) * SW; m += MTH) {
       const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
       S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
     }
-    for (int m = tid; m < HN; m += TTHREADS) {
+    for (int m = tid; m < MHN; m += MTH) {
       const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
       const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
       const long q = in ? (long)gj * imt + gi : 0;
@@ -577,7 +584,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       S.kx[m] = in ? (float)(a.tarea[q] * a.dte[q]) : 0.f;
       S.ky[m] = in ? (float)(a.tarea[q] * a.dts[q]) : 0.f;
     }
-    for (int m = tid; m < FXN + FYN; m += TTHREADS) {
+    for (int m = tid; m < FXN + FYN; m += MTH) {
       int gj, gi;
       if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
       else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
@@ -758,9 +765,9 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
           e_prev = ev;
           f_prev = fv;
         }
-        double* sl = scr + (long)k * 2 * TTHREADS;
+        double* sl = scr + (long)k * 2 * MTH;
         sl[tid] = ev;
-        sl[TTHREADS + tid] = fv;
+        sl[MTH + tid] = fv;
       }
       akt_here = akt_above;
       __syncthreads();
@@ -770,8 +777,8 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       double x = 0.0;
 #pragma unroll 4
       for (int k = 0; k < km; ++k) {
-        const double* sl = scr + (long)k * 2 * TTHREADS;
-        const double ev = sl[tid], fv = sl[TTHREADS + tid];
+        const double* sl = scr + (long)k * 2 * MTH;
+        const double ev = sl[tid], fv = sl[MTH + tid];
         double v;
         if (k < kz) {
           v = (k == 0) ? ev * stf + fv : ev * x + fv;
@@ -799,11 +806,11 @@ __device__ __forceinline__ MxSmem& mixed_smem_init() {
   return S;
 }
 
-__global__ void __launch_bounds__(TTHREADS, kMixedCtasPerSm)
+__global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
     k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
   MxSmem& S = mixed_smem_init();
   uint32_t par = 0, outstanding = 0;
-  double* scr = a.col_scratch + (long)blockIdx.x * a.km * 2 * TTHREADS;
+  double* scr = a.col_scratch + (long)blockIdx.x * a.km * 2 * MTH;
   for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x)
     if (!mixed_item(S, a, maps, scr, ntx, w >> 1, (int)(w & 1), par, outstanding)) return;
 }
@@ -813,11 +820,11 @@ __global__ void __launch_bounds__(TTHREADS, kMixedCtasPerSm)
 // (tile, tracer) items, member after member, so neighbouring CTAs work on
 // neighbouring tiles of the same member.  Each CTA's items ascend, so its
 // member index only moves forward.
-__global__ void __launch_bounds__(TTHREADS, kMixedCtasPerSm)
+__global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
     k_tracer_mixed_batch(const MemberDesc* __restrict__ mem, int nmem, long total, double* scratch, int km_max) {
   MxSmem& S = mixed_smem_init();
   uint32_t par = 0, outstanding = 0;
-  double* scr = scratch + (long)blockIdx.x * km_max * 2 * TTHREADS;
+  double* scr = scratch + (long)blockIdx.x * km_max * 2 * MTH;
   int m = 0;
   for (long w = blockIdx.x; w < total; w += gridDim.x) {
     while (m + 1 < nmem && mem[m + 1].item0 <= w) ++m;
@@ -831,14 +838,14 @@ __global__ void __launch_bounds__(TTHREADS, kMixedCtasPerSm)
 
 int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid) {
   const int ntx = (a.imt + TX - 1) / TX;
-  const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
+  const long ntiles = (long)ntx * ((a.jmt + MY - 1) / MY);
   const size_t sm = sizeof(MxSmem);
   static bool attr = false;
   if (!attr) {
     LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     attr = true;
   }
-  k_tracer_mixed<<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+  k_tracer_mixed<<<grid, MTH, sm, s>>>(a, maps, ntx, ntiles);
   LT_LAUNCHED();
   return LT_OK;
 }
@@ -855,7 +862,7 @@ int prepare_tracer_mixed_batch() {
 // inside a stream capture)
 int launch_tracer_mixed_batch(const MemberDesc* mem, int nmem, long total, double* scratch, int km_max, int grid,
                               cudaStream_t s) {
-  k_tracer_mixed_batch<<<grid, TTHREADS, sizeof(MxSmem), s>>>(mem, nmem, total, scratch, km_max);
+  k_tracer_mixed_batch<<<grid, MTH, sizeof(MxSmem), s>>>(mem, nmem, total, scratch, km_max);
   LT_LAUNCHED();
   return LT_OK;
 }
