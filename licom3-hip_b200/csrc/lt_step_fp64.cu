@@ -775,7 +775,9 @@ struct ExSmem {
   uint64_t bar[NSX];
 };
 
-__device__ void predictor_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0) {
+// Predictor, masked extrema and limiter flag of one cell (hj, hi) of the
+// 1-halo region at level kk; returns the flag (a00 > amax || a00 < amin).
+__device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0) {
   const int km = a.km, imt = a.imt, jmt = a.jmt;
   const double dts = a.p.dts;
   const double* odzp = a.odzp;
@@ -791,12 +793,12 @@ __device__ void predictor_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0)
   double* o00 = S.a00[kk % 3];
   double* omx = S.amx[kk % 3];
   double* omn = S.amn[kk % 3];
-  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
-    const int hj = m / HQX, hi = m % HQX;
+  {
+    const int m = hj * HQX + hi;
     const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
     if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) {
       o00[m] = 0.0; omx[m] = 0.0; omn[m] = 0.0;
-      continue;
+      return false;
     }
     const int r = r2(hj, hi), u = ru(hj, hi), v = rv(hj, hi);
     const long q = (long)gj * imt + gi;
@@ -865,15 +867,17 @@ __device__ void predictor_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0)
     }
     omx[m] = hi_;
     omn[m] = lo_;
+    return o00[m] > hi_ || o00[m] < lo_;
   }
 }
 
-__device__ void del4_first_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0) {
+// First Laplacian of atb at level kk for one cell (hj, hi) of the 1-halo region.
+__device__ __forceinline__ void del4_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0) {
   const double* atb = S.slot[kk % NSX].atb;
-  for (int m = threadIdx.x; m < HN; m += TTHREADS) {
-    const int hj = m / HQX, hi = m % HQX;
+  {
+    const int m = hj * HQX + hi;
     const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
-    if (!(gi >= 1 && gi < a.imt - 1 && gj >= 1 && gj < a.jmt - 1)) { S.d2[m] = 0.0; continue; }
+    if (!(gi >= 1 && gi < a.imt - 1 && gj >= 1 && gj < a.jmt - 1)) { S.d2[m] = 0.0; return; }
     const int r = r2(hj, hi);
     const long q = (long)gj * a.imt + gi;
     double h = 0.0, cc = 0.0;
@@ -885,6 +889,16 @@ __device__ void del4_first_tma(ExSmem& S, const Arena& a, int kk, int x0, int y0
     }
     S.d2[m] = __ldg(a.ahf + q) * (cc * atb[r] + h);
   }
+}
+
+// Every thread handles the interior cell above its column; the 76 ring cells
+// of the 1-halo region go to threads 0 .. 75.
+constexpr int RING64 = HN - TTHREADS;
+__device__ __forceinline__ void ring_cell64(int q, int& hj, int& hi) {
+  if (q < HQX) { hj = 0; hi = q; }
+  else if (q < 2 * HQX) { hj = HQY - 1; hi = q - HQX; }
+  else if (q < 2 * HQX + TY) { hj = q - 2 * HQX + 1; hi = 0; }
+  else { hj = q - 2 * HQX - TY + 1; hi = HQX - 1; }
 }
 
 struct ExactHw {
@@ -916,6 +930,9 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
   }
   __syncthreads();
   uint32_t par = 0, outstanding = 0;
+  const bool has_ring = tid < RING64;
+  int ring_hj = 0, ring_hi = 0;
+  if (has_ring) ring_cell64(tid, ring_hj, ring_hi);
 
   for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x) {
     const long tile = w >> 1;
@@ -963,15 +980,24 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       // a wait that ran out anywhere in the CTA sends every thread out together
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
     }
-    predictor_tma(S, a, km - 1, x0, y0);
+    // limiter flags of the own cell at levels k+1, k (earlier steps) and k-1
+    bool out_kp1 = false, out_k = pred_one64(S, a, km - 1, ty + 1, tx + 1, x0, y0), out_km1 = false;
+    if (has_ring) pred_one64(S, a, km - 1, ring_hj, ring_hi, x0, y0);
 
     for (int k = km - 1; k >= 0; --k) {
+      // ---- phase B1: first Laplacian at level k (arrived in an earlier step)
+      del4_one64(S, a, k, ty + 1, tx + 1, x0, y0);
+      if (has_ring) del4_one64(S, a, k, ring_hj, ring_hi, x0, y0);
       const bool ok = (k >= 2) ? wait(k - 2) : true;
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
-      // ---- phase B
-      if (k >= 1) predictor_tma(S, a, k - 1, x0, y0);
-      del4_first_tma(S, a, k, x0, y0);
-      __syncthreads();
+      // ---- phase B2: predictor one level up.  The column phase below reads
+      // the flags of level k of the neighbours (written in the previous step)
+      // and only its own cell's flags of the levels k-1 and k+1, which this
+      // thread computed: no barrier between the two phases.
+      if (k >= 1) {
+        out_km1 = pred_one64(S, a, k - 1, ty + 1, tx + 1, x0, y0);
+        if (has_ring) pred_one64(S, a, k - 1, ring_hj, ring_hi, x0, y0);
+      }
       // ---- phase C
       if (ring) {
         const LevelSlot<double>& Lk = S.slot[k % NSX];
@@ -989,7 +1015,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         const double hsn = __ldg(a.hts + qo - imt) * __ldg(a.hue + qo - imt);
         const double c = at_c[rc], e = at_c[rc + 1], w = at_c[rc - 1], s = at_c[rc + SW], nn = at_c[rc - SW];
         const double ue = Lk.uw[uc + 1], uwc = Lk.uw[uc], vsc = Lk.vs[vc], vn = Lk.vs[vc - SW];
-        const bool self = out(o00, omx, omn, hc);
+        const bool self = out_k;
         const bool edge_k = (k == 0 || k == km - 1);
         auto lim = [&](int m, bool guard) {
           const bool nb = out(o00, omx, omn, m);
@@ -1008,7 +1034,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         if (k == 0) {
           const double w1 = ws_dn, ad = at_dn;
           zb1 = 0.0;
-          if (self || (out(S.a00[1 % 3], S.amx[1 % 3], S.amn[1 % 3], hc) && k <= km - 2))
+          if (self || (out_kp1 && k <= km - 2))
             zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
           else
             zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
@@ -1016,7 +1042,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           zc = odzp[0] * c * w1;
         } else if (k == km - 1) {
           const double au = at_u[rc];
-          if (self || out(S.a00[(k - 1) % 3], S.amx[(k - 1) % 3], S.amn[(k - 1) % 3], hc))
+          if (self || out_km1)
             zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
           else
             zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
@@ -1025,11 +1051,11 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           zc = -odzp[km - 1] * c * wk;
         } else {
           const double au = at_u[rc], ad = at_dn, w1 = ws_dn;
-          if ((self || out(S.a00[(k - 1) % 3], S.amx[(k - 1) % 3], S.amn[(k - 1) % 3], hc)) && k >= 1)
+          if ((self || out_km1) && k >= 1)
             zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
           else
             zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
-          if ((self || out(S.a00[(k + 1) % 3], S.amx[(k + 1) % 3], S.amn[(k + 1) % 3], hc)) && k <= km - 2)
+          if ((self || out_kp1) && k <= km - 2)
             zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
           else
             zb2 = 0.5 * odzp[k] * w1 * w1 * odzt[k + 1] * (c - ad) * dts;
@@ -1144,6 +1170,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         at_dn = c;
         ws_dn = wk;
       }
+      out_kp1 = out_k;
+      out_k = out_km1;
       __syncthreads();  // level k is no longer read: its slot takes level k-NSX
       if (k - NSX >= 0) issue(k - NSX);
     }
