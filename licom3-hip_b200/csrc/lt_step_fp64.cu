@@ -235,75 +235,113 @@ __global__ void __launch_bounds__(TTHREADS) k_continuity(Arena a) {
   }
 }
 
-// Continuity in two fully parallel passes (used when the arena holds a wka
-// buffer).  k_cont_level: one thread per cell of one level; U-point
-// velocities of a 32 x 8 block plus one column east and one row north staged
-// in shared memory; writes the scaled utf/vtf, both face transports and the
-// masked divergence wka (tracer_1, upwell_2, operators_div,
-// advection_tracer_1_0).  k_cont_column: one thread per column; the column
-// divergence W in level order and w by upward integration (upwell_3/4).
-__global__ void __launch_bounds__(256) k_cont_level(Arena a) {
-  constexpr int BX = 32, BY = 8, UX = BX + 1, UY = BY + 1;
-  __shared__ double s_wkd[UY * UX], s_wkb[UY * UX], s_uk[UY * UX], s_vk[UY * UX];
+// Continuity as one level march per 32 x 8 tile (used when the arena holds a
+// wka buffer; tracer_1, upwell_2, operators_div, advection_tracer_1_0 and
+// upwell_3/4 with the same expressions in the same order): the
+// level-free free-surface factor of the region's U points is formed once, each
+// level's velocities of the next level are loaded into registers while the
+// current one is computed, the column divergence W accumulates in level order
+// during the march, and w is integrated upward afterwards from the wka the
+// march wrote (upwell_3/4).
+__global__ void __launch_bounds__(256) k_cont_march64(Arena a) {
+  constexpr int BX = 32, BY = 8, UX = BX + 1, UY = BY + 1, UN = UX * UY, NT = BX * BY;
+  constexpr int NPT = (UN + NT - 1) / NT;
+  __shared__ double s_wkd[UN], s_wkb[UN], s_uk[UN], s_vk[UN], s_fac[UN];
+  __shared__ unsigned char s_fok[UN];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
-  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, k = blockIdx.z;
-  const int imt = a.imt, jmt = a.jmt;
-  const long lvl = (long)k * a.A;
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A;
   const lt_params& p = a.p;
-  for (int m = tid; m < UY * UX; m += BX * BY) {
+  // the region's U points: the free-surface factor (level-free)
+  for (int m = tid; m < UN; m += NT) {
     const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
-    double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
-    if (uj >= 0 && uj < jmt && ui < imt) {
+    double fac = 0.0;
+    bool ok = false;
+    if (uj >= 0 && uj < jmt && ui < imt && uj < jmt - 1 && ui >= 1) {
       const long q = q2(uj, ui, imt);
-      const long c = lvl + q;
-      wkd = 0.5 * (a.utf[c] * p.oncc) + 0.5 * a.utl[c];
-      wkb = 0.5 * (a.vtf[c] * p.oncc) + 0.5 * a.vtl[c];
-      if (uj < jmt - 1 && ui >= 1) {
-        const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
-                            a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
-        const double fac = 1.0 + work * a.ohbu[q];
-        uk = fac * wkd;
-        vk = fac * wkb;
+      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
+                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
+      fac = 1.0 + work * a.ohbu[q];
+      ok = true;
+    }
+    s_fac[m] = fac;
+    s_fok[m] = ok;
+  }
+  long rq[NPT];
+  bool rin[NPT];
+  double rutf[NPT], rutl[NPT], rvtf[NPT], rvtl[NPT];
+#pragma unroll
+  for (int pt = 0; pt < NPT; ++pt) {
+    const int m = tid + pt * NT;
+    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+    rin[pt] = m < UN && uj >= 0 && uj < jmt && ui < imt;
+    rq[pt] = rin[pt] ? q2(uj, ui, imt) : 0;
+    rutf[pt] = rin[pt] ? a.utf[rq[pt]] : 0.0;
+    rutl[pt] = rin[pt] ? a.utl[rq[pt]] : 0.0;
+    rvtf[pt] = rin[pt] ? a.vtf[rq[pt]] : 0.0;
+    rvtl[pt] = rin[pt] ? a.vtl[rq[pt]] : 0.0;
+  }
+  const int i = x0 + tx, j = y0 + ty;
+  const bool own = i < imt && j < jmt;
+  const bool col = own && j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1;
+  const long qo = own ? q2(j, i, imt) : 0;
+  const int kz = own ? a.kmt[qo] : 0;
+  const double htw_o = own ? a.htw[qo] : 0.0, hts_o = own ? a.hts[qo] : 0.0;
+  const double htw_e = (own && i < imt - 1) ? a.htw[qo + 1] : 0.0;
+  const double hts_n = (own && j >= 1) ? a.hts[qo - imt] : 0.0;
+  const double trr = own ? a.tarea_r[qo] : 0.0;
+  const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
+  double W = 0.0;
+  for (int k = 0; k < km; ++k) {
+    const long lvl = (long)k * A;
+    __syncthreads();   // the previous level is done with the staged values
+#pragma unroll
+    for (int pt = 0; pt < NPT; ++pt) {
+      const int m = tid + pt * NT;
+      if (m < UN) {
+        double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
+        if (rin[pt]) {
+          wkd = 0.5 * (rutf[pt] * p.oncc) + 0.5 * rutl[pt];
+          wkb = 0.5 * (rvtf[pt] * p.oncc) + 0.5 * rvtl[pt];
+          if (s_fok[m]) {
+            uk = s_fac[m] * wkd;
+            vk = s_fac[m] * wkb;
+          }
+        }
+        s_wkd[m] = wkd; s_wkb[m] = wkb; s_uk[m] = uk; s_vk[m] = vk;
       }
     }
-    s_wkd[m] = wkd; s_wkb[m] = wkb; s_uk[m] = uk; s_vk[m] = vk;
+    __syncthreads();
+    if (k + 1 < km) {
+#pragma unroll
+      for (int pt = 0; pt < NPT; ++pt) {
+        if (!rin[pt]) continue;
+        const long c = lvl + A + rq[pt];
+        rutf[pt] = a.utf[c]; rutl[pt] = a.utl[c]; rvtf[pt] = a.vtf[c]; rvtl[pt] = a.vtl[c];
+      }
+    }
+    if (!own) continue;
+    const long c = lvl + qo;
+    a.utf_out[c] = a.utf[c] * p.oncc;
+    a.vtf_out[c] = a.vtf[c] * p.oncc;
+    if (j >= 1 && j < jmt - 1) a.uwf[c] = (s_wkd[mn] + s_wkd[m0]) * htw_o * 0.25;
+    if (i >= 1 && i < imt - 1) a.vsf[c] = (s_wkb[m0] + s_wkb[m0 + 1]) * hts_o * 0.25;
+    double wka = 0.0;
+    if (j >= 1 && i < imt - 1 && k <= kz - 1) {
+      const double east = (s_uk[m0 + 1] + s_uk[mn + 1]) * htw_e;
+      const double west = (s_uk[m0] + s_uk[mn]) * htw_o;
+      const double south = (s_vk[m0 + 1] + s_vk[m0]) * hts_o;
+      const double north = (s_vk[mn + 1] + s_vk[mn]) * hts_n;
+      wka = 0.5 * (east - west + south - north) * trr;
+    }
+    a.wka[c] = wka;
+    if (col) W = W - a.dzp[k] * wka * (k < kz ? 1.0 : 0.0);
   }
-  __syncthreads();
-  const int i = x0 + tx, j = y0 + ty;
-  if (i >= imt || j >= jmt) return;
-  const long qo = q2(j, i, imt);
-  const long c = lvl + qo;
-  const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
-  a.utf_out[c] = a.utf[c] * p.oncc;
-  a.vtf_out[c] = a.vtf[c] * p.oncc;
-  if (j >= 1 && j < jmt - 1) a.uwf[c] = (s_wkd[mn] + s_wkd[m0]) * a.htw[qo] * 0.25;
-  if (i >= 1 && i < imt - 1) a.vsf[c] = (s_wkb[m0] + s_wkb[m0 + 1]) * a.hts[qo] * 0.25;
-  double wka = 0.0;
-  if (j >= 1 && i < imt - 1 && k <= a.kmt[qo] - 1) {
-    const double east = (s_uk[m0 + 1] + s_uk[mn + 1]) * a.htw[qo + 1];
-    const double west = (s_uk[m0] + s_uk[mn]) * a.htw[qo];
-    const double south = (s_vk[m0 + 1] + s_vk[m0]) * a.hts[qo];
-    const double north = (s_vk[mn + 1] + s_vk[mn]) * a.hts[qo - imt];
-    wka = 0.5 * (east - west + south - north) * a.tarea_r[qo];
-  }
-  a.wka[c] = wka;
-}
-
-__global__ void __launch_bounds__(256) k_cont_column(Arena a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int imt = a.imt, jmt = a.jmt, km = a.km;
-  if (!(j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1)) return;
-  const long qo = q2(j, i, imt);
-  const long A = a.A;
-  const int kz = a.kmt[qo];
-  double W = 0.0;
-#pragma unroll 8
-  for (int k = 0; k < km; ++k) W = W - a.dzp[k] * a.wka[(long)k * A + qo] * (k < kz ? 1.0 : 0.0);
+  if (!col) return;
   const double ohbt = a.ohbt[qo];
   const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
   double wsp = a.ws[qo];
-#pragma unroll 8
   for (int k = 1; k < km; ++k) {
     const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + a.wka[(long)(k - 1) * A + qo]));
     a.ws[(long)k * A + qo] = raw * fac;
@@ -1304,11 +1342,8 @@ int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripo
 
 int launch_continuity_fp64(const Arena& a, cudaStream_t s) {
   if (a.wka) {
-    dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8, a.km);
-    k_cont_level<<<g, b, 0, s>>>(a);
-    LT_LAUNCHED();
-    dim3 g2((a.imt + 31) / 32, (a.jmt + 7) / 8);
-    k_cont_column<<<g2, b, 0, s>>>(a);
+    dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
+    k_cont_march64<<<g, b, 0, s>>>(a);
     LT_LAUNCHED();
     return LT_OK;
   }
