@@ -11,11 +11,11 @@ namespace lt {
 // Column tile of the fused tracer kernel: TX columns along i (one warp) by TY
 // rows along j; one thread per column.
 constexpr int TX = 32;
-constexpr int TY = 4;
+constexpr int TY = 8;
 constexpr int TTHREADS = TX * TY;
 // Persistent CTAs per SM of the column kernels (their shared-memory footprint
-// decides): FP64 4 of 128 threads, mixed 3 of 256.
-constexpr int kFp64CtasPerSm = 4;
+// decides): 3 of 256 threads for both.
+constexpr int kFp64CtasPerSm = 3;
 constexpr int kMixedCtasPerSm = 3;
 // The mixed column kernel's tile: TX x kMixedTileY columns, one thread each.
 constexpr int kMixedTileY = 8;

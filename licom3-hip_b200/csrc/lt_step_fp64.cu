@@ -9,9 +9,10 @@
 //                   surface mixing floor, SSS-norm terms       (tracer_1_0, tracer_5/6 surface parts)
 //   tree sum        deterministic SSS-normalisation sum         (tracer.cpp:1849-1868)
 //   halo(net)       in-GPU ghost fill                           (pop_haloupdate_tracer1)
-//   k_continuity    uk/vk, divergence, w by upward integration,
+//   k_cont_march64  uk/vk, divergence, w by upward integration,
 //                   face transports, scaled utf/vtf             (tracer_1, upwell_2..4, advection_tracer_1_0)
-//   k_tracer64      per column tile, both tracers: tspas predictor/limiter,
+//   k_tracer_tma64  per column tile (k_tracer64 where the layout
+//                   does not allow TMA boxes), both tracers: tspas predictor/limiter,
 //                   biharmonic diffusion, shortwave, explicit and implicit
 //                   vertical diffusion, surface terms, update   (advection_tracer_2/3, tracer_del4_1/2,
 //                                                                tracer_5..9, invtrit)
@@ -145,99 +146,9 @@ __global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripol
 }
 
 // ------------------------------------------------------------- continuity
-// One thread per T column of a TX x TY tile.  Per level: U-point velocities
-// of the tile plus one column east and one row north are staged in shared
-// memory; the thread forms
-//   wkd = 0.5*utf*oncc + 0.5*utl, uk = (1 + work*ohbu)*wkd   (tracer_1, upwell_2)
-//   wka = masked divergence of (uk, vk)                          (operators_div)
-//   u_wface, v_sface face transports                             (advection_tracer_1_0)
-// and keeps wka in shared memory for the second, upward pass
-//   ws(k) = vit*(ws(k-1) + dzp(k-1)*(W*ohbt + wka(k-1))) * 1/(1+stf*ohbt)   (upwell_3/4)
-constexpr int CX = TX + 1, CY = TY + 1;  // U-point region: i in [x0, x0+TX], j in [y0-1, y0+TY-1]
-
-__global__ void __launch_bounds__(TTHREADS) k_continuity(Arena a) {
-  extern __shared__ double sh[];
-  double* s_wkd = sh;                 // [CY][CX]
-  double* s_wkb = s_wkd + CY * CX;
-  double* s_uk = s_wkb + CY * CX;
-  double* s_vk = s_uk + CY * CX;
-  double* s_fac = s_vk + CY * CX;     // 1 + work*ohbu per U point
-  double* s_wka = s_fac + CY * CX;    // [km][TTHREADS]
-  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int i = x0 + tx, j = y0 + ty;
-  const int imt = a.imt, jmt = a.jmt, km = a.km;
-  const long A = a.A;
-  const lt_params& p = a.p;
-  const bool own = (i < imt && j < jmt);
-
-  // free-surface factor at the staged U points: tgrid_to_ugrid(stf) (grid.F90:1975-1990)
-  for (int m = tid; m < CY * CX; m += TTHREADS) {
-    const int uj = y0 - 1 + m / CX, ui = x0 + m % CX;
-    double fac = 0.0;
-    if (uj >= 0 && uj < jmt - 1 && ui >= 1 && ui < imt) {
-      const long q = q2(uj, ui, imt);
-      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
-                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
-      fac = 1.0 + work * a.ohbu[q];
-    }
-    s_fac[m] = fac;
-  }
-  const long qo = own ? q2(j, i, imt) : 0;
-  const int kz = own ? a.kmt[qo] : 0;
-  const bool wcol = own && j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1;
-  double W = 0.0;
-
-  for (int k = 0; k < km; ++k) {
-    __syncthreads();
-    for (int m = tid; m < CY * CX; m += TTHREADS) {
-      const int uj = y0 - 1 + m / CX, ui = x0 + m % CX;
-      double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
-      if (uj >= 0 && uj < jmt && ui < imt) {
-        const long c = (long)k * A + q2(uj, ui, imt);
-        wkd = 0.5 * (a.utf[c] * p.oncc) + 0.5 * a.utl[c];
-        wkb = 0.5 * (a.vtf[c] * p.oncc) + 0.5 * a.vtl[c];
-        if (uj < jmt - 1 && ui >= 1) {
-          uk = s_fac[m] * wkd;
-          vk = s_fac[m] * wkb;
-        }
-      }
-      s_wkd[m] = wkd; s_wkb[m] = wkb; s_uk[m] = uk; s_vk[m] = vk;
-    }
-    __syncthreads();
-    if (!own) continue;
-    const long c = (long)k * A + qo;
-    const int m0 = (ty + 1) * CX + tx;      // U point (j, i)
-    const int mn = ty * CX + tx;            // U point (j-1, i)
-    a.utf_out[c] = a.utf[c] * p.oncc;
-    a.vtf_out[c] = a.vtf[c] * p.oncc;
-    if (j >= 1 && j < jmt - 1) a.uwf[c] = (s_wkd[mn] + s_wkd[m0]) * a.htw[qo] * 0.25;
-    if (i >= 1 && i < imt - 1) a.vsf[c] = (s_wkb[m0] + s_wkb[m0 + 1]) * a.hts[qo] * 0.25;
-    double wka = 0.0;
-    if (j >= 1 && i < imt - 1 && k <= kz - 1) {
-      const double east = (s_uk[m0 + 1] + s_uk[mn + 1]) * a.htw[qo + 1];
-      const double west = (s_uk[m0] + s_uk[mn]) * a.htw[qo];
-      const double south = (s_vk[m0 + 1] + s_vk[m0]) * a.hts[qo];
-      const double north = (s_vk[mn + 1] + s_vk[mn]) * a.hts[qo - imt];
-      wka = 0.5 * (east - west + south - north) * a.tarea_r[qo];
-    }
-    s_wka[k * TTHREADS + tid] = wka;
-    if (wcol) W = W - a.dzp[k] * wka * (k < kz ? 1.0 : 0.0);
-  }
-  if (!wcol) return;
-  const double ohbt = a.ohbt[qo];
-  const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
-  double wsp = a.ws[qo];  // level 0 is never written by the step
-  for (int k = 1; k < km; ++k) {
-    const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + s_wka[(k - 1) * TTHREADS + tid]));
-    a.ws[(long)k * A + qo] = raw * fac;
-    wsp = raw;
-  }
-}
-
-// Continuity as one level march per 32 x 8 tile (used when the arena holds a
-// wka buffer; tracer_1, upwell_2, operators_div, advection_tracer_1_0 and
-// upwell_3/4 with the same expressions in the same order): the
+// Continuity as one level march per 32 x 8 tile (tracer_1, upwell_2,
+// operators_div, advection_tracer_1_0 and upwell_3/4 with the same
+// expressions in the same order): the
 // level-free free-surface factor of the region's U points is formed once, each
 // level's velocities of the next level are loaded into registers while the
 // current one is computed, the column divergence W accumulates in level order
@@ -807,7 +718,7 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
 constexpr int NSX = 3;
 struct ExSmem {
   LevelSlot<double> slot[NSX];
-  double a00[3][HN], amx[3][HN], amn[3][HN];
+  unsigned char flag[3][HN];   // limiter flag (a00 > amax || a00 < amin) per level parity of three
   double d2[HN];
   int kmt[(TY + 4) * SW];
   uint64_t bar[NSX];
@@ -828,14 +739,12 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
   const double* ws_d = kk < km - 1 ? S.slot[(kk + 1) % NSX].ws : nullptr;
   const double* uw = Lc.uw;
   const double* vs = Lc.vs;
-  double* o00 = S.a00[kk % 3];
-  double* omx = S.amx[kk % 3];
-  double* omn = S.amn[kk % 3];
+  unsigned char* fl = S.flag[kk % 3];
   {
     const int m = hj * HQX + hi;
     const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
     if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) {
-      o00[m] = 0.0; omx[m] = 0.0; omn[m] = 0.0;
+      fl[m] = 0;   // a00 = amax = amin = 0
       return false;
     }
     const int r = r2(hj, hi), u = ru(hj, hi), v = rv(hj, hi);
@@ -878,7 +787,7 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
     const double xx = -(x0v + xy1 + xy2 + cx);
     const double yy = -(y0v + xy3 + xy4 + cy);
     const double zz = -(zb1 + zb2 + za + zc);
-    o00[m] = c + (xx + yy + zz) * dts;
+    const double a00 = c + (xx + yy + zz) * dts;
     auto vitk = [&](int kl, int rr) { return (kl < S.kmt[rr]) ? 1.0 : 0.0; };
     auto mxv = [&](double t, double vt) { return t * vt + (1.0 - vt) * -1.0e10; };
     auto mnv = [&](double t, double vt) { return t * vt + (1.0 - vt) * 1.0e10; };
@@ -903,9 +812,9 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
       t = mxv(ad, vd); if (hi_ < t) hi_ = t;
       t = mnv(ad, vd); if (lo_ > t) lo_ = t;
     }
-    omx[m] = hi_;
-    omn[m] = lo_;
-    return o00[m] > hi_ || o00[m] < lo_;
+    const bool f = a00 > hi_ || a00 < lo_;
+    fl[m] = f ? 1 : 0;
+    return f;
   }
 }
 
@@ -929,8 +838,8 @@ __device__ __forceinline__ void del4_one64(ExSmem& S, const Arena& a, int kk, in
   }
 }
 
-// Every thread handles the interior cell above its column; the 76 ring cells
-// of the 1-halo region go to threads 0 .. 75.
+// Every thread handles the interior cell above its column; the RING64 ring
+// cells of the 1-halo region go to threads 0 .. RING64-1.
 constexpr int RING64 = HN - TTHREADS;
 __device__ __forceinline__ void ring_cell64(int q, int& hj, int& hi) {
   if (q < HQX) { hj = 0; hi = q; }
@@ -1041,12 +950,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         const LevelSlot<double>& Lk = S.slot[k % NSX];
         const double* at_c = Lk.at;
         const double* at_u = k > 0 ? S.slot[(k - 1) % NSX].at : nullptr;
-        const double* o00 = S.a00[k % 3];
-        const double* omx = S.amx[k % 3];
-        const double* omn = S.amn[k % 3];
-        auto out = [&](const double* a0, const double* mx, const double* mn, int m) {
-          return a0[m] > mx[m] || a0[m] < mn[m];
-        };
+        const unsigned char* fl = S.flag[k % 3];
         const double tr = __ldg(a.tarea_r + qo);
         const double hwe = __ldg(a.htw + qo + 1) * __ldg(a.hun + qo + 1), hww = __ldg(a.htw + qo) * __ldg(a.hun + qo);
         const double hss = __ldg(a.hts + qo) * __ldg(a.hue + qo);
@@ -1056,7 +960,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         const bool self = out_k;
         const bool edge_k = (k == 0 || k == km - 1);
         auto lim = [&](int m, bool guard) {
-          const bool nb = out(o00, omx, omn, m);
+          const bool nb = fl[m] != 0;
           return edge_k ? (self || (nb && guard)) : ((self || nb) && guard);
         };
         double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
@@ -1341,20 +1245,8 @@ int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripo
 }
 
 int launch_continuity_fp64(const Arena& a, cudaStream_t s) {
-  if (a.wka) {
-    dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
-    k_cont_march64<<<g, b, 0, s>>>(a);
-    LT_LAUNCHED();
-    return LT_OK;
-  }
-  dim3 g((a.imt + TX - 1) / TX, (a.jmt + TY - 1) / TY);
-  const size_t sm = sizeof(double) * (5 * CY * CX + (size_t)a.km * TTHREADS);
-  static bool attr = false;
-  if (!attr) {
-    LT_CUDA_OK(cudaFuncSetAttribute(k_continuity, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr = true;
-  }
-  k_continuity<<<g, TTHREADS, sm, s>>>(a);
+  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
+  k_cont_march64<<<g, b, 0, s>>>(a);
   LT_LAUNCHED();
   return LT_OK;
 }
