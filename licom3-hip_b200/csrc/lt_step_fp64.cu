@@ -148,51 +148,84 @@ __global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripol
 // ------------------------------------------------------------- continuity
 // Continuity as one level march per 32 x 8 tile (tracer_1, upwell_2,
 // operators_div, advection_tracer_1_0 and upwell_3/4 with the same
-// expressions in the same order): the
-// level-free free-surface factor of the region's U points is formed once, each
-// level's velocities of the next level are loaded into registers while the
-// current one is computed, the column divergence W accumulates in level order
-// during the march, and w is integrated upward afterwards from the wka the
-// march wrote (upwell_3/4).
+// expressions in the same order).  The U-point velocities of the tile and a
+// one-point halo north and east go through a three-level staging ring filled
+// by per-thread asynchronous copies, so three levels are in flight while one
+// is computed; each thread converts the points it copied itself (mean
+// velocities wkd, wkb and the free-surface scaled uk, vk, whose level-free
+// factor it keeps in registers) into a double-buffered level, read by all
+// after the step's one barrier.  The column divergence W accumulates in level
+// order during the march; w is integrated upward afterwards from the wka the
+// march wrote.
 __global__ void __launch_bounds__(256) k_cont_march64(Arena a) {
   constexpr int BX = 32, BY = 8, UX = BX + 1, UY = BY + 1, UN = UX * UY, NT = BX * BY;
-  constexpr int NPT = (UN + NT - 1) / NT;
-  __shared__ double s_wkd[UN], s_wkb[UN], s_uk[UN], s_vk[UN], s_fac[UN];
-  __shared__ unsigned char s_fok[UN];
+  constexpr int NPT = (UN + NT - 1) / NT, NST = 3;
+  __shared__ double s_st[NST][4][UN];   // staged utf, utl, vtf, vtl of three levels
+  __shared__ double s_wkd[2][UN], s_wkb[2][UN], s_uk[2][UN], s_vk[2][UN];
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
   const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
   const int imt = a.imt, jmt = a.jmt, km = a.km;
   const long A = a.A;
   const lt_params& p = a.p;
-  // the region's U points: the free-surface factor (level-free)
-  for (int m = tid; m < UN; m += NT) {
-    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
-    double fac = 0.0;
-    bool ok = false;
-    if (uj >= 0 && uj < jmt && ui < imt && uj < jmt - 1 && ui >= 1) {
-      const long q = q2(uj, ui, imt);
-      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
-                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
-      fac = 1.0 + work * a.ohbu[q];
-      ok = true;
-    }
-    s_fac[m] = fac;
-    s_fok[m] = ok;
-  }
   long rq[NPT];
-  bool rin[NPT];
-  double rutf[NPT], rutl[NPT], rvtf[NPT], rvtl[NPT];
+  bool rin[NPT], rok[NPT];
+  double rfac[NPT];
 #pragma unroll
   for (int pt = 0; pt < NPT; ++pt) {
     const int m = tid + pt * NT;
     const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
     rin[pt] = m < UN && uj >= 0 && uj < jmt && ui < imt;
     rq[pt] = rin[pt] ? q2(uj, ui, imt) : 0;
-    rutf[pt] = rin[pt] ? a.utf[rq[pt]] : 0.0;
-    rutl[pt] = rin[pt] ? a.utl[rq[pt]] : 0.0;
-    rvtf[pt] = rin[pt] ? a.vtf[rq[pt]] : 0.0;
-    rvtl[pt] = rin[pt] ? a.vtl[rq[pt]] : 0.0;
+    rok[pt] = rin[pt] && uj < jmt - 1 && ui >= 1;
+    rfac[pt] = 0.0;
+    if (rok[pt]) {
+      const long q = rq[pt];
+      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
+                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
+      rfac[pt] = 1.0 + work * a.ohbu[q];
+    }
   }
+  auto issue = [&](int L) {
+    if (L < km) {
+      const long lvl = (long)L * A;
+#pragma unroll
+      for (int pt = 0; pt < NPT; ++pt) {
+        if (!rin[pt]) continue;
+        const int m = tid + pt * NT;
+        const long c = lvl + rq[pt];
+        double(*st)[UN] = s_st[L % NST];
+        cp_async8(&st[0][m], a.utf + c);
+        cp_async8(&st[1][m], a.utl + c);
+        cp_async8(&st[2][m], a.vtf + c);
+        cp_async8(&st[3][m], a.vtl + c);
+      }
+    }
+    cp_async_commit();
+  };
+  // the points this thread copied, level L, into buffer b
+  auto park = [&](int L, int b) {
+    const double(*st)[UN] = s_st[L % NST];
+#pragma unroll
+    for (int pt = 0; pt < NPT; ++pt) {
+      const int m = tid + pt * NT;
+      if (m >= UN) continue;
+      double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
+      if (rin[pt]) {
+        wkd = 0.5 * (st[0][m] * p.oncc) + 0.5 * st[1][m];
+        wkb = 0.5 * (st[2][m] * p.oncc) + 0.5 * st[3][m];
+        if (rok[pt]) {
+          uk = rfac[pt] * wkd;
+          vk = rfac[pt] * wkb;
+        }
+      }
+      s_wkd[b][m] = wkd; s_wkb[b][m] = wkb; s_uk[b][m] = uk; s_vk[b][m] = vk;
+    }
+  };
+  issue(0);
+  issue(1);
+  issue(2);
+  cp_async_wait<2>();
+  park(0, 0);
   const int i = x0 + tx, j = y0 + ty;
   const bool own = i < imt && j < jmt;
   const bool col = own && j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1;
@@ -205,50 +238,38 @@ __global__ void __launch_bounds__(256) k_cont_march64(Arena a) {
   const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
   double W = 0.0;
   for (int k = 0; k < km; ++k) {
-    const long lvl = (long)k * A;
-    __syncthreads();   // the previous level is done with the staged values
-#pragma unroll
-    for (int pt = 0; pt < NPT; ++pt) {
-      const int m = tid + pt * NT;
-      if (m < UN) {
-        double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
-        if (rin[pt]) {
-          wkd = 0.5 * (rutf[pt] * p.oncc) + 0.5 * rutl[pt];
-          wkb = 0.5 * (rvtf[pt] * p.oncc) + 0.5 * rvtl[pt];
-          if (s_fok[m]) {
-            uk = s_fac[m] * wkd;
-            vk = s_fac[m] * wkb;
-          }
-        }
-        s_wkd[m] = wkd; s_wkb[m] = wkb; s_uk[m] = uk; s_vk[m] = vk;
-      }
-    }
+    const int b = k & 1;
+    // level k parked by every thread; buffer b^1 and the staging slot of
+    // level k are no longer read
     __syncthreads();
-    if (k + 1 < km) {
-#pragma unroll
-      for (int pt = 0; pt < NPT; ++pt) {
-        if (!rin[pt]) continue;
-        const long c = lvl + A + rq[pt];
-        rutf[pt] = a.utf[c]; rutl[pt] = a.utl[c]; rvtf[pt] = a.vtf[c]; rvtl[pt] = a.vtl[c];
+    issue(k + 3);
+    if (own) {
+      const double* wd = s_wkd[b];
+      const double* wb = s_wkb[b];
+      const double* uk = s_uk[b];
+      const double* vk = s_vk[b];
+      const long c = (long)k * A + qo;
+      a.utf_out[c] = a.utf[c] * p.oncc;
+      a.vtf_out[c] = a.vtf[c] * p.oncc;
+      if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] + wd[m0]) * htw_o * 0.25;
+      if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25;
+      double wka = 0.0;
+      if (j >= 1 && i < imt - 1 && k <= kz - 1) {
+        const double east = (uk[m0 + 1] + uk[mn + 1]) * htw_e;
+        const double west = (uk[m0] + uk[mn]) * htw_o;
+        const double south = (vk[m0 + 1] + vk[m0]) * hts_o;
+        const double north = (vk[mn + 1] + vk[mn]) * hts_n;
+        wka = 0.5 * (east - west + south - north) * trr;
       }
+      a.wka[c] = wka;
+      if (col) W = W - a.dzp[k] * wka * (k < kz ? 1.0 : 0.0);
     }
-    if (!own) continue;
-    const long c = lvl + qo;
-    a.utf_out[c] = a.utf[c] * p.oncc;
-    a.vtf_out[c] = a.vtf[c] * p.oncc;
-    if (j >= 1 && j < jmt - 1) a.uwf[c] = (s_wkd[mn] + s_wkd[m0]) * htw_o * 0.25;
-    if (i >= 1 && i < imt - 1) a.vsf[c] = (s_wkb[m0] + s_wkb[m0 + 1]) * hts_o * 0.25;
-    double wka = 0.0;
-    if (j >= 1 && i < imt - 1 && k <= kz - 1) {
-      const double east = (s_uk[m0 + 1] + s_uk[mn + 1]) * htw_e;
-      const double west = (s_uk[m0] + s_uk[mn]) * htw_o;
-      const double south = (s_vk[m0 + 1] + s_vk[m0]) * hts_o;
-      const double north = (s_vk[mn + 1] + s_vk[mn]) * hts_n;
-      wka = 0.5 * (east - west + south - north) * trr;
+    if (k + 1 < km) {
+      cp_async_wait<2>();   // this thread's copies of level k+1 have landed
+      park(k + 1, b ^ 1);
     }
-    a.wka[c] = wka;
-    if (col) W = W - a.dzp[k] * wka * (k < kz ? 1.0 : 0.0);
   }
+  cp_async_wait<0>();
   if (!col) return;
   const double ohbt = a.ohbt[qo];
   const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);

@@ -64,7 +64,7 @@ __device__ __forceinline__ float lw_part(float d, float u, float c) { return d *
 
 
 // ------------------------------------------------------------- continuity
-// As the f64 k_cont_level / k_cont_column (tracer_1, upwell_2..4,
+// As the f64 k_cont_march64 (tracer_1, upwell_2..4,
 // operators_div, advection_tracer_1_0) with f32 storage.  The tracer march
 // uses the advective form, whose content change is sum(T * 3-D divergence of
 // the transports it advects with); to keep that divergence zero in exact
