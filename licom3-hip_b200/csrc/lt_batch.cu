@@ -2,10 +2,11 @@
 // batched launches, CUDA-graph replay and the launch-shape autotuner.
 //
 // A batch step is the tracer_ sequence of every member (surface fluxes, SSS
-// norm, net halo, continuity, column march, state halo) with the two heavy
-// kernels batched in mixed precision: one continuity launch over every
-// member's tiles and one persistent column launch over the concatenated
-// (member, tile, tracer) work list.  A kernel's parameters are frozen when a
+// norm, net halo, continuity, column march, state halo), each small kernel
+// one launch over every member, and the two heavy kernels batched in mixed
+// precision: one continuity launch over every member's tiles and one
+// persistent column launch over the concatenated (member, tile, tracer) work
+// list.  A kernel's parameters are frozen when a
 // graph is captured, and each step reads the ping-pong state buffer `cur` and
 // writes the other, so two graphs are kept: parity 0 (every member at the
 // `cur` it had when the descriptors were built) and parity 1 (flipped).
@@ -32,6 +33,7 @@ struct lt_batch {
   MemberDesc* d_desc[2] = {nullptr, nullptr};   // per parity
   double* scratch = nullptr;                     // column scratch, kMixedCtasPerSm CTAs per SM
   int km_max = 0, max_imt = 0, max_jmt = 0;
+  long max_cols = 0;                             // largest member's nx * ny
   long total_items = 0;
   int parity = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -68,6 +70,7 @@ int build_descriptors(lt_batch* b) {
   h[1].resize(n);
   long item = 0;
   b->km_max = b->max_imt = b->max_jmt = 0;
+  b->max_cols = 0;
   b->base_cur.resize(n);
   for (int i = 0; i < n; ++i) {
     lt_domain* d = b->m[i];
@@ -89,6 +92,7 @@ int build_descriptors(lt_batch* b) {
     b->km_max = std::max(b->km_max, a.km);
     b->max_imt = std::max(b->max_imt, a.imt);
     b->max_jmt = std::max(b->max_jmt, a.jmt);
+    b->max_cols = std::max(b->max_cols, (long)a.nx * a.ny);
   }
   b->total_items = item;
   if (b->stream) LT_CUDA_OK(cudaStreamSynchronize(b->stream));
@@ -112,14 +116,9 @@ bool descriptors_stale(const lt_batch* b) {
 // One step of every member at parity p, enqueued on the batch stream.
 int enqueue_step(lt_batch* b, int p) {
   cudaStream_t s = b->stream;
+  const int nmem = (int)b->m.size();
   int rc;
-  for (size_t i = 0; i < b->m.size(); ++i) {
-    Arena a = b->m[i]->a;
-    a.cur = b->base_cur[i] ^ p;
-    if ((rc = launch_surface(a, s))) return rc;
-    if ((rc = launch_interior_sum_sss(a, s))) return rc;
-    if ((rc = launch_halo_r8(a.net, 2, a.imt, a.jmt, a.ew_cyclic, a.tripole, s))) return rc;
-  }
+  if ((rc = launch_small_batch_pre(b->d_desc[p], nmem, b->max_imt, b->max_jmt, b->max_cols, s))) return rc;
   if (b->mixed) {
     if ((rc = launch_continuity_mixed_batch(b->d_desc[p], (int)b->m.size(), b->max_imt, b->max_jmt,
                                             b->cfg.continuity_tile_y, s)))
@@ -137,12 +136,7 @@ int enqueue_step(lt_batch* b, int p) {
       if (rc) return rc;
     }
   }
-  for (size_t i = 0; i < b->m.size(); ++i) {
-    Arena a = b->m[i]->a;
-    a.cur = b->base_cur[i] ^ p;
-    if ((rc = launch_halo_state(a, s))) return rc;
-  }
-  return LT_OK;
+  return launch_halo_state_batch(b->d_desc[p], nmem, b->max_imt, b->km_max, s);
 }
 
 int capture_graphs(lt_batch* b) {

@@ -33,9 +33,7 @@ __device__ __forceinline__ long q2(int j, int i, int imt) { return (long)j * imt
 // SSH mean stf; tracer_del4_2's surface floor on akt(T) (tracer.cpp:1315-1317);
 // salt flux of tracer_5 (tracer.cpp:1480-1520) and heat flux of tracer_6
 // (tracer.cpp:1545-1565) from the previous time level; net (both tracers).
-__global__ void k_surface(Arena a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void surface_col(const Arena& a, int i, int j) {
   if (i >= a.imt || j >= a.jmt) return;
   const long q = q2(j, i, a.imt);
   const lt_params& p = a.p;
@@ -66,15 +64,24 @@ __global__ void k_surface(Arena a) {
   a.stf_n[a.A + q] = sS;
 }
 
+__global__ void k_surface(Arena a) {
+  surface_col(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
+// every member's columns in one launch: blockIdx.z is the member
+__global__ void k_surface_batch(const MemberDesc* __restrict__ mem) {
+  surface_col(mem[blockIdx.z].a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
 // --------------------------------------------------------- deterministic sum
 // Fixed binary tree: blocks of 2048 consecutive terms, pairs (t, t+stride) for
 // stride = 1024..1, zero padding; repeated on the block sums until one value.
 constexpr int RB = 1024;
 
 template <class Term>
-__global__ void k_tree_first(Term term, long n, double* part) {
+__device__ __forceinline__ void tree_block(const Term& term, long n, double* part, long blk) {
   __shared__ double s[2 * RB];
-  const long base = (long)blockIdx.x * 2 * RB;
+  const long base = blk * 2 * RB;
   const int t = threadIdx.x;
   s[t] = (base + t < n) ? term(base + t) : 0.0;
   s[t + RB] = (base + t + RB < n) ? term(base + t + RB) : 0.0;
@@ -82,7 +89,12 @@ __global__ void k_tree_first(Term term, long n, double* part) {
     __syncthreads();
     if (t < stride) s[t] = s[t] + s[t + stride];
   }
-  if (t == 0) part[blockIdx.x] = s[0];
+  if (t == 0) part[blk] = s[0];
+}
+
+template <class Term>
+__global__ void k_tree_first(Term term, long n, double* part) {
+  tree_block(term, n, part, blockIdx.x);
 }
 
 struct ArrayTerm {
@@ -108,6 +120,41 @@ __global__ void k_finish_sss(double* scalars, const double* sum, double area_t) 
   scalars[0] = -sum[0] / area_t;
 }
 
+// The same tree for every member of a batch, pass by pass: pass 0 sums the
+// member's SSS terms into its red_part, pass p > 0 the block sums of pass
+// p-1; blockIdx.y is the member, blocks beyond a member's count at this pass
+// (or members whose tree ended) leave at once.
+__device__ __forceinline__ long tree_blocks(long n) {
+  const long nb = (n + 2 * RB - 1) / (2 * RB);
+  return nb < 1 ? 1 : nb;
+}
+
+__global__ void k_sss_tree_batch(const MemberDesc* __restrict__ mem, int pass) {
+  const Arena& a = mem[blockIdx.y].a;
+  long n = (long)a.nx * a.ny, nb = tree_blocks(n), off = 0;
+  for (int q = 0; q < pass; ++q) {
+    if (nb <= 1) return;
+    off += nb;
+    n = nb;
+    nb = tree_blocks(n);
+  }
+  if ((long)blockIdx.x >= nb) return;
+  if (pass == 0) tree_block(SssTerm{a.tarea, a.net + a.A, a.kmt, a.nx, a.imt}, n, a.red_part, blockIdx.x);
+  else tree_block(ArrayTerm{a.red_part + off - n}, n, a.red_part + off, blockIdx.x);
+}
+
+// the member's total (the last pass's single block sum) and fw_norm2
+__global__ void k_finish_sss_batch(const MemberDesc* __restrict__ mem, int nmem) {
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= nmem) return;
+  const Arena& a = mem[z].a;
+  long nb = tree_blocks((long)a.nx * a.ny), off = 0;
+  while (nb > 1) { off += nb; nb = tree_blocks(nb); }
+  const double sum = a.red_part[off];
+  a.scalars[4] = sum;
+  a.scalars[0] = -sum / a.p.area_t;
+}
+
 template <class Term>
 int tree_sum(Term term, long n, double* part, double* out, cudaStream_t s) {
   long nb = (n + 2 * RB - 1) / (2 * RB);
@@ -130,9 +177,8 @@ int tree_sum(Term term, long n, double* part, double* out, cudaStream_t s) {
 
 // ------------------------------------------------------------------ halo
 // In-place ghost fill of nz levels (e.g. net), one block per level.
-__global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripole) {
+__device__ __forceinline__ void halo_r8_level(double* lvl, int imt, int jmt, int ew_cyclic, int tripole) {
   extern __shared__ double top[];
-  double* lvl = f + (long)blockIdx.x * imt * jmt;
   for (int i = threadIdx.x; i < imt; i += blockDim.x) top[i] = lvl[2L * imt + i];
   __syncthreads();
   HaloCells hc{imt, jmt, tripole};
@@ -143,6 +189,16 @@ __global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripol
     double v;
     if (halo_cell_value(lvl, top, j, i, imt, jmt, ew_cyclic, tripole, v)) lvl[(long)j * imt + i] = v;
   }
+}
+
+__global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripole) {
+  halo_r8_level(f + (long)blockIdx.x * imt * jmt, imt, jmt, ew_cyclic, tripole);
+}
+
+// net (both tracers) of every member: blockIdx.x the level, blockIdx.y the member
+__global__ void k_halo_net_batch(const MemberDesc* __restrict__ mem) {
+  const Arena& a = mem[blockIdx.y].a;
+  halo_r8_level(a.net + (long)blockIdx.x * a.A, a.imt, a.jmt, a.ew_cyclic, a.tripole);
 }
 
 // ------------------------------------------------------------- continuity
@@ -869,10 +925,6 @@ __device__ __forceinline__ void ring_cell64(int q, int& hj, int& hi) {
   else { hj = q - 2 * HQX - TY + 1; hi = HQX - 1; }
 }
 
-struct ExactHw {
-  __device__ double operator()(double a, double b) const { return a * b; }
-};
-
 // kFp64CtasPerSm CTAs per SM: 228 KB of shared memory, 1 KB reserved per CTA
 static_assert(kFp64CtasPerSm * (sizeof(ExSmem) + 1024) <= 228 * 1024,
               "FP64 tracer tile no longer fits kFp64CtasPerSm CTAs per SM");
@@ -1179,9 +1231,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
 // the temperature's final ghost values, which is what vtl holds in the
 // reference between the two passes.
 template <bool DIAG>
-__global__ void k_halo_state(Arena a, int n) {
+__device__ __forceinline__ void halo_state_level(const Arena& a, int n, int k) {
   extern __shared__ double top[];
-  const int k = blockIdx.x;
   const int imt = a.imt, jmt = a.jmt;
   const long A = a.A, F = a.F, FB = a.FB;
   double* lvl = a.at[a.cur ^ 1] + n * F + (long)k * A;
@@ -1218,6 +1269,19 @@ __global__ void k_halo_state(Arena a, int n) {
     lvl[q] = v;
     lvlb[q] = v;
   }
+}
+
+template <bool DIAG>
+__global__ void k_halo_state(Arena a, int n) {
+  halo_state_level<DIAG>(a, n, blockIdx.x);
+}
+
+// tracer n of every member: blockIdx.x the level, blockIdx.y the member
+__global__ void k_halo_state_batch(const MemberDesc* __restrict__ mem, int n) {
+  const Arena& a = mem[blockIdx.y].a;
+  if ((int)blockIdx.x >= a.km) return;
+  if (a.diagnostics) halo_state_level<true>(a, n, blockIdx.x);
+  else halo_state_level<false>(a, n, blockIdx.x);
 }
 
 __global__ void k_vtl_clobber(Arena a) {
@@ -1318,6 +1382,38 @@ int launch_halo_state(const Arena& a, cudaStream_t s) {
   for (int n = 0; n < 2; ++n) {
     if (a.diagnostics) k_halo_state<true><<<a.km, 256, a.imt * sizeof(double), s>>>(a, n);
     else k_halo_state<false><<<a.km, 256, a.imt * sizeof(double), s>>>(a, n);
+    LT_LAUNCHED();
+  }
+  return LT_OK;
+}
+
+// The small kernels of a batch step over every member at once (member
+// descriptors in device memory; the largest member's sizes set the grids).
+int launch_small_batch_pre(const MemberDesc* mem, int nmem, int max_imt, int max_jmt, long max_cols,
+                           cudaStream_t s) {
+  {
+    dim3 b(32, 8), g((max_imt + 31) / 32, (max_jmt + 7) / 8, nmem);
+    k_surface_batch<<<g, b, 0, s>>>(mem);
+    LT_LAUNCHED();
+  }
+  long nb = (max_cols + 2 * RB - 1) / (2 * RB);
+  if (nb < 1) nb = 1;
+  for (int pass = 0;; ++pass) {
+    k_sss_tree_batch<<<dim3((unsigned)nb, nmem), RB, 0, s>>>(mem, pass);
+    LT_LAUNCHED();
+    if (nb <= 1) break;
+    nb = (nb + 2 * RB - 1) / (2 * RB);
+  }
+  k_finish_sss_batch<<<(nmem + 127) / 128, 128, 0, s>>>(mem, nmem);
+  LT_LAUNCHED();
+  k_halo_net_batch<<<dim3(2, nmem), 256, max_imt * sizeof(double), s>>>(mem);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_halo_state_batch(const MemberDesc* mem, int nmem, int max_imt, int km_max, cudaStream_t s) {
+  for (int n = 0; n < 2; ++n) {
+    k_halo_state_batch<<<dim3(km_max, nmem), 256, max_imt * sizeof(double), s>>>(mem, n);
     LT_LAUNCHED();
   }
   return LT_OK;

@@ -133,6 +133,13 @@ int launch_tracer_mixed_batch(const MemberDesc* mem, int nmem, long total, doubl
                               cudaStream_t s);
 int launch_continuity_mixed_batch(const MemberDesc* mem, int nmem, int max_imt, int max_jmt, int cby,
                                   cudaStream_t s);
+// The small kernels of a batch step for every member in one launch each:
+// surface fluxes, the SSS-norm tree (one launch per tree pass; max_cols is
+// the largest member's nx * ny) and its finish, the net halo; and the state
+// halo (two launches, temperature first).
+int launch_small_batch_pre(const MemberDesc* mem, int nmem, int max_imt, int max_jmt, long max_cols,
+                           cudaStream_t s);
+int launch_halo_state_batch(const MemberDesc* mem, int nmem, int max_imt, int km_max, cudaStream_t s);
 size_t mixed_tracer_smem_bytes();
 // sets the batched column kernel's shared-memory size on the current device
 int prepare_tracer_mixed_batch();
