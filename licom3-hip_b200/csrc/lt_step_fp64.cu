@@ -1190,13 +1190,26 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       __syncthreads();  // level k is no longer read: its slot takes level k-NSX
       if (k - NSX >= 0) issue(k - NSX);
     }
-    // ---- substitution, top down
+    // ---- substitution, top down: the elimination coefficients of SUB levels
+    // are loaded together ahead of their stores (the scratch round trip is
+    // paid once per SUB levels, not once per level)
     if (inner) {
       double x = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < km; ++k) {
+      constexpr int SUB = 8;
+      for (int k0 = 0; k0 < km; k0 += SUB) {
+        double evs[SUB], fvs[SUB];
+#pragma unroll
+        for (int c = 0; c < SUB; ++c) {
+          const double* sl = scr + (long)(k0 + c) * NV * TTHREADS;
+          evs[c] = k0 + c < km ? sl[tid] : 0.0;
+          fvs[c] = k0 + c < km ? sl[TTHREADS + tid] : 0.0;
+        }
+#pragma unroll
+      for (int c = 0; c < SUB; ++c) {
+        const int k = k0 + c;
+        if (k >= km) break;
         const double* sl = scr + (long)k * NV * TTHREADS;
-        const double ev = sl[tid], fv = sl[TTHREADS + tid];
+        const double ev = evs[c], fv = fvs[c];
         const long cg = (long)k * A + qo;
         double v;
         if (k < kz) {
@@ -1217,6 +1230,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         }
         at_out[cg] = v;
         atb_out[(long)(k + 1) * A + qo] = v;
+      }
       }
     }
   }

@@ -773,12 +773,25 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       __syncthreads();
       if (k - NSM >= 0) issue(k - NSM);
     }
+    // substitution, top down: the elimination coefficients of SUB levels are
+    // loaded together ahead of their stores (one scratch round trip per SUB
+    // levels)
     if (inner) {
       double x = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < km; ++k) {
-        const double* sl = scr + (long)k * 2 * MTH;
-        const double ev = sl[tid], fv = sl[MTH + tid];
+      constexpr int SUB = 8;
+      for (int k0 = 0; k0 < km; k0 += SUB) {
+        double evs[SUB], fvs[SUB];
+#pragma unroll
+        for (int c = 0; c < SUB; ++c) {
+          const double* sl = scr + (long)(k0 + c) * 2 * MTH;
+          evs[c] = k0 + c < km ? sl[tid] : 0.0;
+          fvs[c] = k0 + c < km ? sl[MTH + tid] : 0.0;
+        }
+#pragma unroll
+      for (int c = 0; c < SUB; ++c) {
+        const int k = k0 + c;
+        if (k >= km) break;
+        const double ev = evs[c], fv = fvs[c];
         double v;
         if (k < kz) {
           v = (k == 0) ? ev * stf + fv : ev * x + fv;
@@ -789,6 +802,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         const long cg = (long)k * A + qo;
         at_out[cg] = v;
         atb_out[(long)(k + 1) * A + qo] = v;
+      }
       }
     }
   }
