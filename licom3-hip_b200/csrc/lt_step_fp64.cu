@@ -330,10 +330,21 @@ __global__ void __launch_bounds__(256) k_cont_march64(Arena a) {
   const double ohbt = a.ohbt[qo];
   const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
   double wsp = a.ws[qo];
-  for (int k = 1; k < km; ++k) {
-    const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + a.wka[(long)(k - 1) * A + qo]));
-    a.ws[(long)k * A + qo] = raw * fac;
-    wsp = raw;
+  // upward integration; the wka of CH levels are loaded together ahead of
+  // their stores (one round trip per CH levels)
+  constexpr int CH = 8;
+  for (int k0 = 1; k0 < km; k0 += CH) {
+    double wk[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) wk[c] = k0 + c < km ? a.wka[(long)(k0 + c - 1) * A + qo] : 0.0;
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const int k = k0 + c;
+      if (k >= km) break;
+      const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + wk[c]));
+      a.ws[(long)k * A + qo] = raw * fac;
+      wsp = raw;
+    }
   }
 }
 
