@@ -157,7 +157,8 @@ int lt_derive_masks(lt_domain* dom);
 int lt_step(lt_domain* dom, int nsteps);
 /* One step taking this step's surface forcing from HOST buffers (swv, nswv,
  * sst, sss, fresh, seaice; each [jmt][imt] f64, any may be NULL to keep the
- * resident field; pinned memory makes the copies asynchronous) and returning
+ * resident field; pinned memory makes the copies asynchronous, on a copy
+ * stream of the domain, overlapped with the step's continuity) and returning
  * fw_norm2 (fw_norm2_out) and, if content2_out is not NULL, the two global
  * tracer integrals sum(tarea*dzp*vit*tracer).  Synchronous. */
 int lt_step_host(lt_domain* dom, const double* const forcing6[6], double* fw_norm2_out, double* content2_out);
@@ -285,9 +286,12 @@ int lt_last_step_ms(lt_domain* dom, float* ms);
  * measures, on the domain's stream, around any sequence of calls. */
 int lt_mark(lt_domain* dom, int which);
 /* Per-phase device timing: lt_profile(dom, 1) records CUDA events around the
- * six launch phases of each step (surface fluxes, SSS-norm sum, net halo,
- * continuity, tracer column kernel, state halo); lt_phase_ms sums them over
- * the recorded steps into ms[0..5] and returns the number of steps. */
+ * six launch phases of each step; lt_phase_ms sums them over the recorded
+ * steps into ms[0..5] = surface fluxes, SSS-norm sum, net halo, continuity
+ * (with the SSH mean it needs), tracer column kernel, state halo, and returns
+ * the number of steps.  The continuity is launched first (it needs no
+ * forcing); with lt_step_host, the surface-flux phase includes any wait for
+ * the forcing copies still in flight after it. */
 int lt_profile(lt_domain* dom, int on);
 int lt_phase_ms(lt_domain* dom, float* ms, int nphase);
 /* Select the tracer column kernel: 1 = TMA-fed pipeline (default where the

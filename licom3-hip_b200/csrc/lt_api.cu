@@ -281,7 +281,7 @@ bool build_tracer_maps(const Arena& a, TracerMaps* m) {
   return ok;
 }
 
-int run_step(lt_domain* d) {
+int run_step(lt_domain* d, cudaEvent_t forcing_ready) {
   Arena& a = d->a;
   cudaStream_t s = d->stream;
   int rc;
@@ -290,26 +290,29 @@ int run_step(lt_domain* d) {
     ev = &d->prof_ev[(size_t)d->prof_steps * (LT_NPHASE + 1)];
     d->prof_steps++;
   }
+  // events bound the phases in launch order (LT_PHASE_ORDER)
   auto mark = [&](int ph) { if (ev) cudaEventRecord(ev[ph], s); };
   mark(0);
-  if ((rc = launch_surface(a, s))) return rc;
+  // continuity first: it reads the SSH mean and the velocities, not the
+  // surface forcing
+  if ((rc = launch_ssh(a, s))) return rc;
+  if (a.precision == LT_PREC_MIXED) rc = launch_continuity_mixed(a, s);
+  else rc = launch_continuity_fp64(a, s);
+  if (rc) return rc;
   mark(1);
-  if ((rc = launch_interior_sum_sss(a, s))) return rc;
+  if (forcing_ready) LT_CUDA_OK(cudaStreamWaitEvent(s, forcing_ready, 0));
+  if ((rc = launch_surface_fluxes(a, s))) return rc;
   mark(2);
-  if ((rc = launch_halo_r8(a.net, 2, a.imt, a.jmt, a.ew_cyclic, a.tripole, s))) return rc;
+  if ((rc = launch_interior_sum_sss(a, s))) return rc;
   mark(3);
+  if ((rc = launch_halo_r8(a.net, 2, a.imt, a.jmt, a.ew_cyclic, a.tripole, s))) return rc;
+  mark(4);
   if (a.precision == LT_PREC_MIXED) {
-    if ((rc = launch_continuity_mixed(a, s))) return rc;
-    mark(4);
     if ((rc = launch_tracer_tma_mixed(a, d->maps, s, d->tma_grid))) return rc;
+  } else if (d->use_tma) {
+    if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid))) return rc;
   } else {
-    if ((rc = launch_continuity_fp64(a, s))) return rc;
-    mark(4);
-    if (d->use_tma) {
-      if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid))) return rc;
-    } else {
-      if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
-    }
+    if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
   }
   mark(5);
   if ((rc = launch_halo_state(a, s))) return rc;
@@ -447,7 +450,7 @@ int lt_phase_ms(lt_domain* d, float* ms, int nphase) {
     for (int p = 0; p < LT_NPHASE; ++p) {
       float t = 0.0f;
       LT_CUDA_OK(cudaEventElapsedTime(&t, ev[p], ev[p + 1]));
-      ms[p] += t;
+      ms[LT_PHASE_ORDER[p]] += t;
     }
   }
   return d->prof_steps;
@@ -519,6 +522,9 @@ int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
   cudaMemsetAsync(base, 0, pl.off, d->stream);
   cudaEventCreate(&d->ev0);
   cudaEventCreate(&d->ev1);
+  cudaEventCreateWithFlags(&d->ev_free, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&d->ev_forcing, cudaEventDisableTiming);
+  cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking);
   // TMA-fed tracer kernel where the row pitch is a multiple of 16 bytes
   d->use_tma = build_tracer_maps(d->a, &d->maps);
   // one persistent CTA per resident slot (kFp64CtasPerSm, kMixedCtasPerSm
@@ -538,8 +544,12 @@ int lt_destroy(lt_domain* d) {
   if (g_shim == d) g_shim = nullptr;
   cudaStreamSynchronize(d->stream);
   for (void* p : d->allocations) cudaFree(p);
+  if (d->copy_stream) cudaStreamSynchronize(d->copy_stream);
   if (d->ev0) cudaEventDestroy(d->ev0);
   if (d->ev1) cudaEventDestroy(d->ev1);
+  if (d->ev_free) cudaEventDestroy(d->ev_free);
+  if (d->ev_forcing) cudaEventDestroy(d->ev_forcing);
+  if (d->copy_stream) cudaStreamDestroy(d->copy_stream);
   for (auto e : d->prof_ev) cudaEventDestroy(e);
   if (d->owns_stream) cudaStreamDestroy(d->stream);
   delete d;
@@ -636,10 +646,19 @@ int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2
   Arena& a = d->a;
   double* dst[6] = {a.swv, a.nswv, a.sst, a.sss, a.fresh, a.seaice};
   const size_t bytes = sizeof(double) * a.A;
-  if (forcing6)
+  // The forcing goes up on the copy stream once the domain's earlier work
+  // (which may read the previous forcing) is done, while the step's
+  // continuity runs; the surface fluxes wait for it.
+  cudaEvent_t ready = nullptr;
+  if (forcing6) {
+    LT_CUDA_OK(cudaEventRecord(d->ev_free, d->stream));
+    LT_CUDA_OK(cudaStreamWaitEvent(d->copy_stream, d->ev_free, 0));
     for (int m = 0; m < 6; ++m)
-      if (forcing6[m]) LT_CUDA_OK(cudaMemcpyAsync(dst[m], forcing6[m], bytes, cudaMemcpyHostToDevice, d->stream));
-  int rc = run_step(d);
+      if (forcing6[m]) LT_CUDA_OK(cudaMemcpyAsync(dst[m], forcing6[m], bytes, cudaMemcpyHostToDevice, d->copy_stream));
+    LT_CUDA_OK(cudaEventRecord(d->ev_forcing, d->copy_stream));
+    ready = d->ev_forcing;
+  }
+  int rc = run_step(d, ready);
   if (rc) return rc;
   if (content2_out) {
     if ((rc = launch_tracer_content(a, d->stream))) return rc;

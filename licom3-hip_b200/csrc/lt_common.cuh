@@ -105,6 +105,10 @@ void set_error(const char* fmt, ...);
 
 // host launchers (defined in the step translation units)
 int launch_surface(const Arena& a, cudaStream_t s);
+// the two parts of launch_surface: the SSH mean (h0f_out, stf_ssh) and the
+// surface fluxes, net and the mixing floor (which read stf_ssh)
+int launch_ssh(const Arena& a, cudaStream_t s);
+int launch_surface_fluxes(const Arena& a, cudaStream_t s);
 int launch_continuity_fp64(const Arena& a, cudaStream_t s);
 int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots);
 int launch_halo_state(const Arena& a, cudaStream_t s);

@@ -6,12 +6,17 @@
 #include "lt_tracer_tma.cuh"
 
 constexpr int LT_NPHASE = 6;       // surface, sss sum, net halo, continuity, tracer, state halo
+// launch order of the phases in a step (continuity first: it needs no
+// forcing, so it runs while lt_step_host's forcing copies are in flight)
+constexpr int LT_PHASE_ORDER[LT_NPHASE] = {3, 0, 1, 2, 4, 5};
 constexpr int LT_PROF_STEPS = 512;  // steps whose phase events are kept
 
 struct lt_domain {
   lt::Arena a;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaStream_t copy_stream = nullptr;          // lt_step_host's forcing copies
+  cudaEvent_t ev_free = nullptr, ev_forcing = nullptr;
   int profile = 0;
   int prof_steps = 0;
   std::vector<cudaEvent_t> prof_ev;   // [LT_PROF_STEPS][LT_NPHASE + 1]
@@ -26,8 +31,9 @@ struct lt_domain {
 };
 
 namespace lt {
-// one tracer step of a domain on its own stream (the tracer_ body)
-int run_step(lt_domain* d);
+// one tracer step of a domain on its own stream (the tracer_ body); the
+// surface fluxes wait for forcing_ready when it is given
+int run_step(lt_domain* d, cudaEvent_t forcing_ready = nullptr);
 // after the stream has drained: LT_E_TIMEOUT once if a column kernel's
 // bounded wait ran out since the last check
 int timeout_status(lt_domain* d);

@@ -33,14 +33,20 @@ __device__ __forceinline__ long q2(int j, int i, int imt) { return (long)j * imt
 // SSH mean stf; tracer_del4_2's surface floor on akt(T) (tracer.cpp:1315-1317);
 // salt flux of tracer_5 (tracer.cpp:1480-1520) and heat flux of tracer_6
 // (tracer.cpp:1545-1565) from the previous time level; net (both tracers).
-__device__ __forceinline__ void surface_col(const Arena& a, int i, int j) {
-  if (i >= a.imt || j >= a.jmt) return;
-  const long q = q2(j, i, a.imt);
+// The SSH part (h0f_out, stf_ssh), which the continuity needs, and the flux
+// part, which needs the surface forcing, are separate so that a step can
+// run the continuity while its forcing is being copied in.
+__device__ __forceinline__ double ssh_col(const Arena& a, long q) {
   const lt_params& p = a.p;
   const double h0 = a.h0f[q] * p.onbc;
   a.h0f_out[q] = h0;
   const double ssh = 0.5 * h0 + 0.5 * a.h0l[q];
   a.stf_ssh[q] = ssh;
+  return ssh;
+}
+
+__device__ __forceinline__ void flux_col(const Arena& a, int i, int j, long q, double ssh) {
+  const lt_params& p = a.p;
   if (i >= 1 && i < a.imt - 1 && j >= 1 && j < a.jmt - 1) {
     if (a.akt) {
       if (a.akt[q] < p.dwndmix) a.akt[q] = p.dwndmix;
@@ -64,8 +70,27 @@ __device__ __forceinline__ void surface_col(const Arena& a, int i, int j) {
   a.stf_n[a.A + q] = sS;
 }
 
+__device__ __forceinline__ void surface_col(const Arena& a, int i, int j) {
+  if (i >= a.imt || j >= a.jmt) return;
+  const long q = q2(j, i, a.imt);
+  flux_col(a, i, j, q, ssh_col(a, q));
+}
+
 __global__ void k_surface(Arena a) {
   surface_col(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
+__global__ void k_ssh(Arena a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.imt || j >= a.jmt) return;
+  ssh_col(a, q2(j, i, a.imt));
+}
+
+__global__ void k_surface_fluxes(Arena a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= a.imt || j >= a.jmt) return;
+  const long q = q2(j, i, a.imt);
+  flux_col(a, i, j, q, a.stf_ssh[q]);
 }
 
 // every member's columns in one launch: blockIdx.z is the member
@@ -1322,6 +1347,20 @@ __global__ void k_vtl_clobber(Arena a) {
 int launch_surface(const Arena& a, cudaStream_t s) {
   dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
   k_surface<<<g, b, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_ssh(const Arena& a, cudaStream_t s) {
+  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
+  k_ssh<<<g, b, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
+int launch_surface_fluxes(const Arena& a, cudaStream_t s) {
+  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
+  k_surface_fluxes<<<g, b, 0, s>>>(a);
   LT_LAUNCHED();
   return LT_OK;
 }
