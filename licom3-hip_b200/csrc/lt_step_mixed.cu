@@ -213,11 +213,18 @@ __global__ void __launch_bounds__(CBX * kContTileY) k_cont_march32(Arena a) {
 
 // every member's tiles in one launch: blockIdx.z is the member; tiles beyond
 // a smaller member's grid leave at once
+// (the member's arena is read from a shared-memory copy, which the march's
+// global stores cannot alias, so its fields stay in registers across levels)
 template <int CBY>
 __global__ void __launch_bounds__(CBX * CBY) k_cont_batch(const MemberDesc* __restrict__ mem) {
-  const Arena& a = mem[blockIdx.z].a;
-  if ((int)blockIdx.x * CBX >= a.imt || (int)blockIdx.y * CBY >= a.jmt) return;
-  cont_tile<CBY>(a, blockIdx.x, blockIdx.y);
+  __shared__ __align__(16) unsigned char s_arena[sizeof(Arena)];
+  const Arena& g = mem[blockIdx.z].a;
+  if ((int)blockIdx.x * CBX >= g.imt || (int)blockIdx.y * CBY >= g.jmt) return;
+  const int tid = threadIdx.y * CBX + threadIdx.x;
+  for (int t = tid; t < (int)(sizeof(Arena) / 16); t += CBX * CBY)
+    reinterpret_cast<uint4*>(s_arena)[t] = reinterpret_cast<const uint4*>(&g)[t];
+  __syncthreads();
+  cont_tile<CBY>(*reinterpret_cast<const Arena*>(s_arena), blockIdx.x, blockIdx.y);
 }
 
 }  // namespace
@@ -834,17 +841,37 @@ __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
 // (tile, tracer) items, member after member, so neighbouring CTAs work on
 // neighbouring tiles of the same member.  Each CTA's items ascend, so its
 // member index only moves forward.
+// The current member's arena is copied into shared memory behind MxSmem:
+// read from there, its fields cannot alias the kernel's global stores, so
+// the compiler keeps them across the level loop instead of reloading them
+// from global memory at every level.
+constexpr size_t kBatchArenaOff = (sizeof(MxSmem) + 15) / 16 * 16;
+constexpr size_t kBatchSmem = kBatchArenaOff + sizeof(Arena);
+static_assert(sizeof(Arena) % 16 == 0, "arena copied as 16-byte words");
+static_assert(kMixedCtasPerSm * (kBatchSmem + 1024) <= 228 * 1024,
+              "batched mixed tracer tile no longer fits kMixedCtasPerSm CTAs per SM");
+
 __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
     k_tracer_mixed_batch(const MemberDesc* __restrict__ mem, int nmem, long total, double* scratch, int km_max) {
   MxSmem& S = mixed_smem_init();
+  extern __shared__ __align__(128) unsigned char smem_mx[];
+  Arena& sa = *reinterpret_cast<Arena*>(smem_mx + kBatchArenaOff);
   uint32_t par = 0, outstanding = 0;
   double* scr = scratch + (long)blockIdx.x * km_max * 2 * MTH;
-  int m = 0;
+  int m = 0, staged = -1;
   for (long w = blockIdx.x; w < total; w += gridDim.x) {
     while (m + 1 < nmem && mem[m + 1].item0 <= w) ++m;
     const MemberDesc& d = mem[m];
+    if (m != staged) {
+      __syncthreads();   // the previous item no longer reads the staged arena
+      const uint4* src = reinterpret_cast<const uint4*>(&d.a);
+      uint4* dst = reinterpret_cast<uint4*>(&sa);
+      for (int t = threadIdx.x; t < (int)(sizeof(Arena) / 16); t += MTH) dst[t] = src[t];
+      __syncthreads();
+      staged = m;
+    }
     const long local = w - d.item0;
-    if (!mixed_item(S, d.a, d.maps, scr, d.ntx, local >> 1, (int)(local & 1), par, outstanding)) return;
+    if (!mixed_item(S, sa, d.maps, scr, d.ntx, local >> 1, (int)(local & 1), par, outstanding)) return;
   }
 }
 
@@ -868,7 +895,7 @@ size_t mixed_tracer_smem_bytes() { return sizeof(MxSmem); }
 
 int prepare_tracer_mixed_batch() {
   LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)sizeof(MxSmem)));
+                                  (int)kBatchSmem));
   return LT_OK;
 }
 
@@ -876,7 +903,7 @@ int prepare_tracer_mixed_batch() {
 // inside a stream capture)
 int launch_tracer_mixed_batch(const MemberDesc* mem, int nmem, long total, double* scratch, int km_max, int grid,
                               cudaStream_t s) {
-  k_tracer_mixed_batch<<<grid, MTH, sizeof(MxSmem), s>>>(mem, nmem, total, scratch, km_max);
+  k_tracer_mixed_batch<<<grid, MTH, kBatchSmem, s>>>(mem, nmem, total, scratch, km_max);
   LT_LAUNCHED();
   return LT_OK;
 }
