@@ -833,6 +833,12 @@ struct ExSmem {
   LevelSlot<double> slot[NSX];
   unsigned char flag[3][HN];   // limiter flag (a00 > amax || a00 < amin) per level parity of three
   double d2[HN];
+  // level-free metric terms of the 1-halo region: tarea_r per cell, htw*hun
+  // at its x faces (west face of column x0-1+fi), hts*hue at its y faces
+  // (south face of row y0-2+fj)
+  double tr[HN];
+  double hw[HQY * (HQX + 1)];
+  double hs[(HQY + 1) * HQX];
   int kmt[(TY + 4) * SW];
   uint64_t bar[NSX];
 };
@@ -861,10 +867,9 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
       return false;
     }
     const int r = r2(hj, hi), u = ru(hj, hi), v = rv(hj, hi);
-    const long q = (long)gj * imt + gi;
-    const double tr = __ldg(a.tarea_r + q);
-    const double hwe = __ldg(a.htw + q + 1) * __ldg(a.hun + q + 1), hww = __ldg(a.htw + q) * __ldg(a.hun + q);
-    const double hss = __ldg(a.hts + q) * __ldg(a.hue + q), hsn = __ldg(a.hts + q - imt) * __ldg(a.hue + q - imt);
+    const double tr = S.tr[m];
+    const double hwe = S.hw[hj * (HQX + 1) + hi + 1], hww = S.hw[hj * (HQX + 1) + hi];
+    const double hss = S.hs[(hj + 1) * HQX + hi], hsn = S.hs[hj * HQX + hi];
     const double c = at_c[r], e = at_c[r + 1], w = at_c[r - 1], s = at_c[r + SW], n = at_c[r - SW];
     const double ue = uw[u + 1], uwc = uw[u];
     const double vsc = vs[v], vn = vs[v - SW];
@@ -1016,6 +1021,22 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
       S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
     }
+    // the level-free metric terms (products formed once, as the reference
+    // forms them at every use)
+    for (int m = tid; m < HN; m += TTHREADS) {
+      const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
+      S.tr[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.tarea_r[(long)gj * imt + gi] : 0.0;
+    }
+    for (int m = tid; m < HQY * (HQX + 1); m += TTHREADS) {
+      const int gj = y0 - 1 + m / (HQX + 1), gi = x0 - 1 + m % (HQX + 1);
+      const long q = (long)gj * imt + gi;
+      S.hw[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.htw[q] * a.hun[q] : 0.0;
+    }
+    for (int m = tid; m < (HQY + 1) * HQX; m += TTHREADS) {
+      const int gj = y0 - 2 + m / HQX, gi = x0 - 1 + m % HQX;
+      const long q = (long)gj * imt + gi;
+      S.hs[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.hts[q] * a.hue[q] : 0.0;
+    }
 
     const bool own = (i < imt && j < jmt);
     const bool ring = own && i >= 1 && i < imt - 1 && j >= 1 && j < jmt - 1;
@@ -1060,10 +1081,9 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         const double* at_c = Lk.at;
         const double* at_u = k > 0 ? S.slot[(k - 1) % NSX].at : nullptr;
         const unsigned char* fl = S.flag[k % 3];
-        const double tr = __ldg(a.tarea_r + qo);
-        const double hwe = __ldg(a.htw + qo + 1) * __ldg(a.hun + qo + 1), hww = __ldg(a.htw + qo) * __ldg(a.hun + qo);
-        const double hss = __ldg(a.hts + qo) * __ldg(a.hue + qo);
-        const double hsn = __ldg(a.hts + qo - imt) * __ldg(a.hue + qo - imt);
+        const double tr = S.tr[hc];
+        const double hwe = S.hw[(ty + 1) * (HQX + 1) + tx + 2], hww = S.hw[(ty + 1) * (HQX + 1) + tx + 1];
+        const double hss = S.hs[(ty + 2) * HQX + tx + 1], hsn = S.hs[(ty + 1) * HQX + tx + 1];
         const double c = at_c[rc], e = at_c[rc + 1], w = at_c[rc - 1], s = at_c[rc + SW], nn = at_c[rc - SW];
         const double ue = Lk.uw[uc + 1], uwc = Lk.uw[uc], vsc = Lk.vs[vc], vn = Lk.vs[vc - SW];
         const bool self = out_k;
