@@ -108,6 +108,10 @@ int admit(lt_server* s) {
       q.inputs = std::async(std::launch::async, build_inputs, q.r.domain);
       q.building = true;
     }
+    // with requests resident, the device keeps stepping them while the head
+    // request's inputs are still being built: admit it at a later iteration
+    // rather than wait here (first come, first served is kept)
+    if (!s->active.empty() && q.inputs.wait_for(std::chrono::seconds(0)) != std::future_status::ready) break;
     auto built = q.inputs.get();
     q.building = false;
     lt_synth* syn = built.second;
