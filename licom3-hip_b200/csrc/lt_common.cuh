@@ -14,8 +14,9 @@ constexpr int TX = 32;
 constexpr int TY = 8;
 constexpr int TTHREADS = TX * TY;
 // Persistent CTAs per SM of the column kernels (their shared-memory footprint
-// decides): 3 of 256 threads for both.
-constexpr int kFp64CtasPerSm = 3;
+// decides): FP64 2 of 256 threads (its tile's metric and biharmonic
+// coefficients staged in shared memory, no register spills), mixed 3 of 256.
+constexpr int kFp64CtasPerSm = 2;
 constexpr int kMixedCtasPerSm = 3;
 // The mixed column kernel's tile: TX x kMixedTileY columns, one thread each.
 constexpr int kMixedTileY = 8;

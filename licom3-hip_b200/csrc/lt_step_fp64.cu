@@ -829,6 +829,7 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
 // the 2-D metric terms are read through L1 (the same 2-D values serve every
 // level), so kFp64CtasPerSm CTAs fit on an SM.
 constexpr int NSX = 3;
+constexpr bool kStageDel4 = kFp64CtasPerSm <= 2;
 struct ExSmem {
   LevelSlot<double> slot[NSX];
   unsigned char flag[3][HN];   // limiter flag (a00 > amax || a00 < amin) per level parity of three
@@ -839,6 +840,9 @@ struct ExSmem {
   double tr[HN];
   double hw[HQY * (HQX + 1)];
   double hs[(HQY + 1) * HQX];
+  // the biharmonic coefficients dtn, dts, dte, dtw, ahf of the 1-halo region
+  // where two CTAs per SM leave the room (read through L1 otherwise)
+  double dt5[kStageDel4 ? 5 : 1][kStageDel4 ? HN : 1];
   int kmt[(TY + 4) * SW];
   uint64_t bar[NSX];
 };
@@ -936,6 +940,13 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
   }
 }
 
+// biharmonic coefficient c (dtn, dts, dte, dtw, ahf) of region cell m at q
+__device__ __forceinline__ double del4c(const ExSmem& S, const Arena& a, int c, int m, long q) {
+  if (kStageDel4) return S.dt5[c][m];
+  const double* f = c == 0 ? a.dtn : c == 1 ? a.dts : c == 2 ? a.dte : c == 3 ? a.dtw : a.ahf;
+  return __ldg(f + q);
+}
+
 // First Laplacian of atb at level kk for one cell (hj, hi) of the 1-halo region.
 __device__ __forceinline__ void del4_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0) {
   const double* atb = S.slot[kk % NSX].atb;
@@ -947,12 +958,12 @@ __device__ __forceinline__ void del4_one64(ExSmem& S, const Arena& a, int kk, in
     const long q = (long)gj * a.imt + gi;
     double h = 0.0, cc = 0.0;
     if (kk <= S.kmt[r] - 1) {
-      if (kk <= S.kmt[r - SW] - 1) { const double cf = __ldg(a.dtn + q); h += cf * atb[r - SW]; cc -= cf; }
-      if (kk <= S.kmt[r + SW] - 1) { const double cf = __ldg(a.dts + q); h += cf * atb[r + SW]; cc -= cf; }
-      if (kk <= S.kmt[r + 1] - 1) { const double cf = __ldg(a.dte + q); h += cf * atb[r + 1]; cc -= cf; }
-      if (kk <= S.kmt[r - 1] - 1) { const double cf = __ldg(a.dtw + q); h += cf * atb[r - 1]; cc -= cf; }
+      if (kk <= S.kmt[r - SW] - 1) { const double cf = del4c(S, a, 0, m, q); h += cf * atb[r - SW]; cc -= cf; }
+      if (kk <= S.kmt[r + SW] - 1) { const double cf = del4c(S, a, 1, m, q); h += cf * atb[r + SW]; cc -= cf; }
+      if (kk <= S.kmt[r + 1] - 1) { const double cf = del4c(S, a, 2, m, q); h += cf * atb[r + 1]; cc -= cf; }
+      if (kk <= S.kmt[r - 1] - 1) { const double cf = del4c(S, a, 3, m, q); h += cf * atb[r - 1]; cc -= cf; }
     }
-    S.d2[m] = __ldg(a.ahf + q) * (cc * atb[r] + h);
+    S.d2[m] = del4c(S, a, 4, m, q) * (cc * atb[r] + h);
   }
 }
 
@@ -1025,7 +1036,16 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // forms them at every use)
     for (int m = tid; m < HN; m += TTHREADS) {
       const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
-      S.tr[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.tarea_r[(long)gj * imt + gi] : 0.0;
+      const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+      const long q = in ? (long)gj * imt + gi : 0;
+      S.tr[m] = in ? a.tarea_r[q] : 0.0;
+      if (kStageDel4) {
+        S.dt5[0][m] = in ? a.dtn[q] : 0.0;
+        S.dt5[1][m] = in ? a.dts[q] : 0.0;
+        S.dt5[2][m] = in ? a.dte[q] : 0.0;
+        S.dt5[3][m] = in ? a.dtw[q] : 0.0;
+        S.dt5[4][m] = in ? a.ahf[q] : 0.0;
+      }
     }
     for (int m = tid; m < HQY * (HQX + 1); m += TTHREADS) {
       const int gj = y0 - 1 + m / (HQX + 1), gi = x0 - 1 + m % (HQX + 1);
@@ -1160,10 +1180,10 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
             const int r = rc;
             double h = 0.0, cc = 0.0;
             if (k <= S.kmt[r] - 1) {
-              if (k <= S.kmt[r - SW] - 1) { const double cf = __ldg(a.dtn + qo); h += cf * S.d2[hc - HQX]; cc -= cf; }
-              if (k <= S.kmt[r + SW] - 1) { const double cf = __ldg(a.dts + qo); h += cf * S.d2[hc + HQX]; cc -= cf; }
-              if (k <= S.kmt[r + 1] - 1) { const double cf = __ldg(a.dte + qo); h += cf * S.d2[hc + 1]; cc -= cf; }
-              if (k <= S.kmt[r - 1] - 1) { const double cf = __ldg(a.dtw + qo); h += cf * S.d2[hc - 1]; cc -= cf; }
+              if (k <= S.kmt[r - SW] - 1) { const double cf = del4c(S, a, 0, hc, qo); h += cf * S.d2[hc - HQX]; cc -= cf; }
+              if (k <= S.kmt[r + SW] - 1) { const double cf = del4c(S, a, 1, hc, qo); h += cf * S.d2[hc + HQX]; cc -= cf; }
+              if (k <= S.kmt[r + 1] - 1) { const double cf = del4c(S, a, 2, hc, qo); h += cf * S.d2[hc + 1]; cc -= cf; }
+              if (k <= S.kmt[r - 1] - 1) { const double cf = del4c(S, a, 3, hc, qo); h += cf * S.d2[hc - 1]; cc -= cf; }
             }
             tf += p.ah * (cc * S.d2[hc] + h);
           }

@@ -235,6 +235,32 @@ def test_step_host_reports_scalars(lt):
     assert bits_equal(dom.get("AT"), o.get("AT"))
 
 
+def test_step_host_new_forcing_every_step(lt):
+    """lt_step_host uploads each step's forcing on a copy stream while the
+    step's continuity runs: several steps, each with its own forcing, match
+    the oracle given the same forcing before each of its steps, bit for bit
+    (mixed-precision domains take the same path)."""
+    syn, f = make(lt, 96, 56, 16, forced=1, cap_north=0)
+    dom = gpu_domain(lt, syn, f)
+    o = oracle_for(syn, f)
+    rng = np.random.default_rng(5)
+    names = ("SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE")
+    for step in range(4):
+        forcing = {}
+        for n in names:
+            a = f[n] * (1.0 + 0.05 * rng.standard_normal(f[n].shape))
+            if n == "SEAICE":
+                a = np.clip(a, 0.0, 1.0)
+            forcing[n] = np.ascontiguousarray(a)
+            o.set(n, forcing[n])
+        fw, _, _ = dom.step_host(forcing)
+        o.step(1)
+        assert fw == o.fw_norm2(), step
+        for name in ("AT", "NET", "AKT"):
+            g, r = dom.get(name), o.get(name)
+            assert bits_equal(g, r), "step %d %s: %s" % (step, name, mismatch(g, r))
+
+
 def test_numeric_scan_flags_injected_nan(lt):
     """Failure detection without a GPU fault: a NaN planted in the state on
     the host is reported as a count and a status, the context stays usable."""
