@@ -830,6 +830,10 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
 // level), so kFp64CtasPerSm CTAs fit on an SM.
 constexpr int NSX = 3;
 constexpr bool kStageDel4 = kFp64CtasPerSm <= 2;
+// the own cell's unlimited horizontal fluxes of a level, as its predictor
+// formed them one step before the column phase needs them (same
+// expressions, same inputs), kept per level parity where the room is
+constexpr bool kCacheXY = kFp64CtasPerSm <= 2;
 struct ExSmem {
   LevelSlot<double> slot[NSX];
   unsigned char flag[3][HN];   // limiter flag (a00 > amax || a00 < amin) per level parity of three
@@ -843,13 +847,15 @@ struct ExSmem {
   // the biharmonic coefficients dtn, dts, dte, dtw, ahf of the 1-halo region
   // where two CTAs per SM leave the room (read through L1 otherwise)
   double dt5[kStageDel4 ? 5 : 1][kStageDel4 ? HN : 1];
+  double xyc[kCacheXY ? 2 : 1][4][kCacheXY ? TTHREADS : 1];
   int kmt[(TY + 4) * SW];
   uint64_t bar[NSX];
 };
 
 // Predictor, masked extrema and limiter flag of one cell (hj, hi) of the
 // 1-halo region at level kk; returns the flag (a00 > amax || a00 < amin).
-__device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0) {
+__device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0,
+                                           double* xy_out = nullptr) {
   const int km = a.km, imt = a.imt, jmt = a.jmt;
   const double dts = a.p.dts;
   const double* odzp = a.odzp;
@@ -883,6 +889,12 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
     const double xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
     const double xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
     const double xy4 = dts * (c - n) * 2.0 * tr * vn * vn / hsn;
+    if (kCacheXY && xy_out) {
+      xy_out[0] = xy1;
+      xy_out[TTHREADS] = xy2;
+      xy_out[2 * TTHREADS] = xy3;
+      xy_out[3 * TTHREADS] = xy4;
+    }
     const double cx = -c * (ue - uwc) * tr * 2.0;
     const double cy = -c * (vsc - vn) * tr * 2.0;
     double za, zb1, zb2, zc;
@@ -1078,7 +1090,9 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
     }
     // limiter flags of the own cell at levels k+1, k (earlier steps) and k-1
-    bool out_kp1 = false, out_k = pred_one64(S, a, km - 1, ty + 1, tx + 1, x0, y0), out_km1 = false;
+    bool out_kp1 = false, out_k = pred_one64(S, a, km - 1, ty + 1, tx + 1, x0, y0, &S.xyc[0][0][0] + tid +
+                                             (kCacheXY ? ((km - 1) & 1) * 4 * TTHREADS : 0)),
+         out_km1 = false;
     if (has_ring) pred_one64(S, a, km - 1, ring_hj, ring_hi, x0, y0);
 
     for (int k = km - 1; k >= 0; --k) {
@@ -1092,7 +1106,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       // and only its own cell's flags of the levels k-1 and k+1, which this
       // thread computed: no barrier between the two phases.
       if (k >= 1) {
-        out_km1 = pred_one64(S, a, k - 1, ty + 1, tx + 1, x0, y0);
+        out_km1 = pred_one64(S, a, k - 1, ty + 1, tx + 1, x0, y0,
+                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 4 * TTHREADS : 0));
         if (has_ring) pred_one64(S, a, k - 1, ring_hj, ring_hi, x0, y0);
       }
       // ---- phase C
@@ -1113,14 +1128,15 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           return edge_k ? (self || (nb && guard)) : ((self || nb) && guard);
         };
         double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
+        const double* xc = &S.xyc[0][0][0] + tid + (kCacheXY ? (k & 1) * 4 * TTHREADS : 0);
         if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
-        else xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
+        else xy1 = kCacheXY ? xc[0] : -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
         if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
-        else xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
+        else xy2 = kCacheXY ? xc[TTHREADS] : dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
         if (lim(hc + HQX, j <= jmt - 3)) xy3 = -(s - c) * fabs(vsc) * tr;
-        else xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
+        else xy3 = kCacheXY ? xc[2 * TTHREADS] : -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
         if (lim(hc - HQX, j >= 2)) xy4 = (c - nn) * fabs(vn) * tr;
-        else xy4 = dts * (c - nn) * 2.0 * tr * vn * vn / hsn;
+        else xy4 = kCacheXY ? xc[3 * TTHREADS] : dts * (c - nn) * 2.0 * tr * vn * vn / hsn;
         const double wk = Lk.ws[uc];
         if (k == 0) {
           const double w1 = ws_dn, ad = at_dn;
