@@ -542,9 +542,64 @@ __device__ __forceinline__ void del4_first_mixed(MxSmem& S, int kk, const HCell&
   if (has_ring) S.d2[ring.m] = d2_cell(S, atb, kk, ring);
 }
 
+// Per-tile 2-D data of the mixed march (kmt with a 2-cell halo, the metric
+// and biharmonic terms of the 1-halo region, the face factors) with fixed
+// trip counts and read-only loads, so a thread's loads of a loop are in
+// flight together.  The batched kernel, whose work items are short and change
+// member often, stages its tiles this way; the single-domain kernel keeps the
+// plain loops in mixed_item, with which it compiles better.
+__device__ __forceinline__ void stage_tile_statics_ahead(MxSmem& S, const Arena& a, int x0, int y0, double dts) {
+  const int tid = threadIdx.x;
+  const int imt = a.imt, jmt = a.jmt;
+#pragma unroll
+  for (int it = 0; it < ((MY + 4) * SW + MTH - 1) / MTH; ++it) {
+    const int m = tid + it * MTH;
+    if (m < (MY + 4) * SW) {
+      const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
+      S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? __ldg(a.kmt + (long)gj * imt + gi) : 0;
+    }
+}
+#pragma unroll
+for (int it = 0; it < (MHN + MTH - 1) / MTH; ++it) {
+  const int m = tid + it * MTH;
+  if (m < MHN) {
+    const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
+    const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
+    const long q = in ? (long)gj * imt + gi : 0;
+    const double tarea = __ldg(a.tarea + q), dte = __ldg(a.dte + q), dtsq = __ldg(a.dts + q);
+    S.tr[m] = in ? (float)__ldg(a.tarea_r + q) : 0.f;
+    S.dtn[m] = in ? (float)__ldg(a.dtn + q) : 0.f;
+    S.dts[m] = in ? (float)dtsq : 0.f;
+    S.dte[m] = in ? (float)dte : 0.f;
+    S.dtw[m] = in ? (float)__ldg(a.dtw + q) : 0.f;
+    S.ahf[m] = in ? (float)__ldg(a.ahf + q) : 0.f;
+    S.kx[m] = in ? (float)(tarea * dte) : 0.f;
+    S.ky[m] = in ? (float)(tarea * dtsq) : 0.f;
+  }
+}
+#pragma unroll
+for (int it = 0; it < (FXN + FYN + MTH - 1) / MTH; ++it) {
+  const int m = tid + it * MTH;
+  if (m < FXN + FYN) {
+    int gj, gi;
+    if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
+    else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
+    const bool inb = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+    const long q = inb ? (long)gj * imt + gi : 0;
+    const double h = (m < FXN) ? __ldg(a.htw + q) : __ldg(a.hts + q);
+    const double hu = (m < FXN) ? __ldg(a.hun + q) : __ldg(a.hue + q);
+    const float v = inb ? (float)(2.0 * dts / (h * hu)) : 0.f;
+    const float hf = inb ? (float)h : 0.f;
+    if (m < FXN) { S.cxf[m] = v; S.hwx[m] = hf; }
+    else { S.cyf[m - FXN] = v; S.hsy[m - FXN] = hf; }
+  }
+}
+}
+
 // One work item (tile, tracer) of the mixed column march.  Returns false if
 // a level wait gave up: the CTA has then recorded the timeout and drained
 // its boxes, and must return.
+template <bool kLoadsAhead>
 __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const TracerMaps& maps, double* scr, int ntx,
                                            long tile, int n, uint32_t& par, uint32_t& outstanding) {
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
@@ -573,37 +628,40 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       return ok;
     };
     for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L);
-    // per-tile 2-D data
-    for (int m = tid; m < (MY + 4) * SW; m += MTH) {
-      const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
-      S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
-    }
-    for (int m = tid; m < MHN; m += MTH) {
-      const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
-      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
-      const long q = in ? (long)gj * imt + gi : 0;
-      S.tr[m] = in ? (float)a.tarea_r[q] : 0.f;
-      S.dtn[m] = in ? (float)a.dtn[q] : 0.f;
-      S.dts[m] = in ? (float)a.dts[q] : 0.f;
-      S.dte[m] = in ? (float)a.dte[q] : 0.f;
-      S.dtw[m] = in ? (float)a.dtw[q] : 0.f;
-      S.ahf[m] = in ? (float)a.ahf[q] : 0.f;
-      S.kx[m] = in ? (float)(a.tarea[q] * a.dte[q]) : 0.f;
-      S.ky[m] = in ? (float)(a.tarea[q] * a.dts[q]) : 0.f;
-    }
-    for (int m = tid; m < FXN + FYN; m += MTH) {
-      int gj, gi;
-      if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
-      else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
-      float v = 0.f;
-      if (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) {
-        const long q = (long)gj * imt + gi;
-        v = (m < FXN) ? (float)(2.0 * dts / (a.htw[q] * a.hun[q])) : (float)(2.0 * dts / (a.hts[q] * a.hue[q]));
+    if constexpr (kLoadsAhead) {
+      stage_tile_statics_ahead(S, a, x0, y0, dts);
+    } else {
+      for (int m = tid; m < (MY + 4) * SW; m += MTH) {
+        const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
+        S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
       }
-      if (m < FXN) S.cxf[m] = v; else S.cyf[m - FXN] = v;
-      const bool inb = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
-      if (m < FXN) S.hwx[m] = inb ? (float)a.htw[(long)gj * imt + gi] : 0.f;
-      else S.hsy[m - FXN] = inb ? (float)a.hts[(long)gj * imt + gi] : 0.f;
+      for (int m = tid; m < MHN; m += MTH) {
+        const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
+        const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
+        const long q = in ? (long)gj * imt + gi : 0;
+        S.tr[m] = in ? (float)a.tarea_r[q] : 0.f;
+        S.dtn[m] = in ? (float)a.dtn[q] : 0.f;
+        S.dts[m] = in ? (float)a.dts[q] : 0.f;
+        S.dte[m] = in ? (float)a.dte[q] : 0.f;
+        S.dtw[m] = in ? (float)a.dtw[q] : 0.f;
+        S.ahf[m] = in ? (float)a.ahf[q] : 0.f;
+        S.kx[m] = in ? (float)(a.tarea[q] * a.dte[q]) : 0.f;
+        S.ky[m] = in ? (float)(a.tarea[q] * a.dts[q]) : 0.f;
+      }
+      for (int m = tid; m < FXN + FYN; m += MTH) {
+        int gj, gi;
+        if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
+        else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
+        float v = 0.f;
+        if (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) {
+          const long q = (long)gj * imt + gi;
+          v = (m < FXN) ? (float)(2.0 * dts / (a.htw[q] * a.hun[q])) : (float)(2.0 * dts / (a.hts[q] * a.hue[q]));
+        }
+        if (m < FXN) S.cxf[m] = v; else S.cyf[m - FXN] = v;
+        const bool inb = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+        if (m < FXN) S.hwx[m] = inb ? (float)a.htw[(long)gj * imt + gi] : 0.f;
+        else S.hsy[m - FXN] = inb ? (float)a.hts[(long)gj * imt + gi] : 0.f;
+      }
     }
 
     const bool own = (i < imt && j < jmt);
@@ -833,7 +891,7 @@ __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
   uint32_t par = 0, outstanding = 0;
   double* scr = a.col_scratch + (long)blockIdx.x * a.km * 2 * MTH;
   for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x)
-    if (!mixed_item(S, a, maps, scr, ntx, w >> 1, (int)(w & 1), par, outstanding)) return;
+    if (!mixed_item<false>(S, a, maps, scr, ntx, w >> 1, (int)(w & 1), par, outstanding)) return;
 }
 
 // Several domains (ensemble members, serving requests; any sizes) in one
@@ -871,7 +929,7 @@ __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
       staged = m;
     }
     const long local = w - d.item0;
-    if (!mixed_item(S, sa, d.maps, scr, d.ntx, local >> 1, (int)(local & 1), par, outstanding)) return;
+    if (!mixed_item<true>(S, sa, d.maps, scr, d.ntx, local >> 1, (int)(local & 1), par, outstanding)) return;
   }
 }
 
