@@ -382,8 +382,9 @@ __device__ __forceinline__ FaceSet face_set(int tid) {
   return f;
 }
 
-__device__ __forceinline__ void faces_level(MxSmem& S, int kk, const FaceSet& f) {
-  const MxSlot& L = S.slot[kk % NSM];
+// sk: the slot of level kk (kk % NSM, carried through the level loop)
+__device__ __forceinline__ void faces_level(MxSmem& S, int kk, int sk, const FaceSet& f) {
+  const MxSlot& L = S.slot[sk];
   face_one(S, L, kk, true, f.own_x, f.own_r);
   face_one(S, L, kk, false, f.own_y, f.own_r - SW);
 #pragma unroll
@@ -437,16 +438,17 @@ struct PredLevel {
   int kk, km;
 };
 
-__device__ __forceinline__ PredLevel pred_level(const MxSmem& S, const Arena& a, int kk) {
+// sc, su, sd: the slots of levels kk, kk-1, kk+1
+__device__ __forceinline__ PredLevel pred_level(const MxSmem& S, const Arena& a, int kk, int sc, int su, int sd) {
   PredLevel P;
   const int km = a.km;
   P.kk = kk;
   P.km = km;
-  P.at_c = S.slot[kk % NSM].at;
-  P.at_u = kk > 0 ? S.slot[(kk - 1) % NSM].at : nullptr;
-  P.at_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].at : nullptr;
-  P.ws_c = S.slot[kk % NSM].ws;
-  P.ws_d = kk < km - 1 ? S.slot[(kk + 1) % NSM].ws : nullptr;
+  P.at_c = S.slot[sc].at;
+  P.at_u = kk > 0 ? S.slot[su].at : nullptr;
+  P.at_d = kk < km - 1 ? S.slot[sd].at : nullptr;
+  P.ws_c = S.slot[sc].ws;
+  P.ws_d = kk < km - 1 ? S.slot[sd].ws : nullptr;
   P.dx = S.fxd[kk & 1];
   P.dy = S.fyd[kk & 1];
   P.ux = S.fxu[kk & 1];
@@ -511,10 +513,10 @@ __device__ __forceinline__ bool pred_cell(const MxSmem& S, const PredLevel& P, c
 
 // Predictor flags of level kk for the thread's own cell and ring cell;
 // returns the own cell's flag.
-__device__ __forceinline__ bool predictor_mixed(MxSmem& S, const Arena& a, int kk, const HCell& own,
-                                                const HCell& ring, bool has_ring) {
-  const PredLevel P = pred_level(S, a, kk);
-  unsigned char* fl = S.flag[kk % 3];
+__device__ __forceinline__ bool predictor_mixed(MxSmem& S, const Arena& a, int kk, int sc, int su, int sd,
+                                                const HCell& own, const HCell& ring, bool has_ring) {
+  const PredLevel P = pred_level(S, a, kk, sc, su, sd);
+  unsigned char* fl = S.flag[sc];   // flags kept per level modulo 3, as the slots
   const bool f = pred_cell(S, P, own);
   fl[own.m] = f ? 1 : 0;
   if (has_ring) fl[ring.m] = pred_cell(S, P, ring) ? 1 : 0;
@@ -535,9 +537,9 @@ __device__ __forceinline__ float d2_cell(const MxSmem& S, const double* atb, int
   return S.ahf[m] * v;
 }
 
-__device__ __forceinline__ void del4_first_mixed(MxSmem& S, int kk, const HCell& own, const HCell& ring,
+__device__ __forceinline__ void del4_first_mixed(MxSmem& S, int kk, int sk, const HCell& own, const HCell& ring,
                                                  bool has_ring) {
-  const double* atb = S.slot[kk % NSM].atb;
+  const double* atb = S.slot[sk].atb;
   S.d2[own.m] = d2_cell(S, atb, kk, own);
   if (has_ring) S.d2[ring.m] = d2_cell(S, atb, kk, ring);
 }
@@ -617,17 +619,17 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     double* atb_out = a.atb[a.cur ^ 1] + n * FB;
 
     __syncthreads();
-    auto issue = [&](int L) {
-      if (tid == 0) issue_mx(S.slot[L % NSM], &S.bar[L % NSM], maps, a.cur, n, km, L, x0, y0);
-      outstanding |= 1u << (L % NSM);
+    // level L goes to slot s = L % NSM
+    auto issue = [&](int L, int s) {
+      if (tid == 0) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, n, km, L, x0, y0);
+      outstanding |= 1u << s;
     };
-    auto wait = [&](int L) -> bool {
-      const int s = L % NSM;
+    auto wait = [&](int s) -> bool {
       const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u, a.wait_limit);
       if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
       return ok;
     };
-    for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L);
+    for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L, L % NSM);
     if constexpr (kLoadsAhead) {
       stage_tile_statics_ahead(S, a, x0, y0, dts);
     } else {
@@ -689,32 +691,36 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
     const float* akt_col = a.akt32 + n * F + qo;
     float akt_here = inner ? __ldg(akt_col + (long)(km - 1) * A) : 0.f;
 
+    // slots of levels k, k-1, k+1 (NSM == 3: level k-2 shares k+1's)
+    static_assert(NSM == 3, "slot rotation below assumes three slots");
+    int sk = (km - 1) % NSM;
+    int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
     {
-      const bool ok = wait(km - 1) && wait(km - 2);
+      const bool ok = wait(sk) && wait(sm1);
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
     }
-    faces_level(S, km - 1, fset);
+    faces_level(S, km - 1, sk, fset);
     __syncthreads();
-    predictor_mixed(S, a, km - 1, own_cell, ring_cell, has_ring);
+    predictor_mixed(S, a, km - 1, sk, sm1, sp1, own_cell, ring_cell, has_ring);
 
     // Level slots: after step k the slot of level k takes level k-NSM.
     for (int k = km - 1; k >= 0; --k) {
       const float akt_above = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
       // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
       // arrived in earlier steps; the previous step ended with a barrier)
-      if (k >= 1) faces_level(S, k - 1, fset);
-      del4_first_mixed(S, k, own_cell, ring_cell, has_ring);
-      const bool ok = (k >= 2) ? wait(k - 2) : true;
+      if (k >= 1) faces_level(S, k - 1, sm1, fset);
+      del4_first_mixed(S, k, sk, own_cell, ring_cell, has_ring);
+      const bool ok = (k >= 2) ? wait(sp1) : true;   // level k-2
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
       // ---- phase B2: predictor one level up.  The column phase below reads
       // the flags of level k (written in the previous step) and, of level
       // k-1, only its own cell's flag, which this thread computes: no barrier
       // between the two phases.
-      const bool flag_up = (k >= 1) ? predictor_mixed(S, a, k - 1, own_cell, ring_cell, has_ring) : false;
+      const bool flag_up = (k >= 1) ? predictor_mixed(S, a, k - 1, sm1, sp1, sk, own_cell, ring_cell, has_ring) : false;
       // ---- phase C: own column at level k
       if (inner) {
-        const MxSlot& Lk = S.slot[k % NSM];
-        const unsigned char* fl = S.flag[k % 3];
+        const MxSlot& Lk = S.slot[sk];
+        const unsigned char* fl = S.flag[sk];
         const bool self = fl[hc] != 0;
         const float* dx = S.fxd[k & 1];
         const float* dy = S.fyd[k & 1];
@@ -751,7 +757,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         double sz = carry;
         if (k > 0) {
           const float wv = Lk.ws[uc];
-          const double d64 = S.slot[(k - 1) % NSM].at[rc] - c;
+          const double d64 = S.slot[sm1].at[rc] - c;
           const float d = (float)d64;
           const bool up = self || flag_up;
           const float Xv = up ? fabsf(wv) * d : (wv * d) * wv * (float)odzt[k] * dtsf;
@@ -783,7 +789,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
           if (k <= S.kmt[rc - SW] - 1) hd -= (double)(S.ky[hc - HQX] * (dc - S.d2[hc - HQX]));
         }
         const double atb_k = Lk.atb[rc];
-        const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSM].atb[rc] : 0.0;
+        const double atb_km1 = k >= 1 ? S.slot[sm1].atb[rc] : 0.0;
         const float wkc_k = akt_here;
         const float wkc_km1 = akt_above;
         // shortwave through the faces above and below (tracer.cpp:1430-1474)
@@ -836,7 +842,11 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
       }
       akt_here = akt_above;
       __syncthreads();
-      if (k - NSM >= 0) issue(k - NSM);
+      if (k - NSM >= 0) issue(k - NSM, sk);   // level k-3 takes level k's slot
+      // one level down: the slots of k-1, k-2, k
+      sp1 = sk;
+      sk = sm1;
+      sm1 = sk == 0 ? 2 : sk - 1;
     }
     // substitution, top down: the elimination coefficients of SUB levels are
     // loaded together ahead of their stores (one scratch round trip per SUB
