@@ -854,21 +854,22 @@ struct ExSmem {
 
 // Predictor, masked extrema and limiter flag of one cell (hj, hi) of the
 // 1-halo region at level kk; returns the flag (a00 > amax || a00 < amin).
-__device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0,
-                                           double* xy_out = nullptr) {
+// sc, su, sd: the slots (and flag sets) of levels kk, kk-1, kk+1
+__device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int sc, int su, int sd, int hj, int hi,
+                                           int x0, int y0, double* xy_out = nullptr) {
   const int km = a.km, imt = a.imt, jmt = a.jmt;
   const double dts = a.p.dts;
   const double* odzp = a.odzp;
   const double* odzt = a.odzt;
-  const LevelSlot<double>& Lc = S.slot[kk % NSX];
+  const LevelSlot<double>& Lc = S.slot[sc];
   const double* at_c = Lc.at;
-  const double* at_u = kk > 0 ? S.slot[(kk - 1) % NSX].at : nullptr;
-  const double* at_d = kk < km - 1 ? S.slot[(kk + 1) % NSX].at : nullptr;
+  const double* at_u = kk > 0 ? S.slot[su].at : nullptr;
+  const double* at_d = kk < km - 1 ? S.slot[sd].at : nullptr;
   const double* ws_c = Lc.ws;
-  const double* ws_d = kk < km - 1 ? S.slot[(kk + 1) % NSX].ws : nullptr;
+  const double* ws_d = kk < km - 1 ? S.slot[sd].ws : nullptr;
   const double* uw = Lc.uw;
   const double* vs = Lc.vs;
-  unsigned char* fl = S.flag[kk % 3];
+  unsigned char* fl = S.flag[sc];
   {
     const int m = hj * HQX + hi;
     const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
@@ -960,8 +961,9 @@ __device__ __forceinline__ double del4c(const ExSmem& S, const Arena& a, int c, 
 }
 
 // First Laplacian of atb at level kk for one cell (hj, hi) of the 1-halo region.
-__device__ __forceinline__ void del4_one64(ExSmem& S, const Arena& a, int kk, int hj, int hi, int x0, int y0) {
-  const double* atb = S.slot[kk % NSX].atb;
+__device__ __forceinline__ void del4_one64(ExSmem& S, const Arena& a, int kk, int sk, int hj, int hi, int x0,
+                                           int y0) {
+  const double* atb = S.slot[sk].atb;
   {
     const int m = hj * HQX + hi;
     const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
@@ -1028,18 +1030,18 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     double* atb_out = a.atb[a.cur ^ 1] + n * FB;
 
     __syncthreads();  // the previous item is done with every slot
-    auto issue = [&](int L) {
-      if (tid == 0) issue_level(S.slot[L % NSX], &S.bar[L % NSX], maps, a.cur, n, km, L, x0, y0);
-      outstanding |= 1u << (L % NSX);
+    // level L goes to slot s = L % NSX
+    auto issue = [&](int L, int s) {
+      if (tid == 0) issue_level(S.slot[s], &S.bar[s], maps, a.cur, n, km, L, x0, y0);
+      outstanding |= 1u << s;
     };
-    auto wait = [&](int L) -> bool {
-      const int s = L % NSX;
+    auto wait = [&](int s) -> bool {
       const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u, a.wait_limit);
       if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
       return ok;
     };
     const int lowest_pro = km - NSX > 0 ? km - NSX : 0;
-    for (int L = km - 1; L >= lowest_pro; --L) issue(L);
+    for (int L = km - 1; L >= lowest_pro; --L) issue(L, L % NSX);
     for (int m = tid; m < (TY + 4) * SW; m += TTHREADS) {
       const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
       S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
@@ -1084,38 +1086,44 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // own cell's at, ws and atb of level k+1, kept from step k+1
     double at_dn = 0.0, ws_dn = 0.0, atb_dn = 0.0;
 
+    // slots of levels k, k-1, k+1 (NSX == 3: level k-2 shares k+1's), carried
+    // through the level loop
+    static_assert(NSX == 3, "slot rotation below assumes three slots");
+    int sk = (km - 1) % NSX;
+    int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
     {
-      const bool ok = wait(km - 1) && wait(km - 2);
+      const bool ok = wait(sk) && wait(sm1);
       // a wait that ran out anywhere in the CTA sends every thread out together
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
     }
     // limiter flags of the own cell at levels k+1, k (earlier steps) and k-1
-    bool out_kp1 = false, out_k = pred_one64(S, a, km - 1, ty + 1, tx + 1, x0, y0, &S.xyc[0][0][0] + tid +
-                                             (kCacheXY ? ((km - 1) & 1) * 4 * TTHREADS : 0)),
+    bool out_kp1 = false,
+         out_k = pred_one64(S, a, km - 1, sk, sm1, sp1, ty + 1, tx + 1, x0, y0,
+                            &S.xyc[0][0][0] + tid + (kCacheXY ? ((km - 1) & 1) * 4 * TTHREADS : 0)),
          out_km1 = false;
-    if (has_ring) pred_one64(S, a, km - 1, ring_hj, ring_hi, x0, y0);
+    if (has_ring) pred_one64(S, a, km - 1, sk, sm1, sp1, ring_hj, ring_hi, x0, y0);
 
     for (int k = km - 1; k >= 0; --k) {
       // ---- phase B1: first Laplacian at level k (arrived in an earlier step)
-      del4_one64(S, a, k, ty + 1, tx + 1, x0, y0);
-      if (has_ring) del4_one64(S, a, k, ring_hj, ring_hi, x0, y0);
-      const bool ok = (k >= 2) ? wait(k - 2) : true;
+      del4_one64(S, a, k, sk, ty + 1, tx + 1, x0, y0);
+      if (has_ring) del4_one64(S, a, k, sk, ring_hj, ring_hi, x0, y0);
+      const bool ok = (k >= 2) ? wait(sp1) : true;   // level k-2
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
       // ---- phase B2: predictor one level up.  The column phase below reads
       // the flags of level k of the neighbours (written in the previous step)
       // and only its own cell's flags of the levels k-1 and k+1, which this
       // thread computed: no barrier between the two phases.
       if (k >= 1) {
-        out_km1 = pred_one64(S, a, k - 1, ty + 1, tx + 1, x0, y0,
+        out_km1 = pred_one64(S, a, k - 1, sm1, sp1, sk, ty + 1, tx + 1, x0, y0,
                              &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 4 * TTHREADS : 0));
-        if (has_ring) pred_one64(S, a, k - 1, ring_hj, ring_hi, x0, y0);
+        if (has_ring) pred_one64(S, a, k - 1, sm1, sp1, sk, ring_hj, ring_hi, x0, y0);
       }
       // ---- phase C
       if (ring) {
-        const LevelSlot<double>& Lk = S.slot[k % NSX];
+        const LevelSlot<double>& Lk = S.slot[sk];
         const double* at_c = Lk.at;
-        const double* at_u = k > 0 ? S.slot[(k - 1) % NSX].at : nullptr;
-        const unsigned char* fl = S.flag[k % 3];
+        const double* at_u = k > 0 ? S.slot[sm1].at : nullptr;
+        const unsigned char* fl = S.flag[sk];
         const double tr = S.tr[hc];
         const double hwe = S.hw[(ty + 1) * (HQX + 1) + tx + 2], hww = S.hw[(ty + 1) * (HQX + 1) + tx + 1];
         const double hss = S.hs[(ty + 2) * HQX + tx + 1], hsn = S.hs[(ty + 1) * HQX + tx + 1];
@@ -1187,10 +1195,10 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           const double vit_k = k < kz ? 1.0 : 0.0;
           const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
           const double atb_k = Lk.atb[rc];
-          const double atb_km1 = k >= 1 ? S.slot[(k - 1) % NSX].atb[rc] : 0.0;
+          const double atb_km1 = k >= 1 ? S.slot[sm1].atb[rc] : 0.0;
           const double atb_kp1 = k < km - 1 ? atb_dn : 0.0;
           const double wkc_k = Lk.akt[ac];
-          const double wkc_km1 = k >= 1 ? S.slot[(k - 1) % NSX].akt[ac] : 0.0;
+          const double wkc_km1 = k >= 1 ? S.slot[sm1].akt[ac] : 0.0;
           double tf = adv * vit_k;
           {
             const int r = rc;
@@ -1280,7 +1288,11 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       out_kp1 = out_k;
       out_k = out_km1;
       __syncthreads();  // level k is no longer read: its slot takes level k-NSX
-      if (k - NSX >= 0) issue(k - NSX);
+      if (k - NSX >= 0) issue(k - NSX, sk);
+      // one level down: the slots of k-1, k-2, k
+      sp1 = sk;
+      sk = sm1;
+      sm1 = sk == 0 ? 2 : sk - 1;
     }
     // ---- substitution, top down: the elimination coefficients of SUB levels
     // are loaded together ahead of their stores (the scratch round trip is
