@@ -436,6 +436,7 @@ struct PredLevel {
   const float *ws_c, *ws_d, *dx, *dy, *ux, *vy;
   float hodz, odzt_k, odzt_k1, dts;
   int kk, km;
+  bool up, dn;   // level kk has a level above / below
 };
 
 // sc, su, sd: the slots of levels kk, kk-1, kk+1
@@ -444,11 +445,16 @@ __device__ __forceinline__ PredLevel pred_level(const MxSmem& S, const Arena& a,
   const int km = a.km;
   P.kk = kk;
   P.km = km;
+  // at the top and bottom levels the missing neighbour level is replaced by
+  // level kk itself: its differences are then exactly zero, and so are the
+  // vertical terms they carry (pred_cell needs no branch on the level)
+  P.up = kk > 0;
+  P.dn = kk < km - 1;
   P.at_c = S.slot[sc].at;
-  P.at_u = kk > 0 ? S.slot[su].at : nullptr;
-  P.at_d = kk < km - 1 ? S.slot[sd].at : nullptr;
+  P.at_u = P.up ? S.slot[su].at : P.at_c;
+  P.at_d = P.dn ? S.slot[sd].at : P.at_c;
   P.ws_c = S.slot[sc].ws;
-  P.ws_d = kk < km - 1 ? S.slot[sd].ws : nullptr;
+  P.ws_d = P.dn ? S.slot[sd].ws : P.ws_c;
   P.dx = S.fxd[kk & 1];
   P.dy = S.fyd[kk & 1];
   P.ux = S.fxu[kk & 1];
@@ -464,7 +470,7 @@ __device__ __forceinline__ PredLevel pred_level(const MxSmem& S, const Arena& a,
 // local bounds (the reference's a00 > amax or a00 < amin).
 __device__ __forceinline__ bool pred_cell(const MxSmem& S, const PredLevel& P, const HCell& h) {
   if (!h.valid) return false;
-  const int kk = P.kk, km = P.km, r = h.r, u = h.u;
+  const int kk = P.kk, r = h.r, u = h.u;
   const int fw = h.fw, fe = fw + 1, fn = h.fn, fs = fn + HQX;
   const float* dx = P.dx;
   const float* dy = P.dy;
@@ -475,18 +481,19 @@ __device__ __forceinline__ bool pred_cell(const MxSmem& S, const PredLevel& P, c
   const float sx = (dx[fe] * ue - lw_part(dx[fe], ue, S.cxf[fe])) + (dx[fw] * uwv + lw_part(dx[fw], uwv, S.cxf[fw]));
   const float sy = (dy[fs] * vs - lw_part(dy[fs], vs, S.cyf[fs])) + (dy[fn] * vn + lw_part(dy[fn], vn, S.cyf[fn]));
   // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
-  float sz = 0.f, dup = 0.f, ddn = 0.f;   // dup, ddn: a_above - c, a_below - c
+  // (at a missing level the difference is 0, the term +-0, and sz stays +0)
+  float sz = 0.f;
   const double c = P.at_c[r];
-  if (kk > 0) {
+  const float dup = (float)(P.at_u[r] - c);   // a_above - c
+  {
     const float w = P.ws_c[u];
-    dup = (float)(P.at_u[r] - c);
     const float A = w * dup;
     sz += A - A * w * P.odzt_k * dts;
   }
-  if (kk < km - 1) {
+  const float d = (float)(c - P.at_d[r]);
+  const float ddn = -d;                         // a_below - c
+  {
     const float w = P.ws_d[u];
-    const float d = (float)(c - P.at_d[r]);
-    ddn = -d;
     const float A = w * d;
     sz += A + A * w * P.odzt_k1 * dts;
   }
@@ -506,8 +513,8 @@ __device__ __forceinline__ bool pred_cell(const MxSmem& S, const PredLevel& P, c
   acc(kk < kt[r - 1], -dx[fw]);
   acc(kk < kt[r + SW], dy[fs]);
   acc(kk < kt[r - SW], -dy[fn]);
-  if (kk > 0) acc(kk - 1 < kt[r], dup);
-  if (kk < km - 1) acc(kk + 1 < kt[r], ddn);
+  acc(P.up && kk - 1 < kt[r], dup);
+  acc(P.dn && kk + 1 < kt[r], ddn);
   return inc > dmax || inc < dmin;
 }
 
