@@ -105,9 +105,9 @@ void count_launches(int n);
 void set_error(const char* fmt, ...);
 
 // host launchers (defined in the step translation units)
-int launch_surface(const Arena& a, cudaStream_t s);
-// the two parts of launch_surface: the SSH mean (h0f_out, stf_ssh) and the
-// surface fluxes, net and the mixing floor (which read stf_ssh)
+// the surface kernel in two parts: the SSH mean (h0f_out, stf_ssh), which the
+// continuity needs, and the surface fluxes, net and the mixing floor (which
+// read stf_ssh and the forcing)
 int launch_ssh(const Arena& a, cudaStream_t s);
 int launch_surface_fluxes(const Arena& a, cudaStream_t s);
 int launch_continuity_fp64(const Arena& a, cudaStream_t s);

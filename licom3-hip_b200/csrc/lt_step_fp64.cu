@@ -5,12 +5,13 @@
 // results match the FP64 CPU oracle bit for bit.
 //
 // Launch sequence of one step (replacing tracer.cpp:1701-1903):
-//   k_surface       surface fluxes of both tracers, SSH mean, net, the
-//                   surface mixing floor, SSS-norm terms       (tracer_1_0, tracer_5/6 surface parts)
-//   tree sum        deterministic SSS-normalisation sum         (tracer.cpp:1849-1868)
-//   halo(net)       in-GPU ghost fill                           (pop_haloupdate_tracer1)
+//   k_ssh           SSH mean (h0f*onbc, stf)                    (tracer_1_0)
 //   k_cont_march64  uk/vk, divergence, w by upward integration,
 //                   face transports, scaled utf/vtf             (tracer_1, upwell_2..4, advection_tracer_1_0)
+//   k_surface_fluxes surface fluxes of both tracers, net, the
+//                   surface mixing floor, SSS-norm terms       (tracer_5/6 surface parts)
+//   tree sum        deterministic SSS-normalisation sum         (tracer.cpp:1849-1868)
+//   halo(net)       in-GPU ghost fill                           (pop_haloupdate_tracer1)
 //   k_tracer_tma64  per column tile (k_tracer64 where the layout
 //                   does not allow TMA boxes), both tracers: tspas predictor/limiter,
 //                   biharmonic diffusion, shortwave, explicit and implicit
@@ -74,10 +75,6 @@ __device__ __forceinline__ void surface_col(const Arena& a, int i, int j) {
   if (i >= a.imt || j >= a.jmt) return;
   const long q = q2(j, i, a.imt);
   flux_col(a, i, j, q, ssh_col(a, q));
-}
-
-__global__ void k_surface(Arena a) {
-  surface_col(a, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
 }
 
 __global__ void k_ssh(Arena a) {
@@ -1412,13 +1409,6 @@ __global__ void k_vtl_clobber(Arena a) {
 }  // namespace
 
 // ---------------------------------------------------------------- launchers
-int launch_surface(const Arena& a, cudaStream_t s) {
-  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
-  k_surface<<<g, b, 0, s>>>(a);
-  LT_LAUNCHED();
-  return LT_OK;
-}
-
 int launch_ssh(const Arena& a, cudaStream_t s) {
   dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
   k_ssh<<<g, b, 0, s>>>(a);

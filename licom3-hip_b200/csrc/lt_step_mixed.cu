@@ -966,8 +966,6 @@ int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t
   return LT_OK;
 }
 
-size_t mixed_tracer_smem_bytes() { return sizeof(MxSmem); }
-
 int prepare_tracer_mixed_batch() {
   LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kBatchSmem));

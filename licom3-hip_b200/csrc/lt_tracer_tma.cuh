@@ -140,7 +140,6 @@ int launch_continuity_mixed_batch(const MemberDesc* mem, int nmem, int max_imt, 
 int launch_small_batch_pre(const MemberDesc* mem, int nmem, int max_imt, int max_jmt, long max_cols,
                            cudaStream_t s);
 int launch_halo_state_batch(const MemberDesc* mem, int nmem, int max_imt, int km_max, cudaStream_t s);
-size_t mixed_tracer_smem_bytes();
 // sets the batched column kernel's shared-memory size on the current device
 int prepare_tracer_mixed_batch();
 int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
