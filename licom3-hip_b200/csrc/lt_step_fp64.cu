@@ -827,9 +827,10 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
 // level), so kFp64CtasPerSm CTAs fit on an SM.
 constexpr int NSX = 3;
 constexpr bool kStageDel4 = kFp64CtasPerSm <= 2;
-// the own cell's unlimited horizontal fluxes of a level, as its predictor
-// formed them one step before the column phase needs them (same
-// expressions, same inputs), kept per level parity where the room is
+// the own cell's unlimited horizontal fluxes and centred transports of a
+// level, as its predictor formed them one step before the column phase
+// needs them (same expressions, same inputs), kept per level parity where
+// the room is
 constexpr bool kCacheXY = kFp64CtasPerSm <= 2;
 struct ExSmem {
   LevelSlot<double> slot[NSX];
@@ -844,7 +845,7 @@ struct ExSmem {
   // the biharmonic coefficients dtn, dts, dte, dtw, ahf of the 1-halo region
   // where two CTAs per SM leave the room (read through L1 otherwise)
   double dt5[kStageDel4 ? 5 : 1][kStageDel4 ? HN : 1];
-  double xyc[kCacheXY ? 2 : 1][4][kCacheXY ? TTHREADS : 1];
+  double xyc[kCacheXY ? 2 : 1][6][kCacheXY ? TTHREADS : 1];
   int kmt[(TY + 4) * SW];
   uint64_t bar[NSX];
 };
@@ -892,6 +893,8 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
       xy_out[TTHREADS] = xy2;
       xy_out[2 * TTHREADS] = xy3;
       xy_out[3 * TTHREADS] = xy4;
+      xy_out[4 * TTHREADS] = x0v;
+      xy_out[5 * TTHREADS] = y0v;
     }
     const double cx = -c * (ue - uwc) * tr * 2.0;
     const double cy = -c * (vsc - vn) * tr * 2.0;
@@ -1096,7 +1099,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // limiter flags of the own cell at levels k+1, k (earlier steps) and k-1
     bool out_kp1 = false,
          out_k = pred_one64(S, a, km - 1, sk, sm1, sp1, ty + 1, tx + 1, x0, y0,
-                            &S.xyc[0][0][0] + tid + (kCacheXY ? ((km - 1) & 1) * 4 * TTHREADS : 0)),
+                            &S.xyc[0][0][0] + tid + (kCacheXY ? ((km - 1) & 1) * 6 * TTHREADS : 0)),
          out_km1 = false;
     if (has_ring) pred_one64(S, a, km - 1, sk, sm1, sp1, ring_hj, ring_hi, x0, y0);
 
@@ -1112,7 +1115,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       // thread computed: no barrier between the two phases.
       if (k >= 1) {
         out_km1 = pred_one64(S, a, k - 1, sm1, sp1, sk, ty + 1, tx + 1, x0, y0,
-                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 4 * TTHREADS : 0));
+                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 6 * TTHREADS : 0));
         if (has_ring) pred_one64(S, a, k - 1, sm1, sp1, sk, ring_hj, ring_hi, x0, y0);
       }
       // ---- phase C
@@ -1133,7 +1136,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           return edge_k ? (self || (nb && guard)) : ((self || nb) && guard);
         };
         double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
-        const double* xc = &S.xyc[0][0][0] + tid + (kCacheXY ? (k & 1) * 4 * TTHREADS : 0);
+        const double* xc = &S.xyc[0][0][0] + tid + (kCacheXY ? (k & 1) * 6 * TTHREADS : 0);
         if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
         else xy1 = kCacheXY ? xc[0] : -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
         if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
@@ -1176,8 +1179,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         }
         const double cx = -c * (ue - uwc) * tr * 2.0;
         const double cy = -c * (vsc - vn) * tr * 2.0;
-        const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
-        const double y0v = ((s + c) * vsc - (c + nn) * vn) * tr;
+        const double x0v = kCacheXY ? xc[4 * TTHREADS] : (e + c) * ue * tr - (c + w) * uwc * tr;
+        const double y0v = kCacheXY ? xc[5 * TTHREADS] : ((s + c) * vsc - (c + nn) * vn) * tr;
         const double xx = -(x0v + xy1 + xy2 + cx);
         const double yy = -(y0v + xy3 + xy4 + cy);
         const double zz = -(za + zb1 + zb2 + zc);
