@@ -75,7 +75,7 @@ __device__ __forceinline__ float lw_part(float d, float u, float c) { return d *
 // f64 and rounded once.  Rounding w to f32 then costs f32 precision of w
 // only, not of the transports.
 //
-// One CTA marches a 32 x 8 column tile down the levels: the 2-D metric and
+// One CTA marches a 32 x CBY column tile down the levels: the 2-D metric and
 // free-surface factors are read once per tile, each level's U-point means
 // (with a one-point halo north and east) pass through shared memory, and the
 // vertical recurrence of upwell_4,
@@ -205,7 +205,7 @@ __device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
   }
 }
 
-constexpr int kContTileY = 8;   // tile height of the single-domain continuity march
+constexpr int kContTileY = 4;   // tile height of the single-domain continuity march
 
 __global__ void __launch_bounds__(CBX * kContTileY) k_cont_march32(Arena a) {
   cont_tile<kContTileY>(a, blockIdx.x, blockIdx.y);
