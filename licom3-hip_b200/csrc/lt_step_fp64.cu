@@ -224,7 +224,9 @@ __global__ void k_halo_net_batch(const MemberDesc* __restrict__ mem) {
 }
 
 // ------------------------------------------------------------- continuity
-// Continuity as one level march per 32 x 8 tile (tracer_1, upwell_2,
+constexpr int kCont64TileY = 8;   // tile height of the FP64 continuity march (4: slower)
+
+// Continuity as one level march per 32 x BY tile (tracer_1, upwell_2,
 // operators_div, advection_tracer_1_0 and upwell_3/4 with the same
 // expressions in the same order).  The U-point velocities of the tile and a
 // one-point halo north and east go through a three-level staging ring filled
@@ -235,8 +237,9 @@ __global__ void k_halo_net_batch(const MemberDesc* __restrict__ mem) {
 // after the step's one barrier.  The column divergence W accumulates in level
 // order during the march; w is integrated upward afterwards from the wka the
 // march wrote.
-__global__ void __launch_bounds__(256) k_cont_march64(Arena a) {
-  constexpr int BX = 32, BY = 8, UX = BX + 1, UY = BY + 1, UN = UX * UY, NT = BX * BY;
+template <int BY>
+__global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
+  constexpr int BX = 32, UX = BX + 1, UY = BY + 1, UN = UX * UY, NT = BX * BY;
   constexpr int NPT = (UN + NT - 1) / NT, NST = 3;
   __shared__ double s_st[NST][4][UN];   // staged utf, utl, vtf, vtl of three levels
   __shared__ double s_wkd[2][UN], s_wkb[2][UN], s_uk[2][UN], s_vk[2][UN];
@@ -1455,8 +1458,9 @@ int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripo
 }
 
 int launch_continuity_fp64(const Arena& a, cudaStream_t s) {
-  dim3 b(32, 8), g((a.imt + 31) / 32, (a.jmt + 7) / 8);
-  k_cont_march64<<<g, b, 0, s>>>(a);
+  constexpr int BY = kCont64TileY;
+  dim3 b(32, BY), g((a.imt + 31) / 32, (a.jmt + BY - 1) / BY);
+  k_cont_march64<BY><<<g, b, 0, s>>>(a);
   LT_LAUNCHED();
   return LT_OK;
 }
