@@ -761,18 +761,18 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const Trac
         double sh = dE * ue64 + dW * uw64 + dS * vs64 + dN * vn64;
         sh += ((double)Xw - (double)Xe) + ((double)Xn - (double)Xs);
         // vertical: face above (k-1|k) computed here, face below carried
+        // (at the top level the level itself stands in for the missing one
+        // above: the difference and both face terms are 0, sz keeps carry)
         double sz = carry;
-        if (k > 0) {
+        {
           const float wv = Lk.ws[uc];
-          const double d64 = S.slot[sm1].at[rc] - c;
+          const double d64 = (k > 0 ? S.slot[sm1].at : Lk.at)[rc] - c;
           const float d = (float)d64;
           const bool up = self || flag_up;
           const float Xv = up ? fabsf(wv) * d : (wv * d) * wv * (float)odzt[k] * dtsf;
           const double Av = (double)wv * d64;
           sz += Av - (double)Xv;
           carry = Av + (double)Xv;
-        } else {
-          carry = 0.0;
         }
         // Face-flux sums are weighted by tarea_r (horizontal) and odzp
         // (vertical) in f64, so a flux leaves one cell and enters the next
