@@ -649,14 +649,22 @@ int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2
   // The forcing goes up on the copy stream once the domain's earlier work
   // (which may read the previous forcing) is done, while the step's
   // continuity runs; the surface fluxes wait for it.
+  // (without a copy stream or its events the copies go on the domain's
+  // stream, in order before the step)
   cudaEvent_t ready = nullptr;
+  const bool overlap = d->copy_stream && d->ev_free && d->ev_forcing;
   if (forcing6) {
-    LT_CUDA_OK(cudaEventRecord(d->ev_free, d->stream));
-    LT_CUDA_OK(cudaStreamWaitEvent(d->copy_stream, d->ev_free, 0));
+    cudaStream_t cs = overlap ? d->copy_stream : d->stream;
+    if (overlap) {
+      LT_CUDA_OK(cudaEventRecord(d->ev_free, d->stream));
+      LT_CUDA_OK(cudaStreamWaitEvent(cs, d->ev_free, 0));
+    }
     for (int m = 0; m < 6; ++m)
-      if (forcing6[m]) LT_CUDA_OK(cudaMemcpyAsync(dst[m], forcing6[m], bytes, cudaMemcpyHostToDevice, d->copy_stream));
-    LT_CUDA_OK(cudaEventRecord(d->ev_forcing, d->copy_stream));
-    ready = d->ev_forcing;
+      if (forcing6[m]) LT_CUDA_OK(cudaMemcpyAsync(dst[m], forcing6[m], bytes, cudaMemcpyHostToDevice, cs));
+    if (overlap) {
+      LT_CUDA_OK(cudaEventRecord(d->ev_forcing, cs));
+      ready = d->ev_forcing;
+    }
   }
   int rc = run_step(d, ready);
   if (rc) return rc;
