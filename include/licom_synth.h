@@ -31,7 +31,7 @@ typedef struct {
   double land_frac;
   uint32_t member;            /* ensemble member (0 = unperturbed) */
   double tpert;               /* K, std of the member's T perturbation */
-  double ah_bihar;            /* m^4/s; 0 = -1e17*(36/nx)^4, stable at every resolution */
+  double ah_bihar;            /* m^4/s; 0 = -min(1e17, half the grid's explicit stability limit) */
 } lt_synth_config;
 
 typedef struct lt_synth lt_synth;

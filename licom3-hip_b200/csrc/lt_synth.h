@@ -493,8 +493,23 @@ inline Domain build_domain(const SynthConfig& c) {
   if (c.ah_bihar != 0.0) {
     d.ah = c.ah_bihar;
   } else {
-    const double r = 36.0 / (double)nx;
-    d.ah = -1.0e17 * (r * r) * (r * r);
+    // The configured -1e17 m^4/s, capped at half the explicit stability limit
+    // of this grid.  The step applies ah * L(AHF * L(atb)) with forward time
+    // stepping (hmix_del4.F90:626-757), stable while dts * |ah| * rho <= 2 with
+    // rho the spectral radius of L AHF L.  Gershgorin bounds |eig(L)| by
+    // 2 (dtn+dts+dte+dtw) per cell, so rho <= max AHF (2 sum d)^2 over the
+    // interior.  -1e17 is below the cap on the reference's 36 x 40 block and
+    // far above it on 1 and 0.1 degree grids (a 360 x 196 oracle run with
+    // -1e17 grows T to 1e51 within 20 steps).
+    double rho = 0.0;
+    for (int j = 2; j < jmt - 2; ++j)
+      for (int i = 2; i < imt - 2; ++i) {
+        const long a = (long)j * imt + i;
+        const double s2 = 2.0 * (d.dtn[a] + d.dts_[a] + d.dte[a] + d.dtw[a]);
+        rho = std::max(rho, d.ahf[a] * s2 * s2);
+      }
+    const double cap = rho > 0.0 ? 0.5 * (2.0 / (c.dts * rho)) : 1.0e17;
+    d.ah = -std::min(1.0e17, cap);
   }
   d.nss = (int)std::lround(86400.0 / c.dts);
   d.area_t = 0.0;

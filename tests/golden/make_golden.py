@@ -3,7 +3,8 @@
 Runs LICOM3-HIP's tracer.cpp, convadj.cpp, icesnow.cpp and readyc.cpp
 (turb_cu and the momentum biharmonic friction), compiled for the CPU by oracle/Makefile (target ``ref``) from the
 reference tree, on seeded
-synthetic inputs at the reference's built-in block size (36 x 40 physical, 55
+synthetic inputs (with the restoring branch on in the cases of
+tests/restore_case.py) at the reference's built-in block size (36 x 40 physical, 55
 levels) and records SHA-256 digests of every output field plus fw_norm2.  The
 icesnow cases start from the cold states of tests/icesnow_state.py; the
 turbulence cases use the closure inputs and stand-in tables of
@@ -27,6 +28,7 @@ import pyoracle  # noqa: E402
 from icesnow_state import ICE_CASES, cold_state  # noqa: E402
 from turb_case import DFRICMX, NCC, TURB_CASES, case, tables  # noqa: E402
 import del4u_case  # noqa: E402
+import restore_case  # noqa: E402
 
 CASES = [(1, 5, 20240611), (0, 3, 7), (1, 2, 99)]
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
@@ -58,6 +60,20 @@ def main():
             "outputs": {n: digest(ref.get(n)) for n in OUT_FIELDS},
             "fw_norm2": ref.fw_norm2(),
             "surface_T_sample": ref.get("AT")[0, 0, 20, 5:15].tolist(),
+            # temperature alone: the SSS-norm sum (salinity only) cannot move it
+            "outputs_T": {n: digest(ref.get(n)[0]) for n in ("AT", "ATB")},
+        }
+    for forced, nsteps, seed in restore_case.RESTORE_CASES:
+        syn, p, inp = restore_case.case(lt, forced, seed)
+        ref = pyoracle.Reference(p)
+        ref.load(inp)
+        for s in range(nsteps):
+            ref.tracer_call(s)
+        ref.convadj()
+        out["restore_forced%d_steps%d_seed%d" % (forced, nsteps, seed)] = {
+            "inputs": {"AT": digest(inp["AT"]), "RESTORE": digest(inp["RESTORE"])},
+            "outputs": {n: digest(ref.get(n)) for n in OUT_FIELDS},
+            "fw_norm2": ref.fw_norm2(),
         }
     for frc_core, nsteps, seed in ICE_CASES:
         syn = lt.Synth(36, 40, 55, forced=1, cap_north=0, cap_south=3, dz_top=5.0, dz_bot=300.0, seed=seed)

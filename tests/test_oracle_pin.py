@@ -18,6 +18,7 @@ import pytest
 from conftest import REPO
 
 import pyoracle
+import restore_case
 
 GOLDEN = os.path.join(REPO, "tests", "golden", "reference_digests.json")
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
@@ -76,6 +77,56 @@ def test_oracle_matches_golden_digests(lt, forced, nsteps, seed):
     for name in OUT_FIELDS:
         assert digest(o.get(name)) == gold[key]["outputs"][name], name
     assert o.fw_norm2() == gold[key]["fw_norm2"]
+
+
+def run_restore_oracle(lt, forced, nsteps, seed):
+    syn, p, f = restore_case.case(lt, forced, seed)
+    o = pyoracle.Oracle(syn.nx, syn.ny, syn.km, p)
+    o.load(f)
+    for _ in range(nsteps):
+        o.tracer_call()
+    o.convadj()
+    return syn, p, f, o
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference tree not built here")
+@pytest.mark.parametrize("forced,nsteps,seed", restore_case.RESTORE_CASES)
+def test_oracle_restoring_bitexact_vs_reference(lt, forced, nsteps, seed):
+    """boundary_restore = 1 (tracer_7's 15-day relaxation below the surface)
+    against the reference's own tracer.cpp, bit for bit."""
+    syn, p, f, o = run_restore_oracle(lt, forced, nsteps, seed)
+    ref = pyoracle.Reference(p)
+    ref.load(f)
+    for s in range(nsteps):
+        ref.tracer_call(s)
+    ref.convadj()
+    assert o.fw_norm2() == ref.fw_norm2()
+    for name in OUT_FIELDS:
+        a, b = o.get(name), ref.get(name)
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+
+
+@pytest.mark.parametrize("forced,nsteps,seed", restore_case.RESTORE_CASES)
+def test_oracle_restoring_matches_golden_digests(lt, forced, nsteps, seed):
+    gold = json.load(open(GOLDEN))
+    key = "restore_forced%d_steps%d_seed%d" % (forced, nsteps, seed)
+    assert key in gold, "regenerate tests/golden with make_golden.py"
+    syn, p, f, o = run_restore_oracle(lt, forced, nsteps, seed)
+    assert digest(f["RESTORE"]) == gold[key]["inputs"]["RESTORE"]
+    assert digest(f["AT"]) == gold[key]["inputs"]["AT"]
+    for name in OUT_FIELDS:
+        assert digest(o.get(name)) == gold[key]["outputs"][name], name
+    assert o.fw_norm2() == gold[key]["fw_norm2"]
+    # the relaxation moved the state: the same run without it differs below the surface
+    off = type(p).from_buffer_copy(p)
+    off.boundary_restore = 0
+    q = pyoracle.Oracle(syn.nx, syn.ny, syn.km, off)
+    q.load(f)
+    for _ in range(nsteps):
+        q.tracer_call()
+    q.convadj()
+    d = np.abs(o.get("AT") - q.get("AT"))
+    assert d[0, 1:].max() > 1e-4 and d[0, 0].max() < d[0, 1:].max()
 
 
 def test_halo_restatement_matches_generator_halo(lt):
@@ -191,3 +242,19 @@ def test_tree_order_only_moves_the_sss_sum(lt):
     assert abs(a.fw_norm2() - b.fw_norm2()) <= 1e-14 * abs(a.fw_norm2())
     ta, tb = a.get("AT"), b.get("AT")
     assert np.max(np.abs(ta - tb)) <= 1e-12 * np.max(np.abs(ta))
+
+
+@pytest.mark.parametrize("forced,nsteps,seed", CASES)
+def test_tree_order_reproduces_reference_temperature(lt, forced, nsteps, seed):
+    """In the device's fixed-tree SSS-norm order the oracle still gives the
+    reference's temperature digests exactly: the sum feeds salinity only."""
+    gold = json.load(open(GOLDEN))["forced%d_steps%d_seed%d" % (forced, nsteps, seed)]
+    syn = ref_config(lt, forced, seed)
+    o = pyoracle.Oracle(syn.nx, syn.ny, syn.km, syn.params)
+    o.load(syn.all_fields())
+    o.sum_order(1)
+    for _ in range(nsteps):
+        o.tracer_call()
+    o.convadj()
+    for n in ("AT", "ATB"):
+        assert digest(o.get(n)[0]) == gold["outputs_T"][n], n
