@@ -11,9 +11,19 @@ One JSON line on rank 0.  Under torchrun each rank advances an independent
 replica of the domain on its own GPU (the path has no cross-domain exchange on
 one device: replicas only, weak scaling); the timed region is bracketed by a
 barrier and a device synchronize and the max over ranks is reported.
-``--impl reference`` times the reference algorithm on the host cores (the FP64
-CPU restatement, bit-exact with the reference's own tracer.cpp) on a bounded
-sample of the same workload.
+
+Beside the headline (the mixed step, device-resident inputs) the default run
+reports the FP64 drop-in, both forms' states compared after 100 steps, the
+global tracer content drift over 100 zero-flux steps in both forms, the FP64
+step with its diagnostics written, a reduced ensemble and serving run, the
+kernels of the next rows, and the CPU baseline.
+
+``--impl reference`` times the reference algorithm on the host cores: the
+FP64 CPU restatement (bit-exact with the reference's own tracer.cpp), fed by
+the host build of the input generator, never the CUDA library.  Each timed
+step is one step of a full-width, full-depth band of the 0.1-degree grid (its
+northern rows, with the fold); the whole grid is stepped twice beside it, and
+a one-thread rate is measured on a narrower band.
 """
 import argparse
 import ctypes as C
@@ -80,6 +90,12 @@ def parse():
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--rate", type=float, default=20.0, help="serving: mean arrivals per second")
+    ap.add_argument("--accuracy-steps", type=int, default=100,
+                    help="steps after which the mixed state is compared with the FP64 state")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the conservation, diagnostics, ensemble and serving figures of the default run")
+    ap.add_argument("--band-rows", type=int, default=0,
+                    help="CPU baseline: physical rows of the band a timed host step advances (default ny/16)")
     return ap.parse_args()
 
 
@@ -161,40 +177,111 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
-def cpu_reference_rate(lt, args, steps, warmup, budget_s=20.0):
-    """The reference algorithm on the host: the FP64 CPU restatement
-    (oracle/licom_oracle.cpp, OpenMP over all host cores), which is bit-exact
-    with the reference's own tracer.cpp compiled for the CPU.  Runs on a
-    bounded sample of the workload: the same generators on a patch of the
-    grid with the full column depth.  Returns (cell-steps/s, details)."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def host_mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
+
+
+def host_synth(args):
+    """The bench configuration's inputs from the host build of the generator
+    (oracle/liblicom_synth_host.so): the CPU baseline never loads the CUDA
+    library."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import pyoracle
-    cores = cpu_cores()
     nx, ny, km = args.grid
     w = workload(args)
-    snx, sny = max(72, nx // 5), max(48, ny // 5)
-    snx += snx % 2
-    syn = lt.Synth(snx, sny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
-    fields = syn.all_fields()
-    o = pyoracle.Oracle(snx, sny, km, syn.params, threads=cores)
-    o.load(fields)
-    o.sum_order(0)
+    return pyoracle, pyoracle.HostSynth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+
+
+def band_rate(pyoracle, hs, rows, threads, steps, warmup):
+    """The FP64 CPU restatement (OpenMP over `threads` host cores, diagnostics
+    off as in the GPU headline) on the northern band of `rows` physical rows
+    of the configuration (full width and depth, tripole fold included).
+    Returns (cell-steps/s, seconds per step); the time is that of the
+    tracer_ calls alone."""
+    o = pyoracle.Oracle(hs.nx, rows, hs.km, hs.params, threads=threads, diagnostics=0)
+    hs.fill(o, rows=rows + 4)
     for _ in range(warmup):
-        o.step(1)
-    done, t_total = 0, 0.0
-    while done < steps:
-        t0 = time.perf_counter()
-        o.step(1)
-        t_total += time.perf_counter() - t0
-        done += 1
-        if t_total > budget_s:
-            break
-    cells = snx * sny * km
-    rate = cells * done / t_total
-    sample = "%dx%dx%d patch (1/25 of the horizontal grid, full depth), %d step(s) after %d warm-up" % (
-        snx, sny, km, done, warmup)
-    return rate, {"unit": "cell-steps/s", "cores": cores, "kind": "port", "sample": sample,
-                  "value": rate}
+        o.step_timed(1)
+    t = sum(o.step_timed(1) for _ in range(steps))
+    del o
+    cells = hs.nx * rows * hs.km
+    return cells * steps / t, t / steps
+
+
+def cpu_baseline(args, steps, warmup, full_grid=False):
+    """CPU baseline on the host cores (the oracle port; see run_reference)."""
+    pyoracle, hs = host_synth(args)
+    cores = cpu_cores()
+    nx, ny, km = args.grid
+    rows = args.band_rows or max(8, ny // 16)
+    rate, sec = band_rate(pyoracle, hs, rows, cores, steps, warmup)
+    rate1, _ = band_rate(pyoracle, hs, 8, 1, 1, 1)
+    pyoracle.Oracle(8, 8, 3, hs.params, threads=cores)   # restore the thread count
+    cb = {"value": rate, "unit": "cell-steps/s", "cores": cores, "kind": "port", "cpu_model": cpu_model(),
+          "sample": "northern band %dx%dx%d of the %dx%dx%d grid (full width and depth, fold included), "
+                    "%d step(s) after %d warm-up, diagnostics off, time inside tracer_ only"
+                    % (nx, rows, km, nx, ny, km, steps, warmup),
+          "ms_per_sample_step": sec * 1e3,
+          "one_thread": {"value": rate1, "sample": "northern band %dx8x%d, 1 step after 1 warm-up" % (nx, km)}}
+    if full_grid:
+        need = 36 * (nx + 4) * (ny + 4) * km * 8
+        avail = host_mem_available()
+        if avail is not None and avail < need:
+            cb["full_grid"] = {"skipped": "host memory %.0f GB available, %.0f GB needed" % (avail / 1e9, need / 1e9)}
+        else:
+            o = pyoracle.Oracle(nx, ny, km, hs.params, threads=cores, diagnostics=0)
+            t0 = time.perf_counter()
+            hs.fill(o)
+            t_fill = time.perf_counter() - t0
+            t = o.step_timed(2)
+            del o
+            cb["full_grid"] = {"value": nx * ny * km * 2 / t, "steps": 2, "ms_per_step": t / 2 * 1e3,
+                               "input_generation_s": t_fill, "cores": cores}
+    return cb
+
+
+def reference_own_code_rate():
+    """The reference's own tracer.cpp compiled for the CPU through the HIP
+    stand-in (oracle/_ref), one 36x40x55 block on one core, when it was built:
+    the stand-in runs every GPU thread of a launch in turn, so this is a
+    measure of that emulation, reported beside the port."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pyoracle
+    if not pyoracle.reference_available():
+        return None
+    hs = pyoracle.HostSynth(36, 40, 55, forced=1, cap_north=0, cap_south=3, dz_top=5.0, dz_bot=300.0)
+    o = pyoracle.Oracle(36, 40, 55, hs.params, threads=1)
+    hs.fill(o)
+    ref = pyoracle.Reference(hs.params)
+    ref.load({n: o.get(n) for n in pyoracle.INPUTS})
+    ref.tracer_call(0)
+    n = 5
+    t0 = time.perf_counter()
+    for s in range(n):
+        ref.tracer_call(s + 1)
+    t = (time.perf_counter() - t0) / n
+    t_port = o.step_timed(n) / n
+    return {"value": 36 * 40 * 55 / t, "unit": "cell-steps/s", "cores": 1,
+            "sample": "one 36x40x55 block (the reference's compiled size), %d steps" % n,
+            "port_same_block_one_thread": 36 * 40 * 55 / t_port}
 
 
 def dist_setup(args):
@@ -240,23 +327,40 @@ def whole_job_rate(cells_per_rank, steps, world, max_ms):
 
 
 def run_reference(args):
+    """The reference arm: the reference algorithm on the host cores, on the
+    same configuration, metric and unit as this build's arm.  The reference
+    has no CPU implementation of this path of its own (its Fortran driver is
+    compiled out and missing); the FP64 restatement is bit-exact with its
+    tracer.cpp compiled for the CPU, whose HIP stand-in runs far slower than
+    real CPU code (reported as reference_own_code), so the restatement is the
+    timed baseline.  Rank 0 alone runs; other ranks exit without work."""
     world, rank, local, pg = dist_setup(args)
-    lt = load_package()
     if rank == 0:
-        rate, cb = cpu_reference_rate(lt, args, args.steps, args.warmup, budget_s=120.0)
         nx, ny, km = args.grid
+        cb = cpu_baseline(args, args.steps, args.warmup, full_grid=True)
+        rate = cb["value"]
         line = {"impl": "reference", "metric": "tracer cell-steps/s (0.1deg 3600x2302x55)", "value": rate,
                 "unit": "cell-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": nx * ny * km / rate * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generators, configuration shapes)",
-                "config": {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
-                           "device": "host cores"},
+                "ms_per_step": cb["ms_per_sample_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generators with the configuration's shapes and distributions)",
+                "config": config_of(args, world),
                 "cpu_baseline": cb,
+                "reference_own_code": reference_own_code_rate(),
                 "e2e": {"value": rate, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def config_of(args, world):
+    """The workload, identical in both arms (the arithmetic is in dtype)."""
+    nx, ny, km = args.grid
+    cells = nx * ny * km
+    return {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)}
 
 
 def measure(lt, args, pg, world, local, precision, keep_state):
@@ -325,8 +429,16 @@ def measure(lt, args, pg, world, local, precision, keep_state):
     e2e = {"value": whole_job_rate(cells, e2e_steps, world, ms_e2e), "unit": "cell-steps/s",
            "h2d_bytes_per_step": 6 * A * 8, "d2h_bytes_per_step": 8,
            "api": "lt_step_host (C ABI), pinned host forcing"}
-    state = dom.get("AT") if keep_state else None
-    kmt = syn.field("KMT") if keep_state else None
+    steps_total = args.warmup + args.steps + 1 + e2e_steps
+    state = kmt = None
+    if keep_state:
+        # both forms advance the same steps from the same inputs, then their
+        # states are compared
+        if steps_total < args.accuracy_steps:
+            dom.step(args.accuracy_steps - steps_total)
+            steps_total = args.accuracy_steps
+        state = dom.get("AT")
+        kmt = syn.field("KMT")
 
     # ---- the sea-ice adjustment that follows each tracer step in the model
     # (icesnow.cpp): its own HBM-bound kernel, timed over repeated launches
@@ -348,7 +460,7 @@ def measure(lt, args, pg, world, local, precision, keep_state):
     dom.close()
     return {"value": value, "ms_per_step": ms / args.steps, "roofline": roofline, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(), "fw_norm2": fw.value, "state": state, "kmt": kmt,
-            "steps_total": args.warmup + args.steps + 1 + e2e_steps, "icesnow": icesnow}
+            "steps_total": steps_total, "icesnow": icesnow}
 
 
 def measure_readyc(lt, args, precision):
@@ -415,6 +527,104 @@ def measure_readyc(lt, args, precision):
     return turb, del4u
 
 
+def measure_conservation(lt, args, precision, steps, diagnostics=False):
+    """Global tracer content (f64, fixed-order tree) before and after `steps`
+    steps with zero surface flux and land rows capping the north and south
+    edges (the fold averages the top row with its mirror, which moves content
+    by design), on the bench grid; with diagnostics on, the step also writes
+    the reference's diagnostic fields.  Returns the relative drift of T and S
+    and the device time per step."""
+    import numpy as np
+    nx, ny, km = args.grid
+    w = dict(workload(args), forced=0, cap_north=3, cap_south=3)
+    syn = lt.Synth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+    dom = syn.domain(precision=lt.PREC_MIXED if precision == "mixed" else lt.PREC_FP64, diagnostics=diagnostics)
+    c0 = np.array(dom.tracer_content())
+    dom.mark(0)
+    dom.step(steps)
+    dom.mark(1)
+    dom.sync()
+    ms = dom.last_step_ms() / steps
+    c1 = np.array(dom.tracer_content())
+    dom.close()
+    rel = np.abs(c1 - c0) / np.abs(c0)
+    return {"T": float(rel[0]), "S": float(rel[1])}, ms
+
+
+def ensemble_figures(lt, nmem, steps, warmup, check):
+    """Configuration 3: nmem members of the 1-degree 360x218x30 grid (T
+    perturbed by seeded N(0, 0.01 K) per member) advanced as ONE batch (one
+    continuity and one persistent column launch per step, CUDA-graph replay,
+    autotuned launch shape), mixed precision.  The first `check` members are
+    compared with their FP64 runs (the FP64 drop-in is bit-exact with the
+    oracle on this grid)."""
+    import numpy as np
+    nx, ny, km = 360, 218, 30
+    syns = [lt.Synth(nx, ny, km, member=m + 1, tpert=0.01, forced=1, cap_north=0) for m in range(nmem)]
+    doms = [s.domain(precision=lt.PREC_MIXED) for s in syns]
+    batch = lt.Batch(doms)
+    cfg = batch.autotune(trial_steps=2)
+    batch.step(warmup)
+    batch.sync()
+    n0 = lt.launch_count()
+    with ClockSampler(0) as clk:
+        batch.step(steps)
+        batch.sync()
+    launches = lt.launch_count() - n0
+    ms = batch.last_ms()
+    value = whole_job_rate(nx * ny * km * nmem, steps, 1, ms)
+    worst_t = worst_s = 0.0
+    for s, d in list(zip(syns, doms))[:check]:
+        ref = s.domain(precision=lt.PREC_FP64)
+        ref.step(warmup + steps)
+        ref.sync()
+        kmt = s.field("KMT")
+        wet = (np.arange(km)[:, None, None] < kmt[None])[:, 2:-2, 2:-2]
+        a, g = ref.get("AT")[:, :, 2:-2, 2:-2], d.get("AT")[:, :, 2:-2, 2:-2]
+        worst_t = max(worst_t, float(np.abs(a[0] - g[0])[wet].max()))
+        worst_s = max(worst_s, float(np.abs(a[1] - g[1])[wet].max()) * 1e3)
+        ref.close()
+    batch.close()
+    for d in doms:
+        d.close()
+    return {"members": nmem, "grid": "%dx%dx%d" % (nx, ny, km), "value": value, "unit": "cell-steps/s",
+            "ms_per_step": ms / steps, "steps": steps, "warmup": warmup, "launch_shape": cfg,
+            "gpu_launches": launches, "clocks": clk.summary(),
+            "accuracy": {"max_abs_dT_K": worst_t, "max_abs_dS_psu": worst_s, "steps": warmup + steps,
+                         "members_checked": check, "against": "each checked member's FP64 run"}}
+
+
+def serving_figures(lt, requests, rate):
+    """Configuration 4: Poisson-arriving requests (mean `rate` per second) for
+    closed regional domains, horizontal area log-uniform from 128x128 to
+    1200x900 (4:3, km 30 below the geometric middle of the range, 55 above),
+    10..200 steps each, mixed precision, through the request server
+    (admission by free HBM, resident state, continuous batching)."""
+    import random
+    rng = random.Random(2024)
+    srv = lt.Server(precision=lt.PREC_MIXED, chunk_steps=10)
+    a_lo, a_hi = 128 * 128, 1200 * 900
+    t, t0 = 0.0, srv.clock()
+    for r in range(requests):
+        t += rng.expovariate(rate)
+        area = math_exp(rng.uniform(math_log(a_lo), math_log(a_hi)))
+        nx = max(64, int(round((area * 4.0 / 3.0) ** 0.5 / 4.0)) * 4)
+        ny = max(48, int(round(area / nx)))
+        km = 30 if area < (a_lo * a_hi) ** 0.5 else 55
+        srv.submit(nx, ny, km, rng.randint(10, 200), arrival=t0 + t, seed=1000 + r,
+                   ew_cyclic=0, tripole=0, forced=1)
+    n0 = lt.launch_count()
+    with ClockSampler(0) as clk:
+        srv.drain()
+    st = srv.stats()
+    srv.close()
+    return {"requests": requests, "rate_per_s": rate, "value": st["cell_steps"] / st["wall_s"],
+            "unit": "cell-steps/s", "latency_s": {"p50": st["latency_p50"], "p99": st["latency_p99"],
+                                                  "max": st["latency_max"]},
+            "device_busy_cell_steps_per_s": st["cell_steps"] / st["busy_s"] if st["busy_s"] else None,
+            "server": st, "gpu_launches": lt.launch_count() - n0, "clocks": clk.summary()}
+
+
 def run_ours(args):
     world, rank, local, pg = dist_setup(args)
     lt = load_package()
@@ -429,7 +639,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        _, cpu = cpu_reference_rate(lt, args, 2, 0)
+        cpu = cpu_baseline(args, 2, 1)
 
     if rank == 0:
         line = {"metric": "tracer cell-steps/s (0.1deg 3600x2302x55)",
@@ -438,9 +648,7 @@ def run_ours(args):
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if main == "fp64" else "f32 arithmetic, f64 state",
                 "data": "synthetic (seeded generators with the configuration's shapes and distributions)",
-                "config": {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
-                           "precision": main, "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)},
+                "config": config_of(args, world),
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"],
                 "clocks": r["clocks"], "fw_norm2": r["fw_norm2"], "icesnow": r["icesnow"]}
         if not args.no_turb and world == 1:
@@ -456,7 +664,27 @@ def run_ours(args):
             line["mixed_over_fp64"] = r["value"] / f["value"]
             line["accuracy"] = {"max_abs_dT_K": float(np.abs(a[0] - g[0])[wet].max()),
                                 "max_abs_dS_psu": float(np.abs(a[1] - g[1])[wet].max()) * 1e3,
-                                "steps": r["steps_total"], "against": "the FP64 drop-in on the same inputs"}
+                                "steps": r["steps_total"], "bound": {"T_K": 1e-4, "S_psu": 1e-5},
+                                "against": "the FP64 drop-in on the same inputs (bit-exact with the oracle)"}
+        if both and world == 1 and not args.no_extras:
+            hbm, hbm_kind = peaks()
+            steps_c = args.accuracy_steps
+            drift_m, _ = measure_conservation(lt, args, "mixed", steps_c)
+            drift_f, ms_diag = measure_conservation(lt, args, "fp64", steps_c, diagnostics=True)
+            line["conservation"] = {"steps": steps_c, "bound": 1e-13, "mixed": drift_m, "fp64": drift_f,
+                                    "workload": "the bench grid with zero surface flux and land rows capping "
+                                                "the north and south edges"}
+            diag_bytes = STEP_BYTES["fp64"] + 104.0
+            line["fp64_diagnostics_on"] = {
+                "value": cells / (ms_diag * 1e-3), "ms_per_step": ms_diag, "steps": steps_c,
+                "bytes_per_cell_step": diag_bytes,
+                "step_frac": diag_bytes * cells / (ms_diag * 1e-3) / 1e9 / hbm, "peak_kind": hbm_kind,
+                "writes": "ax, ay, az, dz, tend, dt_diff (both tracers) and penetrate, as tracer.cpp always does",
+                "workload": "the conservation run above (zero surface flux, capped edges)"}
+            line["ensemble"] = ensemble_figures(lt, args.members, 100, 3, check=4)
+            line["ensemble"]["reduced"] = "4 of %d members checked against their FP64 runs" % args.members
+            line["serving"] = serving_figures(lt, 60, args.rate)
+            line["serving"]["reduced"] = "60 requests (the full workload is 200: bench.py --workload serving)"
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
@@ -464,93 +692,40 @@ def run_ours(args):
 
 
 def run_ensemble(args):
-    """Configuration 3: members of the 1-degree 360x218x30 grid, T perturbed
-    by seeded N(0, 0.01 K) per member, advanced --steps steps as ONE batch
-    (one continuity and one persistent column launch per step, replayed from
-    a CUDA graph, launch shape from the autotuner), mixed precision; every
-    member is then checked against its own FP64 run."""
-    import numpy as np
+    """Configuration 3 on its own line (bench.py --workload ensemble)."""
     lt = load_package()
     lt.set_device(0)
-    nx, ny, km, nmem, steps = 360, 218, 30, args.members, args.steps
-    syns = [lt.Synth(nx, ny, km, member=m + 1, tpert=0.01, forced=1, cap_north=0) for m in range(nmem)]
-    doms = [s.domain(precision=lt.PREC_MIXED) for s in syns]
-    batch = lt.Batch(doms)
-    cfg = batch.autotune(trial_steps=2)
-    batch.step(args.warmup)
-    batch.sync()
-    n0 = lt.launch_count()
-    with ClockSampler(0) as clk:
-        batch.step(steps)
-        batch.sync()
-    launches = lt.launch_count() - n0
-    ms = batch.last_ms()
-    cells = nx * ny * km
-    value = whole_job_rate(cells * nmem, steps, 1, ms)
-    # accuracy of every member against its FP64 run over the same steps
-    worst_t = worst_s = 0.0
-    for s, d in zip(syns, doms):
-        ref = s.domain(precision=lt.PREC_FP64)
-        ref.step(args.warmup + steps)
-        ref.sync()
-        kmt = s.field("KMT")
-        wet = (np.arange(km)[:, None, None] < kmt[None])[:, 2:-2, 2:-2]
-        a, g = ref.get("AT")[:, :, 2:-2, 2:-2], d.get("AT")[:, :, 2:-2, 2:-2]
-        worst_t = max(worst_t, float(np.abs(a[0] - g[0])[wet].max()))
-        worst_s = max(worst_s, float(np.abs(a[1] - g[1])[wet].max()) * 1e3)
-        del ref
+    e = ensemble_figures(lt, args.members, args.steps, args.warmup, check=args.members)
     hbm, hbm_kind = peaks()
-    line = {"metric": "ensemble tracer cell-steps/s (%d x 1deg %dx%dx%d, MIXED, one batch)" % (nmem, nx, ny, km),
-            "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    cells = 360 * 218 * 30
+    line = {"metric": "ensemble tracer cell-steps/s (%d x 1deg 360x218x30, MIXED, one batch)" % args.members,
+            "value": e["value"], "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": e["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 arithmetic, f64 state", "data": "synthetic (seeded generators, perturbed members)",
-            "config": {"workload": "ensemble %d x %dx%dx%d" % (nmem, nx, ny, km), "members": nmem,
-                       "launch_shape": cfg, "l2": "%.1f GB resident, far larger than L2" % (
-                           nmem * 66.8e9 / 4.56e8 * cells / 1e9)},
-            "roofline": {"bound": "hbm", "achieved": value * STEP_BYTES["mixed"] / 1e9, "peak": hbm,
-                         "unit": "GB/s", "frac": value * STEP_BYTES["mixed"] / 1e9 / hbm, "peak_kind": hbm_kind,
+            "config": {"workload": "ensemble %d x 360x218x30" % args.members, "members": args.members,
+                       "launch_shape": e["launch_shape"], "l2": "%.1f GB resident, far larger than L2" % (
+                           args.members * 66.8e9 / 4.56e8 * cells / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": e["value"] * STEP_BYTES["mixed"] / 1e9, "peak": hbm,
+                         "unit": "GB/s", "frac": e["value"] * STEP_BYTES["mixed"] / 1e9 / hbm, "peak_kind": hbm_kind,
                          "basis": "whole step, 100 B per cell-step"},
-            "accuracy": {"max_abs_dT_K": worst_t, "max_abs_dS_psu": worst_s, "steps": args.warmup + steps,
-                         "against": "FP64 run of each member"},
-            "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": None, "e2e": None}
+            "accuracy": e["accuracy"], "gpu_launches": e["gpu_launches"], "clocks": e["clocks"],
+            "cpu_baseline": None, "e2e": None}
     print(json.dumps(line), flush=True)
 
 
 def run_serving(args):
-    """Configuration 4: Poisson-arriving requests (mean --rate per second) for
-    closed regional domains, horizontal area log-uniform from 128x128 to
-    1200x900 (4:3, km 30 below the geometric middle of the range, 55 above),
-    10..200 steps each, mixed precision, through the request server
-    (admission by free HBM, resident state, continuous batching)."""
-    import random
+    """Configuration 4 on its own line (bench.py --workload serving)."""
     lt = load_package()
     lt.set_device(0)
-    rng = random.Random(2024)
-    srv = lt.Server(precision=lt.PREC_MIXED, chunk_steps=10)
-    a_lo, a_hi = 128 * 128, 1200 * 900
-    t, t0 = 0.0, srv.clock()
-    for r in range(args.requests):
-        t += rng.expovariate(args.rate)
-        area = math_exp(rng.uniform(math_log(a_lo), math_log(a_hi)))
-        nx = max(64, int(round((area * 4.0 / 3.0) ** 0.5 / 4.0)) * 4)
-        ny = max(48, int(round(area / nx)))
-        km = 30 if area < (a_lo * a_hi) ** 0.5 else 55
-        srv.submit(nx, ny, km, rng.randint(10, 200), arrival=t0 + t, seed=1000 + r,
-                   ew_cyclic=0, tripole=0, forced=1)
-    n0 = lt.launch_count()
-    with ClockSampler(0) as clk:
-        srv.drain()
-    st = srv.stats()
-    value = st["cell_steps"] / st["wall_s"]
+    sv = serving_figures(lt, args.requests, args.rate)
     line = {"metric": "serving tracer cell-steps/s and latency (Poisson %.0f/s, regional 128x128..1200x900)" % args.rate,
-            "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": None, "warmup": 0,
+            "value": sv["value"], "unit": "cell-steps/s", "n_gpus": 1, "steps": None, "warmup": 0,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 arithmetic, f64 state", "data": "synthetic (seeded generators, seeded arrivals)",
             "config": {"workload": "serving %d requests" % args.requests, "rate_per_s": args.rate,
                        "chunk_steps": 10},
-            "latency_s": {"p50": st["latency_p50"], "p99": st["latency_p99"], "max": st["latency_max"]},
-            "device_busy_cell_steps_per_s": st["cell_steps"] / st["busy_s"] if st["busy_s"] else None,
-            "server": st, "gpu_launches": lt.launch_count() - n0, "clocks": clk.summary(),
+            "latency_s": sv["latency_s"], "device_busy_cell_steps_per_s": sv["device_busy_cell_steps_per_s"],
+            "server": sv["server"], "gpu_launches": sv["gpu_launches"], "clocks": sv["clocks"],
             "cpu_baseline": None, "e2e": None}
     print(json.dumps(line), flush=True)
 

@@ -44,6 +44,11 @@ int lt_synth_params(const lt_synth* s, lt_params* out);
 int lt_synth_grid(const lt_synth* s, lt_grid* out);
 /* Host copy of any input field (3-D fields are generated on the host). */
 int lt_synth_field(const lt_synth* s, int field, void* dst, size_t nbytes);
+/* The same field for the northern band of the domain, rows j < rows (halo
+ * included, 5 <= rows <= jmt): 3-D fields are generated for those rows only
+ * (cell values identical to lt_synth_field's), 2-D fields are their leading
+ * rows, 1-D fields whole.  nbytes is the byte size of the band's field. */
+int lt_synth_field_rows(const lt_synth* s, int field, int rows, void* dst, size_t nbytes);
 /* Element count of a field for this domain. */
 long lt_synth_field_count(const lt_synth* s, int field);
 /* Upload every input of a domain: 2-D/1-D fields from the host, 3-D fields

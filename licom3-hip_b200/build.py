@@ -1,6 +1,6 @@
 """Build recipe for liblicom_tracer.so (sm_100a) and the CPU checker libraries.
 
-Usage: python licom3-hip_b200/build.py [--oracle] [--ref]
+Usage: python licom3-hip_b200/build.py [--oracle [--ref <reference source tree>]]
 
 The CUDA library is compiled per translation unit with nvcc for
 ``arch=compute_100a,code=sm_100a``; files whose results are compared bit for
@@ -84,20 +84,24 @@ def build_cuda(verbose=False, ptxas_info=False):
 
 
 def build_oracle(ref=None):
-    """CPU checker libraries (test infrastructure): the oracle, and the
-    reference's own tracer.cpp/convadj.cpp when the reference tree is present."""
+    """CPU checker libraries (test infrastructure): the oracle and the host
+    input generator; with ``ref`` (or LICOM_REFERENCE_DIR), the directory of
+    the reference's sources, also the reference's own tracer.cpp, convadj.cpp,
+    icesnow.cpp and readyc.cpp compiled for the CPU."""
     oracle_dir = os.path.join(REPO, "oracle")
     env = dict(os.environ)
     env.pop("CXX", None)
     targets = ["all"]
-    ref_tree = ref or "/root/reference"
-    if os.path.isdir(ref_tree):
+    ref_tree = ref or os.environ.get("LICOM_REFERENCE_DIR")
+    args = []
+    if ref_tree and os.path.isfile(os.path.join(ref_tree, "tracer.cpp")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", oracle_dir, "REF=" + ref_tree] + targets, check=True, env=env)
+        args.append("REF=" + ref_tree)
+    subprocess.run(["make", "-s", "-C", oracle_dir] + args + targets, check=True, env=env)
 
 
 if __name__ == "__main__":
     build_cuda(verbose=True, ptxas_info="--ptxas" in sys.argv)
     if "--oracle" in sys.argv:
-        build_oracle()
+        build_oracle(sys.argv[sys.argv.index("--ref") + 1] if "--ref" in sys.argv else None)
     print(LIB)

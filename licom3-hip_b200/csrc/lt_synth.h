@@ -195,10 +195,9 @@ struct SynthConfig {
   double smooth_cells_1deg = 8.0;       // smoothing radius at 1 degree
   int ncc = 1, nbb = 60;
   double dts = 1800.0;
-  // Biharmonic tracer diffusivity (m^4/s).  0 selects the value -1e17 at the
-  // 36-column (10 degree) global grid scaled by (36/nx)^4, i.e. by the fourth
-  // power of the grid spacing, which keeps ah*dts*64/dx^4 (the forward-step
-  // stability number of del4) the same at every resolution.
+  // Biharmonic tracer diffusivity (m^4/s).  0 selects the configured
+  // -1e17, capped at half of this grid's explicit stability limit (see
+  // build_domain).
   double ah_bihar = 0.0;
   double dwndmix = 1.0e-3;
   double gamma_days = 30.0;
@@ -542,20 +541,25 @@ inline Domain build_domain(const SynthConfig& c) {
   return d;
 }
 
-// Fill the dense 3-D inputs of a domain on the host.  at/atb: [2][km(+1)][jmt][imt];
-// velocities: [km][jmt][imt]; akt: [2][km][jmt][imt].  Ghost cells of the
-// tracers are filled with the same halo rule the model applies.
-inline void fill_state(const Domain& d, double* at, double* atb) {
+// Fill the dense 3-D inputs of a domain on the host.  at/atb: [2][km(+1)][rows][imt];
+// velocities: [km][rows][imt]; akt: [2][km][rows][imt], with rows the number of
+// leading rows produced (the whole domain when rows == jmt; fewer give the
+// northern band j < rows of the same fields, with its own ghost cells).
+// Ghost cells of the tracers are filled with the same halo rule the model
+// applies.
+inline void fill_state(const Domain& d, double* at, double* atb, int rows = -1) {
+  if (rows < 0) rows = d.jmt;
   const CellTables t = d.tables();
-  const long A = (long)d.imt * d.jmt, F = A * d.km;
+  const long A = (long)d.imt * rows, F = A * d.km;
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < d.km; ++k)
-    for (int j = 0; j < d.jmt; ++j)
+    for (int j = 0; j < rows; ++j)
       for (int i = 0; i < d.imt; ++i) {
         const long c = (long)k * A + (long)j * d.imt + i;
         at[c] = cell_T(t, k, j, i);
         at[F + c] = cell_S(t, k, j, i);
       }
-  halo_fill(at, 2 * d.km, d.imt, d.jmt, d.cfg.ew_cyclic, d.cfg.tripole);
+  halo_fill(at, 2 * d.km, d.imt, rows, d.cfg.ew_cyclic, d.cfg.tripole);
   const long FB = A * (d.km + 1);
   for (int n = 0; n < 2; ++n) {
     std::memset(atb + n * FB, 0, sizeof(double) * A);
@@ -563,30 +567,38 @@ inline void fill_state(const Domain& d, double* at, double* atb) {
   }
 }
 
-inline void fill_velocity(const Domain& d, double* utf, double* vtf, double* utl, double* vtl) {
+// One velocity component: which = 0 utf, 1 vtf, 2 utl, 3 vtl.
+inline void fill_velocity_one(const Domain& d, int which, double* dst, int rows = -1) {
+  if (rows < 0) rows = d.jmt;
   const CellTables t = d.tables();
-  const long A = (long)d.imt * d.jmt;
+  const long A = (long)d.imt * rows;
   const double ncc1 = (double)(d.cfg.ncc + 1);
+#pragma omp parallel for collapse(2) schedule(static)
   for (int k = 0; k < d.km; ++k)
-    for (int j = 0; j < d.jmt; ++j)
+    for (int j = 0; j < rows; ++j)
       for (int i = 0; i < d.imt; ++i) {
-        const long c = (long)k * A + (long)j * d.imt + i;
-        const double u = cell_U(t, k, j, i), v = cell_V(t, k, j, i);
-        utl[c] = u; vtl[c] = v;
-        utf[c] = ncc1 * u; vtf[c] = ncc1 * v;
+        const double u = (which & 1) ? cell_V(t, k, j, i) : cell_U(t, k, j, i);
+        dst[(long)k * A + (long)j * d.imt + i] = (which < 2) ? ncc1 * u : u;
       }
 }
 
-inline void fill_akt(const Domain& d, double* akt) {
+inline void fill_velocity(const Domain& d, double* utf, double* vtf, double* utl, double* vtl, int rows = -1) {
+  fill_velocity_one(d, 0, utf, rows);
+  fill_velocity_one(d, 1, vtf, rows);
+  fill_velocity_one(d, 2, utl, rows);
+  fill_velocity_one(d, 3, vtl, rows);
+}
+
+inline void fill_akt(const Domain& d, double* akt, int rows = -1) {
+  if (rows < 0) rows = d.jmt;
   const CellTables t = d.tables();
-  const long A = (long)d.imt * d.jmt, F = A * d.km;
+  const long A = (long)d.imt * rows, F = A * d.km;
+#pragma omp parallel for collapse(3) schedule(static)
   for (int n = 0; n < 2; ++n)
     for (int k = 0; k < d.km; ++k)
-      for (int j = 0; j < d.jmt; ++j)
+      for (int j = 0; j < rows; ++j)
         for (int i = 0; i < d.imt; ++i)
           akt[n * F + (long)k * A + (long)j * d.imt + i] = cell_akt(t, n, k, j, i);
 }
-
-
 
 }  // namespace lt

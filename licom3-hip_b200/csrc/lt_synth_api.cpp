@@ -81,36 +81,35 @@ long lt_synth_field_count(const lt_synth* s, int f) {
 }
 
 int lt_synth_field(const lt_synth* s, int f, void* dst, size_t nbytes) {
+  if (!s) return LT_E_INVALID;
+  return lt_synth_field_rows(s, f, s->d.jmt, dst, nbytes);
+}
+
+int lt_synth_field_rows(const lt_synth* s, int f, int rows, void* dst, size_t nbytes) {
   if (!s || !dst || f < 0 || f >= LT_F_COUNT) return LT_E_INVALID;
   const lt::Domain& d = s->d;
-  const size_t need = lt::field_bytes(f, d.imt, d.jmt, d.km);
+  if (rows < 5 || rows > d.jmt) return LT_E_INVALID;
+  const size_t need = lt::field_bytes(f, d.imt, rows, d.km);
   if (nbytes != need) return LT_E_INVALID;
-  const long F = (long)d.imt * d.jmt * d.km;
+  const long F = (long)d.imt * rows * d.km;
   double* o = static_cast<double*>(dst);
+  // 2-D fields [jmt][imt]: the leading rows
   auto copy = [&](const void* src) { std::memcpy(dst, src, nbytes); return LT_OK; };
   switch (f) {
-    case LT_F_AT: {
-      std::vector<double> atb(2 * (size_t)d.imt * d.jmt * (d.km + 1));
-      lt::fill_state(d, o, atb.data());
+    case LT_F_AT: case LT_F_RESTORE: {
+      std::vector<double> atb(2 * (size_t)d.imt * rows * (d.km + 1));
+      lt::fill_state(d, o, atb.data(), rows);
       return LT_OK;
     }
     case LT_F_ATB: {
       std::vector<double> at(2 * (size_t)F);
-      lt::fill_state(d, at.data(), o);
+      lt::fill_state(d, at.data(), o, rows);
       return LT_OK;
     }
-    case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: {
-      std::vector<double> v[4];
-      for (auto& x : v) x.resize(F);
-      lt::fill_velocity(d, v[0].data(), v[1].data(), v[2].data(), v[3].data());
-      return copy(v[f - LT_F_UTF].data());
-    }
-    case LT_F_AKT: lt::fill_akt(d, o); return LT_OK;
-    case LT_F_RESTORE: {
-      std::vector<double> atb(2 * (size_t)d.imt * d.jmt * (d.km + 1));
-      lt::fill_state(d, o, atb.data());
+    case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL:
+      lt::fill_velocity_one(d, f - LT_F_UTF, o, rows);
       return LT_OK;
-    }
+    case LT_F_AKT: lt::fill_akt(d, o, rows); return LT_OK;
     case LT_F_H0F: return copy(d.h0f.data());
     case LT_F_H0L: return copy(d.h0l.data());
     case LT_F_SWV: return copy(d.swv.data());

@@ -98,17 +98,45 @@ struct Oracle {
     return 0;
   }
 
+  // copies of the dynamics inputs that or_step restores before every step
+  std::vector<double> dyn0[5];
+
+  // Fields of the tracer step are allocated at creation; the diagnostics
+  // only while diagnostics are on; the restoring target, the closure's and
+  // the momentum friction's fields on first use (a 0.1-degree oracle then
+  // fits the host memory of one GPU's share of a node).
   Oracle(int nx_, int ny_, int km_) : nx(nx_), ny(ny_), km(km_) {
     imt = nx + 4; jmt = ny + 4;
     A = (long)imt * jmt; F = A * km; FB = A * (km + 1);
     for (int f = 0; f < LT_F_COUNT; ++f) {
-      if (field_info(f).is_int) fi[f].assign(count(f), 0);
-      else fd[f].assign(count(f), 0.0);
+      const int kd = field_info(f).kind;
+      const bool small = kd == K2 || kd == K2I || kd == K2N || kd == K1 || kd == K1C || kd == K1P;
+      const bool step = f == LT_F_AT || f == LT_F_ATB || f == LT_F_UTF || f == LT_F_VTF || f == LT_F_UTL ||
+                        f == LT_F_VTL || f == LT_F_AKT || f == LT_F_WS || f == LT_F_UTF_OUT || f == LT_F_VTF_OUT;
+      if (small || step) ensure(f);
     }
+    set_diagnostics(1);
     for (auto* v : {&vit, &at00, &atmax, &atmin, &uk, &vk, &wka, &wkb, &wkd, &wkc, &tf, &adv_tt, &d2tk,
                     &u_wface, &v_sface, &ori})
       v->assign(F, 0.0);
     work.assign(A, 0.0); stf.assign(A, 0.0); temp11.assign(A, 0.0);
+  }
+
+  void ensure(int f) {
+    if (field_info(f).is_int) {
+      if (fi[f].empty()) fi[f].assign(count(f), 0);
+    } else if (fd[f].empty()) {
+      fd[f].assign(count(f), 0.0);
+    }
+  }
+  void ensure_all() {
+    for (int f = 0; f < LT_F_COUNT; ++f) ensure(f);
+  }
+  void set_diagnostics(int on) {
+    diagnostics = on;
+    if (on)
+      for (int f : {LT_F_AX, LT_F_AY, LT_F_AZ, LT_F_DZ, LT_F_TEND, LT_F_DT_DIFF, LT_F_DT_CONV, LT_F_PENETRATE})
+        ensure(f);
   }
 
   // index helpers
@@ -233,7 +261,9 @@ void tracer_call(Oracle& o) {
   const double* odzp = o.fd[LT_F_ODZP].data();
   const double* odzt = o.fd[LT_F_ODZT].data();
   const double* pen = o.fd[LT_F_PEN].data();
+  if (o.p.boundary_restore == 1) o.ensure(LT_F_RESTORE);
   const double* restore = o.fd[LT_F_RESTORE].data();
+  const bool dg = o.diagnostics != 0;   // diagnostic fields are written only while on
   double* ax = o.fd[LT_F_AX].data();
   double* ay = o.fd[LT_F_AY].data();
   double* az = o.fd[LT_F_AZ].data();
@@ -447,9 +477,11 @@ void tracer_call(Oracle& o) {
           const double yy = -(y0 + xy3 + xy4 + cy);
           const double zz = -(za + zb1 + zb2 + zc);
           adv_tt[c] = xx + yy + zz;
-          ax[n * F + c] = xx;
-          ay[n * F + c] = yy;
-          az[n * F + c] = zz;
+          if (dg) {
+            ax[n * F + c] = xx;
+            ay[n * F + c] = yy;
+            az[n * F + c] = zz;
+          }
         }
     // tracer_del4_1: first masked Laplacian of atb, scaled by ahf
     std::fill(o.d2tk.begin(), o.d2tk.end(), 0.0);
@@ -500,29 +532,33 @@ void tracer_call(Oracle& o) {
             const double w1 = swv[a] * pen[k - 1] * vit[c];
             const double w2 = swv[a] * pen[k] * vit[c + A];
             tf[c] = tf[c] + (w1 - w2) * odzp[k];
-            penetrate[c] = (w1 - w2) * odzp[k];
+            if (dg) penetrate[c] = (w1 - w2) * odzp[k];
           }
           const double w1 = swv[a] * pen[0] * vit[A + a];
           const double w2 = swv[a] * pen[km - 2] * vit[(km - 1) * A + a];
           tf[a] = tf[a] - odzp[0] * w1;
           tf[(km - 1) * A + a] = tf[(km - 1) * A + a] + odzp[km - 1] * w2;
-          penetrate[a] = -w1 * odzp[0];
-          penetrate[(km - 1) * A + a] = w2 * odzp[km - 1];
+          if (dg) {
+            penetrate[a] = -w1 * odzp[0];
+            penetrate[(km - 1) * A + a] = w2 * odzp[km - 1];
+          }
         }
         for (int k = 1; k < km - 1; ++k) {
           const long c = C(k, j, i);
           const double w1 = wkc[c - A] * (atbn[c] - atbn[c + A]) * odzt[k] * vit[c];
           const double w2 = wkc[c] * (atbn[c + A] - atbn[c + 2 * A]) * odzt[k + 1] * vit[c + A];
           tf[c] = tf[c] + odzp[k] * (w1 - w2) * 0.5;
-          dzd[n * F + c] = odzp[k] * (w1 - w2) * 0.5;
+          if (dg) dzd[n * F + c] = odzp[k] * (w1 - w2) * 0.5;
         }
         const double w1 = wkc[a] * (atbn[A + a] - atbn[2 * A + a]) * odzt[1] * vit[A + a];
         const double w2 = wkc[(km - 2) * A + a] * (atbn[(km - 1) * A + a] - atbn[km * A + a]) * odzt[km - 1] *
                           vit[(km - 1) * A + a];
         tf[a] = tf[a] - odzp[0] * w1 * 0.5;
         tf[(km - 1) * A + a] = tf[(km - 1) * A + a] + odzp[km - 1] * w2 * (1.0 - aidif);
-        dzd[n * F + a] = -odzp[0] * w1 * 0.5;
-        dzd[n * F + (km - 1) * A + a] = odzp[km - 1] * w2 * 0.5;
+        if (dg) {
+          dzd[n * F + a] = -odzp[0] * w1 * 0.5;
+          dzd[n * F + (km - 1) * A + a] = odzp[km - 1] * w2 * 0.5;
+        }
       }
     if (n == 1) {
       const double* atbS_top = atb + FB + A;   // S at the surface, previous time level
@@ -632,9 +668,11 @@ void tracer_call(Oracle& o) {
       for (int j = 0; j < jmt; ++j)
         for (int i = 0; i < imt; ++i) {
           const long c = C(k, j, i), a = Q(j, i);
-          if (k == 0) dt_diff[n * F + c] = (vtl[c] - ori[c]) / dts * vit[c] - stf[a] * 0.5 * odzp[0];
-          else dt_diff[n * F + c] = (vtl[c] - ori[c]) / dts * vit[c];
-          tend[n * F + c] = (vtl[c] - at[n * F + c]) / dts * vit[c];
+          if (dg) {
+            if (k == 0) dt_diff[n * F + c] = (vtl[c] - ori[c]) / dts * vit[c] - stf[a] * 0.5 * odzp[0];
+            else dt_diff[n * F + c] = (vtl[c] - ori[c]) / dts * vit[c];
+            tend[n * F + c] = (vtl[c] - at[n * F + c]) / dts * vit[c];
+          }
           at[n * F + c] = vtl[c];
           atbn[c + A] = at[n * F + c];
         }
@@ -643,6 +681,7 @@ void tracer_call(Oracle& o) {
 
 // convadj_cu: per-column convective adjustment (convadj.cpp:29-288)
 void convadj_call(Oracle& o) {
+  o.ensure_all();
   const int km = o.km, imt = o.imt, jmt = o.jmt;
   const long A = o.A, F = o.F, FB = o.FB;
   double* at = o.fd[LT_F_AT].data();
@@ -754,6 +793,7 @@ void convadj_call(Oracle& o) {
 // icesnow_cu over every point of the domain, halo included, with the
 // FRC_CORE reset of licomqice first when reset is set (icesnow.cpp:15-85)
 void icesnow_call(Oracle& o, const lt_icesnow_params& p) {
+  o.ensure_all();
   double* at = o.fd[LT_F_AT].data();
   double* qice = o.fd[LT_F_QICE].data();
   const int* kmt = o.fi[LT_F_KMT].data();
@@ -1093,6 +1133,7 @@ void turb_device(const double* z, const double* t, const double* rh, const doubl
 // (readyc.cpp:1642, 1647, 1668-1671): every column of the interior ring
 // (1 .. imt-2, 1 .. jmt-2) that has a wet top level
 void turb_call(Oracle& o, const lt_turb_tables& T, int ncc, double dfricmx) {
+  o.ensure_all();
   const int km = o.km, imt = o.imt, jmt = o.jmt;
   const long A = o.A, F = o.F;
   double* akmt = o.fd[LT_F_AKMT].data();
@@ -1168,6 +1209,7 @@ void turb_call(Oracle& o, const lt_turb_tables& T, int ncc, double dfricmx) {
 // readyc_'s BIHAR sequence (readyc.cpp:1754-1775) kernel by kernel over the
 // whole domain, one block (ib = jb = 3, ie = imt-2, je = jmt-2)
 void del4u_call(Oracle& o, double am, double c0f) {
+  o.ensure_all();
   const int km = o.km, imt = o.imt, jmt = o.jmt;
   const long A = o.A, F = o.F;
   const int ib = 3, jb = 3, ie = imt - 2, je = jmt - 2;
@@ -1280,6 +1322,41 @@ void del4u_call(Oracle& o, double am, double c0f) {
 }
 }  // namespace
 
+namespace {
+void copy_par(std::vector<double>& dst, const std::vector<double>& src) {
+  dst.resize(src.size());
+  const long n = (long)src.size();
+  double* d = dst.data();
+  const double* q = src.data();
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < n; ++c) d[c] = q[c];
+}
+// nsteps steps with frozen dynamics; *t_tracer (if given) receives the
+// seconds spent inside the tracer_ calls alone, without the copies that
+// restore the dynamics between them.
+int step_frozen(Oracle& o, int nsteps, double* t_tracer) {
+  const int dyn[5] = {LT_F_UTF, LT_F_VTF, LT_F_UTL, LT_F_VTL, LT_F_H0F};
+  for (int m = 0; m < 5; ++m) copy_par(o.dyn0[m], o.fd[dyn[m]]);
+  double t = 0.0;
+  for (int s = 0; s < nsteps; ++s) {
+    for (int m = 0; m < 5; ++m) copy_par(o.fd[dyn[m]], o.dyn0[m]);
+#ifdef _OPENMP
+    const double t0 = omp_get_wtime();
+    tracer_call(o);
+    t += omp_get_wtime() - t0;
+#else
+    tracer_call(o);
+#endif
+  }
+  copy_par(o.fd[LT_F_UTF_OUT], o.fd[LT_F_UTF]);
+  copy_par(o.fd[LT_F_VTF_OUT], o.fd[LT_F_VTF]);
+  copy_par(o.fd[LT_F_H0F_OUT], o.fd[LT_F_H0F]);
+  for (int m : {0, 1, 3, 4}) copy_par(o.fd[dyn[m]], o.dyn0[m]);
+  if (t_tracer) *t_tracer = t;
+  return 0;
+}
+}  // namespace
+
 extern "C" {
 
 void* or_create(int nx, int ny, int km) {
@@ -1299,6 +1376,7 @@ long or_field_count(void* h, int f) {
 int or_set_field(void* h, int f, const void* src, size_t nbytes) {
   Oracle& o = *static_cast<Oracle*>(h);
   if (f < 0 || f >= LT_F_COUNT) return LT_E_INVALID;
+  o.ensure(f);
   const bool isint = field_info(f).is_int;
   const size_t need = (size_t)o.count(f) * (isint ? sizeof(int) : sizeof(double));
   if (nbytes != need) return LT_E_INVALID;
@@ -1309,6 +1387,7 @@ int or_set_field(void* h, int f, const void* src, size_t nbytes) {
 int or_get_field(void* h, int f, void* dst, size_t nbytes) {
   Oracle& o = *static_cast<Oracle*>(h);
   if (f < 0 || f >= LT_F_COUNT) return LT_E_INVALID;
+  o.ensure(f);
   const bool isint = field_info(f).is_int;
   const size_t need = (size_t)o.count(f) * (isint ? sizeof(int) : sizeof(double));
   if (nbytes != need) return LT_E_INVALID;
@@ -1326,20 +1405,30 @@ int or_tracer_call(void* h) {
 // are restored from the given copies (the model's bclinc/barotr would supply
 // fresh ones), then one tracer_ call runs; afterwards UTF/VTF/H0F hold the
 // scaled values of the last step, copied to the *_OUT fields.
+
+// nsteps steps with frozen dynamics: before each step utf, vtf, utl, vtl, h0f
+// are restored from copies taken at entry (the model's bclinc/barotr would
+// supply fresh ones), then one tracer_ call runs; afterwards UTF/VTF/H0F hold
+// the scaled values of the last step, copied to the *_OUT fields.
 int or_step(void* h, int nsteps) {
-  Oracle& o = *static_cast<Oracle*>(h);
-  const std::vector<double> utf0 = o.fd[LT_F_UTF], vtf0 = o.fd[LT_F_VTF], utl0 = o.fd[LT_F_UTL],
-                            vtl0 = o.fd[LT_F_VTL], h0f0 = o.fd[LT_F_H0F];
-  for (int s = 0; s < nsteps; ++s) {
-    o.fd[LT_F_UTF] = utf0; o.fd[LT_F_VTF] = vtf0; o.fd[LT_F_UTL] = utl0; o.fd[LT_F_VTL] = vtl0;
-    o.fd[LT_F_H0F] = h0f0;
-    tracer_call(o);
-  }
-  o.fd[LT_F_UTF_OUT] = o.fd[LT_F_UTF];
-  o.fd[LT_F_VTF_OUT] = o.fd[LT_F_VTF];
-  o.fd[LT_F_H0F_OUT] = o.fd[LT_F_H0F];
-  o.fd[LT_F_UTF] = utf0; o.fd[LT_F_VTF] = vtf0; o.fd[LT_F_VTL] = vtl0; o.fd[LT_F_H0F] = h0f0;
+  return step_frozen(*static_cast<Oracle*>(h), nsteps, nullptr);
+}
+// or_step that also reports the seconds spent in the tracer_ calls.
+int or_step_timed(void* h, int nsteps, double* t_tracer) {
+  return step_frozen(*static_cast<Oracle*>(h), nsteps, t_tracer);
+}
+// 1: write the diagnostics ax, ay, az, dz, penetrate, tend, dt_diff (the
+// reference always does); 0: skip them (the state is the same).
+int or_set_diagnostics(void* h, int on) {
+  static_cast<Oracle*>(h)->set_diagnostics(on != 0);
   return 0;
+}
+// Address of a field's storage (allocated on first use), for filling it in place.
+void* or_field_ptr(void* h, int f) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  if (f < 0 || f >= LT_F_COUNT) return nullptr;
+  o.ensure(f);
+  return field_info(f).is_int ? (void*)o.fi[f].data() : (void*)o.fd[f].data();
 }
 int or_convadj(void* h) {
   convadj_call(*static_cast<Oracle*>(h));

@@ -1,6 +1,9 @@
 """ctypes binding of the CPU checker libraries.  TEST INFRASTRUCTURE ONLY.
 
 ``Oracle`` wraps liblicom_oracle.so (the FP64 restatement in licom_oracle.cpp);
+``HostSynth`` wraps liblicom_synth_host.so, the seeded input generator built
+for the host alone (the CPU baseline uses it so that it never loads the CUDA
+library);
 ``Reference`` wraps oracle/_ref/libref_tracer.so, the reference's own
 tracer.cpp, convadj.cpp and icesnow.cpp compiled for the CPU (present only
 where the reference tree was available at build time).  Field ids are those
@@ -15,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liblicom_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_tracer.so")
 REF_READYC_LIB = os.path.join(HERE, "_ref", "libref_readyc.so")
+SYNTH_HOST_LIB = os.path.join(HERE, "liblicom_synth_host.so")
 
 FIELDS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "NET", "UTF_OUT", "VTF_OUT",
           "H0F_OUT", "SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE",
@@ -56,8 +60,73 @@ def _dtype(name):
     return np.int32 if name in INT else np.float64
 
 
+class Params(C.Structure):
+    """lt_params (include/licom_tracer.h)."""
+    _fields_ = [(n, C.c_double) for n in ("dts", "oncc", "onbc", "dwndmix", "gamma", "od0", "od0cp", "ah", "area_t")] + [
+        ("nss", C.c_int), ("boundary_restore", C.c_int)]
+
+
+class SynthConfig(C.Structure):
+    """lt_synth_config (include/licom_synth.h)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("km", C.c_int), ("lat_s", C.c_double), ("lat_n", C.c_double),
+                ("dz_top", C.c_double), ("dz_bot", C.c_double), ("depth", C.c_double), ("umax", C.c_double),
+                ("seed", C.c_uint64), ("forced", C.c_int), ("cap_north", C.c_int), ("cap_south", C.c_int),
+                ("ew_cyclic", C.c_int), ("tripole", C.c_int), ("land_frac", C.c_double), ("member", C.c_uint32),
+                ("tpert", C.c_double), ("ah_bihar", C.c_double)]
+
+
+class HostSynth:
+    """The seeded synthetic domain of the benchmark configurations, generated
+    on the host (OpenMP) without the CUDA library."""
+
+    def __init__(self, nx, ny, km, **kw):
+        self.lib = lib = C.CDLL(SYNTH_HOST_LIB)
+        lib.lt_synth_defaults.argtypes = [C.c_void_p]
+        lib.lt_synth_build.argtypes = [C.c_void_p, C.c_void_p]
+        lib.lt_synth_free.argtypes = [C.c_void_p]
+        lib.lt_synth_params.argtypes = [C.c_void_p, C.c_void_p]
+        lib.lt_synth_field_rows.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]
+        cfg = SynthConfig()
+        lib.lt_synth_defaults(C.byref(cfg))
+        cfg.nx, cfg.ny, cfg.km = nx, ny, km
+        for k, v in kw.items():
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        self.h = C.c_void_p()
+        if lib.lt_synth_build(C.byref(cfg), C.byref(self.h)):
+            raise ValueError("lt_synth_build")
+        self.params = Params()
+        lib.lt_synth_params(self.h, C.byref(self.params))
+        self.nx, self.ny, self.km = nx, ny, km
+
+    def __del__(self):
+        try:
+            self.lib.lt_synth_free(self.h)
+        except Exception:
+            pass
+
+    def fill(self, oracle, rows=None):
+        """Write every input field of the oracle in place: the whole domain,
+        or (rows) its northern band of that many rows, halo included, for an
+        oracle of ny = rows - 4."""
+        rows = rows or self.ny + 4
+        assert oracle.nx == self.nx and oracle.km == self.km and oracle.ny + 4 == rows
+        for name in INPUTS:
+            n = int(np.prod(shape_of(name, oracle.nx, oracle.ny, oracle.km)))
+            nbytes = n * (4 if name in INT else 8)
+            if self.lib.lt_synth_field_rows(self.h, FID[name], rows, oracle.field_ptr(name), nbytes):
+                raise ValueError("lt_synth_field_rows " + name)
+
+
+# inputs of the tracer step (the generator leaves the others zero)
+INPUTS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "SWV", "NSWV", "SST", "SSS", "FRESH",
+          "SEAICE", "TAREA", "TAREA_R", "HTW", "HTS", "HUN", "HUE", "DXU", "DYU", "AHF", "DTN", "DTS", "DTE", "DTW",
+          "OHBT", "OHBU", "AU0", "AUS", "AUW", "AUSW", "KMT", "KMU", "KMTN", "KMTS", "KMTE", "KMTW", "DZP", "ODZP",
+          "ODZT", "PEN", "TO", "SO", "C"]
+
+
 class Oracle:
-    def __init__(self, nx, ny, km, params, ew_cyclic=1, tripole=1, threads=0):
+    def __init__(self, nx, ny, km, params, ew_cyclic=1, tripole=1, threads=0, diagnostics=1):
         self.lib = lib = C.CDLL(ORACLE_LIB)
         lib.or_create.restype = C.c_void_p
         lib.or_create.argtypes = [C.c_int] * 3
@@ -76,6 +145,10 @@ class Oracle:
         lib.or_icesnow.argtypes = [C.c_void_p, C.c_void_p]
         lib.or_turb.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
         lib.or_hdiffu_del4.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        lib.or_step_timed.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        lib.or_set_diagnostics.argtypes = [C.c_void_p, C.c_int]
+        lib.or_field_ptr.argtypes = [C.c_void_p, C.c_int]
+        lib.or_field_ptr.restype = C.c_void_p
         self.nx, self.ny, self.km = nx, ny, km
         self.h = C.c_void_p(lib.or_create(nx, ny, km))
         if not self.h:
@@ -84,6 +157,8 @@ class Oracle:
         lib.or_set_params(self.h, C.byref(params), int(ew_cyclic), int(tripole))
         if threads:
             lib.or_set_threads(threads)
+        if not diagnostics:
+            lib.or_set_diagnostics(self.h, 0)
 
     def __del__(self):
         try:
@@ -112,6 +187,15 @@ class Oracle:
 
     def tracer_call(self):
         self.lib.or_tracer_call(self.h)
+
+    def step_timed(self, nsteps=1):
+        """step(); returns the seconds spent inside the tracer_ calls."""
+        t = C.c_double()
+        self.lib.or_step_timed(self.h, nsteps, C.byref(t))
+        return t.value
+
+    def field_ptr(self, name):
+        return self.lib.or_field_ptr(self.h, FID[name])
 
     def convadj(self):
         self.lib.or_convadj(self.h)
