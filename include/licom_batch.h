@@ -7,7 +7,7 @@
  * all of one precision.  One batch step advances every member by one tracer
  * step: the per-member surface, SSS-norm and halo kernels, and, in mixed
  * precision, ONE continuity launch and ONE persistent column launch over the
- * concatenated (member, tile, tracer) work list.  The steps are captured in a
+ * concatenated (member, tile) work list.  The steps are captured in a
  * CUDA graph (one per ping-pong parity) and replayed.
  *
  * Each member's state stays in its own arena; after a batch step the domain

@@ -227,7 +227,7 @@ void init_arena_dims(Arena& a, const lt_grid* g, const lt_params* p) {
   a.ew_cyclic = g->ew_cyclic; a.tripole = g->tripole;
   a.diagnostics = g->diagnostics; a.precision = g->precision;
   if (p) a.p = *p;
-  a.nv_scratch = a.diagnostics ? 3 : 2;
+  a.nv_scratch = a.precision == LT_PREC_MIXED ? kMixedScratchPerLevel : (a.diagnostics ? 3 : 2);
   a.wait_limit = 1u << 24;
 }
 
@@ -235,7 +235,9 @@ long slots_for(const Arena& a, int sms) {
   const int ty = a.precision == LT_PREC_MIXED ? kMixedTileY : TY;
   const long ntiles = (long)((a.imt + TX - 1) / TX) * ((a.jmt + ty - 1) / ty);
   long s = (long)sms * (a.precision == LT_PREC_MIXED ? kMixedCtasPerSm : kFp64CtasPerSm);
-  if (s > 2 * ntiles) s = 2 * ntiles;
+  // work items: (tile, tracer) pairs in FP64, tiles (both tracers) in mixed
+  const long items = a.precision == LT_PREC_MIXED ? ntiles : 2 * ntiles;
+  if (s > items) s = items;
   return s;
 }
 
@@ -267,9 +269,10 @@ bool build_tracer_maps(const Arena& a, TracerMaps* m) {
   const bool mx = a.precision == LT_PREC_MIXED;
   const int ty = mx ? kMixedTileY : TY;   // tile rows of the column kernel
   bool ok = true;
+  const int bw64 = mx ? kMixedBoxW64 : SW;   // state box width
   for (int b = 0; b < 2; ++b) {
-    ok = ok && make_tensor_map_3d(&m->at[b], a.at[b], 8, imt, jmt, 2 * km, SW, ty + 4);
-    ok = ok && make_tensor_map_3d(&m->atb[b], a.atb[b], 8, imt, jmt, 2 * (km + 1), SW, ty + 4);
+    ok = ok && make_tensor_map_3d(&m->at[b], a.at[b], 8, imt, jmt, 2 * km, bw64, ty + 4);
+    ok = ok && make_tensor_map_3d(&m->atb[b], a.atb[b], 8, imt, jmt, 2 * (km + 1), bw64, ty + 4);
   }
   const int es = mx ? 4 : 8;
   ok = ok && make_tensor_map_3d(&m->ws, mx ? (const void*)a.ws32 : a.ws, es, imt, jmt, km + 1, SW, ty + 2);

@@ -5,7 +5,7 @@
 // norm, net halo, continuity, column march, state halo), each small kernel
 // one launch over every member, and the two heavy kernels batched in mixed
 // precision: one continuity launch over every member's tiles and one
-// persistent column launch over the concatenated (member, tile, tracer) work
+// persistent column launch over the concatenated (member, tile) work
 // list.  A kernel's parameters are frozen when a
 // graph is captured, and each step reads the ping-pong state buffer `cur` and
 // writes the other, so two graphs are kept: parity 0 (every member at the
@@ -88,7 +88,7 @@ int build_descriptors(lt_batch* b) {
       e.ntiles = ntiles;
       e.ntx = ntx;
     }
-    item += 2 * ntiles;
+    item += ntiles;   // one work item per tile (both tracers)
     b->km_max = std::max(b->km_max, a.km);
     b->max_imt = std::max(b->max_imt, a.imt);
     b->max_jmt = std::max(b->max_jmt, a.jmt);
@@ -239,7 +239,8 @@ int lt_batch_create(lt_domain* const* members, int n, lt_batch** out) {
     return fail(LT_E_CUDA);
   if ((rc = build_descriptors(b))) return fail(rc);
   if (b->mixed) {
-    const size_t bytes = sizeof(double) * (size_t)b->sms * kMixedCtasPerSm * b->km_max * 2 * kMixedThreads;
+    const size_t bytes =
+        sizeof(double) * (size_t)b->sms * kMixedCtasPerSm * b->km_max * kMixedScratchPerLevel * kMixedThreads;
     if (cudaMalloc(&b->scratch, bytes) != cudaSuccess) {
       set_error("lt_batch_create: cudaMalloc(%zu) for the column scratch failed", bytes);
       return fail(LT_E_OOM);
@@ -338,7 +339,7 @@ int lt_batch_autotune(lt_batch* b, int trial_steps, lt_batch_config* chosen) {
   }
   std::vector<lt_batch_config> cands;
   if (b->mixed) {
-    for (int ctas : {1, 2, 3})
+    for (int ctas = 1; ctas <= kMixedCtasPerSm; ++ctas)
       for (int ty : {4, 8, 16}) cands.push_back({ctas, ty, 1});
   } else {
     cands.push_back({b->cfg.column_ctas_per_sm, b->cfg.continuity_tile_y, 1});

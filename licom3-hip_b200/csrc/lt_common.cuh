@@ -15,12 +15,18 @@ constexpr int TY = 8;
 constexpr int TTHREADS = TX * TY;
 // Persistent CTAs per SM of the column kernels (their shared-memory footprint
 // decides): FP64 2 of 256 threads (its tile's metric and biharmonic
-// coefficients staged in shared memory, no register spills), mixed 3 of 256.
+// coefficients staged in shared memory, no register spills), mixed 2 of 256
+// (both tracers' level boxes per CTA).
 constexpr int kFp64CtasPerSm = 2;
-constexpr int kMixedCtasPerSm = 3;
-// The mixed column kernel's tile: TX x kMixedTileY columns, one thread each.
+constexpr int kMixedCtasPerSm = 2;
+// The mixed column kernel's tile: TX x kMixedTileY columns, one thread each
+// (both tracers); its f64 state boxes are kMixedBoxW64 columns wide
+// (x0-2 .. x0+TX+1) and its Thomas sweep keeps four values per level and
+// column (e, f of T and S).
 constexpr int kMixedTileY = 8;
 constexpr int kMixedThreads = TX * kMixedTileY;
+constexpr int kMixedBoxW64 = TX + 4;
+constexpr int kMixedScratchPerLevel = 4;
 
 // Everything the step kernels touch, as raw device pointers (dense
 // [n][k][j][i] layout of the reference, i fastest).

@@ -241,178 +241,209 @@ int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s) {
   return LT_OK;
 }
 
+
 namespace {
 
 // ------------------------------------------------------------ column march
-// Tile of the mixed march: TX x MY columns, one thread per column.  Taller
-// than the FP64 kernel's 32 x 4 tile: the 1-cell halo the predictor, the first
-// Laplacian and the faces are computed on grows less than the tile.
+// Tile of the mixed march: TX x MY columns, one thread per column, and both
+// tracers in every thread.  T and S move through the same faces with the
+// same transports, masks and metric terms, so those are formed and read once
+// for the two; the f32 arithmetic of the predictor runs on (T, S) pairs with
+// the packed sm_100 instructions (fma/add/mul .f32x2).  The column phase, the
+// first and second Laplacians and the sweep compute in f64: on this part the
+// f64 pipe is cheaper than rounding every f64 state difference to f32 and
+// every f32 term back (conversions issue at a quarter of the f64 rate), and
+// the f32 inputs (U-point means, w, the mixing coefficient) are converted
+// once where they enter.
 constexpr int MY = kMixedTileY;
 constexpr int MTH = kMixedThreads;
 constexpr int MHQY = MY + 2;          // tile plus 1-cell halo, rows
 constexpr int MHN = HQX * MHQY;
-// Level slots.  Step k (the march runs downward) reads levels k-2, k-1 and
-// k only, so at the end of step k the slot of level k takes level k-3: three
+// Level slots.  Step k (the march runs upward) reads levels k-2, k-1 and k
+// only, so at the end of step k the slot of level k takes level k-3: three
 // slots keep one step of lead time for every box.
 constexpr int NSM = 3;
+// f64 boxes (state): columns x0-2 .. x0+TX+1, so that the x start stays a
+// multiple of two elements (16 bytes); f32 boxes: columns x0-4 .. x0+TX+3 (SW)
+constexpr int SW64 = kMixedBoxW64;
 constexpr int FXN = (MY + 2) * (TX + 3);   // x faces of the 1-halo region
 constexpr int FYN = (MY + 3) * (TX + 2);   // y faces of the 1-halo region
+constexpr int FN = FXN + FYN;
+constexpr int OXN = MY * (TX + 1);         // x faces of the tile (west sides of columns x0 .. x0+TX)
+constexpr int OYN = (MY + 1) * TX;         // y faces of the tile (north sides of rows y0 .. y0+MY)
 
-// One level of the column tile, filled by five TMA boxes (the mixing
-// coefficient of the own column comes by plain loads, a step ahead).  The f32 fields
-// are w and the U-point means wkd, wkb from which the kernel forms the face
-// transports (face32, face_x64, face_y64).
+// One level of the column tile, filled by seven TMA boxes: T and S of the
+// state and of its previous time level, w and the U-point means wkd, wkb
+// from which the kernel forms the face transports (face32, face_x64,
+// face_y64).
 struct alignas(128) MxSlot {
-  alignas(128) double at[(MY + 4) * SW];   // rows y0-2 .. y0+MY+1
-  alignas(128) double atb[(MY + 4) * SW];  // tracer level L of the previous time level
-  alignas(128) float ws[(MY + 2) * SW];    // rows y0-1 .. y0+MY
-  alignas(128) float wkd[(MY + 3) * SW];   // rows y0-2 .. y0+MY
-  alignas(128) float wkb[(MY + 3) * SW];   // rows y0-2 .. y0+MY
+  alignas(128) double at[2][(MY + 4) * SW64];    // rows y0-2 .. y0+MY+1
+  alignas(128) double atb[2][(MY + 4) * SW64];   // tracer level L of the previous time level
+  alignas(128) float ws[(MY + 2) * SW];          // rows y0-1 .. y0+MY
+  alignas(128) float wkd[(MY + 3) * SW];         // rows y0-2 .. y0+MY
+  alignas(128) float wkb[(MY + 3) * SW];         // rows y0-2 .. y0+MY
 };
+static_assert(((MY + 4) * SW64 * sizeof(double)) % 128 == 0, "each tracer's box starts 128-byte aligned");
 constexpr uint32_t kMxLevelBytes =
-    (uint32_t)(2 * (MY + 4) * SW * sizeof(double) + ((MY + 2) * SW + 2 * (MY + 3) * SW) * sizeof(float));
+    (uint32_t)(4 * (MY + 4) * SW64 * sizeof(double) + ((MY + 2) * SW + 2 * (MY + 3) * SW) * sizeof(float));
+
+// per-level constants of the march (the 1-D vertical grid)
+struct MxLevel {
+  double odzp, odzt;   // odzp(k), odzt(k)
+  double ka, kc;       // odzt(k)*odzp(k)*dts/2, odzt(k+1)*odzp(k)*dts/2 (0 at the bottom)
+  double pu, pd;       // pen(k-1) (0 at the top), pen(k) (0 at the bottom)
+  float hodz, odzt1;   // f32 forms for the predictor: odzp(k)/2, odzt(k+1) (0 at the bottom)
+};
 
 struct MxSmem {
   MxSlot slot[NSM];
-  float fxd[2][FXN];                  // per level parity: face difference d
-  float fyd[2][FYN];
-  unsigned char flag[3][MHN];          // predictor outside its local bounds
-  float d2[MHN];                       // first Laplacian (times ahf)
+  float2 fd[FN];                       // predictor's level: face difference (T, S), 0 where a side is land
+  float fu[FN], fq[FN];                // predictor's level: f32 transport u and Lax-Wendroff factor u*u*cf
+  double ou[OXN + OYN], oq[OXN + OYN]; // column phase's level: the tile's f64 transports and u*u*cf
+  double d2[2][MHN];                   // column phase's level: first Laplacian times ahf (T, S)
+  unsigned char flag[NSM][MHN];        // bit n: tracer n's predictor leaves its local bounds
   float tr[MHN], dtn[MHN], dts[MHN], dte[MHN], dtw[MHN], ahf[MHN];
-  float kx[MHN], ky[MHN];               // del4 face weights tarea*dte (east face), tarea*dts (south face)
-  float cxf[FXN], cyf[FYN];           // 2*dts/(htw*hun), 2*dts/(hts*hue) at the faces
-  float fxu[2][FXN], fyv[2][FYN];    // per level parity: f32 face transports uw, vs
-  float hwx[FXN], hsy[FYN];           // htw, hts at the faces (f32)
-  uint16_t kmt[(MY + 4) * SW];        // bottom level of the tile's columns and their 2-cell halo
+  float cf[FN];                        // 2*dts/(htw*hun) at x faces, 2*dts/(hts*hue) at y faces
+  float hw[FN];                        // htw at x faces, hts at y faces
+  uint16_t kmt[(MY + 4) * SW64];       // bottom level of the tile's columns and their 2-cell halo
   uint64_t bar[NSM];
 };
-// four CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
-// kMixedCtasPerSm CTAs per SM: 228 KB of shared memory, 1 KB of it reserved per CTA
-static_assert(kMixedCtasPerSm * (sizeof(MxSmem) + 1024) <= 228 * 1024,
+// followed by the km level constants (dynamic shared memory)
+constexpr size_t kMxLevOff = (sizeof(MxSmem) + 15) / 16 * 16;
+__host__ __device__ constexpr size_t mx_smem_bytes(int km) { return kMxLevOff + (size_t)km * sizeof(MxLevel); }
+// kMixedCtasPerSm CTAs per SM: 228 KB of shared memory, 1 KB of it reserved
+// per CTA; the largest km the grid check allows must still fit
+static_assert(kMixedCtasPerSm * (mx_smem_bytes(256) + sizeof(Arena) + 16 + 1024) <= 228 * 1024,
               "mixed tracer tile no longer fits kMixedCtasPerSm CTAs per SM");
 
-// Issue the boxes of level L of tracer n into a slot (one thread).
-__device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const TracerMaps& m, int cur, int n, int km,
-                                         int L, int x0, int y0) {
+// x face (fj, fi): row y0-1+fj, west side of column x0-1+fi
+// y face (fj, fi): south side of row y0-2+fj, column x0-1+fi (index FXN + ...)
+__device__ __forceinline__ int fx(int fj, int fi) { return fj * (TX + 3) + fi; }
+__device__ __forceinline__ int fy(int fj, int fi) { return FXN + fj * (TX + 2) + fi; }
+// region cell (hj, hi) = row y0-1+hj, column x0-1+hi in the boxes
+__device__ __forceinline__ int b64(int hj, int hi) { return (hj + 1) * SW64 + hi + 1; }   // at, atb, kmt
+__device__ __forceinline__ int bws(int hj, int hi) { return hj * SW + hi + 3; }           // ws (rows from y0-1)
+__device__ __forceinline__ int b32(int hj, int hi) { return (hj + 1) * SW + hi + 3; }     // wkd, wkb (rows from y0-2)
+
+// Issue the boxes of level L of both tracers into a slot (one thread).
+__device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const TracerMaps& m, int cur, int km, int L,
+                                         int x0, int y0) {
   mbar_expect_tx(bar, kMxLevelBytes);
-  tma_load_3d(sl.at, &m.at[cur], x0 - 4, y0 - 2, n * km + L, bar);
-  tma_load_3d(sl.atb, &m.atb[cur], x0 - 4, y0 - 2, n * (km + 1) + L + 1, bar);
+  tma_load_3d(sl.at[0], &m.at[cur], x0 - 2, y0 - 2, L, bar);
+  tma_load_3d(sl.at[1], &m.at[cur], x0 - 2, y0 - 2, km + L, bar);
+  tma_load_3d(sl.atb[0], &m.atb[cur], x0 - 2, y0 - 2, L + 1, bar);
+  tma_load_3d(sl.atb[1], &m.atb[cur], x0 - 2, y0 - 2, (km + 1) + L + 1, bar);
   tma_load_3d(sl.ws, &m.ws, x0 - 4, y0 - 1, L, bar);
   tma_load_3d(sl.wkd, &m.uw, x0 - 4, y0 - 2, L, bar);
   tma_load_3d(sl.wkb, &m.vs, x0 - 4, y0 - 2, L, bar);
 }
 
-
-// x face (fj, fi): row y0-1+fj, west side of column x0-1+fi
-// y face (fj, fi): south side of row y0-2+fj, column x0-1+fi
-__device__ __forceinline__ int fx(int fj, int fi) { return fj * (TX + 3) + fi; }
-__device__ __forceinline__ int fy(int fj, int fi) { return fj * (TX + 2) + fi; }
-
-// Face quantities of level kk for the 1-halo region, once per face: the f32
-// transport (face32 on the U-point means) and the difference d.  Every later
-// use reads these, so both cells of a face see the same f32 values.
-//
-// A face is described by (kind, index in its array, box index r): an x face
-// by its east cell R = r, a y face by its north cell r.  Each thread forms the
-// west x face and the north y face of its own cell, and up to two of the 192
-// faces on the region's border (FaceSet).
-__device__ __forceinline__ void face_one(MxSmem& S, const MxSlot& L, int kk, bool is_x, int m, int r) {
-  if (is_x) {
-    S.fxd[kk & 1][m] = (float)(L.at[r] - L.at[r - 1]);
-    S.fxu[kk & 1][m] = face32(L.wkd[r - SW], L.wkd[r], S.hwx[m]);
-  } else {
-    S.fyd[kk & 1][m] = (float)(L.at[r + SW] - L.at[r]);
-    S.fyv[kk & 1][m] = face32(L.wkb[r], L.wkb[r + 1], S.hsy[m]);
-  }
-}
-
-constexpr int FX_OWN = TX * MY, FX_EXTRA = FXN - FX_OWN, FY_EXTRA = FYN - TX * MY;
-constexpr int F_EXTRA = FX_EXTRA + FY_EXTRA;   // border faces of the region
-
-struct FaceSet {
-  int own_x, own_y, own_r;   // own cell's west x face, north y face, box index of the cell
-  uint32_t e[2];             // border faces: bit 31 = y face, bits 16..30 index, bits 0..15 box index
-  int ne;
+// ---- f32 faces of the 1-halo region (the predictor's level)
+// A face is described by (kind, index, box index of its east / north cell
+// in the f64 boxes, index of its first U point in the f32 boxes).
+struct FaceRef {
+  int f, r, w;
+  bool x;
 };
 
-__device__ __forceinline__ uint32_t face_desc(bool is_y, int m, int r) {
-  return (is_y ? 0x80000000u : 0u) | ((uint32_t)m << 16) | (uint32_t)r;
+__device__ __forceinline__ FaceRef face_x_ref(int fj, int fi) {
+  // west side of cell (fj, fi): cells (fj, fi-1) | (fj, fi); U points (fj-1, fi), (fj, fi) of rows y0-2+..
+  return {fx(fj, fi), b64(fj, fi), b32(fj - 1, fi), true};
+}
+__device__ __forceinline__ FaceRef face_y_ref(int fj, int fi) {
+  // south side of region row fj-1: cells (fj-1, fi) (north) | (fj, fi) (south); U points (fj-1, fi), (fj-1, fi+1)
+  return {fy(fj, fi), b64(fj - 1, fi), b32(fj - 1, fi), false};
 }
 
-// border face q (0 .. F_EXTRA-1): x faces of the top and bottom rows, x faces
-// of the west column and the two east columns, y faces of rows 0, MY+1, MY+2,
-// y faces of the west and east columns
-__device__ __forceinline__ uint32_t border_face(int q) {
-  int fj, fi;
-  if (q < 2 * (TX + 3)) {
-    fj = q < TX + 3 ? 0 : MY + 1;
-    fi = q % (TX + 3);
-    return face_desc(false, fx(fj, fi), (fj + 1) * SW + fi + 3);
+// Difference a(east) - a(west) for x faces and a(south) - a(north) for y
+// faces (the face's cell of higher index minus the other, j running south)
+// masked to 0 where either cell is land at level kk: the transport through
+// such a face is 0, and a 0 difference stands for the excluded neighbour in
+// the masked extrema.
+__device__ __forceinline__ void face_f32(MxSmem& S, const MxSlot& L, int kk, const FaceRef& q) {
+  int r1, r2;    // the two cells: r1 the one whose value is subtracted
+  float u;
+  if (q.x) {
+    r1 = q.r - 1; r2 = q.r;
+    u = face32(L.wkd[q.w], L.wkd[q.w + SW], S.hw[q.f]);
+  } else {
+    r1 = q.r; r2 = q.r + SW64;
+    u = face32(L.wkb[q.w], L.wkb[q.w + 1], S.hw[q.f]);
   }
+  const bool wet = kk < S.kmt[r1] && kk < S.kmt[r2];
+  float2 d;
+  d.x = wet ? (float)(L.at[0][r2] - L.at[0][r1]) : 0.f;
+  d.y = wet ? (float)(L.at[1][r2] - L.at[1][r1]) : 0.f;
+  S.fd[q.f] = d;
+  S.fu[q.f] = u;
+  S.fq[q.f] = u * u * S.cf[q.f];
+}
+
+// border faces of the region beyond each thread's own west x face and north
+// y face (the faces of cell (ty+1, tx+1)): x faces of region rows 0 and MY+1
+// (all TX+3 columns), x faces of rows 1..MY at columns 0, TX+1, TX+2, y faces
+// of rows 0, MY+1, MY+2 (all TX+2 columns), y faces of rows 1..MY at columns
+// 0 and TX+1
+constexpr int F_EXTRA = FN - 2 * TX * MY;
+static_assert(F_EXTRA <= MTH, "border faces: at most one per thread");
+
+__device__ __forceinline__ FaceRef border_face(int q) {
+  if (q < 2 * (TX + 3)) return face_x_ref(q < TX + 3 ? 0 : MY + 1, q % (TX + 3));
   q -= 2 * (TX + 3);
   if (q < 3 * MY) {
     const int c = q % 3;
-    fj = 1 + q / 3;
-    fi = c == 0 ? 0 : TX + c;
-    return face_desc(false, fx(fj, fi), (fj + 1) * SW + fi + 3);
+    return face_x_ref(1 + q / 3, c == 0 ? 0 : TX + c);
   }
   q -= 3 * MY;
   if (q < 3 * (TX + 2)) {
     const int row = q / (TX + 2);
-    fj = row == 0 ? 0 : MY + row;
-    fi = q % (TX + 2);
-    return face_desc(true, fy(fj, fi), fj * SW + fi + 3);
+    return face_y_ref(row == 0 ? 0 : MY + row, q % (TX + 2));
   }
   q -= 3 * (TX + 2);
-  fj = 1 + q / 2;
-  fi = (q % 2) ? TX + 1 : 0;
-  return face_desc(true, fy(fj, fi), fj * SW + fi + 3);
+  return face_y_ref(1 + q / 2, (q % 2) ? TX + 1 : 0);
 }
 
-__device__ __forceinline__ FaceSet face_set(int tid) {
-  const int tx = tid % TX, ty = tid / TX;
-  FaceSet f;
-  f.own_x = fx(ty + 1, tx + 1);
-  f.own_y = fy(ty + 1, tx + 1);
-  f.own_r = (ty + 2) * SW + tx + 4;
-  f.ne = 0;
-  for (int q = tid; q < F_EXTRA && f.ne < 2; q += MTH) f.e[f.ne++] = border_face(q);
-  if (f.ne < 2) f.e[1] = 0;
-  if (f.ne < 1) f.e[0] = 0;
-  return f;
-}
+// ---- f64 faces of the tile (the column phase's level), as the continuity
+// march formed them: uw(j,i) = (wkd(j-1,i) + wkd(j,i)) * htw(j,i) / 4,
+// vs(j,i) = (wkb(j,i) + wkb(j,i+1)) * hts(j,i) / 4 (face_x64, face_y64)
+struct OwnFace {
+  int o;       // index in ou/oq
+  int w;       // first U point in the f32 boxes
+  int f;       // the same face in the region arrays (for cf)
+  bool x;
+  double h;    // htw or hts of the face
+};
 
-// sk: the slot of level kk (kk % NSM, carried through the level loop)
-__device__ __forceinline__ void faces_level(MxSmem& S, int kk, int sk, const FaceSet& f) {
-  const MxSlot& L = S.slot[sk];
-  face_one(S, L, kk, true, f.own_x, f.own_r);
-  face_one(S, L, kk, false, f.own_y, f.own_r - SW);
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-    if (i < f.ne) {
-      const uint32_t d = f.e[i];
-      face_one(S, L, kk, !(d >> 31), (int)((d >> 16) & 0x7fffu), (int)(d & 0xffffu));
-    }
+// o index of the tile's x face west of column tx in row ty, and of the y
+// face north of row ty at column tx
+__device__ __forceinline__ int ox(int ty, int tx) { return ty * (TX + 1) + tx; }
+__device__ __forceinline__ int oy(int ty, int tx) { return OXN + ty * TX + tx; }
+
+__device__ __forceinline__ void face_f64(MxSmem& S, const MxSlot& L, const OwnFace& q) {
+  double u;
+  if (q.x) u = face_x64(L.wkd[q.w], L.wkd[q.w + SW], q.h);
+  else u = face_y64(L.wkb[q.w], L.wkb[q.w + 1], q.h);
+  S.ou[q.o] = u;
+  S.oq[q.o] = u * u * (double)S.cf[q.f];
 }
-static_assert(F_EXTRA <= 2 * MTH, "border faces: at most two per thread");
 
 // A cell of the 1-halo region as one thread handles it: its index m in the
-// region, box index r (at, atb, kmt boxes), u (ws box), its west x face fw and
-// north y face fn (the east and south faces are fw + 1 and fn + HQX); valid:
-// inside the rows and columns the reference computes (1 .. imt-2, 1 .. jmt-2).
-// Every thread owns the interior cell above its column; the 76 ring cells of
-// the region go to threads 0 .. 75, one each.
+// region, box indices (f64 boxes r, ws box u), its west x face and north y
+// face; valid: inside the rows and columns the reference computes
+// (1 .. imt-2, 1 .. jmt-2).  Every thread owns the interior cell above its
+// column; the ring cells of the region go to threads 0 .. RING-1, one each.
 struct HCell {
   int m, r, u, fw, fn;
   bool valid;
 };
 constexpr int RING = MHN - TX * MY;
+static_assert(RING <= MTH, "ring cells: at most one per thread");
 
 __device__ __forceinline__ HCell hcell(int hj, int hi, int x0, int y0, int imt, int jmt) {
   HCell c;
   c.m = hj * HQX + hi;
-  c.r = r2(hj, hi);
-  c.u = ru(hj, hi);
+  c.r = b64(hj, hi);
+  c.u = bws(hj, hi);
   c.fw = fx(hj, hi);
   c.fn = fy(hj, hi);
   const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
@@ -420,7 +451,6 @@ __device__ __forceinline__ HCell hcell(int hj, int hi, int x0, int y0, int imt, 
   return c;
 }
 
-// ring cell q (0 .. RING-1): top row, bottom row, west column, east column
 __device__ __forceinline__ HCell ring_hcell(int q, int x0, int y0, int imt, int jmt) {
   int hj, hi;
   if (q < HQX) { hj = 0; hi = q; }
@@ -430,461 +460,449 @@ __device__ __forceinline__ HCell ring_hcell(int q, int x0, int y0, int imt, int 
   return hcell(hj, hi, x0, y0, imt, jmt);
 }
 
-// Per-level constants of the predictor at level kk.
-struct PredLevel {
-  const double *at_c, *at_u, *at_d;
-  const float *ws_c, *ws_d, *dx, *dy, *ux, *vy;
-  float hodz, odzt_k, odzt_k1, dts;
-  int kk, km;
-  bool up, dn;   // level kk has a level above / below
-};
-
-// sc, su, sd: the slots of levels kk, kk-1, kk+1
-__device__ __forceinline__ PredLevel pred_level(const MxSmem& S, const Arena& a, int kk, int sc, int su, int sd) {
-  PredLevel P;
-  const int km = a.km;
-  P.kk = kk;
-  P.km = km;
-  // at the top and bottom levels the missing neighbour level is replaced by
-  // level kk itself: its differences are then exactly zero, and so are the
-  // vertical terms they carry (pred_cell needs no branch on the level)
-  P.up = kk > 0;
-  P.dn = kk < km - 1;
-  P.at_c = S.slot[sc].at;
-  P.at_u = P.up ? S.slot[su].at : P.at_c;
-  P.at_d = P.dn ? S.slot[sd].at : P.at_c;
-  P.ws_c = S.slot[sc].ws;
-  P.ws_d = P.dn ? S.slot[sd].ws : P.ws_c;
-  P.dx = S.fxd[kk & 1];
-  P.dy = S.fyd[kk & 1];
-  P.ux = S.fxu[kk & 1];
-  P.vy = S.fyv[kk & 1];
-  P.hodz = 0.5f * (float)a.odzp[kk];
-  P.odzt_k = (float)a.odzt[kk];
-  P.odzt_k1 = kk < km - 1 ? (float)a.odzt[kk + 1] : 0.f;
-  P.dts = (float)a.p.dts;
-  return P;
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
 }
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-// Predictor and bound test of one cell: true if the predictor leaves the
-// local bounds (the reference's a00 > amax or a00 < amin).
-__device__ __forceinline__ bool pred_cell(const MxSmem& S, const PredLevel& P, const HCell& h) {
-  if (!h.valid) return false;
-  const int kk = P.kk, r = h.r, u = h.u;
-  const int fw = h.fw, fe = fw + 1, fn = h.fn, fs = fn + HQX;
-  const float* dx = P.dx;
-  const float* dy = P.dy;
-  const float dts = P.dts;
-  // horizontal: east/west x faces, south/north y faces
-  const float ue = P.ux[fe], uwv = P.ux[fw];
-  const float vs = P.vy[fs], vn = P.vy[fn];
-  const float sx = (dx[fe] * ue - lw_part(dx[fe], ue, S.cxf[fe])) + (dx[fw] * uwv + lw_part(dx[fw], uwv, S.cxf[fw]));
-  const float sy = (dy[fs] * vs - lw_part(dy[fs], vs, S.cyf[fs])) + (dy[fn] * vn + lw_part(dy[fn], vn, S.cyf[fn]));
+// Predictor of level kk for one cell, both tracers: bit n set where tracer
+// n's predictor leaves its local bounds (the reference's a00 > amax or
+// a00 < amin).  sc, su, sd: the slots of levels kk, kk-1, kk+1 (at the top
+// and bottom level the missing neighbour level is replaced by kk itself,
+// whose differences are then 0, and so are the vertical terms they carry).
+__device__ __forceinline__ unsigned pred_cell(const MxSmem& S, const HCell& h, int kk, int km, int sc, int su,
+                                              int sd, const MxLevel& lv, float dts) {
+  if (!h.valid) return 0u;
+  const int r = h.r;
+  const int fe = h.fw + 1, fw = h.fw, fs = h.fn + HQX, fn = h.fn;
+  const float2 de = S.fd[fe], dw = S.fd[fw], ds = S.fd[fs], dn = S.fd[fn];
+  // east face: this cell is the lower one, d*(u - q); west face: upper, d*(u + q)
+  const float2 sx = __ffma2_rn(dw, f2(S.fu[fw] + S.fq[fw]), __fmul2_rn(de, f2(S.fu[fe] - S.fq[fe])));
+  const float2 sy = __ffma2_rn(dn, f2(S.fu[fn] + S.fq[fn]), __fmul2_rn(ds, f2(S.fu[fs] - S.fq[fs])));
   // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
-  // (at a missing level the difference is 0, the term +-0, and sz stays +0)
-  float sz = 0.f;
-  const double c = P.at_c[r];
-  const float dup = (float)(P.at_u[r] - c);   // a_above - c
-  {
-    const float w = P.ws_c[u];
-    const float A = w * dup;
-    sz += A - A * w * P.odzt_k * dts;
-  }
-  const float d = (float)(c - P.at_d[r]);
-  const float ddn = -d;                         // a_below - c
-  {
-    const float w = P.ws_d[u];
-    const float A = w * d;
-    sz += A + A * w * P.odzt_k1 * dts;
-  }
-  const float inc = -(S.tr[h.m] * (sx + sy) + P.hodz * sz) * dts;
-  // Bound test of the predictor c + inc against the masked 7-point extrema
-  // (land excluded: -1e10 for the max, +1e10 for the min), done on
-  // differences from c: c + inc > max_p a_p  <=>  inc > max_p (a_p - c).
-  // The horizontal differences are the face differences already formed;
-  // with no wet point the reference's extrema flag the cell, as -inf does.
-  const uint16_t* kt = S.kmt;
-  float dmax = -INFINITY, dmin = INFINITY;
-  auto acc = [&](bool wet, float d) {
-    if (wet) { dmax = fmaxf(dmax, d); dmin = fminf(dmin, d); }
-  };
-  acc(kk < kt[r], 0.f);
-  acc(kk < kt[r + 1], dx[fe]);
-  acc(kk < kt[r - 1], -dx[fw]);
-  acc(kk < kt[r + SW], dy[fs]);
-  acc(kk < kt[r - SW], -dy[fn]);
-  acc(P.up && kk - 1 < kt[r], dup);
-  acc(P.dn && kk + 1 < kt[r], ddn);
-  return inc > dmax || inc < dmin;
+  const MxSlot& C = S.slot[sc];
+  const MxSlot& U = S.slot[kk > 0 ? su : sc];
+  const MxSlot& D = S.slot[kk < km - 1 ? sd : sc];
+  const double cT = C.at[0][r], cS = C.at[1][r];
+  const float2 dup = make_float2((float)(U.at[0][r] - cT), (float)(U.at[1][r] - cS));   // a_above - c
+  const float2 dlo = make_float2((float)(cT - D.at[0][r]), (float)(cS - D.at[1][r]));   // c - a_below
+  const float wc = C.ws[h.u], wd = D.ws[h.u];
+  const float cu = wc - wc * wc * (float)lv.odzt * dts;
+  const float cd = wd + wd * wd * lv.odzt1 * dts;
+  const float2 sz = __ffma2_rn(dup, f2(cu), __fmul2_rn(dlo, f2(cd)));
+  // inc = -(tr*(sx+sy) + hodz*sz)*dts
+  const float2 inc = __fmul2_rn(__ffma2_rn(f2(lv.hodz), sz, __fmul2_rn(f2(S.tr[h.m]), __fadd2_rn(sx, sy))),
+                                f2(-dts));
+  // Bound test of the predictor c + inc against the masked 7-point extrema,
+  // on differences from c: c + inc > max_p a_p  <=>  inc > max_p (a_p - c).
+  // Land neighbours enter as 0 (the cell itself): horizontally through the
+  // masked face differences, below through the test here; the level above a
+  // wet cell is wet.  The flags of land cells are never used: every face of
+  // a land cell carries no transport.
+  const bool below_wet = kk + 1 < S.kmt[r];
+  const float lx = below_wet ? -dlo.x : 0.f, ly = below_wet ? -dlo.y : 0.f;
+  const float mxT = fmax3f(fmax3f(0.f, de.x, -dw.x), fmax3f(ds.x, -dn.x, dup.x), lx);
+  const float mnT = fmin3f(fmin3f(0.f, de.x, -dw.x), fmin3f(ds.x, -dn.x, dup.x), lx);
+  const float mxS = fmax3f(fmax3f(0.f, de.y, -dw.y), fmax3f(ds.y, -dn.y, dup.y), ly);
+  const float mnS = fmin3f(fmin3f(0.f, de.y, -dw.y), fmin3f(ds.y, -dn.y, dup.y), ly);
+  return ((inc.x > mxT || inc.x < mnT) ? 1u : 0u) | ((inc.y > mxS || inc.y < mnS) ? 2u : 0u);
 }
 
-// Predictor flags of level kk for the thread's own cell and ring cell;
-// returns the own cell's flag.
-__device__ __forceinline__ bool predictor_mixed(MxSmem& S, const Arena& a, int kk, int sc, int su, int sd,
-                                                const HCell& own, const HCell& ring, bool has_ring) {
-  const PredLevel P = pred_level(S, a, kk, sc, su, sd);
-  unsigned char* fl = S.flag[sc];   // flags kept per level modulo 3, as the slots
-  const bool f = pred_cell(S, P, own);
-  fl[own.m] = f ? 1 : 0;
-  if (has_ring) fl[ring.m] = pred_cell(S, P, ring) ? 1 : 0;
-  return f;
-}
-
-// first Laplacian of atb at level kk (f32 on f64 differences), masked
-__device__ __forceinline__ float d2_cell(const MxSmem& S, const double* atb, int kk, const HCell& h) {
-  if (!h.valid) return 0.f;
+// First Laplacian of atb at level kk for one cell, both tracers (f64 on the
+// state differences), masked: land neighbours drop out, a land cell is 0.
+__device__ __forceinline__ void d2_cell(MxSmem& S, const MxSlot& L, int kk, const HCell& h) {
+  double vT = 0.0, vS = 0.0;
   const int r = h.r, m = h.m;
-  const double c = atb[r];
-  if (kk > S.kmt[r] - 1) return 0.f;
-  float v = 0.f;
-  if (kk <= S.kmt[r - SW] - 1) v += S.dtn[m] * (float)(atb[r - SW] - c);
-  if (kk <= S.kmt[r + SW] - 1) v += S.dts[m] * (float)(atb[r + SW] - c);
-  if (kk <= S.kmt[r + 1] - 1) v += S.dte[m] * (float)(atb[r + 1] - c);
-  if (kk <= S.kmt[r - 1] - 1) v += S.dtw[m] * (float)(atb[r - 1] - c);
-  return S.ahf[m] * v;
+  if (h.valid && kk < S.kmt[r]) {
+    const double cT = L.atb[0][r], cS = L.atb[1][r];
+    auto term = [&](int rn, float coef) {
+      if (kk < S.kmt[rn]) {
+        const double c = (double)coef;
+        vT = fma(c, L.atb[0][rn] - cT, vT);
+        vS = fma(c, L.atb[1][rn] - cS, vS);
+      }
+    };
+    term(r - SW64, S.dtn[m]);
+    term(r + SW64, S.dts[m]);
+    term(r + 1, S.dte[m]);
+    term(r - 1, S.dtw[m]);
+    const double ah = (double)S.ahf[m];
+    vT *= ah;
+    vS *= ah;
+  }
+  S.d2[0][m] = vT;
+  S.d2[1][m] = vS;
 }
 
-__device__ __forceinline__ void del4_first_mixed(MxSmem& S, int kk, int sk, const HCell& own, const HCell& ring,
-                                                 bool has_ring) {
-  const double* atb = S.slot[sk].atb;
-  S.d2[own.m] = d2_cell(S, atb, kk, own);
-  if (has_ring) S.d2[ring.m] = d2_cell(S, atb, kk, ring);
-}
-
-// Per-tile 2-D data of the mixed march (kmt with a 2-cell halo, the metric
-// and biharmonic terms of the 1-halo region, the face factors) with fixed
-// trip counts and read-only loads, so a thread's loads of a loop are in
-// flight together.  The batched kernel, whose work items are short and change
-// member often, stages its tiles this way; the single-domain kernel keeps the
-// plain loops in mixed_item, with which it compiles better.
-__device__ __forceinline__ void stage_tile_statics_ahead(MxSmem& S, const Arena& a, int x0, int y0, double dts) {
+// Per-tile 2-D data of the march (kmt with a 2-cell halo, the metric and
+// biharmonic terms of the 1-halo region, the face factors).  kLoadsAhead:
+// fixed trip counts and read-only loads, so a thread's loads of a loop are in
+// flight together (the batched kernel, whose short work items change member
+// often, stages its tiles this way).
+template <bool kLoadsAhead>
+__device__ __forceinline__ void stage_tile(MxSmem& S, const Arena& a, int x0, int y0, double dts) {
   const int tid = threadIdx.x;
   const int imt = a.imt, jmt = a.jmt;
+  auto ld = [&](const double* p) { return kLoadsAhead ? __ldg(p) : *p; };
 #pragma unroll
-  for (int it = 0; it < ((MY + 4) * SW + MTH - 1) / MTH; ++it) {
+  for (int it = 0; it < ((MY + 4) * SW64 + MTH - 1) / MTH; ++it) {
     const int m = tid + it * MTH;
-    if (m < (MY + 4) * SW) {
-      const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
-      S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? __ldg(a.kmt + (long)gj * imt + gi) : 0;
+    if (m < (MY + 4) * SW64) {
+      const int gj = y0 - 2 + m / SW64, gi = x0 - 2 + m % SW64;
+      const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+      S.kmt[m] = in ? (uint16_t)(kLoadsAhead ? __ldg(a.kmt + (long)gj * imt + gi) : a.kmt[(long)gj * imt + gi]) : 0;
     }
-}
-#pragma unroll
-for (int it = 0; it < (MHN + MTH - 1) / MTH; ++it) {
-  const int m = tid + it * MTH;
-  if (m < MHN) {
-    const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
-    const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
-    const long q = in ? (long)gj * imt + gi : 0;
-    const double tarea = __ldg(a.tarea + q), dte = __ldg(a.dte + q), dtsq = __ldg(a.dts + q);
-    S.tr[m] = in ? (float)__ldg(a.tarea_r + q) : 0.f;
-    S.dtn[m] = in ? (float)__ldg(a.dtn + q) : 0.f;
-    S.dts[m] = in ? (float)dtsq : 0.f;
-    S.dte[m] = in ? (float)dte : 0.f;
-    S.dtw[m] = in ? (float)__ldg(a.dtw + q) : 0.f;
-    S.ahf[m] = in ? (float)__ldg(a.ahf + q) : 0.f;
-    S.kx[m] = in ? (float)(tarea * dte) : 0.f;
-    S.ky[m] = in ? (float)(tarea * dtsq) : 0.f;
   }
-}
 #pragma unroll
-for (int it = 0; it < (FXN + FYN + MTH - 1) / MTH; ++it) {
-  const int m = tid + it * MTH;
-  if (m < FXN + FYN) {
-    int gj, gi;
-    if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
-    else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
-    const bool inb = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
-    const long q = inb ? (long)gj * imt + gi : 0;
-    const double h = (m < FXN) ? __ldg(a.htw + q) : __ldg(a.hts + q);
-    const double hu = (m < FXN) ? __ldg(a.hun + q) : __ldg(a.hue + q);
-    const float v = inb ? (float)(2.0 * dts / (h * hu)) : 0.f;
-    const float hf = inb ? (float)h : 0.f;
-    if (m < FXN) { S.cxf[m] = v; S.hwx[m] = hf; }
-    else { S.cyf[m - FXN] = v; S.hsy[m - FXN] = hf; }
+  for (int it = 0; it < (MHN + MTH - 1) / MTH; ++it) {
+    const int m = tid + it * MTH;
+    if (m < MHN) {
+      const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
+      const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+      const long q = in ? (long)gj * imt + gi : 0;
+      S.tr[m] = in ? (float)ld(a.tarea_r + q) : 0.f;
+      S.dtn[m] = in ? (float)ld(a.dtn + q) : 0.f;
+      S.dts[m] = in ? (float)ld(a.dts + q) : 0.f;
+      S.dte[m] = in ? (float)ld(a.dte + q) : 0.f;
+      S.dtw[m] = in ? (float)ld(a.dtw + q) : 0.f;
+      S.ahf[m] = in ? (float)ld(a.ahf + q) : 0.f;
+    }
   }
-}
+#pragma unroll
+  for (int it = 0; it < (FN + MTH - 1) / MTH; ++it) {
+    const int m = tid + it * MTH;
+    if (m < FN) {
+      int gj, gi;
+      if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
+      else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
+      const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+      const long q = in ? (long)gj * imt + gi : 0;
+      const double h = in ? ((m < FXN) ? ld(a.htw + q) : ld(a.hts + q)) : 1.0;
+      const double hu = in ? ((m < FXN) ? ld(a.hun + q) : ld(a.hue + q)) : 1.0;
+      S.cf[m] = in ? (float)(2.0 * dts / (h * hu)) : 0.f;
+      S.hw[m] = in ? (float)h : 0.f;
+    }
+  }
 }
 
-// One work item (tile, tracer) of the mixed column march.  Returns false if
-// a level wait gave up: the CTA has then recorded the timeout and drained
-// its boxes, and must return.
+// The km level constants, once per CTA.
+__device__ __forceinline__ void stage_levels(MxLevel* lv, const Arena& a) {
+  const int km = a.km;
+  const double dts = a.p.dts;
+  for (int k = threadIdx.x; k < km; k += MTH) {
+    MxLevel L;
+    L.odzp = a.odzp[k];
+    L.odzt = a.odzt[k];
+    L.ka = a.odzt[k] * a.odzp[k] * dts * 0.5;
+    L.kc = k < km - 1 ? a.odzt[k + 1] * a.odzp[k] * dts * 0.5 : 0.0;
+    L.pu = k >= 1 ? a.pen[k - 1] : 0.0;
+    L.pd = k < km - 1 ? a.pen[k] : 0.0;
+    L.hodz = 0.5f * (float)a.odzp[k];
+    L.odzt1 = k < km - 1 ? (float)a.odzt[k + 1] : 0.f;
+    lv[k] = L;
+  }
+}
+
+// Column-phase state of one tracer carried up the levels.
+struct ColState {
+  double e, f;      // the sweep's elimination coefficients of the level below
+  double carry;     // vertical face below as seen from above: A + X
+  double wbelow;    // explicit diffusion flux through the face below
+  double stf;       // surface flux
+};
+
+// One work item (a tile, both tracers) of the mixed column march.  Returns
+// false if a level wait gave up: the CTA has then recorded the timeout and
+// drained its boxes, and must return.
 template <bool kLoadsAhead>
-__device__ __forceinline__ bool mixed_item(MxSmem& S, const Arena& a, const TracerMaps& maps, double* scr, int ntx,
-                                           long tile, int n, uint32_t& par, uint32_t& outstanding) {
+__device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict__ lvs, const Arena& a,
+                                           const TracerMaps& maps, double* scr, int ntx, long tile, uint32_t& par,
+                                           uint32_t& outstanding) {
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
   const int imt = a.imt, jmt = a.jmt, km = a.km;
   const long A = a.A, F = a.F, FB = a.FB;
   const lt_params& p = a.p;
   const double dts = p.dts;
   const float dtsf = (float)dts;
-  const double* __restrict__ odzp = a.odzp;
-  const double* __restrict__ odzt = a.odzt;
+  const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * MY;
+  const int i = x0 + tx, j = y0 + ty;
+
+  __syncthreads();   // the previous item no longer reads the slots or the tile data
+  // level L goes to slot s = L % NSM
+  auto issue = [&](int L, int s) {
+    if (tid == 0) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, km, L, x0, y0);
+    outstanding |= 1u << s;
+  };
+  auto wait = [&](int s) -> bool {
+    const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u, a.wait_limit);
+    if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
+    return ok;
+  };
+  for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L, L % NSM);
+  stage_tile<kLoadsAhead>(S, a, x0, y0, dts);
+
+  const bool own = i < imt && j < jmt;
+  const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
+  const long qo = own ? (long)j * imt + i : 0;
+  const int kz = own ? a.kmt[qo] : 0;
+  const int hc = (ty + 1) * HQX + (tx + 1);
+  const int rc = b64(ty + 1, tx + 1), uc = bws(ty + 1, tx + 1);
+  const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
+  const bool has_ring = tid < RING;
+  const HCell ring_cell = ring_hcell(has_ring ? tid : 0, x0, y0, imt, jmt);
+  // f32 faces: the own cell's west x face and north y face, and one border face
+  const FaceRef fo_x = face_x_ref(ty + 1, tx + 1), fo_y = face_y_ref(ty + 1, tx + 1);
+  const bool has_fb = tid < F_EXTRA;
+  const FaceRef fo_b = border_face(has_fb ? tid : 0);
+  // f64 faces of the tile: the own cell's west and north faces, and the east
+  // column's x faces (threads 0 .. MY-1) and the bottom row's y faces
+  // (threads MY .. MY+TX-1)
+  auto hval = [&](const double* h, int gj, int gi) {
+    return (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? h[(long)gj * imt + gi] : 0.0;
+  };
+  const OwnFace of_x = {ox(ty, tx), b32(ty, tx + 1), fx(ty + 1, tx + 1), true, hval(a.htw, j, i)};
+  const OwnFace of_y = {oy(ty, tx), b32(ty, tx + 1), fy(ty + 1, tx + 1), false, hval(a.hts, j - 1, i)};
+  const bool has_ob = tid < MY + TX;
+  OwnFace of_b;
+  if (tid < MY) of_b = {ox(tid, TX), b32(tid, TX + 1), fx(tid + 1, TX + 1), true, hval(a.htw, y0 + tid, x0 + TX)};
+  else if (has_ob) of_b = {oy(MY, tid - MY), b32(MY, tid - MY + 1), fy(MY + 1, tid - MY + 1), false,
+                           hval(a.hts, y0 + MY - 1, x0 + tid - MY)};
+  else of_b = of_x;
+  const int oe = ox(ty, tx + 1), ow = ox(ty, tx), os = oy(ty + 1, tx), on = oy(ty, tx);
+  // second Laplacian face weights K = tarea*dte (x faces), tarea*dts (y faces)
+  // of the own cell's four faces, f64: the same expression in both cells of a face
+  auto kxw = [&](int gj, int gi) {
+    return (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.tarea[(long)gj * imt + gi] * a.dte[(long)gj * imt + gi]
+                                                      : 0.0;
+  };
+  auto kys = [&](int gj, int gi) {
+    return (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.tarea[(long)gj * imt + gi] * a.dts[(long)gj * imt + gi]
+                                                      : 0.0;
+  };
+  const double kxE = inner ? kxw(j, i) : 0.0, kxW = inner ? kxw(j, i - 1) : 0.0;
+  const double kyS = inner ? kys(j, i) : 0.0, kyN = inner ? kys(j - 1, i) : 0.0;
+  const double swv = (inner) ? a.swv[qo] : 0.0;
+  const double err_norm2 = a.scalars[0];
+  const double ah64 = p.ah;
+  const double trc = inner ? a.tarea_r[qo] : 0.0;
+  ColState cs[2];
+  cs[0] = {0.0, 0.0, 0.0, 0.0, own ? a.stf_n[qo] : 0.0};
+  cs[1] = {0.0, 0.0, 0.0, 0.0, own ? a.stf_n[A + qo] : 0.0};
+  // own column's mixing coefficients: level k in akt_here, level k-1 loaded a step ahead
+  const float* akt_col = a.akt32 + qo;
+  float akt_here[2];
+  akt_here[0] = inner ? __ldg(akt_col + (long)(km - 1) * A) : 0.f;
+  akt_here[1] = inner ? __ldg(akt_col + F + (long)(km - 1) * A) : 0.f;
+
+  // slots of levels k, k-1, k+1 (NSM == 3: level k-2 shares k+1's)
+  static_assert(NSM == 3, "slot rotation below assumes three slots");
+  int sk = (km - 1) % NSM;
+  int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
   {
-    const int x0 = (int)(tile % ntx) * TX, y0 = (int)(tile / ntx) * MY;
-    const int i = x0 + tx, j = y0 + ty;
-    double* at_out = a.at[a.cur ^ 1] + n * F;
-    double* atb_out = a.atb[a.cur ^ 1] + n * FB;
+    const bool ok = wait(sk) && wait(sm1);
+    if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
+  }
+  {
+    const MxSlot& L = S.slot[sk];
+    face_f32(S, L, km - 1, fo_x);
+    face_f32(S, L, km - 1, fo_y);
+    if (has_fb) face_f32(S, L, km - 1, fo_b);
+  }
+  __syncthreads();
+  {
+    const MxLevel lv = lvs[km - 1];
+    S.flag[sk][own_cell.m] = (unsigned char)pred_cell(S, own_cell, km - 1, km, sk, sm1, sp1, lv, dtsf);
+    if (has_ring) S.flag[sk][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, km - 1, km, sk, sm1, sp1, lv, dtsf);
+  }
 
-    __syncthreads();
-    // level L goes to slot s = L % NSM
-    auto issue = [&](int L, int s) {
-      if (tid == 0) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, n, km, L, x0, y0);
-      outstanding |= 1u << s;
-    };
-    auto wait = [&](int s) -> bool {
-      const bool ok = mbar_wait(&S.bar[s], (par >> s) & 1u, a.wait_limit);
-      if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
-      return ok;
-    };
-    for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L, L % NSM);
-    if constexpr (kLoadsAhead) {
-      stage_tile_statics_ahead(S, a, x0, y0, dts);
-    } else {
-      for (int m = tid; m < (MY + 4) * SW; m += MTH) {
-        const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
-        S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
-      }
-      for (int m = tid; m < MHN; m += MTH) {
-        const int gj = y0 - 1 + m / HQX, gi = x0 - 1 + m % HQX;
-        const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
-        const long q = in ? (long)gj * imt + gi : 0;
-        S.tr[m] = in ? (float)a.tarea_r[q] : 0.f;
-        S.dtn[m] = in ? (float)a.dtn[q] : 0.f;
-        S.dts[m] = in ? (float)a.dts[q] : 0.f;
-        S.dte[m] = in ? (float)a.dte[q] : 0.f;
-        S.dtw[m] = in ? (float)a.dtw[q] : 0.f;
-        S.ahf[m] = in ? (float)a.ahf[q] : 0.f;
-        S.kx[m] = in ? (float)(a.tarea[q] * a.dte[q]) : 0.f;
-        S.ky[m] = in ? (float)(a.tarea[q] * a.dts[q]) : 0.f;
-      }
-      for (int m = tid; m < FXN + FYN; m += MTH) {
-        int gj, gi;
-        if (m < FXN) { gj = y0 - 1 + m / (TX + 3); gi = x0 - 1 + m % (TX + 3); }
-        else { gj = y0 - 2 + (m - FXN) / (TX + 2); gi = x0 - 1 + (m - FXN) % (TX + 2); }
-        float v = 0.f;
-        if (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) {
-          const long q = (long)gj * imt + gi;
-          v = (m < FXN) ? (float)(2.0 * dts / (a.htw[q] * a.hun[q])) : (float)(2.0 * dts / (a.hts[q] * a.hue[q]));
-        }
-        if (m < FXN) S.cxf[m] = v; else S.cyf[m - FXN] = v;
-        const bool inb = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
-        if (m < FXN) S.hwx[m] = inb ? (float)a.htw[(long)gj * imt + gi] : 0.f;
-        else S.hsy[m - FXN] = inb ? (float)a.hts[(long)gj * imt + gi] : 0.f;
-      }
+  // Level slots: after step k the slot of level k takes level k-NSM.
+  for (int k = km - 1; k >= 0; --k) {
+    float akt_above[2];
+    akt_above[0] = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
+    akt_above[1] = (inner && k >= 1) ? __ldg(akt_col + F + (long)(k - 1) * A) : 0.f;
+    // ---- phase B1: f32 faces one level up (the predictor's), the tile's f64
+    // faces and the first Laplacian here (levels k-1, k arrived in earlier
+    // steps; the previous step ended with a barrier)
+    const MxSlot& Lk = S.slot[sk];
+    if (k >= 1) {
+      const MxSlot& Lu = S.slot[sm1];
+      face_f32(S, Lu, k - 1, fo_x);
+      face_f32(S, Lu, k - 1, fo_y);
+      if (has_fb) face_f32(S, Lu, k - 1, fo_b);
     }
-
-    const bool own = (i < imt && j < jmt);
-    const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
-    const long qo = own ? (long)j * imt + i : 0;
-    const int kz = own ? a.kmt[qo] : 0;
-    const int hc = (ty + 1) * HQX + (tx + 1);
-    const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1);
-    const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
-    const bool has_ring = tid < RING;
-    const HCell ring_cell = ring_hcell(has_ring ? tid : 0, x0, y0, imt, jmt);
-    const FaceSet fset = face_set(tid);
-    const int fe = fx(ty + 1, tx + 2), fwi = fx(ty + 1, tx + 1), fs = fy(ty + 2, tx + 1), fn = fy(ty + 1, tx + 1);
-    const float swv = (inner && n == 0) ? (float)a.swv[qo] : 0.f;
-    const double stf = own ? a.stf_n[n * A + qo] : 0.0;
-    const double err_norm2 = a.scalars[0];
-    const double ah64 = p.ah;
-    const double trc = inner ? a.tarea_r[qo] : 0.0;
-    const double htw_w64 = inner ? a.htw[qo] : 0.0, htw_e64 = inner ? a.htw[qo + 1] : 0.0;
-    const double hts_s64 = inner ? a.hts[qo] : 0.0, hts_n64 = inner ? a.hts[qo - imt] : 0.0;
-    double e_prev = 0.0, f_prev = 0.0;
-    double carry = 0.0;  // lower face of the level below, as seen by the level above: A + X
-    float w_below = 0.f;  // explicit diffusion flux through the bottom face, from the level below
-    // own column's mixing coefficient: level k in akt_here, level k-1 loaded a step ahead
-    const float* akt_col = a.akt32 + n * F + qo;
-    float akt_here = inner ? __ldg(akt_col + (long)(km - 1) * A) : 0.f;
-
-    // slots of levels k, k-1, k+1 (NSM == 3: level k-2 shares k+1's)
-    static_assert(NSM == 3, "slot rotation below assumes three slots");
-    int sk = (km - 1) % NSM;
-    int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
-    {
-      const bool ok = wait(sk) && wait(sm1);
-      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
+    face_f64(S, Lk, of_x);
+    face_f64(S, Lk, of_y);
+    if (has_ob) face_f64(S, Lk, of_b);
+    d2_cell(S, Lk, k, own_cell);
+    if (has_ring) d2_cell(S, Lk, k, ring_cell);
+    const bool ok = (k >= 2) ? wait(sp1) : true;   // level k-2
+    if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
+    // ---- phase B2: predictor one level up.  The column phase below reads
+    // the flags of level k (written in the previous step) and, of level k-1,
+    // only its own cell's, which this thread computes: no barrier between
+    // the two phases.
+    unsigned flag_up = 0;
+    if (k >= 1) {
+      const MxLevel lv = lvs[k - 1];
+      flag_up = pred_cell(S, own_cell, k - 1, km, sm1, sp1, sk, lv, dtsf);
+      S.flag[sm1][own_cell.m] = (unsigned char)flag_up;
+      if (has_ring) S.flag[sm1][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, k - 1, km, sm1, sp1, sk, lv, dtsf);
     }
-    faces_level(S, km - 1, sk, fset);
-    __syncthreads();
-    predictor_mixed(S, a, km - 1, sk, sm1, sp1, own_cell, ring_cell, has_ring);
-
-    // Level slots: after step k the slot of level k takes level k-NSM.
-    for (int k = km - 1; k >= 0; --k) {
-      const float akt_above = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
-      // ---- phase B1: faces one level up, first Laplacian here (levels k-1, k
-      // arrived in earlier steps; the previous step ended with a barrier)
-      if (k >= 1) faces_level(S, k - 1, sm1, fset);
-      del4_first_mixed(S, k, sk, own_cell, ring_cell, has_ring);
-      const bool ok = (k >= 2) ? wait(sp1) : true;   // level k-2
-      if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
-      // ---- phase B2: predictor one level up.  The column phase below reads
-      // the flags of level k (written in the previous step) and, of level
-      // k-1, only its own cell's flag, which this thread computes: no barrier
-      // between the two phases.
-      const bool flag_up = (k >= 1) ? predictor_mixed(S, a, k - 1, sm1, sp1, sk, own_cell, ring_cell, has_ring) : false;
-      // ---- phase C: own column at level k
-      if (inner) {
-        const MxSlot& Lk = S.slot[sk];
-        const unsigned char* fl = S.flag[sk];
-        const bool self = fl[hc] != 0;
-        const float* dx = S.fxd[k & 1];
-        const float* dy = S.fyd[k & 1];
-        const float ue = S.fxu[k & 1][fe], uwv = S.fxu[k & 1][fwi];
-        const float vsv = S.fyv[k & 1][fs], vnv = S.fyv[k & 1][fn];
-        // the same faces in f64, as the continuity march formed them
-        const int xw = (ty + 1) * SW + tx + 4;   // wkd of U point (j-1, i); (j, i) is one row down
-        const double ue64 = face_x64(Lk.wkd[xw + 1], Lk.wkd[xw + 1 + SW], htw_e64);
-        const double uw64 = face_x64(Lk.wkd[xw], Lk.wkd[xw + SW], htw_w64);
-        const int ys = (ty + 2) * SW + tx + 4;   // wkb of U point (j, i); (j, i+1) is next
-        const double vs64 = face_y64(Lk.wkb[ys], Lk.wkb[ys + 1], hts_s64);
-        const double vn64 = face_y64(Lk.wkb[ys - SW], Lk.wkb[ys - SW + 1], hts_n64);
-        // Content bookkeeping.  Both cells of a face receive its centred part
-        // A = d*u with the same sign (the advective form), so any rounding of
-        // A adds up over the domain instead of cancelling: A is formed in f64
-        // from the exact f64 state difference and the f32 transport.  The
-        // upwind / Lax-Wendroff part X (f32) enters the two cells with
-        // opposite signs and cancels exactly in the f64 face sums.
-        const double c = Lk.at[rc];
-        const double dE = Lk.at[rc + 1] - c, dW = c - Lk.at[rc - 1];
-        const double dS = Lk.at[rc + SW] - c, dN = c - Lk.at[rc - SW];
-        float t;
-        t = dx[fe];                                   // east face: this cell is L
-        const float Xe = (self || fl[hc + 1]) ? fabsf(ue) * t : lw_part(t, ue, S.cxf[fe]);
-        t = dx[fwi];
-        const float Xw = (self || fl[hc - 1]) ? fabsf(uwv) * t : lw_part(t, uwv, S.cxf[fwi]);
-        t = dy[fs];
-        const float Xs = (self || fl[hc + HQX]) ? fabsf(vsv) * t : lw_part(t, vsv, S.cyf[fs]);
-        t = dy[fn];
-        const float Xn = (self || fl[hc - HQX]) ? fabsf(vnv) * t : lw_part(t, vnv, S.cyf[fn]);
-        double sh = dE * ue64 + dW * uw64 + dS * vs64 + dN * vn64;
-        sh += ((double)Xw - (double)Xe) + ((double)Xn - (double)Xs);
-        // vertical: face above (k-1|k) computed here, face below carried
-        // (at the top level the level itself stands in for the missing one
-        // above: the difference and both face terms are 0, sz keeps carry)
-        double sz = carry;
-        {
-          const float wv = Lk.ws[uc];
-          const double d64 = (k > 0 ? S.slot[sm1].at : Lk.at)[rc] - c;
-          const float d = (float)d64;
-          const bool up = self || flag_up;
-          const float Xv = up ? fabsf(wv) * d : (wv * d) * wv * (float)odzt[k] * dtsf;
-          const double Av = (double)wv * d64;
-          sz += Av - (double)Xv;
-          carry = Av + (double)Xv;
-        }
-        // Face-flux sums are weighted by tarea_r (horizontal) and odzp
-        // (vertical) in f64, so a flux leaves one cell and enters the next
-        // with weights that cancel against the cell volumes to f64 rounding.
-        const float vit_k = k < kz ? 1.f : 0.f;
-        const float vit_kp1 = (k + 1 < kz) ? 1.f : 0.f;
-        sh *= (double)vit_k;                          // horizontal advection, times -tarea_r
-        const double vadv = -0.5 * sz * (double)vit_k;  // vertical advection, times odzp
-        double vz = 0.0;                              // other vertical face-flux differences, times odzp
-        float tf = 0.f;                               // the remaining tendency terms
-        // second Laplacian as face fluxes K*(d2_R - d2_L), K = tarea*dte
-        // (x) or tarea*dts (y): one f32 value per face, the same in both of
-        // its cells, summed in f64 (dtn/dts/dte/dtw are K*tarea_r of the
-        // cell, hmix_del4.F90:368-385)
+    // ---- phase C: own column at level k, both tracers
+    if (inner) {
+      const MxLevel lv = lvs[k];
+      const unsigned char* fl = S.flag[sk];
+      const unsigned fself = fl[hc];
+      const unsigned fE = fself | fl[hc + 1], fW = fself | fl[hc - 1];
+      const unsigned fS = fself | fl[hc + HQX], fN = fself | fl[hc - HQX];
+      const unsigned fV = fself | flag_up;
+      const double uE = S.ou[oe], uW = S.ou[ow], vS = S.ou[os], vN = S.ou[on];
+      const double qE = S.oq[oe], qW = S.oq[ow], qS = S.oq[os], qN = S.oq[on];
+      const double wv = (double)Lk.ws[uc];
+      const double wq = wv * wv * lv.odzt * dts;       // vertical Lax-Wendroff factor
+      const bool wet = k < kz;
+      const double vit_k = wet ? 1.0 : 0.0;
+      const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
+      // masks of the second Laplacian's faces (hmix_del4.F90:626-757)
+      const bool mself = k <= S.kmt[rc] - 1;
+      const bool mE = mself && k <= S.kmt[rc + 1] - 1, mW = mself && k <= S.kmt[rc - 1] - 1;
+      const bool mS = mself && k <= S.kmt[rc + SW64] - 1, mN = mself && k <= S.kmt[rc - SW64] - 1;
+      const MxSlot& Lu = S.slot[k > 0 ? sm1 : sk];
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        ColState& st = cs[n];
+        const unsigned bit = 1u << n;
+        const double* at = Lk.at[n];
+        // Content bookkeeping.  Both cells of a face receive its centred
+        // part A = d*u with the same sign (the advective form), and the
+        // upwind / Lax-Wendroff part X = c*d with opposite signs: every face
+        // term is one f64 value formed from the same operands in both cells,
+        // weighted by tarea_r (horizontal) and odzp (vertical) in f64, so a
+        // flux leaves one cell and enters the next with weights that cancel
+        // against the cell volumes to f64 rounding.
+        const double c = at[rc];
+        const double dE = at[rc + 1] - c, dW = c - at[rc - 1];
+        const double dS = at[rc + SW64] - c, dN = c - at[rc - SW64];
+        const double Xe = ((fE & bit) ? fabs(uE) : qE) * dE;
+        const double Xw = ((fW & bit) ? fabs(uW) : qW) * dW;
+        const double Xs = ((fS & bit) ? fabs(vS) : qS) * dS;
+        const double Xn = ((fN & bit) ? fabs(vN) : qN) * dN;
+        double sh = dE * uE + dW * uW + dS * vS + dN * vN;
+        sh += (Xw - Xe) + (Xn - Xs);
+        sh *= vit_k;                                   // horizontal advection, times -tarea_r
+        // vertical: face above (k-1|k) computed here, face below carried (at
+        // the top level the level itself stands in for the missing one above:
+        // the difference and both face terms are 0)
+        const double dv = Lu.at[n][rc] - c;
+        const double Xv = ((fV & bit) ? fabs(wv) : wq) * dv;
+        const double Av = wv * dv;
+        const double sz = st.carry + (Av - Xv);
+        st.carry = Av + Xv;
+        const double vadv = -0.5 * sz * vit_k;         // vertical advection, times odzp
+        // second Laplacian as face fluxes K*(d2_R - d2_L)
         double hd = 0.0;
-        if (k <= S.kmt[rc] - 1) {
-          const float dc = S.d2[hc];
-          if (k <= S.kmt[rc + 1] - 1) hd += (double)(S.kx[hc] * (S.d2[hc + 1] - dc));
-          if (k <= S.kmt[rc - 1] - 1) hd -= (double)(S.kx[hc - 1] * (dc - S.d2[hc - 1]));
-          if (k <= S.kmt[rc + SW] - 1) hd += (double)(S.ky[hc] * (S.d2[hc + HQX] - dc));
-          if (k <= S.kmt[rc - SW] - 1) hd -= (double)(S.ky[hc - HQX] * (dc - S.d2[hc - HQX]));
+        {
+          const double* d2 = S.d2[n];
+          const double dc = d2[hc];
+          if (mE) hd += kxE * (d2[hc + 1] - dc);
+          if (mW) hd -= kxW * (dc - d2[hc - 1]);
+          if (mS) hd += kyS * (d2[hc + HQX] - dc);
+          if (mN) hd -= kyN * (dc - d2[hc - HQX]);
         }
-        const double atb_k = Lk.atb[rc];
-        const double atb_km1 = k >= 1 ? S.slot[sm1].atb[rc] : 0.0;
-        const float wkc_k = akt_here;
-        const float wkc_km1 = akt_above;
         // shortwave through the faces above and below (tracer.cpp:1430-1474)
         // and the explicit half of the vertical diffusion: each face flux is
-        // the same f32 expression in the cells above and below it, summed in f64
-        if (n == 0) {
-          if (k >= 1) vz += (double)(swv * (float)a.pen[k - 1] * vit_k);
-          if (k < km - 1) vz -= (double)(swv * (float)a.pen[k] * vit_kp1);
-        }
-        const float w1 = k >= 1 ? wkc_km1 * (float)(atb_km1 - atb_k) * (float)odzt[k] * vit_k : 0.f;
-        const float w2 = w_below;   // = wkc_k * (atb_k - atb_kp1) * odzt[k+1] * vit_kp1, as formed at level k+1
-        w_below = w1;
-        vz += 0.5 * ((double)w1 - (double)w2);
-        // surface flux and the freshwater-norm correction stay f64: the
-        // correction cancels the global salt flux, which f32 would leave at
-        // f32 precision of the flux
+        // one f64 expression in the cells above and below it
+        double vz = 0.0;
+        if (n == 0) vz = swv * lv.pu * vit_k - swv * lv.pd * vit_kp1;
+        const double atb_k = Lk.atb[n][rc];
+        const double wkc_km1 = (double)akt_above[n];
+        const double w1 = k >= 1 ? wkc_km1 * (S.slot[sm1].atb[n][rc] - atb_k) * lv.odzt * vit_k : 0.0;
+        vz += 0.5 * (w1 - st.wbelow);
+        st.wbelow = w1;
+        // surface flux and the freshwater-norm correction
         double sfc = 0.0;
         if (k == 0) {
-          if (kz > 0) sfc = stf * 0.5 * odzp[0];
-          if (n == 1) sfc += err_norm2 * (double)vit_k;
+          if (kz > 0) sfc = st.stf * 0.5 * lv.odzp;
+          if (n == 1) sfc += err_norm2 * vit_k;
         }
+        double tf = 0.0;
         if (p.boundary_restore == 1 && k >= 1)
-          tf += vit_k * (float)(a.restore[n * F + (long)k * A + qo] - atb_k) * (float)(1.0 / (15.0 * 86400.0));
-        const double d8 = c + dts * ((double)tf - trc * sh + odzp[k] * (vz + vadv) + sfc + ah64 * trc * hd);
+          tf = vit_k * (a.restore[n * F + (long)k * A + qo] - atb_k) * (1.0 / (15.0 * 86400.0));
+        const double d8 = c + dts * (tf - trc * sh + lv.odzp * (vz + vadv) + sfc + ah64 * trc * hd);
+        // one elimination step of the implicit half of the vertical
+        // diffusion (invtrit, tracer.cpp:923-978)
         double ev = 0.0, fv = d8;
-        if (k < kz) {
-          double a8, c8, b8;
-          if (k >= 1) a8 = (double)wkc_km1 * odzt[k] * odzp[k] * dts * 0.5;
-          else a8 = odzp[0] * dts * 0.5;
+        if (wet) {
+          const double wkc_k = (double)akt_here[n];
+          const double a8 = k >= 1 ? wkc_km1 * lv.ka : lv.odzp * dts * 0.5;
+          double c8, b8;
           if (k == kz - 1) {
-            c8 = odzp[kz - 1] * dts * 0.5;
+            c8 = lv.odzp * dts * 0.5;
             b8 = 1.0 + a8;
-          } else if (k >= 1) {
-            c8 = (double)wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
-            b8 = 1.0 + a8 + c8;
+            st.e = 0.0;
+            st.f = 0.0;
           } else {
-            c8 = (double)wkc_k * odzt[k + 1] * odzp[k] * dts * 0.5;
-            b8 = 1.0 + c8;
+            c8 = wkc_k * lv.kc;
+            b8 = k >= 1 ? 1.0 + a8 + c8 : 1.0 + c8;
           }
-          if (k == kz - 1) { e_prev = 0.0; f_prev = 0.0; }
-          const double g0 = 1.0 / (b8 - c8 * e_prev);
+          const double g0 = 1.0 / (b8 - c8 * st.e);
           ev = a8 * g0;
-          fv = (d8 + c8 * f_prev) * g0;
-          e_prev = ev;
-          f_prev = fv;
+          fv = (d8 + c8 * st.f) * g0;
+          st.e = ev;
+          st.f = fv;
         }
-        double* sl = scr + (long)k * 2 * MTH;
-        sl[tid] = ev;
-        sl[MTH + tid] = fv;
+        reinterpret_cast<double2*>(scr)[((long)k * 2 + n) * MTH + tid] = make_double2(ev, fv);
       }
-      akt_here = akt_above;
-      __syncthreads();
-      if (k - NSM >= 0) issue(k - NSM, sk);   // level k-3 takes level k's slot
-      // one level down: the slots of k-1, k-2, k
-      sp1 = sk;
-      sk = sm1;
-      sm1 = sk == 0 ? 2 : sk - 1;
     }
-    // substitution, top down: the elimination coefficients of SUB levels are
-    // loaded together ahead of their stores (one scratch round trip per SUB
-    // levels)
-    if (inner) {
-      double x = 0.0;
-      constexpr int SUB = 8;
-      for (int k0 = 0; k0 < km; k0 += SUB) {
-        double evs[SUB], fvs[SUB];
+    akt_here[0] = akt_above[0];
+    akt_here[1] = akt_above[1];
+    __syncthreads();
+    if (k - NSM >= 0) issue(k - NSM, sk);   // level k-3 takes level k's slot
+    // one level down: the slots of k-1, k-2, k
+    sp1 = sk;
+    sk = sm1;
+    sm1 = sk == 0 ? 2 : sk - 1;
+  }
+  // substitution, top down: the elimination coefficients of SUB levels are
+  // loaded together ahead of their stores (one scratch round trip per SUB
+  // levels)
+  if (inner) {
+    double* at_out = a.at[a.cur ^ 1];
+    double* atb_out = a.atb[a.cur ^ 1];
+    double x[2] = {0.0, 0.0};
+    constexpr int SUB = 4;
+    const double2* sc2 = reinterpret_cast<const double2*>(scr);
+    for (int k0 = 0; k0 < km; k0 += SUB) {
+      double2 ef[SUB][2];
 #pragma unroll
-        for (int c = 0; c < SUB; ++c) {
-          const double* sl = scr + (long)(k0 + c) * 2 * MTH;
-          evs[c] = k0 + c < km ? sl[tid] : 0.0;
-          fvs[c] = k0 + c < km ? sl[MTH + tid] : 0.0;
-        }
+      for (int c = 0; c < SUB; ++c)
+#pragma unroll
+        for (int n = 0; n < 2; ++n)
+          ef[c][n] = k0 + c < km ? sc2[((long)(k0 + c) * 2 + n) * MTH + tid] : make_double2(0.0, 0.0);
 #pragma unroll
       for (int c = 0; c < SUB; ++c) {
         const int k = k0 + c;
         if (k >= km) break;
-        const double ev = evs[c], fv = fvs[c];
-        double v;
-        if (k < kz) {
-          v = (k == 0) ? ev * stf + fv : ev * x + fv;
-          x = v;
-        } else {
-          v = fv;
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          const double ev = ef[c][n].x, fv = ef[c][n].y;
+          double v;
+          if (k < kz) {
+            v = (k == 0) ? ev * cs[n].stf + fv : ev * x[n] + fv;
+            x[n] = v;
+          } else {
+            v = fv;
+          }
+          at_out[n * F + (long)k * A + qo] = v;
+          atb_out[n * FB + (long)(k + 1) * A + qo] = v;
         }
-        const long cg = (long)k * A + qo;
-        at_out[cg] = v;
-        atb_out[(long)(k + 1) * A + qo] = v;
-      }
       }
     }
   }
@@ -902,51 +920,57 @@ __device__ __forceinline__ MxSmem& mixed_smem_init() {
   return S;
 }
 
+__device__ __forceinline__ MxLevel* mixed_levels() {
+  extern __shared__ __align__(128) unsigned char smem_mx[];
+  return reinterpret_cast<MxLevel*>(smem_mx + kMxLevOff);
+}
+
 __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
     k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
   MxSmem& S = mixed_smem_init();
+  MxLevel* lv = mixed_levels();
+  stage_levels(lv, a);
   uint32_t par = 0, outstanding = 0;
-  double* scr = a.col_scratch + (long)blockIdx.x * a.km * 2 * MTH;
-  for (long w = blockIdx.x; w < 2 * ntiles; w += gridDim.x)
-    if (!mixed_item<false>(S, a, maps, scr, ntx, w >> 1, (int)(w & 1), par, outstanding)) return;
+  double* scr = a.col_scratch + (long)blockIdx.x * a.km * kMixedScratchPerLevel * MTH;
+  for (long w = blockIdx.x; w < ntiles; w += gridDim.x)
+    if (!mixed_item<false>(S, lv, a, maps, scr, ntx, w, par, outstanding)) return;
 }
 
 // Several domains (ensemble members, serving requests; any sizes) in one
 // persistent launch: the work list is the concatenation of every member's
-// (tile, tracer) items, member after member, so neighbouring CTAs work on
-// neighbouring tiles of the same member.  Each CTA's items ascend, so its
-// member index only moves forward.
-// The current member's arena is copied into shared memory behind MxSmem:
-// read from there, its fields cannot alias the kernel's global stores, so
-// the compiler keeps them across the level loop instead of reloading them
-// from global memory at every level.
-constexpr size_t kBatchArenaOff = (sizeof(MxSmem) + 15) / 16 * 16;
-constexpr size_t kBatchSmem = kBatchArenaOff + sizeof(Arena);
+// tiles, member after member, so neighbouring CTAs work on neighbouring tiles
+// of the same member.  Each CTA's items ascend, so its member index only
+// moves forward.
+// The current member's arena is copied into shared memory behind the level
+// constants: read from there, its fields cannot alias the kernel's global
+// stores, so the compiler keeps them across the level loop instead of
+// reloading them from global memory at every level.
+__host__ __device__ constexpr size_t mx_batch_arena_off(int km) { return (mx_smem_bytes(km) + 15) / 16 * 16; }
+__host__ __device__ constexpr size_t mx_batch_smem(int km) { return mx_batch_arena_off(km) + sizeof(Arena); }
 static_assert(sizeof(Arena) % 16 == 0, "arena copied as 16-byte words");
-static_assert(kMixedCtasPerSm * (kBatchSmem + 1024) <= 228 * 1024,
-              "batched mixed tracer tile no longer fits kMixedCtasPerSm CTAs per SM");
 
 __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
     k_tracer_mixed_batch(const MemberDesc* __restrict__ mem, int nmem, long total, double* scratch, int km_max) {
   MxSmem& S = mixed_smem_init();
   extern __shared__ __align__(128) unsigned char smem_mx[];
-  Arena& sa = *reinterpret_cast<Arena*>(smem_mx + kBatchArenaOff);
+  MxLevel* lv = mixed_levels();
+  Arena& sa = *reinterpret_cast<Arena*>(smem_mx + mx_batch_arena_off(km_max));
   uint32_t par = 0, outstanding = 0;
-  double* scr = scratch + (long)blockIdx.x * km_max * 2 * MTH;
+  double* scr = scratch + (long)blockIdx.x * km_max * kMixedScratchPerLevel * MTH;
   int m = 0, staged = -1;
   for (long w = blockIdx.x; w < total; w += gridDim.x) {
     while (m + 1 < nmem && mem[m + 1].item0 <= w) ++m;
     const MemberDesc& d = mem[m];
     if (m != staged) {
-      __syncthreads();   // the previous item no longer reads the staged arena
+      __syncthreads();   // the previous item no longer reads the staged arena or levels
       const uint4* src = reinterpret_cast<const uint4*>(&d.a);
       uint4* dst = reinterpret_cast<uint4*>(&sa);
       for (int t = threadIdx.x; t < (int)(sizeof(Arena) / 16); t += MTH) dst[t] = src[t];
       __syncthreads();
+      stage_levels(lv, sa);
       staged = m;
     }
-    const long local = w - d.item0;
-    if (!mixed_item<true>(S, sa, d.maps, scr, d.ntx, local >> 1, (int)(local & 1), par, outstanding)) return;
+    if (!mixed_item<true>(S, lv, sa, d.maps, scr, d.ntx, w - d.item0, par, outstanding)) return;
   }
 }
 
@@ -955,11 +979,14 @@ __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
 int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid) {
   const int ntx = (a.imt + TX - 1) / TX;
   const long ntiles = (long)ntx * ((a.jmt + MY - 1) / MY);
-  const size_t sm = sizeof(MxSmem);
-  static bool attr = false;
-  if (!attr) {
-    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    attr = true;
+  const size_t sm = mx_smem_bytes(a.km);
+  static int attr_dev = -1;
+  int dev = 0;
+  LT_CUDA_OK(cudaGetDevice(&dev));
+  if (attr_dev != dev) {
+    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)mx_smem_bytes(256)));
+    attr_dev = dev;
   }
   k_tracer_mixed<<<grid, MTH, sm, s>>>(a, maps, ntx, ntiles);
   LT_LAUNCHED();
@@ -968,7 +995,7 @@ int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t
 
 int prepare_tracer_mixed_batch() {
   LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kBatchSmem));
+                                  (int)mx_batch_smem(256)));
   return LT_OK;
 }
 
@@ -976,7 +1003,7 @@ int prepare_tracer_mixed_batch() {
 // inside a stream capture)
 int launch_tracer_mixed_batch(const MemberDesc* mem, int nmem, long total, double* scratch, int km_max, int grid,
                               cudaStream_t s) {
-  k_tracer_mixed_batch<<<grid, MTH, kBatchSmem, s>>>(mem, nmem, total, scratch, km_max);
+  k_tracer_mixed_batch<<<grid, MTH, mx_batch_smem(km_max), s>>>(mem, nmem, total, scratch, km_max);
   LT_LAUNCHED();
   return LT_OK;
 }

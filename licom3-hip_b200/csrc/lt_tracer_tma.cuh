@@ -120,7 +120,7 @@ __device__ __forceinline__ void load_tile_statics(SM& S, const Arena& a, int x0,
 struct alignas(64) MemberDesc {
   TracerMaps maps;
   Arena a;
-  long item0;    // first (tile, tracer) work item of this member in the batch list
+  long item0;    // first work item (a tile, both tracers) of this member in the batch list
   long ntiles;   // column tiles of this member
   int ntx;       // tiles along i
 };

@@ -38,7 +38,7 @@ def test_batch_equals_members_stepped_alone(lt, precision):
     b.close()
 
 
-@pytest.mark.parametrize("ctas,tile_y,graph", [(3, 8, 1), (2, 8, 1), (2, 4, 1), (1, 16, 1), (3, 16, 0), (1, 8, 0)])
+@pytest.mark.parametrize("ctas,tile_y,graph", [(2, 8, 1), (2, 4, 1), (1, 16, 1), (2, 16, 0), (1, 8, 0)])
 def test_every_launch_shape_gives_the_same_bits(lt, ctas, tile_y, graph):
     syns, doms = members(lt, lt.PREC_MIXED, seed0=5)
     ref = [s.domain(precision=lt.PREC_MIXED) for s in syns]
@@ -81,7 +81,7 @@ def test_autotune_keeps_the_state(lt):
     b = lt.Batch(doms)
     cfg = b.autotune(trial_steps=1)
     assert cfg == b.config()
-    assert cfg["column_ctas_per_sm"] in (1, 2, 3) and cfg["continuity_tile_y"] in (4, 8, 16)
+    assert cfg["column_ctas_per_sm"] in (1, 2) and cfg["continuity_tile_y"] in (4, 8, 16)
     b.step(2)
     b.sync()
     assert_same(doms, ref)
