@@ -99,10 +99,12 @@ typedef enum {
   LT_F_COUNT
 } lt_field;
 
-/* Precision of the step arithmetic.  The state is always f64. */
+/* Precision of the step arithmetic.  The state is always f64.  A mixed
+ * domain stores its dynamics inputs and mixing in f32 and takes at most 128
+ * levels (its per-level constants stay in shared memory). */
 typedef enum {
   LT_PREC_FP64 = 0,   /* plain f64 drop-in: the correctness form */
-  LT_PREC_MIXED = 1   /* f32 flux/stencil/diffusion arithmetic, f64 state and sums */
+  LT_PREC_MIXED = 1   /* f32 storage of the dynamics inputs, f32 predictor, f64 state, fluxes and sums */
 } lt_precision;
 
 typedef struct {

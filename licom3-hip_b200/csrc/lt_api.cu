@@ -168,8 +168,9 @@ bool grid_ok(const lt_grid* g) {
   if (g->nx < 8 || g->ny < 8 || g->km < 3 || g->km > 256) return false;
   if (g->tripole && (g->nx % 2)) return false;
   if (g->precision != LT_PREC_FP64 && g->precision != LT_PREC_MIXED) return false;
-  // the mixed kernel takes its f32 fields by TMA: row pitch a multiple of 16 bytes
-  if (g->precision == LT_PREC_MIXED && ((g->nx + 4) % 4)) return false;
+  // the mixed kernel takes its f32 fields by TMA: row pitch a multiple of 16
+  // bytes; its per-level constants live in shared memory: at most 128 levels
+  if (g->precision == LT_PREC_MIXED && (((g->nx + 4) % 4) || g->km > kMixedMaxLevels)) return false;
   return true;
 }
 

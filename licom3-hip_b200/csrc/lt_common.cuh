@@ -27,6 +27,7 @@ constexpr int kMixedTileY = 8;
 constexpr int kMixedThreads = TX * kMixedTileY;
 constexpr int kMixedBoxW64 = TX + 4;
 constexpr int kMixedScratchPerLevel = 4;
+constexpr int kMixedMaxLevels = 128;
 
 // Everything the step kernels touch, as raw device pointers (dense
 // [n][k][j][i] layout of the reference, i fastest).

@@ -282,10 +282,11 @@ struct alignas(128) MxSlot {
   alignas(128) float ws[(MY + 2) * SW];          // rows y0-1 .. y0+MY
   alignas(128) float wkd[(MY + 3) * SW];         // rows y0-2 .. y0+MY
   alignas(128) float wkb[(MY + 3) * SW];         // rows y0-2 .. y0+MY
+  alignas(128) float akt[2][TX * MY];            // mixing coefficient of the tile's columns (T, S)
 };
 static_assert(((MY + 4) * SW64 * sizeof(double)) % 128 == 0, "each tracer's box starts 128-byte aligned");
 constexpr uint32_t kMxLevelBytes =
-    (uint32_t)(4 * (MY + 4) * SW64 * sizeof(double) + ((MY + 2) * SW + 2 * (MY + 3) * SW) * sizeof(float));
+    (uint32_t)(4 * (MY + 4) * SW64 * sizeof(double) + ((MY + 2) * SW + 2 * (MY + 3) * SW + 2 * TX * MY) * sizeof(float));
 
 // per-level constants of the march (the 1-D vertical grid)
 struct MxLevel {
@@ -312,8 +313,8 @@ struct MxSmem {
 constexpr size_t kMxLevOff = (sizeof(MxSmem) + 15) / 16 * 16;
 __host__ __device__ constexpr size_t mx_smem_bytes(int km) { return kMxLevOff + (size_t)km * sizeof(MxLevel); }
 // kMixedCtasPerSm CTAs per SM: 228 KB of shared memory, 1 KB of it reserved
-// per CTA; the largest km the grid check allows must still fit
-static_assert(kMixedCtasPerSm * (mx_smem_bytes(256) + sizeof(Arena) + 16 + 1024) <= 228 * 1024,
+// per CTA; the largest km a mixed domain may have must still fit
+static_assert(kMixedCtasPerSm * (mx_smem_bytes(kMixedMaxLevels) + sizeof(Arena) + 16 + 1024) <= 228 * 1024,
               "mixed tracer tile no longer fits kMixedCtasPerSm CTAs per SM");
 
 // x face (fj, fi): row y0-1+fj, west side of column x0-1+fi
@@ -336,6 +337,8 @@ __device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const Tracer
   tma_load_3d(sl.ws, &m.ws, x0 - 4, y0 - 1, L, bar);
   tma_load_3d(sl.wkd, &m.uw, x0 - 4, y0 - 2, L, bar);
   tma_load_3d(sl.wkb, &m.vs, x0 - 4, y0 - 2, L, bar);
+  tma_load_3d(sl.akt[0], &m.akt, x0, y0, L, bar);
+  tma_load_3d(sl.akt[1], &m.akt, x0, y0, km + L, bar);
 }
 
 // ---- f32 faces of the 1-halo region (the predictor's level)
@@ -695,11 +698,6 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
   ColState cs[2];
   cs[0] = {0.0, 0.0, 0.0, 0.0, own ? a.stf_n[qo] : 0.0};
   cs[1] = {0.0, 0.0, 0.0, 0.0, own ? a.stf_n[A + qo] : 0.0};
-  // own column's mixing coefficients: level k in akt_here, level k-1 loaded a step ahead
-  const float* akt_col = a.akt32 + qo;
-  float akt_here[2];
-  akt_here[0] = inner ? __ldg(akt_col + (long)(km - 1) * A) : 0.f;
-  akt_here[1] = inner ? __ldg(akt_col + F + (long)(km - 1) * A) : 0.f;
 
   // slots of levels k, k-1, k+1 (NSM == 3: level k-2 shares k+1's)
   static_assert(NSM == 3, "slot rotation below assumes three slots");
@@ -724,9 +722,6 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
 
   // Level slots: after step k the slot of level k takes level k-NSM.
   for (int k = km - 1; k >= 0; --k) {
-    float akt_above[2];
-    akt_above[0] = (inner && k >= 1) ? __ldg(akt_col + (long)(k - 1) * A) : 0.f;
-    akt_above[1] = (inner && k >= 1) ? __ldg(akt_col + F + (long)(k - 1) * A) : 0.f;
     // ---- phase B1: f32 faces one level up (the predictor's), the tile's f64
     // faces and the first Laplacian here (levels k-1, k arrived in earlier
     // steps; the previous step ended with a barrier)
@@ -822,7 +817,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
         double vz = 0.0;
         if (n == 0) vz = swv * lv.pu * vit_k - swv * lv.pd * vit_kp1;
         const double atb_k = Lk.atb[n][rc];
-        const double wkc_km1 = (double)akt_above[n];
+        const double wkc_km1 = k >= 1 ? (double)S.slot[sm1].akt[n][tid] : 0.0;
         const double w1 = k >= 1 ? wkc_km1 * (S.slot[sm1].atb[n][rc] - atb_k) * lv.odzt * vit_k : 0.0;
         vz += 0.5 * (w1 - st.wbelow);
         st.wbelow = w1;
@@ -838,9 +833,8 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
         const double d8 = c + dts * (tf - trc * sh + lv.odzp * (vz + vadv) + sfc + ah64 * trc * hd);
         // one elimination step of the implicit half of the vertical
         // diffusion (invtrit, tracer.cpp:923-978)
-        double ev = 0.0, fv = d8;
         if (wet) {
-          const double wkc_k = (double)akt_here[n];
+          const double wkc_k = (double)Lk.akt[n][tid];
           const double a8 = k >= 1 ? wkc_km1 * lv.ka : lv.odzp * dts * 0.5;
           double c8, b8;
           if (k == kz - 1) {
@@ -853,16 +847,17 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
             b8 = k >= 1 ? 1.0 + a8 + c8 : 1.0 + c8;
           }
           const double g0 = 1.0 / (b8 - c8 * st.e);
-          ev = a8 * g0;
-          fv = (d8 + c8 * st.f) * g0;
-          st.e = ev;
-          st.f = fv;
+          st.e = a8 * g0;
+          st.f = (d8 + c8 * st.f) * g0;
+          reinterpret_cast<double2*>(scr)[((long)k * 2 + n) * MTH + tid] = make_double2(st.e, st.f);
+        } else {
+          // below the column's bottom the sweep leaves the explicit value:
+          // stored at once, the sweep's scratch holds the wet levels only
+          a.at[a.cur ^ 1][n * F + (long)k * A + qo] = d8;
+          a.atb[a.cur ^ 1][n * FB + (long)(k + 1) * A + qo] = d8;
         }
-        reinterpret_cast<double2*>(scr)[((long)k * 2 + n) * MTH + tid] = make_double2(ev, fv);
       }
     }
-    akt_here[0] = akt_above[0];
-    akt_here[1] = akt_above[1];
     __syncthreads();
     if (k - NSM >= 0) issue(k - NSM, sk);   // level k-3 takes level k's slot
     // one level down: the slots of k-1, k-2, k
@@ -870,36 +865,30 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
     sk = sm1;
     sm1 = sk == 0 ? 2 : sk - 1;
   }
-  // substitution, top down: the elimination coefficients of SUB levels are
-  // loaded together ahead of their stores (one scratch round trip per SUB
-  // levels)
+  // substitution, top down through the wet levels: the elimination
+  // coefficients of SUB levels are loaded together ahead of their stores (one
+  // scratch round trip per SUB levels)
   if (inner) {
     double* at_out = a.at[a.cur ^ 1];
     double* atb_out = a.atb[a.cur ^ 1];
     double x[2] = {0.0, 0.0};
     constexpr int SUB = 4;
     const double2* sc2 = reinterpret_cast<const double2*>(scr);
-    for (int k0 = 0; k0 < km; k0 += SUB) {
+    for (int k0 = 0; k0 < kz; k0 += SUB) {
       double2 ef[SUB][2];
 #pragma unroll
       for (int c = 0; c < SUB; ++c)
 #pragma unroll
         for (int n = 0; n < 2; ++n)
-          ef[c][n] = k0 + c < km ? sc2[((long)(k0 + c) * 2 + n) * MTH + tid] : make_double2(0.0, 0.0);
+          ef[c][n] = k0 + c < kz ? sc2[((long)(k0 + c) * 2 + n) * MTH + tid] : make_double2(0.0, 0.0);
 #pragma unroll
       for (int c = 0; c < SUB; ++c) {
         const int k = k0 + c;
-        if (k >= km) break;
+        if (k >= kz) break;
 #pragma unroll
         for (int n = 0; n < 2; ++n) {
-          const double ev = ef[c][n].x, fv = ef[c][n].y;
-          double v;
-          if (k < kz) {
-            v = (k == 0) ? ev * cs[n].stf + fv : ev * x[n] + fv;
-            x[n] = v;
-          } else {
-            v = fv;
-          }
+          const double v = (k == 0) ? ef[c][n].x * cs[n].stf + ef[c][n].y : ef[c][n].x * x[n] + ef[c][n].y;
+          x[n] = v;
           at_out[n * F + (long)k * A + qo] = v;
           atb_out[n * FB + (long)(k + 1) * A + qo] = v;
         }
@@ -985,7 +974,7 @@ int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t
   LT_CUDA_OK(cudaGetDevice(&dev));
   if (attr_dev != dev) {
     LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)mx_smem_bytes(256)));
+                                    (int)mx_smem_bytes(kMixedMaxLevels)));
     attr_dev = dev;
   }
   k_tracer_mixed<<<grid, MTH, sm, s>>>(a, maps, ntx, ntiles);
@@ -995,7 +984,7 @@ int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t
 
 int prepare_tracer_mixed_batch() {
   LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_mixed_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)mx_batch_smem(256)));
+                                  (int)mx_batch_smem(kMixedMaxLevels)));
   return LT_OK;
 }
 
