@@ -388,7 +388,6 @@ __device__ __forceinline__ void face_f32(MxSmem& S, const MxSlot& L, int kk, con
 // of rows 0, MY+1, MY+2 (all TX+2 columns), y faces of rows 1..MY at columns
 // 0 and TX+1
 constexpr int F_EXTRA = FN - 2 * TX * MY;
-static_assert(F_EXTRA <= MTH, "border faces: at most one per thread");
 
 __device__ __forceinline__ FaceRef border_face(int q) {
   if (q < 2 * (TX + 3)) return face_x_ref(q < TX + 3 ? 0 : MY + 1, q % (TX + 3));
@@ -434,7 +433,7 @@ __device__ __forceinline__ void face_f64(MxSmem& S, const MxSlot& L, const OwnFa
 // region, box indices (f64 boxes r, ws box u), its west x face and north y
 // face; valid: inside the rows and columns the reference computes
 // (1 .. imt-2, 1 .. jmt-2).  Every thread owns the interior cell above its
-// column; the ring cells of the region go to threads 0 .. RING-1, one each.
+// column; the ring cells of the region go to the last RING threads, one each.
 struct HCell {
   int m, r, u, fw, fn;
   bool valid;
@@ -482,8 +481,9 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 // whose differences are then 0, and so are the vertical terms they carry).
 __device__ __forceinline__ unsigned pred_cell(const MxSmem& S, const HCell& h, int kk, int km, int sc, int su,
                                               int sd, const MxLevel& lv, float dts) {
-  if (!h.valid) return 0u;
   const int r = h.r;
+  // land cells need no flag: every face of a land cell carries no transport
+  if (!h.valid || kk >= S.kmt[r]) return 0u;
   const int fe = h.fw + 1, fw = h.fw, fs = h.fn + HQX, fn = h.fn;
   const float2 de = S.fd[fe], dw = S.fd[fw], ds = S.fd[fs], dn = S.fd[fn];
   // east face: this cell is the lower one, d*(u - q); west face: upper, d*(u + q)
@@ -621,6 +621,9 @@ struct ColState {
   double stf;       // surface flux
 };
 
+// the thread that issues the level boxes (in a warp with a single border face)
+constexpr int kIssueThread = 4 * TX;
+
 // One work item (a tile, both tracers) of the mixed column march.  Returns
 // false if a level wait gave up: the CTA has then recorded the timeout and
 // drained its boxes, and must return.
@@ -640,7 +643,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
   __syncthreads();   // the previous item no longer reads the slots or the tile data
   // level L goes to slot s = L % NSM
   auto issue = [&](int L, int s) {
-    if (tid == 0) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, km, L, x0, y0);
+    if (tid == kIssueThread) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, km, L, x0, y0);
     outstanding |= 1u << s;
   };
   auto wait = [&](int s) -> bool {
@@ -658,25 +661,37 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
   const int hc = (ty + 1) * HQX + (tx + 1);
   const int rc = b64(ty + 1, tx + 1), uc = bws(ty + 1, tx + 1);
   const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
-  const bool has_ring = tid < RING;
-  const HCell ring_cell = ring_hcell(has_ring ? tid : 0, x0, y0, imt, jmt);
+  // The region's extra cells and faces are spread so that no warp carries
+  // much more than the others between two barriers: the ring cells (first
+  // Laplacian and predictor) go to the last warps, the border faces to the
+  // first ones (two per thread where needed), the TMA issue to a thread of a
+  // warp with a single border face.
+  const bool has_ring = tid >= MTH - RING;
+  const HCell ring_cell = ring_hcell(has_ring ? tid - (MTH - RING) : 0, x0, y0, imt, jmt);
   // f32 faces: the own cell's west x face and north y face, and one border face
   const FaceRef fo_x = face_x_ref(ty + 1, tx + 1), fo_y = face_y_ref(ty + 1, tx + 1);
-  const bool has_fb = tid < F_EXTRA;
+  constexpr int kFaceThreads = MTH - RING - (MTH - RING) % TX;   // the warps without ring cells
+  static_assert(F_EXTRA <= 2 * kFaceThreads, "border faces: at most two per thread");
+  const bool has_fb = tid < kFaceThreads && tid < F_EXTRA;
+  const bool has_fb2 = tid < F_EXTRA - kFaceThreads;
   const FaceRef fo_b = border_face(has_fb ? tid : 0);
+  const FaceRef fo_b2 = border_face(has_fb2 ? tid + kFaceThreads : 0);
   // f64 faces of the tile: the own cell's west and north faces, and the east
-  // column's x faces (threads 0 .. MY-1) and the bottom row's y faces
-  // (threads MY .. MY+TX-1)
+  // column's x faces and the bottom row's y faces (threads kOwnB .. kOwnB+MY-1
+  // and kOwnB+MY .. kOwnB+MY+TX-1, in warps with a single border face)
   auto hval = [&](const double* h, int gj, int gi) {
     return (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? h[(long)gj * imt + gi] : 0.0;
   };
   const OwnFace of_x = {ox(ty, tx), b32(ty, tx + 1), fx(ty + 1, tx + 1), true, hval(a.htw, j, i)};
   const OwnFace of_y = {oy(ty, tx), b32(ty, tx + 1), fy(ty + 1, tx + 1), false, hval(a.hts, j - 1, i)};
-  const bool has_ob = tid < MY + TX;
+  constexpr int kOwnB = 2 * TX;
+  static_assert(F_EXTRA - kFaceThreads <= kOwnB && kOwnB + MY + TX <= kFaceThreads, "f64 border faces");
+  const int tb = tid - kOwnB;
+  const bool has_ob = tb >= 0 && tb < MY + TX;
   OwnFace of_b;
-  if (tid < MY) of_b = {ox(tid, TX), b32(tid, TX + 1), fx(tid + 1, TX + 1), true, hval(a.htw, y0 + tid, x0 + TX)};
-  else if (has_ob) of_b = {oy(MY, tid - MY), b32(MY, tid - MY + 1), fy(MY + 1, tid - MY + 1), false,
-                           hval(a.hts, y0 + MY - 1, x0 + tid - MY)};
+  if (tb >= 0 && tb < MY) of_b = {ox(tb, TX), b32(tb, TX + 1), fx(tb + 1, TX + 1), true, hval(a.htw, y0 + tb, x0 + TX)};
+  else if (has_ob) of_b = {oy(MY, tb - MY), b32(MY, tb - MY + 1), fy(MY + 1, tb - MY + 1), false,
+                           hval(a.hts, y0 + MY - 1, x0 + tb - MY)};
   else of_b = of_x;
   const int oe = ox(ty, tx + 1), ow = ox(ty, tx), os = oy(ty + 1, tx), on = oy(ty, tx);
   // second Laplacian face weights K = tarea*dte (x faces), tarea*dts (y faces)
@@ -712,6 +727,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
     face_f32(S, L, km - 1, fo_x);
     face_f32(S, L, km - 1, fo_y);
     if (has_fb) face_f32(S, L, km - 1, fo_b);
+    if (has_fb2) face_f32(S, L, km - 1, fo_b2);
   }
   __syncthreads();
   {
@@ -731,6 +747,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
       face_f32(S, Lu, k - 1, fo_x);
       face_f32(S, Lu, k - 1, fo_y);
       if (has_fb) face_f32(S, Lu, k - 1, fo_b);
+      if (has_fb2) face_f32(S, Lu, k - 1, fo_b2);
     }
     face_f64(S, Lk, of_x);
     face_f64(S, Lk, of_y);
@@ -750,8 +767,19 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
       S.flag[sm1][own_cell.m] = (unsigned char)flag_up;
       if (has_ring) S.flag[sm1][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, k - 1, km, sm1, sp1, sk, lv, dtsf);
     }
-    // ---- phase C: own column at level k, both tracers
-    if (inner) {
+    // ---- phase C: own column at level k, both tracers.  Below the column's
+    // bottom every term of the step is masked (vit = 0): the new value is the
+    // old one and no face flux leaves the level.
+    if (inner && k >= kz) {
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const double c = Lk.at[n][rc];
+        a.at[a.cur ^ 1][n * F + (long)k * A + qo] = c;
+        a.atb[a.cur ^ 1][n * FB + (long)(k + 1) * A + qo] = c;
+        cs[n].carry = 0.0;
+        cs[n].wbelow = 0.0;
+      }
+    } else if (inner) {
       const MxLevel lv = lvs[k];
       const unsigned char* fl = S.flag[sk];
       const unsigned fself = fl[hc];
@@ -762,8 +790,6 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
       const double qE = S.oq[oe], qW = S.oq[ow], qS = S.oq[os], qN = S.oq[on];
       const double wv = (double)Lk.ws[uc];
       const double wq = wv * wv * lv.odzt * dts;       // vertical Lax-Wendroff factor
-      const bool wet = k < kz;
-      const double vit_k = wet ? 1.0 : 0.0;
       const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
       // masks of the second Laplacian's faces (hmix_del4.F90:626-757)
       const bool mself = k <= S.kmt[rc] - 1;
@@ -791,7 +817,6 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
         const double Xn = ((fN & bit) ? fabs(vN) : qN) * dN;
         double sh = dE * uE + dW * uW + dS * vS + dN * vN;
         sh += (Xw - Xe) + (Xn - Xs);
-        sh *= vit_k;                                   // horizontal advection, times -tarea_r
         // vertical: face above (k-1|k) computed here, face below carried (at
         // the top level the level itself stands in for the missing one above:
         // the difference and both face terms are 0)
@@ -800,7 +825,7 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
         const double Av = wv * dv;
         const double sz = st.carry + (Av - Xv);
         st.carry = Av + Xv;
-        const double vadv = -0.5 * sz * vit_k;         // vertical advection, times odzp
+        const double vadv = -0.5 * sz;                 // vertical advection, times odzp
         // second Laplacian as face fluxes K*(d2_R - d2_L)
         double hd = 0.0;
         {
@@ -815,25 +840,25 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
         // and the explicit half of the vertical diffusion: each face flux is
         // one f64 expression in the cells above and below it
         double vz = 0.0;
-        if (n == 0) vz = swv * lv.pu * vit_k - swv * lv.pd * vit_kp1;
+        if (n == 0) vz = swv * lv.pu - swv * lv.pd * vit_kp1;
         const double atb_k = Lk.atb[n][rc];
         const double wkc_km1 = k >= 1 ? (double)S.slot[sm1].akt[n][tid] : 0.0;
-        const double w1 = k >= 1 ? wkc_km1 * (S.slot[sm1].atb[n][rc] - atb_k) * lv.odzt * vit_k : 0.0;
+        const double w1 = k >= 1 ? wkc_km1 * (S.slot[sm1].atb[n][rc] - atb_k) * lv.odzt : 0.0;
         vz += 0.5 * (w1 - st.wbelow);
         st.wbelow = w1;
         // surface flux and the freshwater-norm correction
         double sfc = 0.0;
         if (k == 0) {
-          if (kz > 0) sfc = st.stf * 0.5 * lv.odzp;
-          if (n == 1) sfc += err_norm2 * vit_k;
+          sfc = st.stf * 0.5 * lv.odzp;
+          if (n == 1) sfc += err_norm2;
         }
         double tf = 0.0;
         if (p.boundary_restore == 1 && k >= 1)
-          tf = vit_k * (a.restore[n * F + (long)k * A + qo] - atb_k) * (1.0 / (15.0 * 86400.0));
+          tf = (a.restore[n * F + (long)k * A + qo] - atb_k) * (1.0 / (15.0 * 86400.0));
         const double d8 = c + dts * (tf - trc * sh + lv.odzp * (vz + vadv) + sfc + ah64 * trc * hd);
         // one elimination step of the implicit half of the vertical
         // diffusion (invtrit, tracer.cpp:923-978)
-        if (wet) {
+        {
           const double wkc_k = (double)Lk.akt[n][tid];
           const double a8 = k >= 1 ? wkc_km1 * lv.ka : lv.odzp * dts * 0.5;
           double c8, b8;
@@ -850,11 +875,6 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
           st.e = a8 * g0;
           st.f = (d8 + c8 * st.f) * g0;
           reinterpret_cast<double2*>(scr)[((long)k * 2 + n) * MTH + tid] = make_double2(st.e, st.f);
-        } else {
-          // below the column's bottom the sweep leaves the explicit value:
-          // stored at once, the sweep's scratch holds the wet levels only
-          a.at[a.cur ^ 1][n * F + (long)k * A + qo] = d8;
-          a.atb[a.cur ^ 1][n * FB + (long)(k + 1) * A + qo] = d8;
         }
       }
     }
