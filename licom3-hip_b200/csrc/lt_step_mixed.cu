@@ -307,6 +307,7 @@ struct MxSmem {
   float cf[FN];                        // 2*dts/(htw*hun) at x faces, 2*dts/(hts*hue) at y faces
   float hw[FN];                        // htw at x faces, hts at y faces
   uint16_t kmt[(MY + 4) * SW64];       // bottom level of the tile's columns and their 2-cell halo
+  int wmax[MTH / 32];                  // per-warp maxima of the region's bottom level
   uint64_t bar[NSM];
 };
 // followed by the km level constants (dynamic shared memory)
@@ -544,16 +545,16 @@ __device__ __forceinline__ void d2_cell(MxSmem& S, const MxSlot& L, int kk, cons
   S.d2[1][m] = vS;
 }
 
-// Per-tile 2-D data of the march (kmt with a 2-cell halo, the metric and
-// biharmonic terms of the 1-halo region, the face factors).  kLoadsAhead:
+// Per-tile 2-D data of the march: kmt with a 2-cell halo (stage_kmt), the
+// metric and biharmonic terms of the 1-halo region and the face factors
+// (stage_tile).  kLoadsAhead:
 // fixed trip counts and read-only loads, so a thread's loads of a loop are in
 // flight together (the batched kernel, whose short work items change member
 // often, stages its tiles this way).
 template <bool kLoadsAhead>
-__device__ __forceinline__ void stage_tile(MxSmem& S, const Arena& a, int x0, int y0, double dts) {
+__device__ __forceinline__ void stage_kmt(MxSmem& S, const Arena& a, int x0, int y0) {
   const int tid = threadIdx.x;
   const int imt = a.imt, jmt = a.jmt;
-  auto ld = [&](const double* p) { return kLoadsAhead ? __ldg(p) : *p; };
 #pragma unroll
   for (int it = 0; it < ((MY + 4) * SW64 + MTH - 1) / MTH; ++it) {
     const int m = tid + it * MTH;
@@ -563,6 +564,13 @@ __device__ __forceinline__ void stage_tile(MxSmem& S, const Arena& a, int x0, in
       S.kmt[m] = in ? (uint16_t)(kLoadsAhead ? __ldg(a.kmt + (long)gj * imt + gi) : a.kmt[(long)gj * imt + gi]) : 0;
     }
   }
+}
+
+template <bool kLoadsAhead>
+__device__ __forceinline__ void stage_tile(MxSmem& S, const Arena& a, int x0, int y0, double dts) {
+  const int tid = threadIdx.x;
+  const int imt = a.imt, jmt = a.jmt;
+  auto ld = [&](const double* p) { return kLoadsAhead ? __ldg(p) : *p; };
 #pragma unroll
   for (int it = 0; it < (MHN + MTH - 1) / MTH; ++it) {
     const int m = tid + it * MTH;
@@ -651,23 +659,57 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
     if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
     return ok;
   };
-  for (int L = km - 1; L >= (km - NSM > 0 ? km - NSM : 0); --L) issue(L, L % NSM);
-  stage_tile<kLoadsAhead>(S, a, x0, y0, dts);
-
   const bool own = i < imt && j < jmt;
   const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
   const long qo = own ? (long)j * imt + i : 0;
-  const int kz = own ? a.kmt[qo] : 0;
   const int hc = (ty + 1) * HQX + (tx + 1);
   const int rc = b64(ty + 1, tx + 1), uc = bws(ty + 1, tx + 1);
   const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
+  const bool has_ring = tid >= MTH - RING;
+  const HCell ring_cell = ring_hcell(has_ring ? tid - (MTH - RING) : 0, x0, y0, imt, jmt);
+  // Levels at and below the deepest bottom of the 1-halo region are land for
+  // every cell the march touches there: the step leaves them as they are.
+  // The march starts at the first of them (or the bottom level), and the
+  // inner cells' values below it are copied.
+  stage_kmt<kLoadsAhead>(S, a, x0, y0);
+  __syncthreads();
+  int kmax = max((int)S.kmt[own_cell.r], has_ring ? (int)S.kmt[ring_cell.r] : 0);
+  kmax = __reduce_max_sync(0xffffffffu, kmax);
+  if (tx == 0) S.wmax[ty] = kmax;
+  __syncthreads();
+#pragma unroll
+  for (int w = 0; w < MTH / 32; ++w) kmax = max(kmax, S.wmax[w]);
+  const int ks = min(km - 1, kmax);   // the march's first (deepest) level
+  for (int L = ks; L >= (ks - NSM + 1 > 0 ? ks - NSM + 1 : 0); --L) issue(L, L % NSM);
+  stage_tile<kLoadsAhead>(S, a, x0, y0, dts);
+  if (inner) {
+    // eight levels' loads in flight ahead of their stores
+    const double* __restrict__ at_in = a.at[a.cur];
+    double* __restrict__ at_out = a.at[a.cur ^ 1];
+    double* __restrict__ atb_out = a.atb[a.cur ^ 1];
+    for (int k0 = ks + 1; k0 < km; k0 += 8) {
+      double v[8][2];
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) v[c][n] = k0 + c < km ? at_in[n * F + (long)(k0 + c) * A + qo] : 0.0;
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (k0 + c < km)
+#pragma unroll
+          for (int n = 0; n < 2; ++n) {
+            at_out[n * F + (long)(k0 + c) * A + qo] = v[c][n];
+            atb_out[n * FB + (long)(k0 + c + 1) * A + qo] = v[c][n];
+          }
+    }
+  }
+
+  const int kz = own ? a.kmt[qo] : 0;
   // The region's extra cells and faces are spread so that no warp carries
   // much more than the others between two barriers: the ring cells (first
   // Laplacian and predictor) go to the last warps, the border faces to the
   // first ones (two per thread where needed), the TMA issue to a thread of a
   // warp with a single border face.
-  const bool has_ring = tid >= MTH - RING;
-  const HCell ring_cell = ring_hcell(has_ring ? tid - (MTH - RING) : 0, x0, y0, imt, jmt);
   // f32 faces: the own cell's west x face and north y face, and one border face
   const FaceRef fo_x = face_x_ref(ty + 1, tx + 1), fo_y = face_y_ref(ty + 1, tx + 1);
   constexpr int kFaceThreads = MTH - RING - (MTH - RING) % TX;   // the warps without ring cells
@@ -716,28 +758,30 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
 
   // slots of levels k, k-1, k+1 (NSM == 3: level k-2 shares k+1's)
   static_assert(NSM == 3, "slot rotation below assumes three slots");
-  int sk = (km - 1) % NSM;
+  // (below ks the slot of level ks+1 holds nothing of this tile: the
+  // predictor of level ks, a land level everywhere, does not read it)
+  int sk = ks % NSM;
   int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
   {
-    const bool ok = wait(sk) && wait(sm1);
+    const bool ok = wait(sk) && (ks == 0 || wait(sm1));
     if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
   }
   {
     const MxSlot& L = S.slot[sk];
-    face_f32(S, L, km - 1, fo_x);
-    face_f32(S, L, km - 1, fo_y);
-    if (has_fb) face_f32(S, L, km - 1, fo_b);
-    if (has_fb2) face_f32(S, L, km - 1, fo_b2);
+    face_f32(S, L, ks, fo_x);
+    face_f32(S, L, ks, fo_y);
+    if (has_fb) face_f32(S, L, ks, fo_b);
+    if (has_fb2) face_f32(S, L, ks, fo_b2);
   }
   __syncthreads();
   {
-    const MxLevel lv = lvs[km - 1];
-    S.flag[sk][own_cell.m] = (unsigned char)pred_cell(S, own_cell, km - 1, km, sk, sm1, sp1, lv, dtsf);
-    if (has_ring) S.flag[sk][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, km - 1, km, sk, sm1, sp1, lv, dtsf);
+    const MxLevel lv = lvs[ks];
+    S.flag[sk][own_cell.m] = (unsigned char)pred_cell(S, own_cell, ks, km, sk, sm1, sp1, lv, dtsf);
+    if (has_ring) S.flag[sk][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, ks, km, sk, sm1, sp1, lv, dtsf);
   }
 
   // Level slots: after step k the slot of level k takes level k-NSM.
-  for (int k = km - 1; k >= 0; --k) {
+  for (int k = ks; k >= 0; --k) {
     // ---- phase B1: f32 faces one level up (the predictor's), the tile's f64
     // faces and the first Laplacian here (levels k-1, k arrived in earlier
     // steps; the previous step ended with a barrier)
