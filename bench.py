@@ -470,7 +470,7 @@ def measure_readyc(lt, args, precision):
     with the stand-in closure tables, and the momentum biharmonic friction
     (lt_hdiffu_del4).  Device time per launch over 10 launches after 3
     untimed ones."""
-    sys.path.insert(0, PKG_DIR)
+    sys.path.insert(0, os.path.join(REPO, "tests"))   # the stand-in closure and friction inputs
     import turb_synth
     nx, ny, km = 720, 460, 55
     w = workload(args)

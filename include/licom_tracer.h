@@ -273,8 +273,9 @@ int lt_tracer_content(lt_domain* dom, double* out2);
  * every GPU that loads it until exit), which caps nx*ny*km at about 5.3e8
  * cells; larger sizes return LT_E_INVALID.  All calls share that array, so
  * calls that overlap on the GPU race.  The first call on each device looks up
- * the array's address and should come before any stream capture.  Allocates
- * nothing. */
+ * the array's address and should come before any stream capture; later calls
+ * outside a capture look it up again (so a call after cudaDeviceReset finds
+ * the reloaded array).  Allocates nothing. */
 int lt_tracer_content_noalloc(const double* at, const double* tarea, const double* dzp, const int* kmt,
                               int nx, int ny, int km, double* out2, void* stream);
 /* fw_norm2 of the last step (tracer.cpp:1862-1865). */

@@ -63,7 +63,7 @@ class TurbTablesStruct(C.Structure):
 
 
 def turb_tables_struct(t):
-    """lt_turb_tables over a dict of arrays and scalars (turb_synth.tables()
+    """lt_turb_tables over a dict of arrays and scalars (tests/turb_synth.py tables()
     layout); the arrays must stay alive while the struct is used."""
     st = TurbTablesStruct()
     for n in TURB_TABLE_ARRAYS:
@@ -457,7 +457,7 @@ class TracerDomain:
 
 class TurbTab:
     """The closure's tables copied to the current device (lt_turb_tables_create);
-    ``tables`` is a dict in the turb_synth.tables() layout."""
+    ``tables`` is a dict in the tests/turb_synth.py tables() layout."""
 
     def __init__(self, tables):
         st = turb_tables_struct(tables)

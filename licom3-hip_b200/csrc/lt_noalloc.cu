@@ -19,7 +19,11 @@
 //
 // The first call on each device looks up the array's device address
 // (cudaGetSymbolAddress, with that device current); make that first call
-// before any stream capture begins.
+// before any stream capture begins.  Later calls look the address up again
+// unless their stream is capturing, so a call after cudaDeviceReset (which
+// unloads the library image from the device) finds the array where the
+// reloaded image put it; inside a capture the address of the last call
+// outside one is used.
 //
 // The sum is the same fixed binary tree as lt_tracer_content's (blocks of 2048
 // consecutive wet-cell terms T*tarea*dz over k, j, i of the interior, pairs
@@ -45,17 +49,19 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 double* g_scratch_ptr[kMaxDevices] = {};
 
-// Resolves the scratch address on the current device (first call on that
-// device only).
-int scratch_on_current_device(double** out) {
+// Resolves the scratch address on the current device: on the first call on
+// that device, and on every call whose stream is not capturing.
+int scratch_on_current_device(cudaStream_t stream, double** out) {
   int dev = 0;
   LT_CUDA_OK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("lt_tracer_content_noalloc: device %d beyond the %d devices supported", dev, kMaxDevices);
     return LT_E_INVALID;
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  LT_CUDA_OK(cudaStreamIsCapturing(stream, &cap));
   std::lock_guard<std::mutex> g(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
+  if (!g_scratch_ptr[dev] || cap == cudaStreamCaptureStatusNone) {
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_content_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_content_scratch)");
@@ -111,11 +117,11 @@ extern "C" int lt_tracer_content_noalloc(const double* at, const double* tarea, 
               nx, ny, km, n, need, kScratchValues, (kScratchValues - 8) * 2 * RB);
     return LT_E_INVALID;
   }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* part = nullptr;
-  int rc = scratch_on_current_device(&part);
+  int rc = scratch_on_current_device(s, &part);
   if (rc) return rc;
 
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int imt = nx + 4, jmt = ny + 4;
   const long A = (long)imt * jmt, F = A * km;
   const long nb = (n + 2 * RB - 1) / (2 * RB);

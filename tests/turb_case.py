@@ -1,6 +1,6 @@
 """Seeded cases of the turbulence closure for the tests: a synthetic domain,
-its closure inputs and the stand-in closure tables (licom3-hip_b200/
-turb_synth.py), at the reference's built-in block size by default."""
+its closure inputs and the stand-in closure tables (tests/turb_synth.py), at
+the reference's built-in block size by default."""
 import functools
 
 import numpy as np
@@ -13,13 +13,13 @@ TURB_CASES = [(3, 1), (8, 0), (21, 1)]
 
 @functools.lru_cache(maxsize=1)
 def tables(lt):
-    from licom3_hip_b200 import turb_synth
+    import turb_synth
     return turb_synth.tables()
 
 
 def case(lt, seed, forced=1, nx=36, ny=40, km=55, **kw):
     """(synth, fields) with the closure inputs added to the synth's fields."""
-    from licom3_hip_b200 import turb_synth
+    import turb_synth
     opts = dict(cap_north=0, cap_south=3, dz_top=5.0, dz_bot=300.0)
     opts.update(kw)
     syn = lt.Synth(nx, ny, km, seed=seed, forced=forced, **opts)
