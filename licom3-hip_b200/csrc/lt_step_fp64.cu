@@ -850,14 +850,23 @@ struct ExSmem {
   double dt5[kStageDel4 ? 5 : 1][kStageDel4 ? HN : 1];
   double xyc[kCacheXY ? 2 : 1][6][kCacheXY ? TTHREADS : 1];
   int kmt[(TY + 4) * SW];
+  int wmax[TTHREADS / 32];       // per-warp maxima of the region's bottom level
   uint64_t bar[NSX];
 };
 
 // Predictor, masked extrema and limiter flag of one cell (hj, hi) of the
 // 1-halo region at level kk; returns the flag (a00 > amax || a00 < amin).
 // sc, su, sd: the slots (and flag sets) of levels kk, kk-1, kk+1
+// dry_out: the flag of a land cell whose four horizontal faces carry no
+// transport is left 0 without computing its predictor: a flag only chooses
+// between the upwind and Lax-Wendroff forms of its faces' fluxes, which are
+// the same zero for a zero transport, and the vertical faces below a
+// column's bottom carry w = 0.  Not for a cell whose cached fluxes (xy_out)
+// the column phase reads.  (Model velocities vanish on land faces; the
+// reference's literal tracer_ sequence, which leaves vtl holding S, does not
+// keep them zero, hence the test.)
 __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int sc, int su, int sd, int hj, int hi,
-                                           int x0, int y0, double* xy_out = nullptr) {
+                                           int x0, int y0, double* xy_out = nullptr, bool dry_out = false) {
   const int km = a.km, imt = a.imt, jmt = a.jmt;
   const double dts = a.p.dts;
   const double* odzp = a.odzp;
@@ -879,6 +888,10 @@ __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, in
       return false;
     }
     const int r = r2(hj, hi), u = ru(hj, hi), v = rv(hj, hi);
+    if (dry_out && kk >= S.kmt[r] && uw[u] == 0.0 && uw[u + 1] == 0.0 && vs[v] == 0.0 && vs[v - SW] == 0.0) {
+      fl[m] = 0;
+      return false;
+    }
     const double tr = S.tr[m];
     const double hwe = S.hw[hj * (HQX + 1) + hi + 1], hww = S.hw[hj * (HQX + 1) + hi];
     const double hss = S.hs[(hj + 1) * HQX + hi], hsn = S.hs[hj * HQX + hi];
@@ -1043,12 +1056,30 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       if (ok) { par ^= 1u << s; outstanding &= ~(1u << s); }
       return ok;
     };
-    const int lowest_pro = km - NSX > 0 ? km - NSX : 0;
-    for (int L = km - 1; L >= lowest_pro; --L) issue(L, L % NSX);
     for (int m = tid; m < (TY + 4) * SW; m += TTHREADS) {
       const int gj = y0 - 2 + m / SW, gi = x0 - 4 + m % SW;
       S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
     }
+    // Without diagnostics, levels at and below the deepest bottom of the
+    // 1-halo region are land for every cell the march touches there: the
+    // reference's arithmetic leaves them as they are (every term is masked,
+    // the new value is at + dts * 0), so the march starts at the first of
+    // them and the inner cells' values below it are copied.  With
+    // diagnostics every level is marched (the reference writes them
+    // everywhere).
+    int ks = km - 1;
+    if (!DIAG) {
+      __syncthreads();
+      int kmax = max((int)S.kmt[r2(ty + 1, tx + 1)], has_ring ? (int)S.kmt[r2(ring_hj, ring_hi)] : 0);
+      kmax = __reduce_max_sync(0xffffffffu, kmax);
+      if (tx == 0) S.wmax[ty] = kmax;
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < TTHREADS / 32; ++q) kmax = max(kmax, S.wmax[q]);
+      ks = min(km - 1, kmax);
+    }
+    const int lowest_pro = ks - NSX + 1 > 0 ? ks - NSX + 1 : 0;
+    for (int L = ks; L >= lowest_pro; --L) issue(L, L % NSX);
     // the level-free metric terms (products formed once, as the reference
     // forms them at every use)
     for (int m = tid; m < HN; m += TTHREADS) {
@@ -1080,6 +1111,23 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
     const long qo = own ? (long)j * imt + i : 0;
     const int kz = own ? a.kmt[qo] : 0;
+    if (!DIAG && inner) {
+      // eight levels' loads in flight ahead of their stores
+      const double* __restrict__ src = at_in;
+      double* __restrict__ d1 = at_out;
+      double* __restrict__ d2 = atb_out;
+      for (int k0 = ks + 1; k0 < km; k0 += 8) {
+        double v[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) v[c] = k0 + c < km ? src[(long)(k0 + c) * A + qo] : 0.0;
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          if (k0 + c < km) {
+            d1[(long)(k0 + c) * A + qo] = v[c];
+            d2[(long)(k0 + c + 1) * A + qo] = v[c];
+          }
+      }
+    }
     const int hc = (ty + 1) * HQX + (tx + 1);
     const int rc = r2(ty + 1, tx + 1), uc = ru(ty + 1, tx + 1), vc = rv(ty + 1, tx + 1), ac = ty * TX + tx;
     const double swv = (inner && n == 0) ? a.swv[qo] : 0.0;
@@ -1092,21 +1140,23 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // slots of levels k, k-1, k+1 (NSX == 3: level k-2 shares k+1's), carried
     // through the level loop
     static_assert(NSX == 3, "slot rotation below assumes three slots");
-    int sk = (km - 1) % NSX;
+    // (below ks the slot of level ks+1 holds nothing of this tile: level ks
+    // is land everywhere in the region, and nothing of it reads that slot)
+    int sk = ks % NSX;
     int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
     {
-      const bool ok = wait(sk) && wait(sm1);
+      const bool ok = wait(sk) && (ks == 0 || wait(sm1));
       // a wait that ran out anywhere in the CTA sends every thread out together
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
     }
     // limiter flags of the own cell at levels k+1, k (earlier steps) and k-1
     bool out_kp1 = false,
-         out_k = pred_one64(S, a, km - 1, sk, sm1, sp1, ty + 1, tx + 1, x0, y0,
-                            &S.xyc[0][0][0] + tid + (kCacheXY ? ((km - 1) & 1) * 6 * TTHREADS : 0)),
+         out_k = pred_one64(S, a, ks, sk, sm1, sp1, ty + 1, tx + 1, x0, y0,
+                            &S.xyc[0][0][0] + tid + (kCacheXY ? (ks & 1) * 6 * TTHREADS : 0), !DIAG),
          out_km1 = false;
-    if (has_ring) pred_one64(S, a, km - 1, sk, sm1, sp1, ring_hj, ring_hi, x0, y0);
+    if (has_ring) pred_one64(S, a, ks, sk, sm1, sp1, ring_hj, ring_hi, x0, y0, nullptr, true);
 
-    for (int k = km - 1; k >= 0; --k) {
+    for (int k = ks; k >= 0; --k) {
       // ---- phase B1: first Laplacian at level k (arrived in an earlier step)
       del4_one64(S, a, k, sk, ty + 1, tx + 1, x0, y0);
       if (has_ring) del4_one64(S, a, k, sk, ring_hj, ring_hi, x0, y0);
@@ -1118,11 +1168,21 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       // thread computed: no barrier between the two phases.
       if (k >= 1) {
         out_km1 = pred_one64(S, a, k - 1, sm1, sp1, sk, ty + 1, tx + 1, x0, y0,
-                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 6 * TTHREADS : 0));
-        if (has_ring) pred_one64(S, a, k - 1, sm1, sp1, sk, ring_hj, ring_hi, x0, y0);
+                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 6 * TTHREADS : 0), !DIAG);
+        if (has_ring) pred_one64(S, a, k - 1, sm1, sp1, sk, ring_hj, ring_hi, x0, y0, nullptr, true);
       }
-      // ---- phase C
-      if (ring) {
+      // ---- phase C.  Without diagnostics an inner cell below its column's
+      // bottom keeps its value (every term of the step is masked) and only
+      // hands its level's values up to the level above.
+      if (!DIAG && inner && k >= kz) {
+        const LevelSlot<double>& Lk = S.slot[sk];
+        const double c = Lk.at[rc];
+        at_out[(long)k * A + qo] = c;
+        atb_out[(long)(k + 1) * A + qo] = c;
+        at_dn = c;
+        ws_dn = Lk.ws[uc];
+        atb_dn = Lk.atb[rc];
+      } else if (ring) {
         const LevelSlot<double>& Lk = S.slot[sk];
         const double* at_c = Lk.at;
         const double* at_u = k > 0 ? S.slot[sm1].at : nullptr;
@@ -1303,18 +1363,19 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     if (inner) {
       double x = 0.0;
       constexpr int SUB = 8;
-      for (int k0 = 0; k0 < km; k0 += SUB) {
+      const int kend = DIAG ? km : min(kz, ks + 1);   // the levels the march left in the scratch
+      for (int k0 = 0; k0 < kend; k0 += SUB) {
         double evs[SUB], fvs[SUB];
 #pragma unroll
         for (int c = 0; c < SUB; ++c) {
           const double* sl = scr + (long)(k0 + c) * NV * TTHREADS;
-          evs[c] = k0 + c < km ? sl[tid] : 0.0;
-          fvs[c] = k0 + c < km ? sl[TTHREADS + tid] : 0.0;
+          evs[c] = k0 + c < kend ? sl[tid] : 0.0;
+          fvs[c] = k0 + c < kend ? sl[TTHREADS + tid] : 0.0;
         }
 #pragma unroll
       for (int c = 0; c < SUB; ++c) {
         const int k = k0 + c;
-        if (k >= km) break;
+        if (k >= kend) break;
         const double* sl = scr + (long)k * NV * TTHREADS;
         const double ev = evs[c], fv = fvs[c];
         const long cg = (long)k * A + qo;
