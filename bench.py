@@ -48,9 +48,10 @@ FALLBACK_HBM_GBS = 6650.0
 STEP_BYTES = {"fp64": 136.0, "mixed": 100.0}
 TRACER_KERNEL_BYTES = {"fp64": 104.0, "mixed": 84.0}
 # DRAM bytes per cell (read + write) of the column kernel, from one ncu
-# --set full capture of a 720x460x55 launch; traffic grows with the cells, so
-# it scales to the bench's launch
-TRACER_KERNEL_TRAFFIC = {"fp64": 3.072e9 / (720 * 460 * 55), "mixed": 2.885e9 / (720 * 460 * 55)}
+# --set full capture of a 720x460x55 launch (profiles/); traffic grows with
+# the cells, so it scales to the bench's launch
+TRACER_KERNEL_TRAFFIC = {"fp64": (1.106355e9 + 0.653346e9) / (720 * 460 * 55),
+                         "mixed": (0.963681e9 + 0.646199e9) / (720 * 460 * 55)}
 
 
 def ICESNOW_BYTES_PER_POINT(km):
