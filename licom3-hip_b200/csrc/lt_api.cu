@@ -282,6 +282,11 @@ bool build_tracer_maps(const Arena& a, TracerMaps* m) {
   ok = ok && make_tensor_map_3d(&m->uw, mx ? (const void*)a.wkd32 : a.uwf, es, imt, jmt, km, SW, mx ? ty + 3 : ty + 2);
   ok = ok && make_tensor_map_3d(&m->vs, mx ? (const void*)a.wkb32 : a.vsf, es, imt, jmt, km, SW, ty + 3);
   ok = ok && make_tensor_map_3d(&m->akt, mx ? (const void*)a.akt32 : a.akt, es, imt, jmt, 2 * km, TX, ty);
+  if (mx) {
+    const float* vel[4] = {a.utf32, a.vtf32, a.utl32, a.vtl32};
+    for (int v = 0; v < 4; ++v)
+      ok = ok && make_tensor_map_3d(&m->vel[v], vel[v], 4, imt, jmt, km, kMixedContBoxW, kMixedContTileY + 1);
+  }
   return ok;
 }
 
@@ -300,7 +305,7 @@ int run_step(lt_domain* d, cudaEvent_t forcing_ready) {
   // continuity first: it reads the SSH mean and the velocities, not the
   // surface forcing
   if ((rc = launch_ssh(a, s))) return rc;
-  if (a.precision == LT_PREC_MIXED) rc = launch_continuity_mixed(a, s);
+  if (a.precision == LT_PREC_MIXED) rc = launch_continuity_mixed(a, d->maps, d->use_tma, s);
   else rc = launch_continuity_fp64(a, s);
   if (rc) return rc;
   mark(1);

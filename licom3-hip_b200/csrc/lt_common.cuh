@@ -28,6 +28,11 @@ constexpr int kMixedThreads = TX * kMixedTileY;
 constexpr int kMixedBoxW64 = TX + 4;
 constexpr int kMixedScratchPerLevel = 4;
 constexpr int kMixedMaxLevels = 128;
+// The mixed continuity march: tiles of 32 x kMixedContTileY columns, each
+// level's U-point velocities as boxes kMixedContBoxW wide (x0-4 .. x0+35)
+// and kMixedContTileY+1 rows (y0-1 .. y0+kMixedContTileY-1).
+constexpr int kMixedContTileY = 4;
+constexpr int kMixedContBoxW = 40;
 
 // Everything the step kernels touch, as raw device pointers (dense
 // [n][k][j][i] layout of the reference, i fastest).
@@ -131,7 +136,7 @@ int launch_del4u(const Arena& a, double am, double c0f, cudaStream_t s);
 int launch_check_numeric(const Arena& a, cudaStream_t s);
 int launch_derive_masks(const Arena& a, cudaStream_t s);
 int launch_vtl_clobber(const Arena& a, cudaStream_t s);
-int launch_continuity_mixed(const Arena& a, cudaStream_t s);
+
 int launch_f64_to_f32(const double* x, float* y, long n, cudaStream_t s);
 int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s);
 int tracer_slots(const Arena& a);

@@ -85,6 +85,70 @@ __device__ __forceinline__ float lw_part(float d, float u, float c) { return d *
 //   raw(k) = ws(0) + W * ohbt * Z(k) + P(k),  Z(k) = sum_{k'<k} dzp,
 // with P(k) parked in the ws field between the two passes.
 constexpr int CBX = 32;
+
+// The U-point mean velocity wkd = (utf*oncc + utl)/2 (wkb likewise), with
+// every rounding spelled out: the plain-load and the TMA-fed march form it
+// in different code, and must give the same bits.
+__device__ __forceinline__ float u_mean32(float f, float l, float oncc) {
+  return __fadd_rn(__fmul_rn(0.5f, __fmul_rn(f, oncc)), __fmul_rn(0.5f, l));
+}
+
+// Horizontal divergence of one T cell at one level (tracer_1, upwell_2,
+// operators_div; the four faces as the tracer kernel forms them, face_x64 /
+// face_y64, with the free-surface correction: (uk_1 + uk_2) * htw = 4 * uw +
+// htw * (fm1_1 * wkd_1 + fm1_2 * wkd_2)), roundings spelled out for the same
+// reason.  d*: wkd at the U points (j-1,i), (j,i), (j-1,i+1), (j,i+1); b*:
+// wkb at the same points; f*: the free-surface factors minus one there.
+struct ContCell {
+  double htw_c, htw_e, hts_c, hts_n, tr;
+};
+__device__ __forceinline__ double cont_wka(const ContCell& g, float dn, float d0, float dn1, float d01, float bn,
+                                           float b0, float bn1, float b01, float fn, float f0, float fn1,
+                                           float f01) {
+  auto corr = [](float f1, float w1, float f2, float w2) {
+    return __dadd_rn(__dmul_rn((double)f1, (double)w1), __dmul_rn((double)f2, (double)w2));
+  };
+  const double uw_w = face_x64(dn, d0, g.htw_c);
+  const double uw_e = face_x64(dn1, d01, g.htw_e);
+  const double vs_s = face_y64(b0, b01, g.hts_c);
+  const double vs_n = face_y64(bn, bn1, g.hts_n);
+  const double east = __fma_rn(g.htw_e, corr(f01, d01, fn1, dn1), __dmul_rn(4.0, uw_e));
+  const double west = __fma_rn(g.htw_c, corr(f0, d0, fn, dn), __dmul_rn(4.0, uw_w));
+  const double south = __fma_rn(g.hts_c, corr(f01, b01, f0, b0), __dmul_rn(4.0, vs_s));
+  const double north = __fma_rn(g.hts_n, corr(fn1, bn1, fn, bn), __dmul_rn(4.0, vs_n));
+  return __dmul_rn(__dmul_rn(0.5, __dadd_rn(__dsub_rn(east, west), __dsub_rn(south, north))), g.tr);
+}
+
+// Final pass of the march: ws(k) from the partial sums P(k), parked in the ws
+// field (ps null) or in shared memory (ps[k * ps_stride]), eight levels'
+// loads ahead of their stores.
+__device__ __forceinline__ void cont_finish(const Arena& a, long qo, int kz, double P, const float* ps = nullptr,
+                                            int ps_stride = 0) {
+  const int km = a.km;
+  const long A = a.A;
+  const double ohbt = a.ohbt[qo];
+  const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
+  const double W = -P;
+  float* __restrict__ ws = a.ws32;
+  const double ws0 = ws[qo];
+  const double* __restrict__ dzp = a.dzp;
+  double Z = 0.0;
+  for (int k0 = 1; k0 < km; k0 += 8) {
+    float pk[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      pk[c] = (k0 + c < km && k0 + c < kz) ? (ps ? ps[(k0 + c) * ps_stride] : ws[(long)(k0 + c) * A + qo]) : 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int k = k0 + c;
+      if (k >= km) break;
+      Z = __dadd_rn(Z, dzp[k - 1]);
+      ws[(long)k * A + qo] =
+          (k < kz) ? (float)__dmul_rn(fac, __dadd_rn(__fma_rn(__dmul_rn(W, ohbt), Z, ws0), (double)pk[c])) : 0.f;
+    }
+  }
+}
+
 template <int CBY>
 __device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
   constexpr int UX = CBX + 1, UY = CBY + 1, UN = UX * UY, NT = CBX * CBY;
@@ -150,8 +214,8 @@ __device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
     for (int p = 0; p < NPT; ++p) {
       const int m = tid + p * NT;
       if (m < UN) {
-        s_wkd[b][m] = rin[p] ? 0.5f * (ruf[p] * oncc) + 0.5f * rul[p] : 0.f;
-        s_wkb[b][m] = rin[p] ? 0.5f * (rvf[p] * oncc) + 0.5f * rvl[p] : 0.f;
+        s_wkd[b][m] = rin[p] ? u_mean32(ruf[p], rul[p], oncc) : 0.f;
+        s_wkb[b][m] = rin[p] ? u_mean32(rvf[p], rvl[p], oncc) : 0.f;
       }
     }
   };
@@ -171,41 +235,131 @@ __device__ __forceinline__ void cont_tile(const Arena& a, int bx, int by) {
       a.wkd32[c] = wd[m0];
       a.wkb32[c] = wb[m0];
       if (col_here && k < kz) {
-        // the four faces, as the tracer kernel forms them (face_x64/face_y64)
-        const double uw_w = face_x64(wd[mn], wd[m0], htw_cd);
-        const double uw_e = face_x64(wd[mn + 1], wd[m0 + 1], htw_ed);
-        const double vs_s = face_y64(wb[m0], wb[m0 + 1], hts_cd);
-        const double vs_n = face_y64(wb[mn], wb[mn + 1], hts_nd);
-        // (uk_1 + uk_2) * htw = 4 * uw + htw * (fm1_1 * wkd_1 + fm1_2 * wkd_2)
-        auto corr = [&](const float* s, int m1, int m2) {
-          return (double)s_fm1[m1] * (double)s[m1] + (double)s_fm1[m2] * (double)s[m2];
-        };
-        const double east = 4.0 * uw_e + htw_ed * corr(wd, m0 + 1, mn + 1);
-        const double west = 4.0 * uw_w + htw_cd * corr(wd, m0, mn);
-        const double south = 4.0 * vs_s + hts_cd * corr(wb, m0 + 1, m0);
-        const double north = 4.0 * vs_n + hts_nd * corr(wb, mn + 1, mn);
-        const double wka = 0.5 * (east - west + south - north) * tr;
+        const ContCell g{htw_cd, htw_ed, hts_cd, hts_nd, tr};
+        const double wka = cont_wka(g, wd[mn], wd[m0], wd[mn + 1], wd[m0 + 1], wb[mn], wb[m0], wb[mn + 1],
+                                    wb[m0 + 1], s_fm1[mn], s_fm1[m0], s_fm1[mn + 1], s_fm1[m0 + 1]);
         if (k >= 1) a.ws32[c] = (float)P;
-        P += a.dzp[k] * wka;
+        P = __fma_rn(a.dzp[k], wka, P);
       }
     }
     // buffer b^1 was last read in step k-1, before this step's barrier
     if (k + 1 < km) park(b ^ 1);
   }
   if (!col_here) return;
-  const double ohbt = a.ohbt[qo];
-  const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
-  const double W = -P;
-  const double ws0 = a.ws32[qo];
-  double Z = 0.0;
-  for (int k = 1; k < km; ++k) {
-    Z += a.dzp[k - 1];
-    const long c = (long)k * A + qo;
-    a.ws32[c] = (k < kz) ? (float)(fac * (ws0 + W * ohbt * Z + (double)a.ws32[c])) : 0.f;
-  }
+  cont_finish(a, qo, kz, P);
 }
 
-constexpr int kContTileY = 4;   // tile height of the single-domain continuity march
+constexpr int kContTileY = kMixedContTileY;   // tile height of the single-domain continuity march
+
+// The single-domain march fed by TMA: each level's raw U-point velocities
+// (utf, vtf, utl, vtl over the tile plus a row above and a column east) come
+// as four boxes into a ring of kContRing level slots, so kContRing levels of
+// loads are in flight; each thread forms the U-point means it needs from
+// them (u_mean32, the same bits as the plain-load march).  The partial sums
+// P(k) of the upward integration stay in shared memory behind the ring (km
+// floats per column) instead of making a round trip through the ws field.
+constexpr int kContRing = 6;
+constexpr int CRW = kMixedContBoxW, CRR = kMixedContTileY + 1;
+struct alignas(128) ContSlot {
+  struct alignas(128) Box { float v[CRR * CRW]; };
+  Box f[4];   // utf, vtf, utl, vtl
+};
+struct ContSmem {
+  ContSlot slot[kContRing];
+  float fm1[CRR * (CBX + 1)];
+  uint64_t bar[kContRing];
+};
+constexpr uint32_t kContLevelBytes = 4 * CRR * CRW * sizeof(float);
+
+__global__ void __launch_bounds__(CBX * kContTileY) k_cont_tma32(Arena a, const __grid_constant__ TracerMaps maps) {
+  extern __shared__ __align__(128) unsigned char smem_ct[];
+  ContSmem& S = *reinterpret_cast<ContSmem*>(smem_ct);
+  constexpr int UX = CBX + 1, NT = CBX * kContTileY;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CBX + tx;
+  float* ps = reinterpret_cast<float*>(smem_ct + sizeof(ContSmem)) + tid;   // P(k) at ps[k * NT]
+  const int x0 = blockIdx.x * CBX, y0 = blockIdx.y * kContTileY;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A;
+  const float oncc = (float)a.p.oncc;
+  if (tid == 0) {
+    for (int r = 0; r < kContRing; ++r) mbar_init(&S.bar[r], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](int k) {
+    if (tid == 0 && k < km) {
+      const int r = k % kContRing;
+      mbar_expect_tx(&S.bar[r], kContLevelBytes);
+      for (int v = 0; v < 4; ++v) tma_load_3d(S.slot[r].f[v].v, &maps.vel[v], x0 - 4, y0 - 1, k, &S.bar[r]);
+    }
+  };
+  for (int k = 0; k < kContRing; ++k) issue(k);
+  for (int m = tid; m < CRR * UX; m += NT) {
+    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+    float fm1 = -1.f;
+    if (uj >= 0 && uj < jmt - 1 && ui >= 1 && ui < imt) {
+      const long q = (long)uj * imt + ui;
+      const double work = a.au0[q] * a.stf_ssh[q] + a.aus[q] * a.stf_ssh[q + imt] +
+                          a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
+      fm1 = (float)(work * a.ohbu[q]);
+    }
+    S.fm1[m] = fm1;
+  }
+  const int i = x0 + tx, j = y0 + ty;
+  const bool own = i < imt && j < jmt;
+  const bool div_here = own && j >= 1 && i < imt - 1;
+  const bool col_here = own && j >= 1 && j < jmt - 1 && i >= 1 && i < imt - 1;
+  const long qo = own ? (long)j * imt + i : 0;
+  const int kz = own ? a.kmt[qo] : 0;
+  const ContCell g{own ? a.htw[qo] : 0.0, div_here ? a.htw[qo + 1] : 0.0, own ? a.hts[qo] : 0.0,
+                   div_here ? a.hts[qo - imt] : 0.0, div_here ? a.tarea_r[qo] : 0.0};
+  // box index of U point (j, i) and (j-1, i); region index for the factors
+  const int b0 = (ty + 1) * CRW + tx + 4, bn = ty * CRW + tx + 4;
+  const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
+  __syncthreads();
+  const float fn = S.fm1[mn], f0 = S.fm1[m0], fn1 = S.fm1[mn + 1], f01 = S.fm1[m0 + 1];
+  // outside the domain the boxes read zeros, as the plain-load march does
+  const bool in_n = j >= 1 && i < imt, in_0 = own, in_n1 = j >= 1 && i + 1 < imt, in_01 = j < jmt && i + 1 < imt;
+  double P = 0.0;
+  // level k is the (k / kContRing)-th use of its slot: that use's phase parity
+  auto parity = [](int k) { return (uint32_t)((k / kContRing) & 1); };
+  for (int k = 0; k < km; ++k) {
+    const int r = k % kContRing;
+    const bool ok = mbar_wait(&S.bar[r], parity(k), a.wait_limit);
+    if (__syncthreads_or(!ok)) {
+      // a wait ran out: record it, let the boxes still in flight land
+      // (bounded) and leave together
+      if (tid == 0) {
+        atomicExch(a.status + 1, 1);
+        for (int l = k; l < km && l < k + kContRing; ++l)
+          mbar_wait(&S.bar[l % kContRing], parity(l));   // the full bound, whatever a.wait_limit is
+      }
+      __syncthreads();
+      return;
+    }
+    const ContSlot& L = S.slot[r];
+    auto mean = [&](int f, int l, int b, bool in) { return in ? u_mean32(L.f[f].v[b], L.f[l].v[b], oncc) : 0.f; };
+    if (own) {
+      const long c = (long)k * A + qo;
+      const float d0 = mean(0, 2, b0, in_0), e0 = mean(1, 3, b0, in_0);
+      a.utf_out32[c] = L.f[0].v[b0] * oncc;
+      a.vtf_out32[c] = L.f[1].v[b0] * oncc;
+      a.wkd32[c] = d0;
+      a.wkb32[c] = e0;
+      if (col_here && k < kz) {
+        const double wka = cont_wka(g, mean(0, 2, bn, in_n), d0, mean(0, 2, bn + 1, in_n1), mean(0, 2, b0 + 1, in_01),
+                                    mean(1, 3, bn, in_n), e0, mean(1, 3, bn + 1, in_n1), mean(1, 3, b0 + 1, in_01),
+                                    fn, f0, fn1, f01);
+        if (k >= 1) ps[k * NT] = (float)P;
+        P = __fma_rn(a.dzp[k], wka, P);
+      }
+    }
+    __syncthreads();   // level k's slot is read: it takes level k + kContRing
+    issue(k + kContRing);
+  }
+  if (!col_here) return;
+  cont_finish(a, qo, kz, P, ps, NT);
+}
 
 __global__ void __launch_bounds__(CBX * kContTileY) k_cont_march32(Arena a) {
   cont_tile<kContTileY>(a, blockIdx.x, blockIdx.y);
@@ -1074,9 +1228,22 @@ int launch_continuity_mixed_batch(const MemberDesc* mem, int nmem, int max_imt, 
   return LT_OK;
 }
 
-int launch_continuity_mixed(const Arena& a, cudaStream_t s) {
+int launch_continuity_mixed(const Arena& a, const TracerMaps& maps, bool tma, cudaStream_t s) {
   dim3 b(CBX, kContTileY), g((a.imt + CBX - 1) / CBX, (a.jmt + kContTileY - 1) / kContTileY);
-  k_cont_march32<<<g, b, 0, s>>>(a);
+  if (tma) {
+    static int attr_dev = -1;
+    int dev = 0;
+    LT_CUDA_OK(cudaGetDevice(&dev));
+    const size_t psm = sizeof(float) * CBX * kContTileY;   // partial sums per level
+    if (attr_dev != dev) {
+      LT_CUDA_OK(cudaFuncSetAttribute(k_cont_tma32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(sizeof(ContSmem) + psm * kMixedMaxLevels)));
+      attr_dev = dev;
+    }
+    k_cont_tma32<<<g, b, sizeof(ContSmem) + psm * a.km, s>>>(a, maps);
+  } else {
+    k_cont_march32<<<g, b, 0, s>>>(a);
+  }
   LT_LAUNCHED();
   return LT_OK;
 }

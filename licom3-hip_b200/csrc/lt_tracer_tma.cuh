@@ -27,6 +27,7 @@ constexpr int HN = HQX * HQY;
 
 struct TracerMaps {
   CUtensorMap at[2], atb[2], ws, uw, vs, akt;
+  CUtensorMap vel[4];   // mixed: utf, vtf, utl, vtl (f32) in the continuity march's boxes
 };
 
 template <class VT>
@@ -91,6 +92,9 @@ int launch_halo_state_batch(const MemberDesc* mem, int nmem, int max_imt, int km
 // sets the batched column kernel's shared-memory size on the current device
 int prepare_tracer_mixed_batch();
 int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
+// The mixed continuity: TMA-fed when the domain has its maps (tma), else
+// plain loads.
+int launch_continuity_mixed(const Arena& a, const TracerMaps& maps, bool tma, cudaStream_t s);
 // Build the tensor maps of a domain; false if the layout does not allow TMA
 // (row pitch not a multiple of 16 bytes for some field).
 bool build_tracer_maps(const Arena& a, TracerMaps* maps);
