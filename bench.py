@@ -609,7 +609,7 @@ def serving_figures(lt, requests, rate):
     for r in range(requests):
         t += rng.expovariate(rate)
         area = math_exp(rng.uniform(math_log(a_lo), math_log(a_hi)))
-        nx = max(64, int(round((area * 4.0 / 3.0) ** 0.5 / 4.0)) * 4)
+        nx = max(64, int(round((area * 4.0 / 3.0) ** 0.5)))
         ny = max(48, int(round(area / nx)))
         km = 30 if area < (a_lo * a_hi) ** 0.5 else 55
         srv.submit(nx, ny, km, rng.randint(10, 200), arrival=t0 + t, seed=1000 + r,

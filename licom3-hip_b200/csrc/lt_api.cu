@@ -168,9 +168,8 @@ bool grid_ok(const lt_grid* g) {
   if (g->nx < 8 || g->ny < 8 || g->km < 3 || g->km > 256) return false;
   if (g->tripole && (g->nx % 2)) return false;
   if (g->precision != LT_PREC_FP64 && g->precision != LT_PREC_MIXED) return false;
-  // the mixed kernel takes its f32 fields by TMA: row pitch a multiple of 16
-  // bytes; its per-level constants live in shared memory: at most 128 levels
-  if (g->precision == LT_PREC_MIXED && (((g->nx + 4) % 4) || g->km > kMixedMaxLevels)) return false;
+  // the mixed kernel's per-level constants live in shared memory: at most 128 levels
+  if (g->precision == LT_PREC_MIXED && g->km > kMixedMaxLevels) return false;
   return true;
 }
 
@@ -317,7 +316,7 @@ int run_step(lt_domain* d, cudaEvent_t forcing_ready) {
   if ((rc = launch_halo_r8(a.net, 2, a.imt, a.jmt, a.ew_cyclic, a.tripole, s))) return rc;
   mark(4);
   if (a.precision == LT_PREC_MIXED) {
-    if ((rc = launch_tracer_tma_mixed(a, d->maps, s, d->tma_grid))) return rc;
+    if ((rc = launch_tracer_tma_mixed(a, d->maps, d->use_tma, s, d->tma_grid))) return rc;
   } else if (d->use_tma) {
     if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid))) return rc;
   } else {

@@ -87,6 +87,7 @@ int build_descriptors(lt_batch* b) {
       e.item0 = item;
       e.ntiles = ntiles;
       e.ntx = ntx;
+      e.tma = d->use_tma ? 1 : 0;
     }
     item += ntiles;   // one work item per tile (both tracers)
     b->km_max = std::max(b->km_max, a.km);
@@ -221,11 +222,6 @@ int lt_batch_create(lt_domain* const* members, int n, lt_batch** out) {
     lt_domain* d = members[i];
     if (!d || (d->a.precision == LT_PREC_MIXED) != b->mixed) {
       set_error("lt_batch_create: member %d is missing or of another precision", i);
-      delete b;
-      return LT_E_INVALID;
-    }
-    if (b->mixed && !d->use_tma) {
-      set_error("lt_batch_create: mixed member %d has no TMA maps", i);
       delete b;
       return LT_E_INVALID;
     }

@@ -496,6 +496,52 @@ __device__ __forceinline__ void issue_mx(MxSlot& sl, uint64_t* bar, const Tracer
   tma_load_3d(sl.akt[1], &m.akt, x0, y0, km + L, bar);
 }
 
+// The same level by per-thread asynchronous copies, for grids whose row
+// pitch TMA cannot take (not a multiple of 16 bytes): every thread copies
+// its share of the boxes' elements (zeros outside the domain, as TMA fills)
+// and the slot's mbarrier counts one arrival per thread once its copies have
+// landed.  The slot layout and the waits are the TMA path's.
+constexpr int kF64Elems = 4 * (MY + 4) * SW64;
+constexpr int kWsElems = (MY + 2) * SW, kWkElems = (MY + 3) * SW, kAktElems = TX * MY;
+constexpr int kF32Elems = kWsElems + 2 * kWkElems + 2 * kAktElems;
+__device__ __forceinline__ void copy_level_mx(MxSlot& sl, uint64_t* bar, const Arena& a, int km, int L, int x0,
+                                              int y0) {
+  const int imt = a.imt, jmt = a.jmt;
+  const long A = a.A, F = a.F, FB = a.FB;
+  for (int e = threadIdx.x; e < kF64Elems; e += MTH) {
+    constexpr int BOX = (MY + 4) * SW64;
+    const int b = e / BOX, r = e % BOX;
+    const int gj = y0 - 2 + r / SW64, gi = x0 - 2 + r % SW64;
+    const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+    const int n = b & 1;
+    const double* src = (b < 2) ? a.at[a.cur] + n * F + (long)L * A : a.atb[a.cur] + n * FB + (long)(L + 1) * A;
+    double* dst = (b < 2) ? sl.at[n] : sl.atb[n];
+    cp_async8z(dst + r, src + (in ? (long)gj * imt + gi : 0), in);
+  }
+  for (int e = threadIdx.x; e < kF32Elems; e += MTH) {
+    const float* base;
+    float* dst;
+    int r, w, gj0, gi0;
+    if (e < kWsElems) {
+      r = e; w = SW; gj0 = y0 - 1; gi0 = x0 - 4; base = a.ws32 + (long)L * A; dst = sl.ws;
+    } else if (e < kWsElems + 2 * kWkElems) {
+      const int q = e - kWsElems, b = q / kWkElems;
+      r = q % kWkElems; w = SW; gj0 = y0 - 2; gi0 = x0 - 4;
+      base = (b == 0 ? a.wkd32 : a.wkb32) + (long)L * A;
+      dst = b == 0 ? sl.wkd : sl.wkb;
+    } else {
+      const int q = e - kWsElems - 2 * kWkElems, n = q / kAktElems;
+      r = q % kAktElems; w = TX; gj0 = y0; gi0 = x0;
+      base = a.akt32 + n * F + (long)L * A;
+      dst = sl.akt[n];
+    }
+    const int gj = gj0 + r / w, gi = gi0 + r % w;
+    const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+    cp_async4z(dst + r, base + (in ? (long)gj * imt + gi : 0), in);
+  }
+  cp_async_mbar_arrive(bar);
+}
+
 // ---- f32 faces of the 1-halo region (the predictor's level)
 // A face is described by (kind, index, box index of its east / north cell
 // in the f64 boxes, index of its first U point in the f32 boxes).
@@ -790,7 +836,7 @@ constexpr int kIssueThread = 4 * TX;
 // false if a level wait gave up: the CTA has then recorded the timeout and
 // drained its boxes, and must return.
 template <bool kLoadsAhead>
-__device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict__ lvs, const Arena& a,
+__device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* __restrict__ lvs, const Arena& a,
                                            const TracerMaps& maps, double* scr, int ntx, long tile, uint32_t& par,
                                            uint32_t& outstanding) {
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
@@ -804,8 +850,15 @@ __device__ __forceinline__ bool mixed_item(MxSmem& S, const MxLevel* __restrict_
 
   __syncthreads();   // the previous item no longer reads the slots or the tile data
   // level L goes to slot s = L % NSM
+  // every thread arrives on the slot's barrier once per level: by TMA (the
+  // issuing thread with the level's byte count) or after its own copies
   auto issue = [&](int L, int s) {
-    if (tid == kIssueThread) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, km, L, x0, y0);
+    if (tma) {
+      if (tid == kIssueThread) issue_mx(S.slot[s], &S.bar[s], maps, a.cur, km, L, x0, y0);
+      else mbar_arrive(&S.bar[s]);
+    } else {
+      copy_level_mx(S.slot[s], &S.bar[s], a, km, L, x0, y0);
+    }
     outstanding |= 1u << s;
   };
   auto wait = [&](int s) -> bool {
@@ -1120,7 +1173,7 @@ __device__ __forceinline__ MxSmem& mixed_smem_init() {
   extern __shared__ __align__(128) unsigned char smem_mx[];
   MxSmem& S = *reinterpret_cast<MxSmem*>(smem_mx);
   if (threadIdx.x == 0) {
-    for (int s = 0; s < NSM; ++s) mbar_init(&S.bar[s], 1);
+    for (int s = 0; s < NSM; ++s) mbar_init(&S.bar[s], MTH);   // one arrival per thread and level
     mbar_fence_init();
   }
   __syncthreads();
@@ -1133,14 +1186,14 @@ __device__ __forceinline__ MxLevel* mixed_levels() {
 }
 
 __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
-    k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
+    k_tracer_mixed(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles, int tma) {
   MxSmem& S = mixed_smem_init();
   MxLevel* lv = mixed_levels();
   stage_levels(lv, a);
   uint32_t par = 0, outstanding = 0;
   double* scr = a.col_scratch + (long)blockIdx.x * a.km * kMixedScratchPerLevel * MTH;
   for (long w = blockIdx.x; w < ntiles; w += gridDim.x)
-    if (!mixed_item<false>(S, lv, a, maps, scr, ntx, w, par, outstanding)) return;
+    if (!mixed_item<false>(tma != 0, S, lv, a, maps, scr, ntx, w, par, outstanding)) return;
 }
 
 // Several domains (ensemble members, serving requests; any sizes) in one
@@ -1177,13 +1230,13 @@ __global__ void __launch_bounds__(MTH, kMixedCtasPerSm)
       stage_levels(lv, sa);
       staged = m;
     }
-    if (!mixed_item<true>(S, lv, sa, d.maps, scr, d.ntx, w - d.item0, par, outstanding)) return;
+    if (!mixed_item<true>(d.tma != 0, S, lv, sa, d.maps, scr, d.ntx, w - d.item0, par, outstanding)) return;
   }
 }
 
 }  // namespace
 
-int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid) {
+int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, bool tma, cudaStream_t s, int grid) {
   const int ntx = (a.imt + TX - 1) / TX;
   const long ntiles = (long)ntx * ((a.jmt + MY - 1) / MY);
   const size_t sm = mx_smem_bytes(a.km);
@@ -1195,7 +1248,7 @@ int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t
                                     (int)mx_smem_bytes(kMixedMaxLevels)));
     attr_dev = dev;
   }
-  k_tracer_mixed<<<grid, MTH, sm, s>>>(a, maps, ntx, ntiles);
+  k_tracer_mixed<<<grid, MTH, sm, s>>>(a, maps, ntx, ntiles, tma ? 1 : 0);
   LT_LAUNCHED();
   return LT_OK;
 }

@@ -72,6 +72,7 @@ struct alignas(64) MemberDesc {
   long item0;    // first work item (a tile, both tracers) of this member in the batch list
   long ntiles;   // column tiles of this member
   int ntx;       // tiles along i
+  int tma;       // 1: level boxes by TMA; 0: by per-thread copies (row pitch TMA cannot take)
 };
 
 int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
@@ -91,7 +92,8 @@ int launch_small_batch_pre(const MemberDesc* mem, int nmem, int max_imt, int max
 int launch_halo_state_batch(const MemberDesc* mem, int nmem, int max_imt, int km_max, cudaStream_t s);
 // sets the batched column kernel's shared-memory size on the current device
 int prepare_tracer_mixed_batch();
-int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
+// The mixed column kernel; tma: its level boxes by TMA (else per-thread copies)
+int launch_tracer_tma_mixed(const Arena& a, const TracerMaps& maps, bool tma, cudaStream_t s, int grid);
 // The mixed continuity: TMA-fed when the domain has its maps (tma), else
 // plain loads.
 int launch_continuity_mixed(const Arena& a, const TracerMaps& maps, bool tma, cudaStream_t s);

@@ -53,6 +53,28 @@ def test_every_launch_shape_gives_the_same_bits(lt, ctas, tile_y, graph):
     b.close()
 
 
+def test_batch_with_members_of_any_row_pitch(lt):
+    """Members whose row pitch TMA cannot take (nx + 4 odd or not a multiple
+    of 4) step in the same batch as the others, each exactly as alone."""
+    sizes = [(49, 30, 12), (64, 40, 20), (50, 34, 30)]
+    kw = dict(forced=1, ew_cyclic=0, tripole=0)
+    syns = [lt.Synth(nx, ny, km, seed=40 + i, **kw) for i, (nx, ny, km) in enumerate(sizes)]
+    doms = [lt.TracerDomain(s.nx, s.ny, s.km, s.params, precision=lt.PREC_MIXED, ew_cyclic=False, tripole=False)
+            for s in syns]
+    alone = [lt.TracerDomain(s.nx, s.ny, s.km, s.params, precision=lt.PREC_MIXED, ew_cyclic=False, tripole=False)
+             for s in syns]
+    for s, d, e in zip(syns, doms, alone):
+        s.upload(d)
+        s.upload(e)
+        e.step(4)
+        e.sync()
+    b = lt.Batch(doms)
+    b.step(4)
+    b.sync()
+    assert_same(doms, alone)
+    b.close()
+
+
 def test_batch_steps_mix_with_single_steps(lt):
     """A member stepped on its own between batch steps is picked up correctly."""
     syns, doms = members(lt, lt.PREC_MIXED, seed0=21)

@@ -77,7 +77,40 @@ def test_conservation_100_steps(lt, precision):
     assert rel[0] < 1e-13 and rel[1] < 1e-13, rel
 
 
-def test_mixed_rejects_unaligned_pitch(lt):
-    syn = lt.Synth(50, 30, 10, ew_cyclic=0, tripole=0)   # imt = 54, not a multiple of 4
-    with pytest.raises(lt.LtError):
-        lt.TracerDomain(50, 30, 10, syn.params, precision=lt.PREC_MIXED, ew_cyclic=False, tripole=False)
+@pytest.mark.parametrize("nx", [49, 50, 51])
+def test_mixed_any_row_pitch_vs_oracle(lt, nx):
+    """Grids whose row pitch TMA cannot take (imt = nx + 4 not a multiple of
+    4 floats) run the mixed step with per-thread copies of the same level
+    boxes: within the bounds of the oracle after 20 steps."""
+    import pyoracle
+    syn = lt.Synth(nx, 30, 12, forced=1, cap_north=2, ew_cyclic=0, tripole=0)
+    f = syn.all_fields()
+    dom = lt.TracerDomain(nx, 30, 12, syn.params, precision=lt.PREC_MIXED, ew_cyclic=False, tripole=False)
+    for n in lt.INPUT_FIELDS:
+        dom.set(n, f[n])
+    dom.step(20)
+    o = pyoracle.Oracle(nx, 30, 12, syn.params, ew_cyclic=0, tripole=0)
+    o.load(f)
+    o.sum_order(1)
+    o.step(20)
+    kmt = f["KMT"]
+    wet = (np.arange(12)[:, None, None] < kmt[None])[:, 2:-2, 2:-2]
+    a, b = o.get("AT")[:, :, 2:-2, 2:-2], dom.get("AT")[:, :, 2:-2, 2:-2]
+    dt = np.abs(a[0] - b[0])[wet].max()
+    ds = np.abs(a[1] - b[1])[wet].max() * 1e3
+    print("nx=%d mixed vs oracle after 20 steps: %.3e K, %.3e psu" % (nx, dt, ds))
+    assert dt <= 1e-5 and ds <= 1e-6, (dt, ds)
+    assert dom.check_numeric() == 0
+
+
+def test_mixed_copy_path_equals_tma_path(lt):
+    """On a grid TMA can take, the per-thread copy path fills the same level
+    slots: both give the same bits."""
+    syn = lt.Synth(124, 60, 24, forced=1, cap_north=0)
+    a = syn.domain(precision=lt.PREC_MIXED)
+    b = syn.domain(precision=lt.PREC_MIXED)
+    b.use_tma(False)
+    a.step(6)
+    b.step(6)
+    for n in ("AT", "ATB", "WS", "NET"):
+        np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)

@@ -47,6 +47,23 @@ def test_results_same_alone_and_in_the_mix(lt):
     srv.close()
 
 
+def test_unrounded_sizes_same_alone_and_in_the_mix(lt):
+    """Requests of any size (row pitches TMA cannot take among them) are
+    served and give the same result as alone."""
+    reqs = [(101, 77, 30, 5, 0.0, 31), (64, 48, 30, 6, 0.0, 32), (150, 90, 55, 4, 0.01, 33), (57, 61, 30, 7, 0.0, 34)]
+    srv = lt.Server(precision=lt.PREC_MIXED, chunk_steps=3)
+    t0 = srv.clock()
+    ids = [srv.submit(nx, ny, km, steps, arrival=t0 + arr, keep_state=True, seed=seed, **CLOSED)
+           for nx, ny, km, steps, arr, seed in reqs]
+    srv.drain()
+    assert srv.stats()["requests_done"] == len(reqs)
+    for rid, (nx, ny, km, steps, arr, seed) in zip(ids, reqs):
+        at_alone, content_alone = run_alone(lt, nx, ny, km, steps, seed)
+        np.testing.assert_array_equal(srv.state(rid), at_alone)
+        assert tuple(srv.status(rid)["content"]) == tuple(content_alone)
+    srv.close()
+
+
 def test_admission_waits_for_memory(lt):
     """A budget that holds two of these requests at a time: never more than
     two resident, and every request still finishes."""
