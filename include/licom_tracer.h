@@ -110,7 +110,8 @@ typedef enum {
 typedef struct {
   int nx, ny, km;        /* physical sizes; imt = nx+4, jmt = ny+4 */
   int precision;         /* lt_precision */
-  int diagnostics;       /* nonzero: write AX..PENETRATE */
+  int diagnostics;       /* nonzero: write AX..PENETRATE, TEND, DT_DIFF (FP64 form only; a mixed
+                            domain with diagnostics is refused with LT_E_INVALID) */
   int ew_cyclic;         /* 1 cyclic east-west, 0 closed */
   int tripole;           /* 1 tripole north fold, 0 closed north */
 } lt_grid;
@@ -164,6 +165,17 @@ int lt_step(lt_domain* dom, int nsteps);
  * fw_norm2 (fw_norm2_out) and, if content2_out is not NULL, the two global
  * tracer integrals sum(tarea*dzp*vit*tracer).  Synchronous. */
 int lt_step_host(lt_domain* dom, const double* const forcing6[6], double* fw_norm2_out, double* content2_out);
+/* The same step, asynchronous: enqueues the forcing copies, the step and the
+ * reads of fw_norm2 (and the integrals) into the given host addresses, and
+ * returns.  The domain keeps two device sets of the six forcing fields (the
+ * second allocated on the first call) and the step reads the set this call
+ * filled, so a step's copies overlap the previous step's work.  Host buffers
+ * must stay unchanged, and the outputs unread, until lt_sync; pinned memory
+ * makes the copies asynchronous.  A NULL field keeps the previous step's
+ * values.  A batch holding the domain picks up the swapped set at its next
+ * step (its descriptors are rebuilt).  No counterpart in the reference,
+ * whose tracer_ copies synchronously (tracer.cpp:1838). */
+int lt_step_host_async(lt_domain* dom, const double* const forcing6[6], double* fw_norm2_out, double* content2_out);
 /* Convective adjustment of the current state (convadj.cpp:29-288). */
 int lt_convadj(lt_domain* dom);
 

@@ -173,6 +173,7 @@ _SIGS = {
     "lt_derive_masks": ([_vp], _i),
     "lt_step": ([_vp, _i], _i),
     "lt_step_host": ([_vp, C.POINTER(_vp), C.POINTER(C.c_double), C.POINTER(C.c_double)], _i),
+    "lt_step_host_async": ([_vp, C.POINTER(_vp), _vp, _vp], _i),
     "lt_profile": ([_vp, _i], _i),
     "lt_mark": ([_vp, _i], _i),
     "lt_use_tma": ([_vp, _i], _i),
@@ -368,6 +369,13 @@ class TracerDomain:
         fw_norm2 written to a ctypes double; the timed end-to-end path."""
         arr = (_vp * 6)(*ptrs)
         _check(lib.lt_step_host(self.h, arr, C.byref(fw_out), None), "lt_step_host")
+
+    def step_host_async_ptrs(self, ptrs, fw_addr, content_addr=None):
+        """lt_step_host_async: forcing at raw host addresses (6 ints, 0 =
+        keep), fw_norm2 (and the two integrals) delivered to raw host
+        addresses once the step has run; returns at once (see sync())."""
+        arr = (_vp * 6)(*ptrs)
+        _check(lib.lt_step_host_async(self.h, arr, fw_addr, content_addr), "lt_step_host_async")
 
     def use_tma(self, on=True):
         _check(lib.lt_use_tma(self.h, int(on)), "lt_use_tma")

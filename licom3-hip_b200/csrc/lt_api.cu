@@ -484,6 +484,10 @@ size_t lt_domain_bytes(const lt_grid* g) {
 
 int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
   if (!out || !grid_ok(g) || !p) { set_error("lt_create: invalid grid or params"); return LT_E_INVALID; }
+  if (g->precision == LT_PREC_MIXED && g->diagnostics) {
+    set_error("lt_create: the diagnostics (AX .. PENETRATE, TEND, DT_DIFF) are written by the FP64 form only");
+    return LT_E_INVALID;
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("lt_create: no CUDA device");
@@ -557,6 +561,10 @@ int lt_destroy(lt_domain* d) {
   if (d->ev1) cudaEventDestroy(d->ev1);
   if (d->ev_free) cudaEventDestroy(d->ev_free);
   if (d->ev_forcing) cudaEventDestroy(d->ev_forcing);
+  for (int k = 0; k < 2; ++k) {
+    if (d->ev_set_used[k]) cudaEventDestroy(d->ev_set_used[k]);
+    if (d->ev_set_ready[k]) cudaEventDestroy(d->ev_set_ready[k]);
+  }
   if (d->copy_stream) cudaStreamDestroy(d->copy_stream);
   for (auto e : d->prof_ev) cudaEventDestroy(e);
   if (d->owns_stream) cudaStreamDestroy(d->stream);
@@ -683,6 +691,63 @@ int lt_step_host(lt_domain* d, const double* const forcing6[6], double* fw_norm2
   if (fw_norm2_out) LT_CUDA_OK(cudaMemcpyAsync(fw_norm2_out, a.scalars, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
   LT_CUDA_OK(cudaStreamSynchronize(d->stream));
   return timeout_status(d);
+}
+
+int lt_step_host_async(lt_domain* d, const double* const forcing6[6], double* fw_norm2_out, double* content2_out) {
+  if (!d) return LT_E_INVALID;
+  Arena& a = d->a;
+  double** field[6] = {&a.swv, &a.nswv, &a.sst, &a.sss, &a.fresh, &a.seaice};
+  const size_t bytes = sizeof(double) * a.A;
+  if (!d->forcing_set[1][0]) {
+    // first asynchronous step: the second set and the events
+    char* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, 6 * bytes);
+    if (e != cudaSuccess) {
+      set_error("lt_step_host_async: cudaMalloc(%zu) for the second forcing set failed", 6 * bytes);
+      return LT_E_OOM;
+    }
+    d->allocations.push_back(p);
+    for (int m = 0; m < 6; ++m) {
+      d->forcing_set[0][m] = *field[m];
+      d->forcing_set[1][m] = reinterpret_cast<double*>(p) + (size_t)m * a.A;
+    }
+    for (int s = 0; s < 2; ++s) {
+      LT_CUDA_OK(cudaEventCreateWithFlags(&d->ev_set_used[s], cudaEventDisableTiming));
+      LT_CUDA_OK(cudaEventCreateWithFlags(&d->ev_set_ready[s], cudaEventDisableTiming));
+      LT_CUDA_OK(cudaEventRecord(d->ev_set_used[s], d->stream));
+    }
+    d->forcing_cur = 0;
+  }
+  // This step reads the other set: its copies wait only for the last step
+  // that read that set (two steps back), so they overlap the previous step.
+  const int nb = d->forcing_cur ^ 1;
+  cudaStream_t cs = d->copy_stream;
+  LT_CUDA_OK(cudaStreamWaitEvent(cs, d->ev_set_used[nb], 0));
+  bool keeps = !forcing6;
+  for (int m = 0; m < 6 && !keeps; ++m) keeps = !forcing6[m];
+  if (keeps) {   // the current set may have been written on the domain's stream (lt_set_field)
+    LT_CUDA_OK(cudaEventRecord(d->ev_free, d->stream));
+    LT_CUDA_OK(cudaStreamWaitEvent(cs, d->ev_free, 0));
+  }
+  for (int m = 0; m < 6; ++m) {
+    if (forcing6 && forcing6[m])
+      LT_CUDA_OK(cudaMemcpyAsync(d->forcing_set[nb][m], forcing6[m], bytes, cudaMemcpyHostToDevice, cs));
+    else   // a field kept resident: the current set's copy, once its writers are done
+      LT_CUDA_OK(cudaMemcpyAsync(d->forcing_set[nb][m], d->forcing_set[d->forcing_cur][m], bytes,
+                                 cudaMemcpyDeviceToDevice, cs));
+  }
+  LT_CUDA_OK(cudaEventRecord(d->ev_set_ready[nb], cs));
+  for (int m = 0; m < 6; ++m) *field[m] = d->forcing_set[nb][m];
+  d->forcing_cur = nb;
+  int rc = run_step(d, d->ev_set_ready[nb]);
+  if (rc) return rc;
+  LT_CUDA_OK(cudaEventRecord(d->ev_set_used[nb], d->stream));
+  if (content2_out) {
+    if ((rc = launch_tracer_content(a, d->stream))) return rc;
+    LT_CUDA_OK(cudaMemcpyAsync(content2_out, a.scalars + 1, 2 * sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  }
+  if (fw_norm2_out) LT_CUDA_OK(cudaMemcpyAsync(fw_norm2_out, a.scalars, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+  return LT_OK;
 }
 
 int lt_convadj(lt_domain* d) {

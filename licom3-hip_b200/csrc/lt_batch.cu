@@ -25,6 +25,7 @@ using namespace lt;
 struct lt_batch {
   std::vector<lt_domain*> m;
   std::vector<int> base_cur;        // member cur when the descriptors were built
+  std::vector<const double*> base_forcing;   // member forcing set (lt_step_host_async swaps it)
   int dev = 0, sms = 148;
   bool mixed = false;
   cudaStream_t stream = nullptr;
@@ -72,12 +73,14 @@ int build_descriptors(lt_batch* b) {
   b->km_max = b->max_imt = b->max_jmt = 0;
   b->max_cols = 0;
   b->base_cur.resize(n);
+  b->base_forcing.resize(n);
   for (int i = 0; i < n; ++i) {
     lt_domain* d = b->m[i];
     const Arena& a = d->a;
     const int ntx = (a.imt + TX - 1) / TX;
     const long ntiles = (long)ntx * ((a.jmt + kMixedTileY - 1) / kMixedTileY);
     b->base_cur[i] = a.cur;
+    b->base_forcing[i] = a.swv;
     for (int p = 0; p < 2; ++p) {
       MemberDesc& e = h[p][i];
       std::memset(&e, 0, sizeof(e));
@@ -107,10 +110,11 @@ int build_descriptors(lt_batch* b) {
 }
 
 // Members stepped outside the batch since the descriptors were built (their
-// cur moved without the batch's parity) need new descriptors.
+// cur moved without the batch's parity, or their forcing set was swapped)
+// need new descriptors.
 bool descriptors_stale(const lt_batch* b) {
   for (size_t i = 0; i < b->m.size(); ++i)
-    if (b->m[i]->a.cur != (b->base_cur[i] ^ b->parity)) return true;
+    if (b->m[i]->a.cur != (b->base_cur[i] ^ b->parity) || b->m[i]->a.swv != b->base_forcing[i]) return true;
   return false;
 }
 

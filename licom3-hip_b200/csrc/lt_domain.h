@@ -17,6 +17,12 @@ struct lt_domain {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaStream_t copy_stream = nullptr;          // lt_step_host's forcing copies
   cudaEvent_t ev_free = nullptr, ev_forcing = nullptr;
+  // lt_step_host_async: two sets of the six forcing fields (set 0 the
+  // arena's, set 1 allocated on first use), the set the current step reads,
+  // and per set an event after its last reader and one after its copies
+  double* forcing_set[2][6] = {};
+  int forcing_cur = 0;
+  cudaEvent_t ev_set_used[2] = {}, ev_set_ready[2] = {};
   int profile = 0;
   int prof_steps = 0;
   std::vector<cudaEvent_t> prof_ev;   // [LT_PROF_STEPS][LT_NPHASE + 1]

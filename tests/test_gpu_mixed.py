@@ -114,3 +114,11 @@ def test_mixed_copy_path_equals_tma_path(lt):
     b.step(6)
     for n in ("AT", "ATB", "WS", "NET"):
         np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+
+
+def test_mixed_refuses_diagnostics(lt):
+    """The diagnostic fields are the FP64 form's: a mixed domain asking for
+    them is refused, not silently left without them."""
+    syn = lt.Synth(64, 40, 12)
+    with pytest.raises(lt.LtError):
+        lt.TracerDomain(64, 40, 12, syn.params, precision=lt.PREC_MIXED, diagnostics=True)

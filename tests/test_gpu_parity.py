@@ -276,6 +276,52 @@ def test_step_host_new_forcing_every_step(lt):
             assert bits_equal(g, r), "step %d %s: %s" % (step, name, mismatch(g, r))
 
 
+def test_step_host_async_double_buffered_forcing(lt):
+    """lt_step_host_async: each step's forcing goes into the other of two
+    device sets while the previous step runs.  A run of asynchronous steps
+    (some keeping a field from the step before), then a synchronous one and a
+    device step, match the oracle given the same forcing, bit for bit, with
+    every step's fw_norm2 delivered to pinned host memory."""
+    import torch
+    syn, f = make(lt, 96, 56, 16, forced=1, cap_north=0)
+    dom = gpu_domain(lt, syn, f)
+    o = oracle_for(syn, f)
+    rng = np.random.default_rng(9)
+    names = ("SWV", "NSWV", "SST", "SSS", "FRESH", "SEAICE")
+    A = f["SST"].size
+    nsteps = 6
+    keep = {2: ("SST",), 4: names}          # step -> fields left NULL (kept)
+    host = torch.empty((nsteps, 6, A), dtype=torch.float64, pin_memory=True)
+    fw = torch.zeros(nsteps, dtype=torch.float64, pin_memory=True)
+    fw_ref = []
+    for step in range(nsteps):
+        ptrs = [0] * 6
+        for m, n in enumerate(names):
+            if n in keep.get(step, ()):
+                continue
+            a = f[n] * (1.0 + 0.05 * rng.standard_normal(f[n].shape))
+            if n == "SEAICE":
+                a = np.clip(a, 0.0, 1.0)
+            host[step, m] = torch.from_numpy(np.ascontiguousarray(a).ravel())
+            ptrs[m] = host[step, m].data_ptr()
+            o.set(n, a)
+        dom.step_host_async_ptrs(ptrs, fw.data_ptr() + 8 * step)
+        o.step(1)
+        fw_ref.append(o.fw_norm2())
+    dom.sync()
+    assert fw.tolist() == fw_ref
+    for name in ("AT", "NET", "AKT", "SST", "SWV"):
+        g, r = dom.get(name), o.get(name)
+        assert bits_equal(g, r), "%s: %s" % (name, mismatch(g, r))
+    # a synchronous step and a device step go on from the set last filled
+    forcing = {"SSS": np.ascontiguousarray(f["SSS"] * 1.01)}
+    o.set("SSS", forcing["SSS"])
+    fw1, _, _ = dom.step_host(forcing)
+    dom.step(1)
+    o.step(2)
+    assert bits_equal(dom.get("AT"), o.get("AT"))
+
+
 def test_numeric_scan_flags_injected_nan(lt):
     """Failure detection without a GPU fault: a NaN planted in the state on
     the host is reported as a count and a status, the context stays usable."""
