@@ -116,6 +116,16 @@ typedef struct {
   int tripole;           /* 1 tripole north fold, 0 closed north */
 } lt_grid;
 
+/* Tracer advection scheme: pconst_mod adv_tracer, which tracer_ matches as
+ * "centered" / "flux" / "tspas" (tracer.cpp:1712-1714) and passes to the
+ * advection kernels as Str 0 / 1 / 2.  The centred and flux forms run in the
+ * FP64 form only (a mixed domain refuses them with LT_E_INVALID). */
+typedef enum {
+  LT_ADV_TSPAS = 0,     /* two-step shape-preserving (Str 2, advection_tracer_1_0/2/3), the default */
+  LT_ADV_CENTERED = 1,  /* centred differences of the tracer across each face (Str 0, advection_tracer_1) */
+  LT_ADV_FLUX = 2       /* face means times dx/dy-weighted transports (Str 1, advection_tracer_1_0/1) */
+} lt_adv_scheme;
+
 /* Scalars read by tracer_ from Fortran module variables (tracer.cpp:1712-1896). */
 typedef struct {
   double dts;            /* pconst_mod dts */
@@ -129,6 +139,7 @@ typedef struct {
   double area_t;         /* grid area_t (global ocean surface area) */
   int nss;               /* pconst_mod nss */
   int boundary_restore;  /* pconst_mod boundary_restore (1 = 15-day restoring) */
+  int adv_tracer;        /* lt_adv_scheme from pconst_mod adv_tracer (0 = tspas) */
 } lt_params;
 
 typedef struct lt_domain lt_domain;

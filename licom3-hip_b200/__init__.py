@@ -24,6 +24,9 @@ lib = C.CDLL(LIB_PATH)
 
 LT_OK, LT_E_INVALID, LT_E_OOM, LT_E_CUDA, LT_E_NUMERIC, LT_E_TIMEOUT, LT_E_STATE, LT_E_NODEVICE = range(8)
 PREC_FP64, PREC_MIXED = 0, 1
+# lt_adv_scheme: pconst_mod adv_tracer "tspas", "centered", "flux"
+ADV_TSPAS, ADV_CENTERED, ADV_FLUX = 0, 1, 2
+ADV_SCHEMES = {"tspas": ADV_TSPAS, "centered": ADV_CENTERED, "flux": ADV_FLUX}
 
 
 class LtError(RuntimeError):
@@ -40,7 +43,7 @@ class Grid(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("dts", "oncc", "onbc", "dwndmix", "gamma", "od0", "od0cp", "ah", "area_t")] + [
-        ("nss", C.c_int), ("boundary_restore", C.c_int)]
+        ("nss", C.c_int), ("boundary_restore", C.c_int), ("adv_tracer", C.c_int)]
 
 
 class IcesnowParams(C.Structure):
@@ -334,6 +337,11 @@ class TracerDomain:
     def set(self, name, array):
         a = np.ascontiguousarray(array, dtype=field_dtype(name))
         _check(lib.lt_set_field(self.h, FIELD_ID[name], a.ctypes.data, a.nbytes), "lt_set_field(%s)" % name)
+
+    def set_params(self, params):
+        """New scalars (lt_set_params) for the following steps."""
+        _check(lib.lt_set_params(self.h, C.byref(params)), "lt_set_params")
+        self.params = params
 
     def get(self, name):
         a = np.empty(self.shape(name), dtype=field_dtype(name))

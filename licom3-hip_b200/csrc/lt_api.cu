@@ -317,7 +317,9 @@ int run_step(lt_domain* d, cudaEvent_t forcing_ready) {
   mark(4);
   if (a.precision == LT_PREC_MIXED) {
     if ((rc = launch_tracer_tma_mixed(a, d->maps, d->use_tma, s, d->tma_grid))) return rc;
-  } else if (d->use_tma) {
+  } else if (d->use_tma && a.p.adv_tracer == LT_ADV_TSPAS) {
+    // the TMA column kernel is the tspas scheme's; the centred and flux
+    // schemes run in the plain-load kernel
     if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid))) return rc;
   } else {
     if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
@@ -482,12 +484,26 @@ size_t lt_domain_bytes(const lt_grid* g) {
   return pl.off;
 }
 
+// the advection scheme: one of lt_adv_scheme, and tspas in mixed precision
+static bool scheme_ok(int precision, const lt_params* p, const char* where) {
+  if (p->adv_tracer < LT_ADV_TSPAS || p->adv_tracer > LT_ADV_FLUX) {
+    set_error("%s: adv_tracer %d is not an lt_adv_scheme", where, p->adv_tracer);
+    return false;
+  }
+  if (precision == LT_PREC_MIXED && p->adv_tracer != LT_ADV_TSPAS) {
+    set_error("%s: the centred and flux advection schemes run in the FP64 form only", where);
+    return false;
+  }
+  return true;
+}
+
 int lt_create(const lt_grid* g, const lt_params* p, lt_domain** out) {
   if (!out || !grid_ok(g) || !p) { set_error("lt_create: invalid grid or params"); return LT_E_INVALID; }
   if (g->precision == LT_PREC_MIXED && g->diagnostics) {
     set_error("lt_create: the diagnostics (AX .. PENETRATE, TEND, DT_DIFF) are written by the FP64 form only");
     return LT_E_INVALID;
   }
+  if (!scheme_ok(g->precision, p, "lt_create")) return LT_E_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     set_error("lt_create: no CUDA device");
@@ -574,6 +590,7 @@ int lt_destroy(lt_domain* d) {
 
 int lt_set_params(lt_domain* d, const lt_params* p) {
   if (!d || !p) return LT_E_INVALID;
+  if (!scheme_ok(d->a.precision, p, "lt_set_params")) return LT_E_INVALID;
   if (p->boundary_restore == 1 && !d->a.restore) {
     set_error("lt_set_params: boundary_restore needs a domain created with it");
     return LT_E_STATE;

@@ -36,7 +36,7 @@ constexpr int kMixedContBoxW = 40;
 
 // Everything the step kernels touch, as raw device pointers (dense
 // [n][k][j][i] layout of the reference, i fastest).
-struct Arena {
+struct alignas(16) Arena {   // copied into shared memory as 16-byte words
   int nx, ny, km, imt, jmt;
   long A, F, FB;
   int ew_cyclic, tripole, diagnostics, precision;

@@ -13,7 +13,8 @@
 //   tree sum        deterministic SSS-normalisation sum         (tracer.cpp:1849-1868)
 //   halo(net)       in-GPU ghost fill                           (pop_haloupdate_tracer1)
 //   k_tracer_tma64  per column tile (k_tracer64 where the layout
-//                   does not allow TMA boxes), both tracers: tspas predictor/limiter,
+//                   does not allow TMA boxes, and for the centred and
+//                   flux schemes), both tracers: tspas predictor/limiter,
 //                   biharmonic diffusion, shortwave, explicit and implicit
 //                   vertical diffusion, surface terms, update   (advection_tracer_2/3, tracer_del4_1/2,
 //                                                                tracer_5..9, invtrit)
@@ -315,6 +316,11 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   const double htw_o = own ? a.htw[qo] : 0.0, hts_o = own ? a.hts[qo] : 0.0;
   const double htw_e = (own && i < imt - 1) ? a.htw[qo + 1] : 0.0;
   const double hts_n = (own && j >= 1) ? a.hts[qo - imt] : 0.0;
+  // flux scheme: each U-point mean weighted by its own dyu (west face) or
+  // dxu (south face) before the face mean (advection_tracer_1_0, Str 1)
+  const bool flux = p.adv_tracer == LT_ADV_FLUX;
+  const double dyu_o = (flux && own) ? a.dyu[qo] : 0.0, dyu_n = (flux && own && j >= 1) ? a.dyu[qo - imt] : 0.0;
+  const double dxu_o = (flux && own) ? a.dxu[qo] : 0.0, dxu_e = (flux && own && i < imt - 1) ? a.dxu[qo + 1] : 0.0;
   const double trr = own ? a.tarea_r[qo] : 0.0;
   const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
   double W = 0.0;
@@ -332,8 +338,13 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
       const long c = (long)k * A + qo;
       a.utf_out[c] = a.utf[c] * p.oncc;
       a.vtf_out[c] = a.vtf[c] * p.oncc;
-      if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] + wd[m0]) * htw_o * 0.25;
-      if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25;
+      if (flux) {
+        if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] * dyu_n + wd[m0] * dyu_o) * 0.25;
+        if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] * dxu_o + wb[m0 + 1] * dxu_e) * 0.25;
+      } else {
+        if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] + wd[m0]) * htw_o * 0.25;
+        if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25;
+      }
       double wka = 0.0;
       if (j >= 1 && i < imt - 1 && k <= kz - 1) {
         const double east = (uk[m0 + 1] + uk[mn + 1]) * htw_e;
@@ -518,7 +529,47 @@ __device__ void del4_first(TSmem& S, const Arena& a, int kk, int x0, int y0) {
   }
 }
 
-template <bool DIAG>
+// advection_tracer_1 for the centred (Str 0) and flux (Str 1) schemes at one
+// inner cell of level k (tracer.cpp:120-289), from the tile's level slots.
+// The centred form accumulates ax, ay, az with weight 1/nss, once per level
+// (the reference repeats its top- and bottom-level statements in every
+// level thread of its launch, so there those two levels' accumulations race).
+template <int ADV, bool DIAG>
+__device__ __forceinline__ double simple_adv(const TSmem& S, const Arena& a, int k, int n, long cg, int rc, int hc,
+                                             int uc, int vc, const double* at_c, const double* at_u,
+                                             const double* at_d) {
+  const int km = a.km;
+  const double* odzp = a.odzp;
+  const double tr = S.tr[hc];
+  const double c = at_c[rc], e = at_c[rc + 1], w = at_c[rc - 1], s = at_c[rc + RX], nn = at_c[rc - RX];
+  const double* uw = S.uw[k & 1];
+  const double* vs = S.vs[k & 1];
+  const double ue = uw[uc + 1], uwc = uw[uc], vsc = vs[vc], vn = vs[vc - QX];
+  const double wk = S.ws[slot3(k)][hc];
+  const double w1 = k < km - 1 ? S.ws[slot3(k + 1)][hc] : 0.0;
+  if (ADV == LT_ADV_CENTERED) {
+    const double h = (-uwc * (c - w) - ue * (e - c) - vsc * (s - c) - vn * (c - nn)) * tr;
+    double z;
+    if (k == 0) z = 0.5 * odzp[0] * (w1 * (c - at_d[rc]));
+    else if (k == km - 1) z = 0.5 * odzp[km - 1] * (wk * (at_u[rc] - c));
+    else z = 0.5 * odzp[k] * (wk * (at_u[rc] - c) + w1 * (c - at_d[rc]));
+    if (DIAG) {
+      const long q = (long)n * a.F + cg;
+      const double nss = (double)a.p.nss;
+      a.ax[q] = a.ax[q] + (-uwc * (c - w) - ue * (e - c)) * tr / nss;
+      a.ay[q] = a.ay[q] + (-vsc * (s - c) - vn * (c - nn)) * tr / nss;
+      a.az[q] = a.az[q] - z / nss;
+    }
+    return h - z;
+  } else {
+    const double h = (-uwc * (c + w) + ue * (e + c) - vn * (c + nn) + vsc * (s + c)) * tr;
+    const double z1 = k == 0 ? 0.0 : wk * (at_u[rc] + c) * 0.5;
+    const double z2 = k == km - 1 ? 0.0 : w1 * (c + at_d[rc]) * 0.5;
+    return h - odzp[k] * (z2 - z1);
+  }
+}
+
+template <bool DIAG, int ADV>
 __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long ntiles) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TSmem& S = *reinterpret_cast<TSmem*>(smem_raw);
@@ -578,7 +629,7 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
     load_region(S.uw[(km - 1) & 1], a.uwf + (long)(km - 1) * A, y0 - 1, x0 - 2, QY, RX, imt, jmt);
     load_region(S.vs[(km - 1) & 1], a.vsf + (long)(km - 1) * A, y0 - 2, x0 - 1, QY + 1, QX, imt, jmt);
     __syncthreads();
-    predictor_level(S, a, km - 1, x0, y0);
+    if (ADV == LT_ADV_TSPAS) predictor_level(S, a, km - 1, x0, y0);
 
     const bool own = (i < imt && j < jmt);
     const bool ring = own && i >= 1 && i < imt - 1 && j >= 1 && j < jmt - 1;
@@ -611,14 +662,19 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
       if (k == km - 1) wkc_k = 0.0;
       __syncthreads();
       // ---- phase B: predictor one level up, first Laplacian at this level
-      if (k >= 1) predictor_level(S, a, k - 1, x0, y0);
+      if (ADV == LT_ADV_TSPAS && k >= 1) predictor_level(S, a, k - 1, x0, y0);
       del4_first(S, a, k, x0, y0);
       __syncthreads();
       // ---- phase C: own column
-      if (ring) {
+      if (ADV == LT_ADV_TSPAS ? ring : inner) {
         const double* at_c = S.at[slot4(k)];
         const double* at_u = k > 0 ? S.at[slot4(k - 1)] : nullptr;
         const double* at_d = k < km - 1 ? S.at[slot4(k + 1)] : nullptr;
+        const long cg = (long)k * A + qo;
+        double adv;
+        if constexpr (ADV != LT_ADV_TSPAS) {
+          adv = simple_adv<ADV, DIAG>(S, a, k, n, cg, rc, hc, uc, vc, at_c, at_u, at_d);
+        } else {
         const double* o00 = S.a00[slot3(k)];
         const double* omx = S.amx[slot3(k)];
         const double* omn = S.amn[slot3(k)];
@@ -684,13 +740,13 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
         const double xx = -(x0v + xy1 + xy2 + cx);
         const double yy = -(y0v + xy3 + xy4 + cy);
         const double zz = -(za + zb1 + zb2 + zc);
-        const double adv = xx + yy + zz;
-        const long cg = (long)k * A + qo;
+        adv = xx + yy + zz;
         if (DIAG) {
           a.ax[n * F + cg] = xx;
           a.ay[n * F + cg] = yy;
           a.az[n * F + cg] = zz;
         }
+        }  // tspas
         if (inner) {
           const double vit_k = k < kz ? 1.0 : 0.0;
           const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
@@ -755,7 +811,7 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
           }
           // explicit update (tracer_8) and one elimination step of the
           // implicit sweep (invtrit, tracer.cpp:923-978)
-          const double d8 = c + dts * tf;
+          const double d8 = at_c[rc] + dts * tf;
           double ev = 0.0, fv = d8;
           if (k < kz) {
             double a8, c8, b8;
@@ -1540,14 +1596,21 @@ int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots) {
   const int ntx = (a.imt + TX - 1) / TX;
   const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
   const size_t sm = sizeof(TSmem);
+  // [scheme][diagnostics]: lt_adv_scheme order
+  using Kern = void (*)(Arena, int, long);
+  static const Kern kern[3][2] = {
+      {k_tracer64<false, LT_ADV_TSPAS>, k_tracer64<true, LT_ADV_TSPAS>},
+      {k_tracer64<false, LT_ADV_CENTERED>, k_tracer64<true, LT_ADV_CENTERED>},
+      {k_tracer64<false, LT_ADV_FLUX>, k_tracer64<true, LT_ADV_FLUX>}};
   static bool attr = false;
   if (!attr) {
-    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    LT_CUDA_OK(cudaFuncSetAttribute(k_tracer64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    for (auto& row : kern)
+      for (Kern k : row) LT_CUDA_OK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     attr = true;
   }
-  if (a.diagnostics) k_tracer64<true><<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
-  else k_tracer64<false><<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
+  const int adv = a.p.adv_tracer;
+  if (adv < LT_ADV_TSPAS || adv > LT_ADV_FLUX) return LT_E_INVALID;
+  kern[adv][a.diagnostics ? 1 : 0]<<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
   LT_LAUNCHED();
   return LT_OK;
 }

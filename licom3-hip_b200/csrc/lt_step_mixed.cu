@@ -58,9 +58,6 @@ __device__ __forceinline__ double face_y64(float wc, float we, double hts) {
   return ((double)wc + (double)we) * hts * 0.25;
 }
 __device__ __forceinline__ float face32(float w1, float w2, float h) { return (w1 + w2) * h * 0.25f; }
-// Lax-Wendroff part of a face flux, d*u*u*(2 dts / (h_t h_u)): one expression
-// wherever a face is used, so both cells of the face get the same value
-__device__ __forceinline__ float lw_part(float d, float u, float c) { return d * u * u * c; }
 
 
 // ------------------------------------------------------------- continuity

@@ -64,6 +64,7 @@ int lt_synth_params(const lt_synth* s, lt_params* p) {
   p->dts = d.dts; p->oncc = d.oncc; p->onbc = d.onbc; p->dwndmix = d.dwndmix; p->gamma = d.gamma;
   p->od0 = d.od0; p->od0cp = d.od0cp; p->ah = d.ah; p->area_t = d.area_t; p->nss = d.nss;
   p->boundary_restore = 0;
+  p->adv_tracer = LT_ADV_TSPAS;
   return LT_OK;
 }
 

@@ -213,6 +213,60 @@ void halo_r8(double* a, int nz, int imt, int jmt, int ew_cyclic, int tripole) {
   }
 }
 
+// advection_tracer_1 for Str 0 (centered) and Str 1 (flux), tracer.cpp:120-289:
+// adv_tt on the inner cells (2 <= j < jmt-2, 2 <= i < imt-2) of every level.
+// The centred form also accumulates the diagnostics ax, ay, az with weight
+// 1/nss.  The reference writes its top- and bottom-level statements without a
+// level guard, so every thread of the launch's level dimension repeats them
+// and their diagnostic accumulations race; here each level is accumulated
+// once (adv_tt itself gets the same value from every repetition).
+void advect_simple(Oracle& o, int n, const double* atn, const double* uw, const double* vs, const double* ws,
+                   double* adv_tt, bool dg) {
+  const int km = o.km, imt = o.imt, jmt = o.jmt;
+  const long A = o.A, F = o.F;
+  const double* tarea_r = o.fd[LT_F_TAREA_R].data();
+  const double* odzp = o.fd[LT_F_ODZP].data();
+  double* ax = o.fd[LT_F_AX].data();
+  double* ay = o.fd[LT_F_AY].data();
+  double* az = o.fd[LT_F_AZ].data();
+  const double nss = (double)o.p.nss;
+  const bool centered = o.p.adv_tracer == LT_ADV_CENTERED;
+#pragma omp parallel for
+  for (int k = 0; k < km; ++k)
+    for (int j = 2; j < jmt - 2; ++j)
+      for (int i = 2; i < imt - 2; ++i) {
+        const long c = (long)k * A + (long)j * imt + i;
+        const double tr = tarea_r[(long)j * imt + i];
+        const double ac = atn[c], ae = atn[c + 1], aw = atn[c - 1], as = atn[c + imt], an = atn[c - imt];
+        if (centered) {
+          const double h = (-uw[c] * (ac - aw) - uw[c + 1] * (ae - ac) - vs[c] * (as - ac) - vs[c - imt] * (ac - an)) * tr;
+          if (dg) {
+            ax[n * F + c] = ax[n * F + c] + (-uw[c] * (ac - aw) - uw[c + 1] * (ae - ac)) * tr / nss;
+            ay[n * F + c] = ay[n * F + c] + (-vs[c] * (as - ac) - vs[c - imt] * (ac - an)) * tr / nss;
+          }
+          double z;
+          if (k == 0) {
+            const double z2 = ws[c + A] * (ac - atn[c + A]);
+            z = 0.5 * odzp[0] * z2;
+          } else if (k == km - 1) {
+            const double z1 = ws[c] * (atn[c - A] - ac);
+            z = 0.5 * odzp[km - 1] * z1;
+          } else {
+            const double z1 = ws[c] * (atn[c - A] - ac);
+            const double z2 = ws[c + A] * (ac - atn[c + A]);
+            z = 0.5 * odzp[k] * (z1 + z2);
+          }
+          adv_tt[c] = h - z;
+          if (dg) az[n * F + c] = az[n * F + c] - z / nss;
+        } else {
+          const double h = (-uw[c] * (ac + aw) + uw[c + 1] * (ae + ac) - vs[c - imt] * (ac + an) + vs[c] * (as + ac)) * tr;
+          const double z1 = k == 0 ? 0.0 : ws[c] * (atn[c - A] + ac) * 0.5;
+          const double z2 = k == km - 1 ? 0.0 : ws[c + A] * (ac + atn[c + A]) * 0.5;
+          adv_tt[c] = h - odzp[k] * (z2 - z1);
+        }
+      }
+}
+
 // ------------------------------------------------------------ the step
 void tracer_call(Oracle& o) {
   const int km = o.km, imt = o.imt, jmt = o.jmt;
@@ -241,6 +295,8 @@ void tracer_call(Oracle& o) {
   const double* hts = o.fd[LT_F_HTS].data();
   const double* hun = o.fd[LT_F_HUN].data();
   const double* hue = o.fd[LT_F_HUE].data();
+  const double* dxu = o.fd[LT_F_DXU].data();
+  const double* dyu = o.fd[LT_F_DYU].data();
   const double* ahf = o.fd[LT_F_AHF].data();
   const double* dtn = o.fd[LT_F_DTN].data();
   const double* dts_c = o.fd[LT_F_DTS].data();
@@ -359,14 +415,25 @@ void tracer_call(Oracle& o) {
     double* atbn = atb + n * FB;
     std::fill(o.tf.begin(), o.tf.end(), 0.0);
     std::fill(o.adv_tt.begin(), o.adv_tt.end(), 0.0);
-    // advection_tracer_1_0 (tspas): face transports
+    // advection_tracer_1_0: face transports, the U-point means times the
+    // face lengths (tspas, centered) or times dxu / dyu before the mean (flux)
+    const bool flux_faces = p.adv_tracer == LT_ADV_FLUX;
 #pragma omp parallel for
     for (int k = 0; k < km; ++k)
       for (int j = 0; j < jmt; ++j)
         for (int i = 0; i < imt; ++i) {
-          if (i >= 1 && i < imt - 1) vs[C(k, j, i)] = (wkb[C(k, j, i)] + wkb[C(k, j, i + 1)]) * hts[Q(j, i)] * 0.25;
-          if (j >= 1 && j < jmt - 1) uw[C(k, j, i)] = (wkd[C(k, j - 1, i)] + wkd[C(k, j, i)]) * htw[Q(j, i)] * 0.25;
+          if (flux_faces) {
+            if (i >= 1 && i < imt - 1)
+              vs[C(k, j, i)] = (wkb[C(k, j, i)] * dxu[Q(j, i)] + wkb[C(k, j, i + 1)] * dxu[Q(j, i + 1)]) * 0.25;
+            if (j >= 1 && j < jmt - 1)
+              uw[C(k, j, i)] = (wkd[C(k, j - 1, i)] * dyu[Q(j - 1, i)] + wkd[C(k, j, i)] * dyu[Q(j, i)]) * 0.25;
+          } else {
+            if (i >= 1 && i < imt - 1) vs[C(k, j, i)] = (wkb[C(k, j, i)] + wkb[C(k, j, i + 1)]) * hts[Q(j, i)] * 0.25;
+            if (j >= 1 && j < jmt - 1) uw[C(k, j, i)] = (wkd[C(k, j - 1, i)] + wkd[C(k, j, i)]) * htw[Q(j, i)] * 0.25;
+          }
         }
+    if (p.adv_tracer != LT_ADV_TSPAS) advect_simple(o, n, atn, uw, vs, ws, adv_tt, dg);
+    else {
     // advection_tracer_2: predictor at00 and masked 7-point extrema
 #pragma omp parallel for
     for (int k = 0; k < km; ++k)
@@ -483,6 +550,7 @@ void tracer_call(Oracle& o) {
             az[n * F + c] = zz;
           }
         }
+    }  // tspas
     // tracer_del4_1: first masked Laplacian of atb, scaled by ahf
     std::fill(o.d2tk.begin(), o.d2tk.end(), 0.0);
     auto lap = [&](const double* fld, long c, long a, int k) {

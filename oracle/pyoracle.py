@@ -63,7 +63,7 @@ def _dtype(name):
 class Params(C.Structure):
     """lt_params (include/licom_tracer.h)."""
     _fields_ = [(n, C.c_double) for n in ("dts", "oncc", "onbc", "dwndmix", "gamma", "od0", "od0cp", "ah", "area_t")] + [
-        ("nss", C.c_int), ("boundary_restore", C.c_int)]
+        ("nss", C.c_int), ("boundary_restore", C.c_int), ("adv_tracer", C.c_int)]
 
 
 class SynthConfig(C.Structure):
@@ -154,6 +154,7 @@ class Oracle:
         if not self.h:
             raise ValueError("oracle: bad sizes")
         self._params = params
+        self._boundaries = (int(ew_cyclic), int(tripole))
         lib.or_set_params(self.h, C.byref(params), int(ew_cyclic), int(tripole))
         if threads:
             lib.or_set_threads(threads)
@@ -181,6 +182,10 @@ class Oracle:
     def load(self, inputs):
         for n, a in inputs.items():
             self.set(n, a)
+
+    def set_params(self, params):
+        self._params = params
+        self.lib.or_set_params(self.h, C.byref(params), *self._boundaries)
 
     def step(self, nsteps=1):
         self.lib.or_step(self.h, nsteps)

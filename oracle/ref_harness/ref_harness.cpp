@@ -186,6 +186,11 @@ int ref_set_params(const lt_params* p, int ew_cyclic, int tripole) {
   pconst_mod_mp_dwndmix_ = p->dwndmix; pconst_mod_mp_gamma_ = p->gamma; pconst_mod_mp_od0_ = p->od0;
   pconst_mod_mp_od0cp_ = p->od0cp; hmix_del4_mp_ah_ = p->ah; grid_mp_area_t_ = p->area_t;
   pconst_mod_mp_nss_ = p->nss; pconst_mod_mp_boundary_restore_ = p->boundary_restore;
+  // the namelist string tracer_ matches (tracer.cpp:1712-1714), blank-padded
+  // like a Fortran CHARACTER variable
+  const char* scheme = p->adv_tracer == LT_ADV_CENTERED ? "centered" : p->adv_tracer == LT_ADV_FLUX ? "flux" : "tspas";
+  std::memset(pconst_mod_mp_adv_tracer_, ' ', sizeof(pconst_mod_mp_adv_tracer_));
+  std::memcpy(pconst_mod_mp_adv_tracer_, scheme, std::strlen(scheme));
   g_ew_cyclic = ew_cyclic; g_tripole = tripole;
   return 0;
 }

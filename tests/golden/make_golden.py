@@ -4,7 +4,8 @@ Runs LICOM3-HIP's tracer.cpp, convadj.cpp, icesnow.cpp and readyc.cpp
 (turb_cu and the momentum biharmonic friction), compiled for the CPU by oracle/Makefile (target ``ref``) from the
 reference tree, on seeded
 synthetic inputs (with the restoring branch on in the cases of
-tests/restore_case.py) at the reference's built-in block size (36 x 40 physical, 55
+tests/restore_case.py, the centred and flux advection schemes in those of
+tests/scheme_case.py) at the reference's built-in block size (36 x 40 physical, 55
 levels) and records SHA-256 digests of every output field plus fw_norm2.  The
 icesnow cases start from the cold states of tests/icesnow_state.py; the
 turbulence cases use the closure inputs and stand-in tables of
@@ -29,6 +30,7 @@ from icesnow_state import ICE_CASES, cold_state  # noqa: E402
 from turb_case import DFRICMX, NCC, TURB_CASES, case, tables  # noqa: E402
 import del4u_case  # noqa: E402
 import restore_case  # noqa: E402
+import scheme_case  # noqa: E402
 
 CASES = [(1, 5, 20240611), (0, 3, 7), (1, 2, 99)]
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
@@ -73,6 +75,19 @@ def main():
         out["restore_forced%d_steps%d_seed%d" % (forced, nsteps, seed)] = {
             "inputs": {"AT": digest(inp["AT"]), "RESTORE": digest(inp["RESTORE"])},
             "outputs": {n: digest(ref.get(n)) for n in OUT_FIELDS},
+            "fw_norm2": ref.fw_norm2(),
+        }
+    for scheme, forced, nsteps, seed in scheme_case.SCHEME_CASES:
+        syn, p, inp = scheme_case.case(lt, scheme, forced, seed)
+        ref = pyoracle.Reference(p)
+        ref.load(inp)
+        for s in range(nsteps):
+            ref.tracer_call(s)
+        ref.convadj()
+        out["scheme_%s_forced%d_steps%d_seed%d" % (scheme, forced, nsteps, seed)] = {
+            "inputs": {"AT": digest(inp["AT"])},
+            # the centred scheme's racy diagnostic levels left out
+            "outputs": {n: digest(scheme_case.comparable(scheme, n, ref.get(n))) for n in OUT_FIELDS},
             "fw_norm2": ref.fw_norm2(),
         }
     for frc_core, nsteps, seed in ICE_CASES:

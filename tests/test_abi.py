@@ -81,3 +81,19 @@ def test_domain_bytes_admission(lt):
     assert nbytes < 180e9
     bad = lt.Grid(3601, 2302, 55, 0, 0, 1, 1)  # tripole needs even nx
     assert lt.lib.lt_domain_bytes(C.byref(bad)) == 0
+
+
+def test_advection_scheme_checked_before_device_work(lt):
+    """The scheme is validated on the host (no device needed): an unknown
+    scheme, and the centred / flux schemes in mixed precision, are
+    LT_E_INVALID with a message."""
+    syn = lt.Synth(16, 12, 5)
+    h = C.c_void_p()
+    for prec, adv, ok in ((lt.PREC_MIXED, lt.ADV_CENTERED, False), (lt.PREC_MIXED, lt.ADV_FLUX, False),
+                          (lt.PREC_FP64, 3, False), (lt.PREC_FP64, -1, False)):
+        p = type(syn.params).from_buffer_copy(syn.params)
+        p.adv_tracer = adv
+        g = lt.Grid(16, 12, 5, prec, 0, 1, 1)
+        rc = lt.lib.lt_create(C.byref(g), C.byref(p), C.byref(h))
+        assert rc == lt.LT_E_INVALID, (prec, adv)
+        assert b"adv" in lt.lib.lt_last_error() or b"FP64 form only" in lt.lib.lt_last_error()

@@ -19,6 +19,7 @@ from conftest import REPO
 
 import pyoracle
 import restore_case
+import scheme_case
 
 GOLDEN = os.path.join(REPO, "tests", "golden", "reference_digests.json")
 OUT_FIELDS = ["AT", "ATB", "WS", "NET", "UTF", "VTF", "VTL", "H0F", "AKT", "AX", "AY", "AZ", "DZ", "TEND",
@@ -127,6 +128,66 @@ def test_oracle_restoring_matches_golden_digests(lt, forced, nsteps, seed):
     q.convadj()
     d = np.abs(o.get("AT") - q.get("AT"))
     assert d[0, 1:].max() > 1e-4 and d[0, 0].max() < d[0, 1:].max()
+
+
+def run_scheme_oracle(lt, scheme, forced, nsteps, seed):
+    syn, p, f = scheme_case.case(lt, scheme, forced, seed)
+    o = pyoracle.Oracle(syn.nx, syn.ny, syn.km, p)
+    o.load(f)
+    for _ in range(nsteps):
+        o.tracer_call()
+    o.convadj()
+    return syn, p, f, o
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference tree not built here")
+@pytest.mark.parametrize("scheme,forced,nsteps,seed", scheme_case.SCHEME_CASES)
+def test_oracle_scheme_bitexact_vs_reference(lt, scheme, forced, nsteps, seed):
+    """The centred and flux advection schemes against the reference's own
+    tracer.cpp, bit for bit (the centred scheme's racy diagnostic levels left
+    out; their emulated value is the once-per-level one times the number of
+    level threads of the launch)."""
+    syn, p, f, o = run_scheme_oracle(lt, scheme, forced, nsteps, seed)
+    ref = pyoracle.Reference(p)
+    ref.load(f)
+    for s in range(nsteps):
+        ref.tracer_call(s)
+    ref.convadj()
+    assert o.fw_norm2() == ref.fw_norm2()
+    for name in OUT_FIELDS:
+        a = scheme_case.comparable(scheme, name, o.get(name))
+        b = scheme_case.comparable(scheme, name, ref.get(name))
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), name
+    if scheme == "centered":
+        repeats = -(-syn.km // 4) * 4     # the launch's level threads (blocks of 4 levels)
+        for name in scheme_case.RACY_DIAG:
+            a, b = o.get(name), ref.get(name)
+            assert np.abs(a[:, 0]).max() > 0
+            for k in (0, syn.km - 1):
+                assert np.allclose(b[:, k], repeats * a[:, k], rtol=1e-9, atol=0), (name, k)
+    else:
+        assert not np.any(o.get("AX"))   # the flux scheme writes no diagnostics
+    # the scheme matters: the tspas run of the same inputs differs
+    tspas = type(p).from_buffer_copy(p)
+    tspas.adv_tracer = lt.ADV_TSPAS
+    q = pyoracle.Oracle(syn.nx, syn.ny, syn.km, tspas)
+    q.load(f)
+    for _ in range(nsteps):
+        q.tracer_call()
+    q.convadj()
+    assert np.abs(o.get("AT") - q.get("AT")).max() > 1e-6
+
+
+@pytest.mark.parametrize("scheme,forced,nsteps,seed", scheme_case.SCHEME_CASES)
+def test_oracle_scheme_matches_golden_digests(lt, scheme, forced, nsteps, seed):
+    gold = json.load(open(GOLDEN))
+    key = "scheme_%s_forced%d_steps%d_seed%d" % (scheme, forced, nsteps, seed)
+    assert key in gold, "regenerate tests/golden with make_golden.py"
+    syn, p, f, o = run_scheme_oracle(lt, scheme, forced, nsteps, seed)
+    assert digest(f["AT"]) == gold[key]["inputs"]["AT"]
+    for name in OUT_FIELDS:
+        assert digest(scheme_case.comparable(scheme, name, o.get(name))) == gold[key]["outputs"][name], name
+    assert o.fw_norm2() == gold[key]["fw_norm2"]
 
 
 def test_halo_restatement_matches_generator_halo(lt):
