@@ -235,9 +235,11 @@ constexpr int kCont64TileY = 8;   // tile height of the FP64 continuity march (4
 // is computed; each thread converts the points it copied itself (mean
 // velocities wkd, wkb and the free-surface scaled uk, vk, whose level-free
 // factor it keeps in registers) into a double-buffered level, read by all
-// after the step's one barrier.  The column divergence W accumulates in level
-// order during the march; w is integrated upward afterwards from the wka the
-// march wrote.
+// after the step's one barrier.  Each thread's first copy is its own cell's
+// point, so the scaled utf, vtf it writes come from its own staged copies
+// (a global re-read of them per level cost 9.00 -> 7.67 ms per 0.1-degree
+// step).  The column divergence W accumulates in level order during the
+// march; w is integrated upward afterwards from the wka the march wrote.
 template <int BY>
 __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   constexpr int BX = 32, UX = BX + 1, UY = BY + 1, UN = UX * UY, NT = BX * BY;
@@ -249,14 +251,24 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   const int imt = a.imt, jmt = a.jmt, km = a.km;
   const long A = a.A;
   const lt_params& p = a.p;
+  static_assert(NPT == 2 && UN - NT == UX + BY, "own point plus one of the row above or the column east");
+  // region point of this thread's copy pt: its own cell's U point first (so
+  // that the own point's raw velocities are this thread's own copies, read
+  // without a barrier), then one point of the row above the tile (threads
+  // 0 .. UX-1) or of the column east of it (threads UX .. UX+BY-1)
+  auto point_of = [&](int pt) {
+    if (pt == 0) return (ty + 1) * UX + tx;
+    return tid < UX ? tid : (tid - UX + 1) * UX + BX;
+  };
+  const bool has_extra = tid < UX + BY;
   long rq[NPT];
   bool rin[NPT], rok[NPT];
   double rfac[NPT];
 #pragma unroll
   for (int pt = 0; pt < NPT; ++pt) {
-    const int m = tid + pt * NT;
+    const int m = point_of(pt);
     const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
-    rin[pt] = m < UN && uj >= 0 && uj < jmt && ui < imt;
+    rin[pt] = (pt == 0 || has_extra) && uj >= 0 && uj < jmt && ui < imt;
     rq[pt] = rin[pt] ? q2(uj, ui, imt) : 0;
     rok[pt] = rin[pt] && uj < jmt - 1 && ui >= 1;
     rfac[pt] = 0.0;
@@ -273,7 +285,7 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
 #pragma unroll
       for (int pt = 0; pt < NPT; ++pt) {
         if (!rin[pt]) continue;
-        const int m = tid + pt * NT;
+        const int m = point_of(pt);
         const long c = lvl + rq[pt];
         double(*st)[UN] = s_st[L % NST];
         cp_async8(&st[0][m], a.utf + c);
@@ -284,13 +296,19 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
     }
     cp_async_commit();
   };
-  // the points this thread copied, level L, into buffer b
+  // the points this thread copied, level L, into buffer b; the own point's
+  // raw utf, vtf of level L into own_utf, own_vtf
+  double own_utf = 0.0, own_vtf = 0.0;
   auto park = [&](int L, int b) {
     const double(*st)[UN] = s_st[L % NST];
 #pragma unroll
     for (int pt = 0; pt < NPT; ++pt) {
-      const int m = tid + pt * NT;
-      if (m >= UN) continue;
+      if (pt > 0 && !has_extra) continue;
+      const int m = point_of(pt);
+      if (pt == 0) {
+        own_utf = rin[0] ? st[0][m] : 0.0;
+        own_vtf = rin[0] ? st[2][m] : 0.0;
+      }
       double wkd = 0.0, wkb = 0.0, uk = 0.0, vk = 0.0;
       if (rin[pt]) {
         wkd = 0.5 * (st[0][m] * p.oncc) + 0.5 * st[1][m];
@@ -324,8 +342,11 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   const double trr = own ? a.tarea_r[qo] : 0.0;
   const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
   double W = 0.0;
+  double dzp_k = a.dzp[0];
   for (int k = 0; k < km; ++k) {
     const int b = k & 1;
+    const double dzp_c = dzp_k;
+    if (k + 1 < km) dzp_k = a.dzp[k + 1];
     // level k parked by every thread; buffer b^1 and the staging slot of
     // level k are no longer read
     __syncthreads();
@@ -336,8 +357,8 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
       const double* uk = s_uk[b];
       const double* vk = s_vk[b];
       const long c = (long)k * A + qo;
-      a.utf_out[c] = a.utf[c] * p.oncc;
-      a.vtf_out[c] = a.vtf[c] * p.oncc;
+      a.utf_out[c] = own_utf * p.oncc;
+      a.vtf_out[c] = own_vtf * p.oncc;
       if (flux) {
         if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] * dyu_n + wd[m0] * dyu_o) * 0.25;
         if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] * dxu_o + wb[m0 + 1] * dxu_e) * 0.25;
@@ -354,7 +375,7 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
         wka = 0.5 * (east - west + south - north) * trr;
       }
       a.wka[c] = wka;
-      if (col) W = W - a.dzp[k] * wka * (k < kz ? 1.0 : 0.0);
+      if (col) W = W - dzp_c * wka * (k < kz ? 1.0 : 0.0);
     }
     if (k + 1 < km) {
       cp_async_wait<2>();   // this thread's copies of level k+1 have landed

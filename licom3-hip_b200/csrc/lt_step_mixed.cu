@@ -254,8 +254,11 @@ constexpr int kContTileY = kMixedContTileY;   // tile height of the single-domai
 // loads are in flight; each thread forms the U-point means it needs from
 // them (u_mean32, the same bits as the plain-load march).  The partial sums
 // P(k) of the upward integration stay in shared memory behind the ring (km
-// floats per column) instead of making a round trip through the ws field.
-constexpr int kContRing = 6;
+// floats per column) instead of making a round trip through the ws field
+// (through ws: 3.77 -> 3.93 ms per 0.1-degree step, the round trip reaches
+// DRAM).  Four slots leave room for five CTAs per SM (six slots: four CTAs,
+// 3.77 ms; four slots: 3.55 ms).
+constexpr int kContRing = 4;
 constexpr int CRW = kMixedContBoxW, CRR = kMixedContTileY + 1;
 struct alignas(128) ContSlot {
   struct alignas(128) Box { float v[CRR * CRW]; };
