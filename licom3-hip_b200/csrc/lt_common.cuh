@@ -29,10 +29,11 @@ constexpr int kMixedBoxW64 = TX + 4;
 constexpr int kMixedScratchPerLevel = 4;
 constexpr int kMixedMaxLevels = 128;
 // The mixed continuity march: tiles of 32 x kMixedContTileY columns, each
-// level's U-point velocities as boxes kMixedContBoxW wide (x0-4 .. x0+35)
-// and kMixedContTileY+1 rows (y0-1 .. y0+kMixedContTileY-1).
+// level's U-point velocities as boxes kMixedContBoxW wide (x0 .. x0+35: the
+// 33 columns the march reads, rounded up to 16 bytes) and kMixedContTileY+1
+// rows (y0-1 .. y0+kMixedContTileY-1).
 constexpr int kMixedContTileY = 4;
-constexpr int kMixedContBoxW = 40;
+constexpr int kMixedContBoxW = 36;
 
 // Everything the step kernels touch, as raw device pointers (dense
 // [n][k][j][i] layout of the reference, i fastest).

@@ -256,17 +256,22 @@ constexpr int kContTileY = kMixedContTileY;   // tile height of the single-domai
 // P(k) of the upward integration stay in shared memory behind the ring (km
 // floats per column) instead of making a round trip through the ws field
 // (through ws: 3.77 -> 3.93 ms per 0.1-degree step, the round trip reaches
-// DRAM).  Four slots leave room for five CTAs per SM (six slots: four CTAs,
-// 3.77 ms; four slots: 3.55 ms).
-constexpr int kContRing = 4;
+// DRAM).  The ring's depth and the boxes' width set how many CTAs fit on an
+// SM: six slots of 40-column boxes, four CTAs (3.77 ms); four slots, five
+// CTAs (3.55 ms); three slots of 36-column boxes with the free-surface
+// factors in registers, six CTAs (3.54 ms: the march runs at about 72 % of
+// the measured copy bandwidth in either of the last two shapes).
+constexpr int kContRing = 3;
 constexpr int CRW = kMixedContBoxW, CRR = kMixedContTileY + 1;
+// A tiled TMA load writes to a 128-byte aligned shared-memory address: every
+// box starts on a 128-byte boundary (a 16-byte aligned box faulted with a
+// misaligned address).
 struct alignas(128) ContSlot {
   struct alignas(128) Box { float v[CRR * CRW]; };
   Box f[4];   // utf, vtf, utl, vtl
 };
 struct ContSmem {
   ContSlot slot[kContRing];
-  float fm1[CRR * (CBX + 1)];
   uint64_t bar[kContRing];
 };
 constexpr uint32_t kContLevelBytes = 4 * CRR * CRW * sizeof(float);
@@ -274,7 +279,7 @@ constexpr uint32_t kContLevelBytes = 4 * CRR * CRW * sizeof(float);
 __global__ void __launch_bounds__(CBX * kContTileY) k_cont_tma32(Arena a, const __grid_constant__ TracerMaps maps) {
   extern __shared__ __align__(128) unsigned char smem_ct[];
   ContSmem& S = *reinterpret_cast<ContSmem*>(smem_ct);
-  constexpr int UX = CBX + 1, NT = CBX * kContTileY;
+  constexpr int NT = CBX * kContTileY;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * CBX + tx;
   float* ps = reinterpret_cast<float*>(smem_ct + sizeof(ContSmem)) + tid;   // P(k) at ps[k * NT]
   const int x0 = blockIdx.x * CBX, y0 = blockIdx.y * kContTileY;
@@ -290,12 +295,13 @@ __global__ void __launch_bounds__(CBX * kContTileY) k_cont_tma32(Arena a, const 
     if (tid == 0 && k < km) {
       const int r = k % kContRing;
       mbar_expect_tx(&S.bar[r], kContLevelBytes);
-      for (int v = 0; v < 4; ++v) tma_load_3d(S.slot[r].f[v].v, &maps.vel[v], x0 - 4, y0 - 1, k, &S.bar[r]);
+      for (int v = 0; v < 4; ++v) tma_load_3d(S.slot[r].f[v].v, &maps.vel[v], x0, y0 - 1, k, &S.bar[r]);
     }
   };
   for (int k = 0; k < kContRing; ++k) issue(k);
-  for (int m = tid; m < CRR * UX; m += NT) {
-    const int uj = y0 - 1 + m / UX, ui = x0 + m % UX;
+  // the free-surface factor minus one at U point (uj, ui), -1 where the
+  // reference's uk/vk are zero (as cont_tile forms it for its region)
+  auto fm1_at = [&](int uj, int ui) {
     float fm1 = -1.f;
     if (uj >= 0 && uj < jmt - 1 && ui >= 1 && ui < imt) {
       const long q = (long)uj * imt + ui;
@@ -303,8 +309,8 @@ __global__ void __launch_bounds__(CBX * kContTileY) k_cont_tma32(Arena a, const 
                           a.auw[q] * a.stf_ssh[q - 1] + a.ausw[q] * a.stf_ssh[q + imt - 1];
       fm1 = (float)(work * a.ohbu[q]);
     }
-    S.fm1[m] = fm1;
-  }
+    return fm1;
+  };
   const int i = x0 + tx, j = y0 + ty;
   const bool own = i < imt && j < jmt;
   const bool div_here = own && j >= 1 && i < imt - 1;
@@ -313,11 +319,9 @@ __global__ void __launch_bounds__(CBX * kContTileY) k_cont_tma32(Arena a, const 
   const int kz = own ? a.kmt[qo] : 0;
   const ContCell g{own ? a.htw[qo] : 0.0, div_here ? a.htw[qo + 1] : 0.0, own ? a.hts[qo] : 0.0,
                    div_here ? a.hts[qo - imt] : 0.0, div_here ? a.tarea_r[qo] : 0.0};
-  // box index of U point (j, i) and (j-1, i); region index for the factors
-  const int b0 = (ty + 1) * CRW + tx + 4, bn = ty * CRW + tx + 4;
-  const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
-  __syncthreads();
-  const float fn = S.fm1[mn], f0 = S.fm1[m0], fn1 = S.fm1[mn + 1], f01 = S.fm1[m0 + 1];
+  // box index of U point (j, i) and (j-1, i)
+  const int b0 = (ty + 1) * CRW + tx, bn = ty * CRW + tx;
+  const float fn = fm1_at(j - 1, i), f0 = fm1_at(j, i), fn1 = fm1_at(j - 1, i + 1), f01 = fm1_at(j, i + 1);
   // outside the domain the boxes read zeros, as the plain-load march does
   const bool in_n = j >= 1 && i < imt, in_0 = own, in_n1 = j >= 1 && i + 1 < imt, in_01 = j < jmt && i + 1 < imt;
   double P = 0.0;
