@@ -214,8 +214,45 @@ __device__ __forceinline__ void halo_r8_level(double* lvl, int imt, int jmt, int
   }
 }
 
+// A level's ghost cells spread over kHaloParts blocks (one block per level
+// left most SMs idle: 55 blocks per tracer, each thread walking ~120 cells
+// in turn).  With the fold, part 0 takes rows 0..2 (the only cells that read
+// the staged top row, and the only ones that rewrite it; rows 0 and 1 read
+// interior columns of rows 3 and 4, which no part rewrites) and the other
+// parts share the rest; without it the parts share all cells.
+constexpr int kHaloParts = 8;
+__device__ __forceinline__ bool halo_part(long nc, int imt, int tripole, int part, long& m0, long& m1) {
+  long base = 0, parts = kHaloParts;
+  if (tripole) {
+    if (part == 0) { m0 = 0; m1 = 3L * imt; return true; }
+    base = 3L * imt;
+    parts = kHaloParts - 1;
+    part -= 1;
+  }
+  const long per = (nc - base + parts - 1) / parts;
+  m0 = base + part * per;
+  m1 = m0 + per < nc ? m0 + per : nc;
+  return m0 < m1;
+}
+
+// part blockIdx.x of level blockIdx.y
 __global__ void k_halo_r8(double* f, int imt, int jmt, int ew_cyclic, int tripole) {
-  halo_r8_level(f + (long)blockIdx.x * imt * jmt, imt, jmt, ew_cyclic, tripole);
+  double* lvl = f + (long)blockIdx.y * imt * jmt;
+  HaloCells hc{imt, jmt, tripole};
+  long m0, m1;
+  if (!halo_part(hc.count(), imt, tripole, blockIdx.x, m0, m1)) return;
+  extern __shared__ double top[];
+  const bool fold = tripole && blockIdx.x == 0;
+  if (fold) {
+    for (int i = threadIdx.x; i < imt; i += blockDim.x) top[i] = lvl[2L * imt + i];
+    __syncthreads();
+  }
+  for (long m = m0 + threadIdx.x; m < m1; m += blockDim.x) {
+    int j, i;
+    hc.cell(m, j, i);
+    double v;
+    if (halo_cell_value(lvl, top, j, i, imt, jmt, ew_cyclic, tripole, v)) lvl[(long)j * imt + i] = v;
+  }
 }
 
 // net (both tracers) of every member: blockIdx.x the level, blockIdx.y the member
@@ -1535,6 +1572,36 @@ __global__ void k_halo_state(Arena a, int n) {
   halo_state_level<DIAG>(a, n, blockIdx.x);
 }
 
+// Without diagnostics the two tracers' ghost fills are independent: one
+// launch, part blockIdx.x (as k_halo_r8) of level blockIdx.y of tracer
+// blockIdx.z, the same values as halo_state_level<false>.
+__global__ void k_halo_state_parts(Arena a) {
+  const int n = blockIdx.z, k = blockIdx.y;
+  const int imt = a.imt, jmt = a.jmt;
+  HaloCells hc{imt, jmt, a.tripole};
+  long m0, m1;
+  if (!halo_part(hc.count(), imt, a.tripole, blockIdx.x, m0, m1)) return;
+  const long A = a.A, F = a.F, FB = a.FB;
+  double* lvl = a.at[a.cur ^ 1] + n * F + (long)k * A;
+  double* lvlb = a.atb[a.cur ^ 1] + n * FB + (long)(k + 1) * A;
+  const double* vin = a.vtl ? a.vtl + (long)k * A : nullptr;
+  const float* vin32 = a.vtl32 ? a.vtl32 + (long)k * A : nullptr;
+  extern __shared__ double top[];
+  if (a.tripole && blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < imt; i += blockDim.x) top[i] = lvl[2L * imt + i];
+    __syncthreads();
+  }
+  for (long m = m0 + threadIdx.x; m < m1; m += blockDim.x) {
+    int j, i;
+    hc.cell(m, j, i);
+    const long q = (long)j * imt + i;
+    double v;
+    if (!halo_cell_value(lvl, top, j, i, imt, jmt, a.ew_cyclic, a.tripole, v)) v = vin ? vin[q] : (double)vin32[q];
+    lvl[q] = v;
+    lvlb[q] = v;
+  }
+}
+
 // tracer n of every member: blockIdx.x the level, blockIdx.y the member
 __global__ void k_halo_state_batch(const MemberDesc* __restrict__ mem, int n) {
   const Arena& a = mem[blockIdx.y].a;
@@ -1590,7 +1657,7 @@ int launch_tree_sum(const double* x, long n, double* part, double* out, cudaStre
 }
 
 int launch_halo_r8(double* f, int nz, int imt, int jmt, int ew_cyclic, int tripole, cudaStream_t s) {
-  k_halo_r8<<<nz, 256, imt * sizeof(double), s>>>(f, imt, jmt, ew_cyclic, tripole);
+  k_halo_r8<<<dim3(kHaloParts, nz), 256, imt * sizeof(double), s>>>(f, imt, jmt, ew_cyclic, tripole);
   LT_LAUNCHED();
   return LT_OK;
 }
@@ -1653,6 +1720,12 @@ int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, 
 }
 
 int launch_halo_state(const Arena& a, cudaStream_t s) {
+  if (!a.diagnostics) {
+    k_halo_state_parts<<<dim3(kHaloParts, a.km, 2), 256, a.imt * sizeof(double), s>>>(a);
+    LT_LAUNCHED();
+    return LT_OK;
+  }
+  // with diagnostics, salinity's dt_diff reads temperature's new ghost values
   for (int n = 0; n < 2; ++n) {
     if (a.diagnostics) k_halo_state<true><<<a.km, 256, a.imt * sizeof(double), s>>>(a, n);
     else k_halo_state<false><<<a.km, 256, a.imt * sizeof(double), s>>>(a, n);
