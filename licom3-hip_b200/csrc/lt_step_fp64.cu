@@ -975,8 +975,8 @@ struct ExSmem {
 // transport is left 0 without computing its predictor: a flag only chooses
 // between the upwind and Lax-Wendroff forms of its faces' fluxes, which are
 // the same zero for a zero transport, and the vertical faces below a
-// column's bottom carry w = 0.  Not for a cell whose cached fluxes (xy_out)
-// the column phase reads.  (Model velocities vanish on land faces; the
+// column's bottom carry w = 0.  The column phase forms such a cell's
+// cached terms (xy_out) itself.  (Model velocities vanish on land faces; the
 // reference's literal tracer_ sequence, which leaves vtl holding S, does not
 // keep them zero, hence the test.)
 __device__ __forceinline__ bool pred_one64(ExSmem& S, const Arena& a, int kk, int sc, int su, int sd, int hj, int hi,
@@ -1266,7 +1266,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // limiter flags of the own cell at levels k+1, k (earlier steps) and k-1
     bool out_kp1 = false,
          out_k = pred_one64(S, a, ks, sk, sm1, sp1, ty + 1, tx + 1, x0, y0,
-                            &S.xyc[0][0][0] + tid + (kCacheXY ? (ks & 1) * 6 * TTHREADS : 0), !DIAG),
+                            &S.xyc[0][0][0] + tid + (kCacheXY ? (ks & 1) * 6 * TTHREADS : 0), true),
          out_km1 = false;
     if (has_ring) pred_one64(S, a, ks, sk, sm1, sp1, ring_hj, ring_hi, x0, y0, nullptr, true);
 
@@ -1282,7 +1282,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       // thread computed: no barrier between the two phases.
       if (k >= 1) {
         out_km1 = pred_one64(S, a, k - 1, sm1, sp1, sk, ty + 1, tx + 1, x0, y0,
-                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 6 * TTHREADS : 0), !DIAG);
+                             &S.xyc[0][0][0] + tid + (kCacheXY ? ((k - 1) & 1) * 6 * TTHREADS : 0), true);
         if (has_ring) pred_one64(S, a, k - 1, sm1, sp1, sk, ring_hj, ring_hi, x0, y0, nullptr, true);
       }
       // ---- phase C.  Without diagnostics an inner cell below its column's
@@ -1314,14 +1314,18 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         };
         double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
         const double* xc = &S.xyc[0][0][0] + tid + (kCacheXY ? (k & 1) * 6 * TTHREADS : 0);
+        // the predictor of a dry cell whose faces carry no transport was
+        // skipped (pred_one64's dry_out), so its cached terms are stale:
+        // formed here from the same expressions
+        const bool cached = kCacheXY && !(k >= kz && ue == 0.0 && uwc == 0.0 && vsc == 0.0 && vn == 0.0);
         if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
-        else xy1 = kCacheXY ? xc[0] : -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
+        else xy1 = cached ? xc[0] : -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
         if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
-        else xy2 = kCacheXY ? xc[TTHREADS] : dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
+        else xy2 = cached ? xc[TTHREADS] : dts * (c - w) * 2.0 * tr * uwc * uwc / hww;
         if (lim(hc + HQX, j <= jmt - 3)) xy3 = -(s - c) * fabs(vsc) * tr;
-        else xy3 = kCacheXY ? xc[2 * TTHREADS] : -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
+        else xy3 = cached ? xc[2 * TTHREADS] : -dts * (s - c) * 2.0 * tr * vsc * vsc / hss;
         if (lim(hc - HQX, j >= 2)) xy4 = (c - nn) * fabs(vn) * tr;
-        else xy4 = kCacheXY ? xc[3 * TTHREADS] : dts * (c - nn) * 2.0 * tr * vn * vn / hsn;
+        else xy4 = cached ? xc[3 * TTHREADS] : dts * (c - nn) * 2.0 * tr * vn * vn / hsn;
         const double wk = Lk.ws[uc];
         if (k == 0) {
           const double w1 = ws_dn, ad = at_dn;
@@ -1356,8 +1360,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         }
         const double cx = -c * (ue - uwc) * tr * 2.0;
         const double cy = -c * (vsc - vn) * tr * 2.0;
-        const double x0v = kCacheXY ? xc[4 * TTHREADS] : (e + c) * ue * tr - (c + w) * uwc * tr;
-        const double y0v = kCacheXY ? xc[5 * TTHREADS] : ((s + c) * vsc - (c + nn) * vn) * tr;
+        const double x0v = cached ? xc[4 * TTHREADS] : (e + c) * ue * tr - (c + w) * uwc * tr;
+        const double y0v = cached ? xc[5 * TTHREADS] : ((s + c) * vsc - (c + nn) * vn) * tr;
         const double xx = -(x0v + xy1 + xy2 + cx);
         const double yy = -(y0v + xy3 + xy4 + cy);
         const double zz = -(za + zb1 + zb2 + zc);
@@ -1376,8 +1380,13 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           const double atb_kp1 = k < km - 1 ? atb_dn : 0.0;
           const double wkc_k = Lk.akt[ac];
           const double wkc_km1 = k >= 1 ? S.slot[sm1].akt[ac] : 0.0;
+          // below the column's bottom every term of the step is masked (its
+          // new value is at + dts*0 = at): with diagnostics only they are
+          // formed there, and the state is copied (without diagnostics such
+          // cells take the copy path above)
+          const bool dry = DIAG && k >= kz;
           double tf = adv * vit_k;
-          {
+          if (!dry) {
             const int r = rc;
             double h = 0.0, cc = 0.0;
             if (k <= S.kmt[r] - 1) {
@@ -1418,6 +1427,17 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
             tf = tf + odzp[km - 1] * w2 * (1.0 - aidif);
             if (DIAG) a.dzd[n * F + cg] = odzp[km - 1] * w2 * 0.5;
           }
+          if (dry) {
+            // tracer_9's diagnostics of the unchanged cell, formed as for
+            // any cell: v = d8 = at
+            const double v = c;
+            a.tend[n * F + cg] = (v - c) / dts * vit_k;
+            if (k == 0) a.dt_diff[n * F + cg] = (v - v) / dts * vit_k - stf * 0.5 * odzp[0];
+            else a.dt_diff[n * F + cg] = (v - v) / dts * vit_k;
+            if (j == 2 && a.tripole) a.fold_save[((long)(n * km + k)) * imt + i] = v;
+            at_out[cg] = v;
+            atb_out[(long)(k + 1) * A + qo] = v;
+          } else {
           if (k == 0) {
             if (n == 1) {
               if (kz > 0) tf = tf + stf * (1.0 - aidif) * odzp[0];
@@ -1457,6 +1477,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           sl[tid] = ev;
           sl[TTHREADS + tid] = fv;
           if (DIAG) sl[2 * TTHREADS + tid] = d8;
+          }  // wet
           atb_dn = atb_k;
         }
         at_dn = c;
@@ -1477,7 +1498,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     if (inner) {
       double x = 0.0;
       constexpr int SUB = 8;
-      const int kend = DIAG ? km : min(kz, ks + 1);   // the levels the march left in the scratch
+      const int kend = min(kz, ks + 1);   // the levels the march left in the scratch (the wet ones)
       for (int k0 = 0; k0 < kend; k0 += SUB) {
         double evs[SUB], fvs[SUB];
 #pragma unroll
