@@ -1316,8 +1316,11 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
         const double* xc = &S.xyc[0][0][0] + tid + (kCacheXY ? (k & 1) * 6 * TTHREADS : 0);
         // the predictor of a dry cell whose faces carry no transport was
         // skipped (pred_one64's dry_out), so its cached terms are stale:
-        // formed here from the same expressions
-        const bool cached = kCacheXY && !(k >= kz && ue == 0.0 && uwc == 0.0 && vsc == 0.0 && vn == 0.0);
+        // with diagnostics they are formed here from the same expressions
+        // (without, such a cell is inner and copied above, or on the ring,
+        // where its tendency is not used)
+        const bool cached =
+            kCacheXY && !(DIAG && k >= kz && ue == 0.0 && uwc == 0.0 && vsc == 0.0 && vn == 0.0);
         if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
         else xy1 = cached ? xc[0] : -dts * (e - c) * 2.0 * tr * ue * ue / hwe;
         if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
