@@ -210,6 +210,7 @@ void plan_arena(Arena& a, Plan& pl) {
     D(&a.ax, 2 * F); D(&a.ay, 2 * F); D(&a.az, 2 * F); D(&a.dzd, 2 * F);
     D(&a.tend, 2 * F); D(&a.dt_diff, 2 * F); D(&a.dt_conv, 2 * F); D(&a.penetrate, F);
     D(&a.fold_save, 2 * km * (size_t)a.imt);
+    I(&a.kfz, A);
   } else {
     D(&a.dt_conv, 2 * F);  // convadj writes it
     D(&a.tend, 2 * F);     // convadj accumulates into it

@@ -68,6 +68,10 @@ struct alignas(16) Arena {   // copied into shared memory as 16-byte words
   double *duc, *dum, *dun, *dus, *due, *duw, *dmc, *dmn, *dms, *dme, *dmw, *amf, *uarea_r, *dxur, *dyur;
   // diagnostics (null when off)
   double *ax, *ay, *az, *dzd, *tend, *dt_diff, *dt_conv, *penetrate;
+  // [jmt][imt], with diagnostics: one past the deepest level at which the
+  // column's west or south face transport or its w is nonzero (written by
+  // the continuity; the column kernel's deep-level shortcut reads it)
+  int* kfz;
 
   // step scratch
   double *uwf, *vsf;          // face transports u_wface, v_sface [km][jmt][imt]

@@ -380,6 +380,7 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   const int m0 = (ty + 1) * UX + tx, mn = ty * UX + tx;
   double W = 0.0;
   double dzp_k = a.dzp[0];
+  int kf = 0;   // one past the deepest level with a nonzero west/south face transport or w here
   for (int k = 0; k < km; ++k) {
     const int b = k & 1;
     const double dzp_c = dzp_k;
@@ -396,13 +397,15 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
       const long c = (long)k * A + qo;
       a.utf_out[c] = own_utf * p.oncc;
       a.vtf_out[c] = own_vtf * p.oncc;
+      double uwv = 0.0, vsv = 0.0;   // the faces outside these ranges stay zero
       if (flux) {
-        if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] * dyu_n + wd[m0] * dyu_o) * 0.25;
-        if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] * dxu_o + wb[m0 + 1] * dxu_e) * 0.25;
+        if (j >= 1 && j < jmt - 1) a.uwf[c] = uwv = (wd[mn] * dyu_n + wd[m0] * dyu_o) * 0.25;
+        if (i >= 1 && i < imt - 1) a.vsf[c] = vsv = (wb[m0] * dxu_o + wb[m0 + 1] * dxu_e) * 0.25;
       } else {
-        if (j >= 1 && j < jmt - 1) a.uwf[c] = (wd[mn] + wd[m0]) * htw_o * 0.25;
-        if (i >= 1 && i < imt - 1) a.vsf[c] = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25;
+        if (j >= 1 && j < jmt - 1) a.uwf[c] = uwv = (wd[mn] + wd[m0]) * htw_o * 0.25;
+        if (i >= 1 && i < imt - 1) a.vsf[c] = vsv = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25;
       }
+      if (uwv != 0.0 || vsv != 0.0) kf = k + 1;
       double wka = 0.0;
       if (j >= 1 && i < imt - 1 && k <= kz - 1) {
         const double east = (uk[m0 + 1] + uk[mn + 1]) * htw_e;
@@ -420,7 +423,10 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
     }
   }
   cp_async_wait<0>();
-  if (!col) return;
+  if (!col) {
+    if (a.kfz && own) a.kfz[qo] = kf;
+    return;
+  }
   const double ohbt = a.ohbt[qo];
   const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
   double wsp = a.ws[qo];
@@ -436,10 +442,13 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
       const int k = k0 + c;
       if (k >= km) break;
       const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + wk[c]));
-      a.ws[(long)k * A + qo] = raw * fac;
+      const double wv = raw * fac;
+      a.ws[(long)k * A + qo] = wv;
+      if (wv != 0.0) kf = max(kf, k + 1);
       wsp = raw;
     }
   }
+  if (a.kfz) a.kfz[qo] = kf;
 }
 
 // ------------------------------------------------------------- tracer march
@@ -1125,6 +1134,18 @@ __device__ __forceinline__ void ring_cell64(int q, int& hj, int& hi) {
 static_assert(kFp64CtasPerSm * (sizeof(ExSmem) + 1024) <= 228 * 1024,
               "FP64 tracer tile no longer fits kFp64CtasPerSm CTAs per SM");
 
+// With diagnostics: the level from which a ring cell (where diagnostics are
+// written) is below its bottom and carries no transport through its four
+// faces or w (kfz of its own column covers its west and south faces and
+// w, its east and north neighbours' cover the other two faces).  From there
+// down its diagnostics need no limiter flag: a zero transport gives the same
+// signed zero in the upwind and Lax-Wendroff form of every face flux.
+__device__ __forceinline__ int deep_start_cell(const Arena& a, int i, int j) {
+  if (!(i >= 1 && i < a.imt - 1 && j >= 1 && j < a.jmt - 1)) return 0;
+  const long q = (long)j * a.imt + i;
+  return max(max(a.kmt[q], a.kfz[q]), max(a.kfz[q + 1], a.kfz[q - a.imt]));
+}
+
 template <bool DIAG>
 __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     k_tracer_tma64(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
@@ -1179,10 +1200,18 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // reference's arithmetic leaves them as they are (every term is masked,
     // the new value is at + dts * 0), so the march starts at the first of
     // them and the inner cells' values below it are copied.  With
-    // diagnostics every level is marched (the reference writes them
-    // everywhere).
+    // diagnostics the march starts at the deepest deep_start_cell of the
+    // tile and k_diag_deep writes the levels below it.
     int ks = km - 1;
-    if (!DIAG) {
+    if (DIAG) {
+      int kmax = deep_start_cell(a, i, j);
+      kmax = __reduce_max_sync(0xffffffffu, kmax);
+      if (tx == 0) S.wmax[ty] = kmax;
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < TTHREADS / 32; ++q) kmax = max(kmax, S.wmax[q]);
+      ks = min(km - 1, kmax);
+    } else {
       __syncthreads();
       int kmax = max((int)S.kmt[r2(ty + 1, tx + 1)], has_ring ? (int)S.kmt[r2(ring_hj, ring_hi)] : 0);
       kmax = __reduce_max_sync(0xffffffffu, kmax);
@@ -1248,8 +1277,14 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     const double stf = own ? a.stf_n[n * A + qo] : 0.0;
     const double err_norm2 = a.scalars[0];
     double e_prev = 0.0, f_prev = 0.0;
-    // own cell's at, ws and atb of level k+1, kept from step k+1
+    // own cell's at, ws and atb of level k+1, kept from step k+1 (with
+    // diagnostics, those of the level below the first marched one)
     double at_dn = 0.0, ws_dn = 0.0, atb_dn = 0.0;
+    if (DIAG && own && ks < km - 1) {
+      at_dn = at_in[(long)(ks + 1) * A + qo];
+      ws_dn = a.ws[(long)(ks + 1) * A + qo];
+      atb_dn = a.atb[a.cur][n * FB + (long)(ks + 2) * A + qo];
+    }
 
     // slots of levels k, k-1, k+1 (NSX == 3: level k-2 shares k+1's), carried
     // through the level loop
@@ -1542,6 +1577,108 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
   }
 }
 
+// ------------------------------------------------- deep levels (diagnostics)
+// The levels k_tracer_tma64<true> leaves to this kernel: below the deepest
+// deep_start_cell of a tile every ring cell of the tile is below its bottom
+// and carries no transport, so per cell and level it writes the diagnostics
+// of advection_tracer_3 (the upwind forms of the face fluxes, the same bits
+// as any form at a zero transport), of tracer_5 (penetrate, dz) and of
+// tracer_9 (tend, dt_diff, with the state unchanged: every term is masked),
+// reading the level fields directly.  Block = one tile (the column kernel's
+// decomposition), blockIdx.y = tracer.
+__global__ void __launch_bounds__(TTHREADS) k_diag_deep(Arena a, int ntx) {
+  __shared__ int wmax[TTHREADS / 32];
+  const int n = blockIdx.y, tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int x0 = (int)(blockIdx.x % ntx) * TX, y0 = (int)(blockIdx.x / ntx) * TY;
+  const int i = x0 + tx, j = y0 + ty;
+  const int imt = a.imt, jmt = a.jmt, km = a.km;
+  const long A = a.A, F = a.F, FB = a.FB;
+  int kmax = deep_start_cell(a, i, j);
+  kmax = __reduce_max_sync(0xffffffffu, kmax);
+  if (tx == 0) wmax[ty] = kmax;
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < TTHREADS / 32; ++q) kmax = max(kmax, wmax[q]);
+  const int ks = min(km - 1, kmax);
+  const bool own = i < imt && j < jmt;
+  const bool ring = own && i >= 1 && i < imt - 1 && j >= 1 && j < jmt - 1;
+  const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
+  if (!ring || ks >= km - 1) return;
+  const long qo = (long)j * imt + i;
+  const double dts = a.p.dts;
+  const double* __restrict__ at = a.at[a.cur] + n * F;
+  const double* __restrict__ atb = a.atb[a.cur] + n * FB;
+  const double* __restrict__ akt = a.akt + n * F;
+  const double* __restrict__ uwf = a.uwf;
+  const double* __restrict__ vsf = a.vsf;
+  const double* __restrict__ ws = a.ws;
+  const double* __restrict__ odzp = a.odzp;
+  const double* __restrict__ odzt = a.odzt;
+  const double tr = __ldg(a.tarea_r + qo);
+  const double swv = (inner && n == 0) ? __ldg(a.swv + qo) : 0.0;
+  const double vit_k = 0.0, vit_kp1 = 0.0;   // below the bottom
+  for (int k = ks + 1; k < km; ++k) {
+    const long cg = (long)k * A + qo;
+    const double c = __ldg(at + cg), e = __ldg(at + cg + 1), w = __ldg(at + cg - 1);
+    const double s = __ldg(at + cg + imt), nn = __ldg(at + cg - imt);
+    const double au = __ldg(at + cg - A);
+    const double ue = __ldg(uwf + cg + 1), uwc = __ldg(uwf + cg), vsc = __ldg(vsf + cg), vn = __ldg(vsf + cg - imt);
+    const double wk = __ldg(ws + cg);
+    const double xy1 = -(e - c) * fabs(ue) * tr;
+    const double xy2 = (c - w) * fabs(uwc) * tr;
+    const double xy3 = -(s - c) * fabs(vsc) * tr;
+    const double xy4 = (c - nn) * fabs(vn) * tr;
+    double zb1, zb2, za, zc;
+    if (k == km - 1) {
+      zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
+      zb2 = 0.0;
+      za = 0.5 * odzp[km - 1] * wk * (c + au);
+      zc = -odzp[km - 1] * c * wk;
+    } else {
+      const double ad = __ldg(at + cg + A), w1 = __ldg(ws + cg + A);
+      zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
+      zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
+      za = 0.5 * odzp[k] * wk * (c + au) - 0.5 * odzp[k] * w1 * (c + ad);
+      zc = -odzp[k] * c * (wk - w1);
+    }
+    const double cx = -c * (ue - uwc) * tr * 2.0;
+    const double cy = -c * (vsc - vn) * tr * 2.0;
+    const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
+    const double y0v = ((s + c) * vsc - (c + nn) * vn) * tr;
+    a.ax[n * F + cg] = -(x0v + xy1 + xy2 + cx);
+    a.ay[n * F + cg] = -(y0v + xy3 + xy4 + cy);
+    a.az[n * F + cg] = -(za + zb1 + zb2 + zc);
+    if (!inner) continue;
+    const double atb_k = __ldg(atb + cg + A), atb_km1 = __ldg(atb + cg);
+    const double wkc_km1 = __ldg(akt + cg - A);
+    if (k < km - 1) {
+      if (n == 0) {
+        const double w1p = swv * a.pen[k - 1] * vit_k;
+        const double w2p = swv * a.pen[k] * vit_kp1;
+        a.penetrate[cg] = (w1p - w2p) * odzp[k];
+      }
+      const double atb_kp1 = __ldg(atb + cg + 2 * A), wkc_k = __ldg(akt + cg);
+      const double w1 = wkc_km1 * (atb_km1 - atb_k) * odzt[k] * vit_k;
+      const double w2 = wkc_k * (atb_k - atb_kp1) * odzt[k + 1] * vit_kp1;
+      a.dzd[n * F + cg] = odzp[k] * (w1 - w2) * 0.5;
+    } else {
+      if (n == 0) {
+        const double w2p = swv * a.pen[km - 2] * vit_k;
+        a.penetrate[cg] = w2p * odzp[km - 1];
+      }
+      const double w2 = wkc_km1 * (atb_km1 - atb_k) * odzt[km - 1] * vit_k;
+      a.dzd[n * F + cg] = odzp[km - 1] * w2 * 0.5;
+    }
+    // tracer_8, invtrit and tracer_9 of a masked cell: v = d8 = at
+    const double v = c;
+    a.tend[n * F + cg] = (v - c) / dts * vit_k;
+    a.dt_diff[n * F + cg] = (v - v) / dts * vit_k;
+    if (j == 2 && a.tripole) a.fold_save[((long)(n * km + k)) * imt + i] = v;
+    a.at[a.cur ^ 1][n * F + cg] = v;
+    a.atb[a.cur ^ 1][n * FB + (long)(k + 1) * A + qo] = v;
+  }
+}
+
 // ------------------------------------------------------------- state halo
 // One block per (level, tracer): ghost cells of the new state take the halo
 // values (pop_haloupdate_tracer2 then tracer_9 for every point); cells the
@@ -1737,8 +1874,14 @@ int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, 
     LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_tma64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     attr = true;
   }
-  if (a.diagnostics) k_tracer_tma64<true><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
-  else k_tracer_tma64<false><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+  if (a.diagnostics) {
+    k_tracer_tma64<true><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+    LT_LAUNCHED();
+    // the levels below each tile's march
+    k_diag_deep<<<dim3((unsigned)ntiles, 2), TTHREADS, 0, s>>>(a, ntx);
+  } else {
+    k_tracer_tma64<false><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+  }
   LT_LAUNCHED();
   return LT_OK;
 }
