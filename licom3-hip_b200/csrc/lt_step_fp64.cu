@@ -1196,12 +1196,16 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       S.kmt[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? a.kmt[(long)gj * imt + gi] : 0;
     }
     // Without diagnostics, levels at and below the deepest bottom of the
-    // 1-halo region are land for every cell the march touches there: the
-    // reference's arithmetic leaves them as they are (every term is masked,
-    // the new value is at + dts * 0), so the march starts at the first of
-    // them and the inner cells' values below it are copied.  With
-    // diagnostics the march starts at the deepest deep_start_cell of the
-    // tile and k_diag_deep writes the levels below it.
+    // tile's own columns are land for every cell the march updates there:
+    // the reference's arithmetic leaves them as they are (every term is
+    // masked, the new value is at + dts * 0), so the march starts at the
+    // first of them and the inner cells' values below it are copied.  (At
+    // that level a wetter cell of the halo may form its limiter flag from the
+    // level below, which is not loaded; the flag only meets the tile's cells
+    // through faces and a w that carry no transport there, where every form
+    // of the flux gives the same bits.)  With diagnostics the march starts at
+    // the deepest deep_start_cell of the tile and k_diag_deep writes the
+    // levels below it.
     int ks = km - 1;
     if (DIAG) {
       int kmax = deep_start_cell(a, i, j);
@@ -1213,7 +1217,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       ks = min(km - 1, kmax);
     } else {
       __syncthreads();
-      int kmax = max((int)S.kmt[r2(ty + 1, tx + 1)], has_ring ? (int)S.kmt[r2(ring_hj, ring_hi)] : 0);
+      int kmax = (int)S.kmt[r2(ty + 1, tx + 1)];
       kmax = __reduce_max_sync(0xffffffffu, kmax);
       if (tx == 0) S.wmax[ty] = kmax;
       __syncthreads();

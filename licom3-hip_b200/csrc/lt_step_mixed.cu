@@ -878,13 +878,15 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
   const HCell own_cell = hcell(ty + 1, tx + 1, x0, y0, imt, jmt);
   const bool has_ring = tid >= MTH - RING;
   const HCell ring_cell = ring_hcell(has_ring ? tid - (MTH - RING) : 0, x0, y0, imt, jmt);
-  // Levels at and below the deepest bottom of the 1-halo region are land for
-  // every cell the march touches there: the step leaves them as they are.
-  // The march starts at the first of them (or the bottom level), and the
-  // inner cells' values below it are copied.
+  // Levels at and below the deepest bottom of the tile's own columns are land
+  // for every cell the march updates there: the step leaves them as they
+  // are.  The march starts at the first of them (or the bottom level), and
+  // the inner cells' values below it are copied.  (A wetter halo cell's flag
+  // at that level, formed without the level below, meets the tile's cells
+  // only through faces and a w that carry no transport there.)
   stage_kmt<kLoadsAhead>(S, a, x0, y0);
   __syncthreads();
-  int kmax = max((int)S.kmt[own_cell.r], has_ring ? (int)S.kmt[ring_cell.r] : 0);
+  int kmax = (int)S.kmt[own_cell.r];
   kmax = __reduce_max_sync(0xffffffffu, kmax);
   if (tx == 0) S.wmax[ty] = kmax;
   __syncthreads();
