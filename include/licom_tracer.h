@@ -320,8 +320,10 @@ int lt_mark(lt_domain* dom, int which);
  * the forcing copies still in flight after it. */
 int lt_profile(lt_domain* dom, int on);
 int lt_phase_ms(lt_domain* dom, float* ms, int nphase);
-/* Select the tracer column kernel: 1 = TMA-fed pipeline (default where the
- * row pitch allows 16-byte strides), 0 = plain-load variant. */
+/* How the column kernels' level slots are filled: 1 = TMA boxes (the default
+ * where the row pitch allows 16-byte strides; refused with LT_E_INVALID
+ * elsewhere), 0 = per-thread asynchronous copies into the same slots (the
+ * default where it does not).  The results are the same bits either way. */
 int lt_use_tma(lt_domain* dom, int on);
 /* Failure-detection hook.  Each level wait of the TMA-fed column kernels polls
  * its mbarrier at most `polls` times (default 2^24) before the CTA records a

@@ -318,10 +318,11 @@ int run_step(lt_domain* d, cudaEvent_t forcing_ready) {
   mark(4);
   if (a.precision == LT_PREC_MIXED) {
     if ((rc = launch_tracer_tma_mixed(a, d->maps, d->use_tma, s, d->tma_grid))) return rc;
-  } else if (d->use_tma && a.p.adv_tracer == LT_ADV_TSPAS) {
-    // the TMA column kernel is the tspas scheme's; the centred and flux
-    // schemes run in the plain-load kernel
-    if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid))) return rc;
+  } else if (a.p.adv_tracer == LT_ADV_TSPAS) {
+    // the TMA-slot column kernel is the tspas scheme's (its level boxes by
+    // per-thread copies where the row pitch does not allow TMA); the centred
+    // and flux schemes run in the plain-load kernel
+    if ((rc = launch_tracer_tma64(a, d->maps, s, d->tma_grid, d->use_tma))) return rc;
   } else {
     if ((rc = launch_tracer_fp64(a, s, d->slots))) return rc;
   }

@@ -137,8 +137,8 @@ int enqueue_step(lt_batch* b, int p) {
       Arena a = d->a;
       a.cur = b->base_cur[i] ^ p;
       if ((rc = launch_continuity_fp64(a, s))) return rc;
-      rc = (d->use_tma && a.p.adv_tracer == LT_ADV_TSPAS) ? launch_tracer_tma64(a, d->maps, s, d->tma_grid)
-                                                          : launch_tracer_fp64(a, s, d->slots);
+      rc = a.p.adv_tracer == LT_ADV_TSPAS ? launch_tracer_tma64(a, d->maps, s, d->tma_grid, d->use_tma)
+                                          : launch_tracer_fp64(a, s, d->slots);
       if (rc) return rc;
     }
   }

@@ -12,9 +12,10 @@
 //                   surface mixing floor, SSS-norm terms       (tracer_5/6 surface parts)
 //   tree sum        deterministic SSS-normalisation sum         (tracer.cpp:1849-1868)
 //   halo(net)       in-GPU ghost fill                           (pop_haloupdate_tracer1)
-//   k_tracer_tma64  per column tile (k_tracer64 where the layout
-//                   does not allow TMA boxes, and for the centred and
-//                   flux schemes), both tracers: tspas predictor/limiter,
+//   k_tracer_tma64  per column tile (its level boxes by per-thread copies
+//                   where the layout does not allow TMA boxes; k_tracer64
+//                   for the centred and flux schemes), both tracers:
+//                   tspas predictor/limiter,
 //                   biharmonic diffusion, shortwave, explicit and implicit
 //                   vertical diffusion, surface terms, update   (advection_tracer_2/3, tracer_del4_1/2,
 //                                                                tracer_5..9, invtrit)
@@ -451,22 +452,23 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   if (a.kfz) a.kfz[qo] = kf;
 }
 
-// ------------------------------------------------------------- tracer march
+// ------------------------------------------- plain-load march (centred, flux)
+// The column march of the centred and flux advection schemes (no predictor
+// or limiter), with each level's region loaded by plain loads.
 // Shared-memory regions of a TX x TY column tile:
 //   H2: rows y0-2..y0+TY+1, cols x0-2..x0+TX+1   (RY x RX)   tracer, atb, kmt
-//   H1: rows y0-1..y0+TY,   cols x0-1..x0+TX     (QY x QX)   predictor, extrema, w, d2tk
+//   H1: rows y0-1..y0+TY,   cols x0-1..x0+TX     (QY x QX)   w, d2tk
 constexpr int RX = TX + 4, RY = TY + 4, QX = TX + 2, QY = TY + 2;
 constexpr int UWN = QY * RX;          // u_wface: H1 rows, cols x0-2..x0+TX+1
 constexpr int VSN = (QY + 1) * QX;    // v_sface: rows y0-2..y0+TY, H1 cols
 
 struct TSmem {
   double at[4][RY * RX];
-  double a00[3][QY * QX], amx[3][QY * QX], amn[3][QY * QX];
   double ws[3][QY * QX];
   double uw[2][UWN], vs[2][VSN];
   double atb[RY * RX];
   double d2[QY * QX];
-  double tr[QY * QX], hw[UWN], hs[VSN];
+  double tr[QY * QX];
   double dtn[QY * QX], dts[QY * QX], dte[QY * QX], dtw[QY * QX], ahf[QY * QX];
   int kmt[RY * RX];
 };
@@ -481,100 +483,6 @@ __device__ __forceinline__ void load_region(double* dst, const double* lvl, int 
   for (int m = threadIdx.x; m < nyr * nxr; m += TTHREADS) {
     const int gj = r0 + m / nxr, gi = c0 + m % nxr;
     dst[m] = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt) ? lvl[(long)gj * imt + gi] : 0.0;
-  }
-}
-
-// tspas predictor at00 and masked extrema at level kk for every H1 point
-// (advection_tracer_2, tracer.cpp:291-547).  s_at slots hold kk-1, kk, kk+1.
-__device__ void predictor_level(TSmem& S, const Arena& a, int kk, int x0, int y0) {
-  const int km = a.km, imt = a.imt, jmt = a.jmt;
-  const double dts = a.p.dts;
-  const double* odzp = a.odzp;
-  const double* odzt = a.odzt;
-  const double* at_c = S.at[slot4(kk)];
-  const double* at_u = kk > 0 ? S.at[slot4(kk - 1)] : nullptr;        // level above
-  const double* at_d = kk < km - 1 ? S.at[slot4(kk + 1)] : nullptr;   // level below
-  const double* ws_c = S.ws[slot3(kk)];
-  const double* ws_d = kk < km - 1 ? S.ws[slot3(kk + 1)] : nullptr;
-  const double* uw = S.uw[kk & 1];
-  const double* vs = S.vs[kk & 1];
-  double* o00 = S.a00[slot3(kk)];
-  double* omx = S.amx[slot3(kk)];
-  double* omn = S.amn[slot3(kk)];
-  for (int m = threadIdx.x; m < QY * QX; m += TTHREADS) {
-    const int hj = m / QX, hi = m % QX;
-    const int gj = y0 - 1 + hj, gi = x0 - 1 + hi;
-    if (!(gi >= 1 && gi < imt - 1 && gj >= 1 && gj < jmt - 1)) {
-      o00[m] = 0.0; omx[m] = 0.0; omn[m] = 0.0;
-      continue;
-    }
-    const int r = (hj + 1) * RX + (hi + 1);   // H2 index of this point
-    const int u = hj * RX + (hi + 1);          // uw index of column gi (row gj)
-    const int v = (hj + 1) * QX + hi;          // vs index of row gj
-    const double tr = S.tr[m];
-    const double c = at_c[r], e = at_c[r + 1], w = at_c[r - 1], s = at_c[r + RX], n = at_c[r - RX];
-    const double ue = uw[u + 1], uwc = uw[u];
-    const double vsc = vs[v], vn = vs[v - QX];
-    const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
-    const double y0v = ((s + c) * vsc - (c + n) * vn) * tr;
-    const double xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / S.hw[u + 1];
-    const double xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / S.hw[u];
-    const double xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / S.hs[v];
-    const double xy4 = dts * (c - n) * 2.0 * tr * vn * vn / S.hs[v - QX];
-    const double cx = -c * (ue - uwc) * tr * 2.0;
-    const double cy = -c * (vsc - vn) * tr * 2.0;
-    double za, zb1, zb2, zc;
-    const double wk = ws_c[m];
-    if (kk == 0) {
-      const double w1 = ws_d[m], ad = at_d[r];
-      za = -0.5 * odzp[0] * w1 * (ad + c);
-      zb1 = 0.0;
-      zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
-      zc = odzp[0] * c * w1;
-    } else if (kk == km - 1) {
-      const double au = at_u[r];
-      za = 0.5 * odzp[km - 1] * wk * (c + au);
-      zb1 = -0.5 * odzp[km - 1] * wk * wk * odzt[km - 1] * (au - c) * dts;
-      zb2 = 0.0;
-      zc = -odzp[km - 1] * c * wk;
-    } else {
-      const double au = at_u[r], ad = at_d[r], w1 = ws_d[m];
-      za = 0.5 * odzp[kk] * wk * (c + au) - 0.5 * odzp[kk] * w1 * (c + ad);
-      zb1 = -0.5 * odzp[kk] * wk * wk * odzt[kk] * (au - c) * dts;
-      zb2 = 0.5 * odzp[kk] * w1 * w1 * odzt[kk + 1] * (c - ad) * dts;
-      zc = -odzp[kk] * c * (wk - w1);
-    }
-    const double xx = -(x0v + xy1 + xy2 + cx);
-    const double yy = -(y0v + xy3 + xy4 + cy);
-    const double zz = -(zb1 + zb2 + za + zc);
-    o00[m] = c + (xx + yy + zz) * dts;
-    // masked 7-point extrema, land weighted to -/+1e10 (tracer.cpp:418-546)
-    auto vitk = [&](int kl, int rr) { return (kl < S.kmt[rr]) ? 1.0 : 0.0; };
-    auto mxv = [&](double t, double vt) { return t * vt + (1.0 - vt) * -1.0e10; };
-    auto mnv = [&](double t, double vt) { return t * vt + (1.0 - vt) * 1.0e10; };
-    const double vc = vitk(kk, r), vn_ = vitk(kk, r - RX), vs_ = vitk(kk, r + RX), vw = vitk(kk, r - 1),
-                 ve = vitk(kk, r + 1);
-    double hi_ = mxv(c, vc), lo_ = mnv(c, vc), t;
-    t = mxv(n, vn_); if (hi_ < t) hi_ = t;
-    t = mxv(s, vs_); if (hi_ < t) hi_ = t;
-    t = mxv(w, vw); if (hi_ < t) hi_ = t;
-    t = mxv(e, ve); if (hi_ < t) hi_ = t;
-    t = mnv(n, vn_); if (lo_ > t) lo_ = t;
-    t = mnv(s, vs_); if (lo_ > t) lo_ = t;
-    t = mnv(w, vw); if (lo_ > t) lo_ = t;
-    t = mnv(e, ve); if (lo_ > t) lo_ = t;
-    if (kk > 0) {
-      const double au = at_u[r], vu = vitk(kk - 1, r);
-      t = mxv(au, vu); if (hi_ < t) hi_ = t;
-      t = mnv(au, vu); if (lo_ > t) lo_ = t;
-    }
-    if (kk < km - 1) {
-      const double ad = at_d[r], vd = vitk(kk + 1, r);
-      t = mxv(ad, vd); if (hi_ < t) hi_ = t;
-      t = mnv(ad, vd); if (lo_ > t) lo_ = t;
-    }
-    omx[m] = hi_;
-    omn[m] = lo_;
   }
 }
 
@@ -638,6 +546,7 @@ __device__ __forceinline__ double simple_adv(const TSmem& S, const Arena& a, int
 
 template <bool DIAG, int ADV>
 __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long ntiles) {
+  static_assert(ADV == LT_ADV_CENTERED || ADV == LT_ADV_FLUX, "the tspas scheme runs in k_tracer_tma64");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TSmem& S = *reinterpret_cast<TSmem*>(smem_raw);
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
@@ -679,27 +588,14 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
       S.dtw[m] = in ? a.dtw[q] : 0.0;
       S.ahf[m] = in ? a.ahf[q] : 0.0;
     }
-    for (int m = tid; m < UWN; m += TTHREADS) {
-      const int gj = y0 - 1 + m / RX, gi = x0 - 2 + m % RX;
-      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
-      S.hw[m] = in ? a.htw[q2(gj, gi, imt)] * a.hun[q2(gj, gi, imt)] : 1.0;
-    }
-    for (int m = tid; m < VSN; m += TTHREADS) {
-      const int gj = y0 - 2 + m / QX, gi = x0 - 1 + m % QX;
-      const bool in = (gj >= 0 && gj < jmt && gi >= 0 && gi < imt);
-      S.hs[m] = in ? a.hts[q2(gj, gi, imt)] * a.hue[q2(gj, gi, imt)] : 1.0;
-    }
     // ---- prologue: levels km-1 and km-2 of the tracer, w and faces at km-1
     load_region(S.at[slot4(km - 1)], at_in + (long)(km - 1) * A, y0 - 2, x0 - 2, RY, RX, imt, jmt);
     load_region(S.at[slot4(km - 2)], at_in + (long)(km - 2) * A, y0 - 2, x0 - 2, RY, RX, imt, jmt);
     load_region(S.ws[slot3(km - 1)], a.ws + (long)(km - 1) * A, y0 - 1, x0 - 1, QY, QX, imt, jmt);
     load_region(S.uw[(km - 1) & 1], a.uwf + (long)(km - 1) * A, y0 - 1, x0 - 2, QY, RX, imt, jmt);
     load_region(S.vs[(km - 1) & 1], a.vsf + (long)(km - 1) * A, y0 - 2, x0 - 1, QY + 1, QX, imt, jmt);
-    __syncthreads();
-    if (ADV == LT_ADV_TSPAS) predictor_level(S, a, km - 1, x0, y0);
 
     const bool own = (i < imt && j < jmt);
-    const bool ring = own && i >= 1 && i < imt - 1 && j >= 1 && j < jmt - 1;
     const bool inner = own && i >= 2 && i < imt - 2 && j >= 2 && j < jmt - 2;
     const long qo = own ? q2(j, i, imt) : 0;
     const int kz = own ? a.kmt[qo] : 0;
@@ -728,92 +624,16 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
       const double wkc_km1 = (own && k >= 1) ? akt[(long)(k - 1) * A + qo] : 0.0;
       if (k == km - 1) wkc_k = 0.0;
       __syncthreads();
-      // ---- phase B: predictor one level up, first Laplacian at this level
-      if (ADV == LT_ADV_TSPAS && k >= 1) predictor_level(S, a, k - 1, x0, y0);
+      // ---- phase B: first Laplacian at this level
       del4_first(S, a, k, x0, y0);
       __syncthreads();
       // ---- phase C: own column
-      if (ADV == LT_ADV_TSPAS ? ring : inner) {
+      if (inner) {
         const double* at_c = S.at[slot4(k)];
         const double* at_u = k > 0 ? S.at[slot4(k - 1)] : nullptr;
         const double* at_d = k < km - 1 ? S.at[slot4(k + 1)] : nullptr;
         const long cg = (long)k * A + qo;
-        double adv;
-        if constexpr (ADV != LT_ADV_TSPAS) {
-          adv = simple_adv<ADV, DIAG>(S, a, k, n, cg, rc, hc, uc, vc, at_c, at_u, at_d);
-        } else {
-        const double* o00 = S.a00[slot3(k)];
-        const double* omx = S.amx[slot3(k)];
-        const double* omn = S.amn[slot3(k)];
-        auto out = [&](const double* a0, const double* mx, const double* mn, int m) {
-          return a0[m] > mx[m] || a0[m] < mn[m];
-        };
-        const double tr = S.tr[hc];
-        const double c = at_c[rc], e = at_c[rc + 1], w = at_c[rc - 1], s = at_c[rc + RX], nn = at_c[rc - RX];
-        const double* uw = S.uw[k & 1];
-        const double* vs = S.vs[k & 1];
-        const double ue = uw[uc + 1], uwc = uw[uc], vsc = vs[vc], vn = vs[vc - QX];
-        const bool self = out(o00, omx, omn, hc);
-        const bool edge_k = (k == 0 || k == km - 1);
-        auto lim = [&](int m, bool guard) {
-          const bool nb = out(o00, omx, omn, m);
-          return edge_k ? (self || (nb && guard)) : ((self || nb) && guard);
-        };
-        double xy1, xy2, xy3, xy4, zb1, zb2, za, zc;
-        if (lim(hc + 1, i <= imt - 3)) xy1 = -(e - c) * fabs(ue) * tr;
-        else xy1 = -dts * (e - c) * 2.0 * tr * ue * ue / S.hw[uc + 1];
-        if (lim(hc - 1, i >= 2)) xy2 = (c - w) * fabs(uwc) * tr;
-        else xy2 = dts * (c - w) * 2.0 * tr * uwc * uwc / S.hw[uc];
-        if (lim(hc + QX, j <= jmt - 3)) xy3 = -(s - c) * fabs(vsc) * tr;
-        else xy3 = -dts * (s - c) * 2.0 * tr * vsc * vsc / S.hs[vc];
-        if (lim(hc - QX, j >= 2)) xy4 = (c - nn) * fabs(vn) * tr;
-        else xy4 = dts * (c - nn) * 2.0 * tr * vn * vn / S.hs[vc - QX];
-        const double wk = S.ws[slot3(k)][hc];
-        if (k == 0) {
-          const double w1 = S.ws[slot3(1)][hc], ad = at_d[rc];
-          zb1 = 0.0;
-          if (self || (out(S.a00[slot3(1)], S.amx[slot3(1)], S.amn[slot3(1)], hc) && k <= km - 2))
-            zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
-          else
-            zb2 = 0.5 * odzp[0] * w1 * w1 * odzt[1] * (c - ad) * dts;
-          za = -0.5 * odzp[0] * w1 * (ad + c);
-          zc = odzp[0] * c * w1;
-        } else if (k == km - 1) {
-          const double au = at_u[rc];
-          if (self || out(S.a00[slot3(k - 1)], S.amx[slot3(k - 1)], S.amn[slot3(k - 1)], hc))
-            zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
-          else
-            zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
-          zb2 = 0.0;
-          za = 0.5 * odzp[km - 1] * wk * (c + au);
-          zc = -odzp[km - 1] * c * wk;
-        } else {
-          const double au = at_u[rc], ad = at_d[rc], w1 = S.ws[slot3(k + 1)][hc];
-          if ((self || out(S.a00[slot3(k - 1)], S.amx[slot3(k - 1)], S.amn[slot3(k - 1)], hc)) && k >= 1)
-            zb1 = -0.5 * fabs(wk) * odzp[k] * (au - c);
-          else
-            zb1 = -0.5 * odzp[k] * wk * wk * odzt[k] * (au - c) * dts;
-          if ((self || out(S.a00[slot3(k + 1)], S.amx[slot3(k + 1)], S.amn[slot3(k + 1)], hc)) && k <= km - 2)
-            zb2 = 0.5 * fabs(w1) * odzp[k] * (c - ad);
-          else
-            zb2 = 0.5 * odzp[k] * w1 * w1 * odzt[k + 1] * (c - ad) * dts;
-          za = 0.5 * odzp[k] * wk * (c + au) - 0.5 * odzp[k] * w1 * (c + ad);
-          zc = -odzp[k] * c * (wk - w1);
-        }
-        const double cx = -c * (ue - uwc) * tr * 2.0;
-        const double cy = -c * (vsc - vn) * tr * 2.0;
-        const double x0v = (e + c) * ue * tr - (c + w) * uwc * tr;
-        const double y0v = ((s + c) * vsc - (c + nn) * vn) * tr;
-        const double xx = -(x0v + xy1 + xy2 + cx);
-        const double yy = -(y0v + xy3 + xy4 + cy);
-        const double zz = -(za + zb1 + zb2 + zc);
-        adv = xx + yy + zz;
-        if (DIAG) {
-          a.ax[n * F + cg] = xx;
-          a.ay[n * F + cg] = yy;
-          a.az[n * F + cg] = zz;
-        }
-        }  // tspas
+        const double adv = simple_adv<ADV, DIAG>(S, a, k, n, cg, rc, hc, uc, vc, at_c, at_u, at_d);
         if (inner) {
           const double vit_k = k < kz ? 1.0 : 0.0;
           const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
@@ -944,7 +764,10 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
 }
 
 // -------------------------------------------- tracer march, TMA pipeline
-// Same arithmetic as k_tracer64 (term for term), data staged by TMA boxes.
+// The tspas column march (advection_tracer_2/3 with tracer_del4_1/2,
+// tracer_5..9 and invtrit, each expression in the reference's order), its
+// level data staged by TMA boxes (or, where the row pitch does not allow
+// TMA, by per-thread asynchronous copies into the same slots).
 // Three level slots: step k reads levels k-2 .. k from shared memory; the
 // own cell's at, ws and atb of level k+1 that the column phase also needs are
 // carried in registers from step k+1, so the slot of level k takes level k-3
@@ -1134,6 +957,47 @@ __device__ __forceinline__ void ring_cell64(int q, int& hj, int& hi) {
 static_assert(kFp64CtasPerSm * (sizeof(ExSmem) + 1024) <= 228 * 1024,
               "FP64 tracer tile no longer fits kFp64CtasPerSm CTAs per SM");
 
+// The six boxes of level L of tracer n by per-thread asynchronous copies, for
+// grids whose row pitch TMA cannot take (not a multiple of 16 bytes): every
+// thread copies its share of the boxes' elements (zeros outside the domain,
+// as TMA fills them) and the slot's mbarrier counts one arrival per thread
+// once its copies have landed.  The slot layout and the waits are the TMA
+// path's (issue_level).
+__device__ __forceinline__ void copy_level64(LevelSlot<double>& sl, uint64_t* bar, const Arena& a, int n, int L,
+                                             int x0, int y0) {
+  const int imt = a.imt, jmt = a.jmt;
+  const long A = a.A, F = a.F, FB = a.FB;
+  constexpr int NAT = (TY + 4) * SW, NWS = (TY + 2) * SW, NUW = (TY + 2) * SW, NVS = (TY + 3) * SW, NAK = TY * TX;
+  constexpr int TOT = 2 * NAT + NWS + NUW + NVS + NAK;
+  for (int e = threadIdx.x; e < TOT; e += TTHREADS) {
+    const double* base;
+    double* dst;
+    int r, w, gj0, gi0;
+    if (e < 2 * NAT) {
+      const int b = e / NAT;
+      r = e % NAT; w = SW; gj0 = y0 - 2; gi0 = x0 - 4;
+      base = b == 0 ? a.at[a.cur] + n * F + (long)L * A : a.atb[a.cur] + n * FB + (long)(L + 1) * A;
+      dst = b == 0 ? sl.at : sl.atb;
+    } else if (e < 2 * NAT + NWS) {
+      r = e - 2 * NAT; w = SW; gj0 = y0 - 1; gi0 = x0 - 4;
+      base = a.ws + (long)L * A; dst = sl.ws;
+    } else if (e < 2 * NAT + NWS + NUW) {
+      r = e - 2 * NAT - NWS; w = SW; gj0 = y0 - 1; gi0 = x0 - 4;
+      base = a.uwf + (long)L * A; dst = sl.uw;
+    } else if (e < 2 * NAT + NWS + NUW + NVS) {
+      r = e - 2 * NAT - NWS - NUW; w = SW; gj0 = y0 - 2; gi0 = x0 - 4;
+      base = a.vsf + (long)L * A; dst = sl.vs;
+    } else {
+      r = e - 2 * NAT - NWS - NUW - NVS; w = TX; gj0 = y0; gi0 = x0;
+      base = a.akt + n * F + (long)L * A; dst = sl.akt;
+    }
+    const int gj = gj0 + r / w, gi = gi0 + r % w;
+    const bool in = gj >= 0 && gj < jmt && gi >= 0 && gi < imt;
+    cp_async8z(dst + r, base + (in ? (long)gj * imt + gi : 0), in);
+  }
+  cp_async_mbar_arrive(bar);
+}
+
 // With diagnostics: the level from which a ring cell (where diagnostics are
 // written) is below its bottom and carries no transport through its four
 // faces or w (kfz of its own column covers its west and south faces and
@@ -1148,7 +1012,7 @@ __device__ __forceinline__ int deep_start_cell(const Arena& a, int i, int j) {
 
 template <bool DIAG>
 __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
-    k_tracer_tma64(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles) {
+    k_tracer_tma64(Arena a, const __grid_constant__ TracerMaps maps, int ntx, long ntiles, int tma) {
   extern __shared__ __align__(128) unsigned char smem_tma[];
   ExSmem& S = *reinterpret_cast<ExSmem*>(smem_tma);
   const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
@@ -1162,7 +1026,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
   const int NV = a.nv_scratch;
   double* scr = a.col_scratch + (long)blockIdx.x * km * NV * TTHREADS;
   if (tid == 0) {
-    for (int s = 0; s < NSX; ++s) mbar_init(&S.bar[s], 1);
+    for (int s = 0; s < NSX; ++s) mbar_init(&S.bar[s], TTHREADS);   // one arrival per thread and level
     mbar_fence_init();
   }
   __syncthreads();
@@ -1183,7 +1047,12 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     __syncthreads();  // the previous item is done with every slot
     // level L goes to slot s = L % NSX
     auto issue = [&](int L, int s) {
-      if (tid == 0) issue_level(S.slot[s], &S.bar[s], maps, a.cur, n, km, L, x0, y0);
+      if (tma) {
+        if (tid == 0) issue_level(S.slot[s], &S.bar[s], maps, a.cur, n, km, L, x0, y0);
+        else mbar_arrive(&S.bar[s]);
+      } else {
+        copy_level64(S.slot[s], &S.bar[s], a, n, L, x0, y0);
+      }
       outstanding |= 1u << s;
     };
     auto wait = [&](int s) -> bool {
@@ -1293,12 +1162,16 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
     // slots of levels k, k-1, k+1 (NSX == 3: level k-2 shares k+1's), carried
     // through the level loop
     static_assert(NSX == 3, "slot rotation below assumes three slots");
-    // (below ks the slot of level ks+1 holds nothing of this tile: level ks
-    // is land everywhere in the region, and nothing of it reads that slot)
+    // (below ks the slot of level ks+1 holds level ks-2: the first
+    // predictor's limiter flags of level ks meet the tile's cells only
+    // through zero transports.)  Every level the prologue issued is waited
+    // before any of them is used: with the third one still in flight the
+    // results came out different at a cell's bottom wet level in some runs,
+    // in the cells of the threads that also carry a ring cell.
     int sk = ks % NSX;
     int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
     {
-      const bool ok = wait(sk) && (ks == 0 || wait(sm1));
+      const bool ok = wait(sk) && (ks == 0 || wait(sm1)) && (ks < 2 || wait(sp1));
       // a wait that ran out anywhere in the CTA sends every thread out together
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
     }
@@ -1313,7 +1186,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       // ---- phase B1: first Laplacian at level k (arrived in an earlier step)
       del4_one64(S, a, k, sk, ty + 1, tx + 1, x0, y0);
       if (has_ring) del4_one64(S, a, k, sk, ring_hj, ring_hi, x0, y0);
-      const bool ok = (k >= 2) ? wait(sp1) : true;   // level k-2
+      const bool ok = (k >= 2 && k != ks) ? wait(sp1) : true;   // level k-2 (the prologue waited ks-2)
       if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return; }
       // ---- phase B2: predictor one level up.  The column phase below reads
       // the flags of level k of the neighbours (written in the previous step)
@@ -1849,10 +1722,9 @@ int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots) {
   const int ntx = (a.imt + TX - 1) / TX;
   const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
   const size_t sm = sizeof(TSmem);
-  // [scheme][diagnostics]: lt_adv_scheme order
+  // [scheme - 1][diagnostics]: the centred and flux schemes (lt_adv_scheme order)
   using Kern = void (*)(Arena, int, long);
-  static const Kern kern[3][2] = {
-      {k_tracer64<false, LT_ADV_TSPAS>, k_tracer64<true, LT_ADV_TSPAS>},
+  static const Kern kern[2][2] = {
       {k_tracer64<false, LT_ADV_CENTERED>, k_tracer64<true, LT_ADV_CENTERED>},
       {k_tracer64<false, LT_ADV_FLUX>, k_tracer64<true, LT_ADV_FLUX>}};
   static bool attr = false;
@@ -1862,13 +1734,13 @@ int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots) {
     attr = true;
   }
   const int adv = a.p.adv_tracer;
-  if (adv < LT_ADV_TSPAS || adv > LT_ADV_FLUX) return LT_E_INVALID;
-  kern[adv][a.diagnostics ? 1 : 0]<<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
+  if (adv != LT_ADV_CENTERED && adv != LT_ADV_FLUX) return LT_E_INVALID;
+  kern[adv - 1][a.diagnostics ? 1 : 0]<<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
   LT_LAUNCHED();
   return LT_OK;
 }
 
-int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid) {
+int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid, bool tma) {
   const int ntx = (a.imt + TX - 1) / TX;
   const long ntiles = (long)ntx * ((a.jmt + TY - 1) / TY);
   const size_t sm = sizeof(ExSmem);
@@ -1879,12 +1751,12 @@ int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, 
     attr = true;
   }
   if (a.diagnostics) {
-    k_tracer_tma64<true><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+    k_tracer_tma64<true><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles, tma ? 1 : 0);
     LT_LAUNCHED();
     // the levels below each tile's march
     k_diag_deep<<<dim3((unsigned)ntiles, 2), TTHREADS, 0, s>>>(a, ntx);
   } else {
-    k_tracer_tma64<false><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles);
+    k_tracer_tma64<false><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles, tma ? 1 : 0);
   }
   LT_LAUNCHED();
   return LT_OK;

@@ -976,7 +976,9 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
   int sk = ks % NSM;
   int sm1 = sk == 0 ? 2 : sk - 1, sp1 = sk == 2 ? 0 : sk + 1;
   {
-    const bool ok = wait(sk) && (ks == 0 || wait(sm1));
+    // every level the prologue issued is waited before any of them is used
+    // (as in the FP64 kernel)
+    const bool ok = wait(sk) && (ks == 0 || wait(sm1)) && (ks < 2 || wait(sp1));
     if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
   }
   {
@@ -1011,7 +1013,7 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
     if (has_ob) face_f64(S, Lk, of_b);
     d2_cell(S, Lk, k, own_cell);
     if (has_ring) d2_cell(S, Lk, k, ring_cell);
-    const bool ok = (k >= 2) ? wait(sp1) : true;   // level k-2
+    const bool ok = (k >= 2 && k != ks) ? wait(sp1) : true;   // level k-2 (the prologue waited ks-2)
     if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
     // ---- phase B2: predictor one level up.  The column phase below reads
     // the flags of level k (written in the previous step) and, of level k-1,

@@ -75,7 +75,9 @@ struct alignas(64) MemberDesc {
   int tma;       // 1: level boxes by TMA; 0: by per-thread copies (row pitch TMA cannot take)
 };
 
-int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid);
+// The FP64 column kernel of the tspas scheme; tma: its level boxes by TMA (else
+// per-thread copies, for row pitches TMA cannot take)
+int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, int grid, bool tma);
 // Batched forms (mixed precision): nmem members, total work items, one
 // persistent column launch of `grid` CTAs with per-CTA scratch of km_max
 // levels; continuity over every member's tiles with tiles of 32 x cby columns.

@@ -121,7 +121,8 @@ def test_multistep_medium_grid(lt):
 
 @pytest.mark.parametrize("tma", [True, False])
 def test_both_column_kernels(lt, tma):
-    """The TMA-fed column kernel and the plain-load variant give the same bits."""
+    """The column kernel's level slots filled by TMA boxes or by per-thread
+    asynchronous copies: the same bits as the oracle either way."""
     syn, f = make(lt, 100, 60, 20, forced=1, cap_north=0)
     dom = gpu_domain(lt, syn, f, diagnostics=True)
     dom.use_tma(tma)
@@ -133,17 +134,23 @@ def test_both_column_kernels(lt, tma):
         assert bits_equal(g, r), n + ": " + mismatch(g, r)
 
 
-def test_odd_row_pitch_uses_plain_kernel(lt):
+@pytest.mark.parametrize("diagnostics", [False, True])
+def test_odd_row_pitch_copy_fill(lt, diagnostics):
     """nx = 49 (closed domain): the row pitch is not a multiple of 16 bytes,
-    the TMA path is refused and the plain kernel still matches."""
+    TMA boxes are refused, and the column kernel's slots filled by per-thread
+    copies still match the oracle bit for bit (with the diagnostics, also
+    below the tile's march)."""
     syn, f = make(lt, 49, 30, 10, forced=1, cap_north=2, ew_cyclic=0, tripole=0)
-    dom = gpu_domain(lt, syn, f)
+    dom = gpu_domain(lt, syn, f, diagnostics=diagnostics)
     with pytest.raises(lt.LtError):
         dom.use_tma(True)
     dom.step(3)
     o = oracle_for(syn, f)
     o.step(3)
-    assert bits_equal(dom.get("AT"), o.get("AT"))
+    names = ["AT", "ATB", "WS"] + (["AX", "AY", "AZ", "DZ", "PENETRATE", "TEND", "DT_DIFF"] if diagnostics else [])
+    for n in names:
+        g, r = dom.get(n), o.get(n)
+        assert bits_equal(g, r), n + ": " + mismatch(g, r)
 
 
 def test_closed_boundaries(lt):
