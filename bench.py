@@ -95,6 +95,9 @@ def parse():
                     help="steps after which the mixed state is compared with the FP64 state")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the conservation, diagnostics, ensemble and serving figures of the default run")
+    ap.add_argument("--hypsometry", type=int, default=0, choices=[0, 1],
+                    help="ocean depths of the generator: 0 = linear in the land field (mostly shallow), "
+                         "1 = the global ocean's area-depth curve (mean depth about 3.7 km)")
     ap.add_argument("--band-rows", type=int, default=0,
                     help="CPU baseline: physical rows of the band a timed host step advances (default ny/16)")
     return ap.parse_args()
@@ -104,7 +107,21 @@ def workload(args):
     nx, ny, km = args.grid
     deep = km >= 50
     return dict(nx=nx, ny=ny, km=km, umax=0.3 if deep else 0.1, dz_top=5.0 if deep else 10.0,
-                dz_bot=300.0 if deep else 250.0, cap_north=0, forced=1)
+                dz_bot=300.0 if deep else 250.0, cap_north=0, forced=1, hypsometry=args.hypsometry)
+
+
+HYPSOMETRY = {0: "KMT linear in the land field above its 30 % threshold (3..km levels, mostly shallow)",
+              1: "the global ocean's area-depth curve (mean ocean depth about 3.7 km)"}
+
+
+def bathymetry(syn, km):
+    """Wet share of the grid's cell-levels and of the ocean columns' levels."""
+    import numpy as np
+    kmt = syn.field("KMT")[2:-2, 2:-2]
+    ocean = kmt[kmt > 0]
+    return {"wet_cell_levels_frac": round(float(kmt.mean()) / km, 4),
+            "ocean_mean_kmt": round(float(ocean.mean()), 2) if ocean.size else 0.0,
+            "land_columns_frac": round(float((kmt == 0).mean()), 4)}
 
 
 class ClockSampler:
@@ -360,6 +377,7 @@ def config_of(args, world):
     nx, ny, km = args.grid
     cells = nx * ny * km
     return {"workload": "0.1deg tracer step %dx%dx%d" % (nx, ny, km), "nx": nx, "ny": ny, "km": km,
+            "hypsometry": args.hypsometry, "depths": HYPSOMETRY[args.hypsometry],
             "parallelism": "replicas" if world > 1 else "single",
             "l2": "inputs (~%.0f GB) far larger than L2; no flush" % (cells * 8 * 16 / 1e9)}
 
@@ -372,6 +390,7 @@ def measure(lt, args, pg, world, local, precision, keep_state):
     w = workload(args)
     prec = lt.PREC_MIXED if precision == "mixed" else lt.PREC_FP64
     syn = lt.Synth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+    bathy = bathymetry(syn, km)
     dom = syn.domain(precision=prec)
     cells = nx * ny * km
 
@@ -466,7 +485,42 @@ def measure(lt, args, pg, world, local, precision, keep_state):
     dom.close()
     return {"value": value, "ms_per_step": ms / args.steps, "roofline": roofline, "e2e": e2e,
             "gpu_launches": launches, "clocks": clk.summary(), "fw_norm2": fw.value, "state": state, "kmt": kmt,
-            "steps_total": steps_total, "icesnow": icesnow}
+            "steps_total": steps_total, "icesnow": icesnow, "bathymetry": bathy}
+
+
+def deep_ocean_figures(lt, args, steps=5, warmup=3):
+    """The bench grid with the global ocean's area-depth curve instead of
+    the linear depth map (--hypsometry 1): most columns are abyssal, so the
+    column march runs through most levels of most tiles.  Device-resident
+    step rate of both forms (inputs far larger than L2), the same timing as
+    the headline."""
+    nx, ny, km = args.grid
+    w = dict(workload(args), hypsometry=1)
+    cells = nx * ny * km
+    hbm, hbm_kind = peaks()
+    out = {"hypsometry": 1, "depths": HYPSOMETRY[1], "steps": steps, "warmup": warmup}
+    for precision in ("fp64", "mixed"):
+        syn = lt.Synth(nx, ny, km, **{k: v for k, v in w.items() if k not in ("nx", "ny", "km")})
+        out["bathymetry"] = bathymetry(syn, km)
+        dom = syn.domain(precision=lt.PREC_MIXED if precision == "mixed" else lt.PREC_FP64)
+        dom.step(warmup)
+        dom.sync()
+        dom.profile(True)
+        with ClockSampler(0) as clk:
+            dom.step(steps)
+            dom.sync()
+        ms = dom.last_step_ms() / steps
+        nprof, ph = dom.phase_ms()
+        dom.close()
+        t_col = ph["tracer"] / max(nprof, 1)
+        out[precision] = {"value": cells / (ms * 1e-3), "ms_per_step": ms,
+                          "step_frac": STEP_BYTES[precision] * cells / (ms * 1e-3) / 1e9 / hbm,
+                          "column_kernel_frac": TRACER_KERNEL_BYTES[precision] * cells / (t_col * 1e-3) / 1e9 / hbm,
+                          "peak_kind": hbm_kind,
+                          "phase_ms_per_step": {k: v / max(nprof, 1) for k, v in ph.items()},
+                          "clocks": clk.summary()}
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
 
 
 def measure_readyc(lt, args, precision):
@@ -656,7 +710,8 @@ def run_ours(args):
                 "data": "synthetic (seeded generators with the configuration's shapes and distributions)",
                 "config": config_of(args, world),
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["gpu_launches"],
-                "clocks": r["clocks"], "fw_norm2": r["fw_norm2"], "icesnow": r["icesnow"]}
+                "clocks": r["clocks"], "fw_norm2": r["fw_norm2"], "icesnow": r["icesnow"],
+                "bathymetry": r["bathymetry"]}
         if not args.no_turb and world == 1:
             line["turb"], line["hdiffu_del4"] = measure_readyc(lt, args, main)
         if both:
@@ -687,6 +742,8 @@ def run_ours(args):
                 "step_frac": diag_bytes * cells / (ms_diag * 1e-3) / 1e9 / hbm, "peak_kind": hbm_kind,
                 "writes": "ax, ay, az, dz, tend, dt_diff (both tracers) and penetrate, as tracer.cpp always does",
                 "workload": "the conservation run above (zero surface flux, capped edges)"}
+            if args.hypsometry == 0:
+                line["deep_ocean"] = deep_ocean_figures(lt, args)
             line["ensemble"] = ensemble_figures(lt, args.members, 100, 3, check=4)
             line["ensemble"]["reduced"] = "4 of %d members checked against their FP64 runs" % args.members
             line["serving"] = serving_figures(lt, 60, args.rate)

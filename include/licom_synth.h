@@ -32,6 +32,9 @@ typedef struct {
   uint32_t member;            /* ensemble member (0 = unperturbed) */
   double tpert;               /* K, std of the member's T perturbation */
   double ah_bihar;            /* m^4/s; 0 = -min(1e17, half the grid's explicit stability limit) */
+  int hypsometry;             /* ocean depths: 0 = linear in the land field above its threshold (3 .. km
+                                 levels, mostly shallow); 1 = the global ocean's area-depth curve
+                                 (mean depth about 3.7 km, 30 % of the ocean deeper than 5 km) */
 } lt_synth_config;
 
 typedef struct lt_synth lt_synth;

@@ -134,7 +134,7 @@ class SynthConfig(C.Structure):
                 ("dz_top", C.c_double), ("dz_bot", C.c_double), ("depth", C.c_double), ("umax", C.c_double),
                 ("seed", C.c_uint64), ("forced", C.c_int), ("cap_north", C.c_int), ("cap_south", C.c_int),
                 ("ew_cyclic", C.c_int), ("tripole", C.c_int), ("land_frac", C.c_double), ("member", C.c_uint32),
-                ("tpert", C.c_double), ("ah_bihar", C.c_double)]
+                ("tpert", C.c_double), ("ah_bihar", C.c_double), ("hypsometry", C.c_int)]
 
 
 class BatchConfig(C.Structure):

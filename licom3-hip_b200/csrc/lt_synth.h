@@ -199,6 +199,11 @@ struct SynthConfig {
   // -1e17, capped at half of this grid's explicit stability limit (see
   // build_domain).
   double ah_bihar = 0.0;
+  // Ocean depth map: 0 = KMT linear in the land field above its threshold
+  // (3 .. km levels); 1 = depths by the rank of the land field among the
+  // ocean cells on the global ocean's area-depth curve (hypsometry), so the
+  // shallow cells sit next to the coast and most of the ocean is abyssal.
+  int hypsometry = 0;
   double dwndmix = 1.0e-3;
   double gamma_days = 30.0;
   double tnoise = 0.1, snoise_psu = 0.01;
@@ -366,12 +371,42 @@ inline Domain build_domain(const SynthConfig& c) {
     std::nth_element(sorted.begin(), sorted.begin() + q, sorted.end());
     const int64_t thr = sorted[q];
     int64_t fmax = *std::max_element(f.begin(), f.end());
+    // hypsometry 1: the ocean cells' rank in the land field (ties by
+    // position) read as the fraction q of the ocean shallower than the cell,
+    // mapped through the global ocean's area-depth curve (piecewise linear
+    // between these published fractions: 7.5 % shallower than 200 m, 12 %
+    // than 1 km, 16.5 % than 2 km, 25 % than 3 km, 46 % than 4 km, 78 % than
+    // 5 km, 99 % than 6 km), depth clipped to the grid's; KMT = the levels
+    // whose centre lies above that depth, at least 3
+    std::vector<int> hyps_k;
+    if (c.hypsometry == 1) {
+      std::vector<std::pair<int64_t, long>> ocean;
+      for (long q = 0; q < (long)f.size(); ++q)
+        if (f[q] > thr) ocean.push_back({f[q], q});
+      std::sort(ocean.begin(), ocean.end());
+      static const double zq[][2] = {{0.0, 0.0},       {200.0, 0.075},  {1000.0, 0.12}, {2000.0, 0.165},
+                                     {3000.0, 0.25},   {4000.0, 0.46},  {5000.0, 0.78}, {6000.0, 0.99},
+                                     {11000.0, 1.0}};
+      hyps_k.assign(f.size(), 0);
+      const long n = (long)ocean.size();
+      for (long r = 0; r < n; ++r) {
+        const double q = (r + 0.5) / (double)n;
+        int s = 1;
+        while (s < 8 && zq[s][1] < q) ++s;
+        const double z = zq[s - 1][0] + (zq[s][0] - zq[s - 1][0]) * (q - zq[s - 1][1]) / (zq[s][1] - zq[s - 1][1]);
+        int k = 0;
+        while (k < km && -0.5 * (d.zkp[k] + d.zkp[k + 1]) < z) ++k;
+        hyps_k[ocean[r].second] = std::max(3, k);
+      }
+    }
     d.kmt.assign(A, 0);
     for (int j = 0; j < ny; ++j)
       for (int i = 0; i < nx; ++i) {
         const int64_t v = f[(long)j * nx + i];
         int k = 0;
-        if (v > thr) {
+        if (v > thr && c.hypsometry == 1) {
+          k = hyps_k[(long)j * nx + i];
+        } else if (v > thr) {
           const int64_t span = std::max<int64_t>(fmax - thr, 1);
           k = 3 + (int)(((v - thr) * (int64_t)(km - 3)) / span);
           if (k > km) k = km;

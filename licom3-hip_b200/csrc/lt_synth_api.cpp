@@ -20,6 +20,7 @@ lt::SynthConfig to_cfg(const lt_synth_config& c) {
   s.ew_cyclic = c.ew_cyclic; s.tripole = c.tripole;
   s.land_frac = c.land_frac; s.member = c.member; s.tpert = c.tpert;
   s.ah_bihar = c.ah_bihar;
+  s.hypsometry = c.hypsometry;
   return s;
 }
 }  // namespace
@@ -36,6 +37,7 @@ void lt_synth_defaults(lt_synth_config* c) {
   c->ew_cyclic = s.ew_cyclic; c->tripole = s.tripole;
   c->land_frac = s.land_frac; c->member = s.member; c->tpert = s.tpert;
   c->ah_bihar = s.ah_bihar;
+  c->hypsometry = s.hypsometry;
 }
 
 int lt_synth_build(const lt_synth_config* cfg, lt_synth** out) {

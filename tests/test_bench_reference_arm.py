@@ -40,5 +40,6 @@ def test_reference_arm_runs_without_the_product_library():
 
     class A:
         grid = [120, 80, 30]
+        hypsometry = 0
     assert line["config"] == b.config_of(A, 1)
     assert line["ms_per_step"] * line["steps"] < 60e3

@@ -43,6 +43,17 @@ def test_mixed_error_bounds_100_steps(lt):
     assert mix.check_numeric() == 0
 
 
+def test_mixed_error_bounds_deep_ocean(lt):
+    """The same bounds on the 1-degree grid with the global ocean's
+    area-depth curve: most columns wet through most of the 30 levels."""
+    syn, ref, mix = run_pair(lt, 360, 218, 30, 100, forced=1, cap_north=0, hypsometry=1)
+    dt, ds = ocean_errors(syn, ref, mix)
+    print("deep ocean, mixed vs fp64 after 100 steps: max |dT| = %.3e K, max |dS| = %.3e psu" % (dt, ds))
+    assert dt <= T_TOL_K, dt
+    assert ds <= S_TOL_PSU, ds
+    assert mix.check_numeric() == 0
+
+
 def test_mixed_small_grid_close(lt):
     syn, ref, mix = run_pair(lt, 64, 40, 20, 10, forced=1, cap_north=0)
     dt, ds = ocean_errors(syn, ref, mix)

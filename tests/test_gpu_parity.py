@@ -119,6 +119,21 @@ def test_multistep_medium_grid(lt):
         assert bits_equal(g, r), n + ": " + mismatch(g, r)
 
 
+@pytest.mark.parametrize("diagnostics", [False, True])
+def test_deep_ocean_bitexact(lt, diagnostics):
+    """Depths from the global ocean's area-depth curve: the column march
+    starts at the bottom level in most tiles and the deep-level paths (copies
+    below the tile's bottom, the diagnostics' deep kernel) see few levels."""
+    syn, f = make(lt, 120, 80, 30, forced=1, cap_north=0, hypsometry=1)
+    dom = gpu_domain(lt, syn, f, diagnostics=diagnostics)
+    dom.step(10)
+    o = oracle_for(syn, f)
+    o.step(10)
+    for n in ("AT", "ATB", "WS") + (("AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF") if diagnostics else ()):
+        g, r = dom.get(n), o.get(n)
+        assert bits_equal(g, r), n + ": " + mismatch(g, r)
+
+
 @pytest.mark.parametrize("tma", [True, False])
 def test_both_column_kernels(lt, tma):
     """The column kernel's level slots filled by TMA boxes or by per-thread

@@ -34,3 +34,26 @@ def test_host_generator_matches_product_generator(lt):
         assert np.array_equal(a, b[..., :16, :]), n
     a, b = ob.get("AT"), syn.field("AT")
     assert np.array_equal(a[:, :, :14], b[:, :, :14])
+
+
+def test_hypsometry_keeps_the_land_and_deepens_the_ocean(lt):
+    """hypsometry 1 keeps the land mask of the linear depth map and places
+    the ocean's depths on the global area-depth curve: shallow next to the
+    coast (the lowest land-field values), most of the ocean abyssal; the
+    host build agrees bit for bit."""
+    kw = dict(forced=1, cap_north=0)
+    lin = lt.Synth(120, 80, 30, **kw).field("KMT")[2:-2, 2:-2]
+    syn = lt.Synth(120, 80, 30, hypsometry=1, **kw)
+    hyp = syn.field("KMT")[2:-2, 2:-2]
+    assert np.array_equal(lin == 0, hyp == 0)
+    ocean = hyp[hyp > 0]
+    assert hyp[1:][hyp[1:] > 0].min() >= 3 and ocean.max() == 30   # (row 0 mirrors the fold)
+    zkp = np.concatenate([[0.0], np.cumsum(syn.field("DZP"))])
+    depth = 0.5 * (zkp[ocean - 1] + zkp[ocean])            # centre depth of the bottom level
+    assert 3000.0 < depth.mean() < 4300.0, depth.mean()
+    assert 0.15 < (depth < 2000.0).mean() < 0.25
+    assert (hyp[hyp > 0].mean()) > 2.0 * lin[lin > 0].mean()
+    hs = pyoracle.HostSynth(120, 80, 30, hypsometry=1, **kw)
+    o = pyoracle.Oracle(120, 80, 30, hs.params)
+    hs.fill(o)
+    assert np.array_equal(o.get("KMT"), syn.field("KMT"))
