@@ -994,6 +994,13 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
     S.flag[sk][own_cell.m] = (unsigned char)pred_cell(S, own_cell, ks, km, sk, sm1, sp1, lv, dtsf);
     if (has_ring) S.flag[sk][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, ks, km, sk, sm1, sp1, lv, dtsf);
   }
+  // The first step's phase B1 overwrites the face arrays these predictors
+  // read (its faces are of level ks-1).  Without this barrier a warp that
+  // finished its predictors early changed a neighbouring cell's faces while
+  // that cell's predictor still read them: the limiter flags of level ks came
+  // out different from run to run in tiles whose level ks is wet (a column
+  // reaching the bottom level), at the tile's edge columns.
+  __syncthreads();
 
   // Level slots: after step k the slot of level k takes level k-NSM.
   for (int k = ks; k >= 0; --k) {
