@@ -568,7 +568,8 @@ __device__ __forceinline__ FaceRef face_y_ref(int fj, int fi) {
 // masked to 0 where either cell is land at level kk: the transport through
 // such a face is 0, and a 0 difference stands for the excluded neighbour in
 // the masked extrema.
-__device__ __forceinline__ void face_f32(MxSmem& S, const MxSlot& L, int kk, const FaceRef& q) {
+__device__ __forceinline__ void face_f32(MxSmem& S, const MxSlot& L, int kk, const FaceRef& q, int k1 = -1,
+                                         int k2 = -1) {
   int r1, r2;    // the two cells: r1 the one whose value is subtracted
   float u;
   if (q.x) {
@@ -578,7 +579,7 @@ __device__ __forceinline__ void face_f32(MxSmem& S, const MxSlot& L, int kk, con
     r1 = q.r; r2 = q.r + SW64;
     u = face32(L.wkb[q.w], L.wkb[q.w + 1], S.hw[q.f]);
   }
-  const bool wet = kk < S.kmt[r1] && kk < S.kmt[r2];
+  const bool wet = kk < (k1 >= 0 ? k1 : (int)S.kmt[r1]) && kk < (k2 >= 0 ? k2 : (int)S.kmt[r2]);
   float2 d;
   d.x = wet ? (float)(L.at[0][r2] - L.at[0][r1]) : 0.f;
   d.y = wet ? (float)(L.at[1][r2] - L.at[1][r1]) : 0.f;
@@ -685,10 +686,11 @@ __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 // and bottom level the missing neighbour level is replaced by kk itself,
 // whose differences are then 0, and so are the vertical terms they carry).
 __device__ __forceinline__ unsigned pred_cell(const MxSmem& S, const HCell& h, int kk, int km, int sc, int su,
-                                              int sd, const MxLevel& lv, float dts) {
+                                              int sd, const MxLevel& lv, float dts, int kself = -1) {
   const int r = h.r;
+  const int kr = kself >= 0 ? kself : (int)S.kmt[r];
   // land cells need no flag: every face of a land cell carries no transport
-  if (!h.valid || kk >= S.kmt[r]) return 0u;
+  if (!h.valid || kk >= kr) return 0u;
   const int fe = h.fw + 1, fw = h.fw, fs = h.fn + HQX, fn = h.fn;
   const float2 de = S.fd[fe], dw = S.fd[fw], ds = S.fd[fs], dn = S.fd[fn];
   // east face: this cell is the lower one, d*(u - q); west face: upper, d*(u + q)
@@ -714,7 +716,7 @@ __device__ __forceinline__ unsigned pred_cell(const MxSmem& S, const HCell& h, i
   // masked face differences, below through the test here; the level above a
   // wet cell is wet.  The flags of land cells are never used: every face of
   // a land cell carries no transport.
-  const bool below_wet = kk + 1 < S.kmt[r];
+  const bool below_wet = kk + 1 < kr;
   const float lx = below_wet ? -dlo.x : 0.f, ly = below_wet ? -dlo.y : 0.f;
   const float mxT = fmax3f(fmax3f(0.f, de.x, -dw.x), fmax3f(ds.x, -dn.x, dup.x), lx);
   const float mnT = fmin3f(fmin3f(0.f, de.x, -dw.x), fmin3f(ds.x, -dn.x, dup.x), lx);
@@ -725,22 +727,26 @@ __device__ __forceinline__ unsigned pred_cell(const MxSmem& S, const HCell& h, i
 
 // First Laplacian of atb at level kk for one cell, both tracers (f64 on the
 // state differences), masked: land neighbours drop out, a land cell is 0.
-__device__ __forceinline__ void d2_cell(MxSmem& S, const MxSlot& L, int kk, const HCell& h) {
+struct Kmt5 {
+  int c, n, s, e, w;
+};
+__device__ __forceinline__ void d2_cell(MxSmem& S, const MxSlot& L, int kk, const HCell& h,
+                                        const Kmt5* kq = nullptr) {
   double vT = 0.0, vS = 0.0;
   const int r = h.r, m = h.m;
-  if (h.valid && kk < S.kmt[r]) {
+  if (h.valid && kk < (kq ? kq->c : (int)S.kmt[r])) {
     const double cT = L.atb[0][r], cS = L.atb[1][r];
-    auto term = [&](int rn, float coef) {
-      if (kk < S.kmt[rn]) {
+    auto term = [&](int rn, float coef, int kn) {
+      if (kk < (kq ? kn : (int)S.kmt[rn])) {
         const double c = (double)coef;
         vT = fma(c, L.atb[0][rn] - cT, vT);
         vS = fma(c, L.atb[1][rn] - cS, vS);
       }
     };
-    term(r - SW64, S.dtn[m]);
-    term(r + SW64, S.dts[m]);
-    term(r + 1, S.dte[m]);
-    term(r - 1, S.dtw[m]);
+    term(r - SW64, S.dtn[m], kq ? kq->n : 0);
+    term(r + SW64, S.dts[m], kq ? kq->s : 0);
+    term(r + 1, S.dte[m], kq ? kq->e : 0);
+    term(r - 1, S.dtw[m], kq ? kq->w : 0);
     const double ah = (double)S.ahf[m];
     vT *= ah;
     vS *= ah;
@@ -886,7 +892,8 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
   // only through faces and a w that carry no transport there.)
   stage_kmt<kLoadsAhead>(S, a, x0, y0);
   __syncthreads();
-  int kmax = (int)S.kmt[own_cell.r];
+  const Kmt5 kq = {S.kmt[rc], S.kmt[rc - SW64], S.kmt[rc + SW64], S.kmt[rc + 1], S.kmt[rc - 1]};
+  int kmax = kq.c;
   kmax = __reduce_max_sync(0xffffffffu, kmax);
   if (tx == 0) S.wmax[ty] = kmax;
   __syncthreads();
@@ -983,15 +990,15 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
   }
   {
     const MxSlot& L = S.slot[sk];
-    face_f32(S, L, ks, fo_x);
-    face_f32(S, L, ks, fo_y);
+    face_f32(S, L, ks, fo_x, kq.w, kq.c);
+    face_f32(S, L, ks, fo_y, kq.n, kq.c);
     if (has_fb) face_f32(S, L, ks, fo_b);
     if (has_fb2) face_f32(S, L, ks, fo_b2);
   }
   __syncthreads();
   {
     const MxLevel lv = lvs[ks];
-    S.flag[sk][own_cell.m] = (unsigned char)pred_cell(S, own_cell, ks, km, sk, sm1, sp1, lv, dtsf);
+    S.flag[sk][own_cell.m] = (unsigned char)pred_cell(S, own_cell, ks, km, sk, sm1, sp1, lv, dtsf, kq.c);
     if (has_ring) S.flag[sk][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, ks, km, sk, sm1, sp1, lv, dtsf);
   }
   // The first step's phase B1 overwrites the face arrays these predictors
@@ -1010,15 +1017,15 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
     const MxSlot& Lk = S.slot[sk];
     if (k >= 1) {
       const MxSlot& Lu = S.slot[sm1];
-      face_f32(S, Lu, k - 1, fo_x);
-      face_f32(S, Lu, k - 1, fo_y);
+      face_f32(S, Lu, k - 1, fo_x, kq.w, kq.c);
+      face_f32(S, Lu, k - 1, fo_y, kq.n, kq.c);
       if (has_fb) face_f32(S, Lu, k - 1, fo_b);
       if (has_fb2) face_f32(S, Lu, k - 1, fo_b2);
     }
     face_f64(S, Lk, of_x);
     face_f64(S, Lk, of_y);
     if (has_ob) face_f64(S, Lk, of_b);
-    d2_cell(S, Lk, k, own_cell);
+    d2_cell(S, Lk, k, own_cell, &kq);
     if (has_ring) d2_cell(S, Lk, k, ring_cell);
     const bool ok = (k >= 2 && k != ks) ? wait(sp1) : true;   // level k-2 (the prologue waited ks-2)
     if (__syncthreads_or(!ok)) { tma_bail(S, a, par, outstanding); return false; }
@@ -1029,7 +1036,7 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
     unsigned flag_up = 0;
     if (k >= 1) {
       const MxLevel lv = lvs[k - 1];
-      flag_up = pred_cell(S, own_cell, k - 1, km, sm1, sp1, sk, lv, dtsf);
+      flag_up = pred_cell(S, own_cell, k - 1, km, sm1, sp1, sk, lv, dtsf, kq.c);
       S.flag[sm1][own_cell.m] = (unsigned char)flag_up;
       if (has_ring) S.flag[sm1][ring_cell.m] = (unsigned char)pred_cell(S, ring_cell, k - 1, km, sm1, sp1, sk, lv, dtsf);
     }
@@ -1058,9 +1065,9 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
       const double wq = wv * wv * lv.odzt * dts;       // vertical Lax-Wendroff factor
       const double vit_kp1 = (k + 1 < kz) ? 1.0 : 0.0;
       // masks of the second Laplacian's faces (hmix_del4.F90:626-757)
-      const bool mself = k <= S.kmt[rc] - 1;
-      const bool mE = mself && k <= S.kmt[rc + 1] - 1, mW = mself && k <= S.kmt[rc - 1] - 1;
-      const bool mS = mself && k <= S.kmt[rc + SW64] - 1, mN = mself && k <= S.kmt[rc - SW64] - 1;
+      const bool mself = k <= kq.c - 1;
+      const bool mE = mself && k <= kq.e - 1, mW = mself && k <= kq.w - 1;
+      const bool mS = mself && k <= kq.s - 1, mN = mself && k <= kq.n - 1;
       const MxSlot& Lu = S.slot[k > 0 ? sm1 : sk];
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
