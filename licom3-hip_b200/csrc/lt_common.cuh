@@ -147,4 +147,38 @@ int launch_f32_to_f64(const float* x, double* y, long n, cudaStream_t s);
 int tracer_slots(const Arena& a);
 size_t tree_sum_part_elems(long n);
 
+// L2 policies of the column sweeps' scratch.  The elimination coefficients of
+// a work item's wet levels are written during its march and read once, in
+// reverse order, by its substitution.  Written with evict_last they stay in
+// L2 against the streaming level boxes and state stores (on a deep ocean the
+// scratch of all resident CTAs is close to the L2's size); read with
+// evict_first they leave it once used.  The kernels write the new state with
+// streaming stores (__stcs): nothing reads it again within the step.
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void st_l2(double* p, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ double ld_l2(const double* p, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_l2(double2* p, double2 v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y), "l"(pol) : "memory");
+}
+__device__ __forceinline__ double2 ld_l2(const double2* p, uint64_t pol) {
+  double2 v;
+  asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(p), "l"(pol));
+  return v;
+}
+
 }  // namespace lt

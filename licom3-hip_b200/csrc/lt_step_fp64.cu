@@ -1139,8 +1139,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
 #pragma unroll
         for (int c = 0; c < 8; ++c)
           if (k0 + c < km) {
-            d1[(long)(k0 + c) * A + qo] = v[c];
-            d2[(long)(k0 + c + 1) * A + qo] = v[c];
+            __stcs(d1 + (long)(k0 + c) * A + qo, v[c]);
+            __stcs(d2 + (long)(k0 + c + 1) * A + qo, v[c]);
           }
       }
     }
@@ -1203,8 +1203,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       if (!DIAG && inner && k >= kz) {
         const LevelSlot<double>& Lk = S.slot[sk];
         const double c = Lk.at[rc];
-        at_out[(long)k * A + qo] = c;
-        atb_out[(long)(k + 1) * A + qo] = c;
+        __stcs(at_out + (long)k * A + qo, c);
+        __stcs(atb_out + (long)(k + 1) * A + qo, c);
         at_dn = c;
         ws_dn = Lk.ws[uc];
         atb_dn = Lk.atb[rc];
@@ -1389,9 +1389,10 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
             f_prev = fv;
           }
           double* sl = scr + (long)k * NV * TTHREADS;
-          sl[tid] = ev;
-          sl[TTHREADS + tid] = fv;
-          if (DIAG) sl[2 * TTHREADS + tid] = d8;
+          const uint64_t pl = l2_evict_last();
+          st_l2(sl + tid, ev, pl);
+          st_l2(sl + TTHREADS + tid, fv, pl);
+          if (DIAG) st_l2(sl + 2 * TTHREADS + tid, d8, pl);
           }  // wet
           atb_dn = atb_k;
         }
@@ -1414,13 +1415,14 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
       double x = 0.0;
       constexpr int SUB = 8;
       const int kend = min(kz, ks + 1);   // the levels the march left in the scratch (the wet ones)
+      const uint64_t pf = l2_evict_first();
       for (int k0 = 0; k0 < kend; k0 += SUB) {
         double evs[SUB], fvs[SUB];
 #pragma unroll
         for (int c = 0; c < SUB; ++c) {
           const double* sl = scr + (long)(k0 + c) * NV * TTHREADS;
-          evs[c] = k0 + c < kend ? sl[tid] : 0.0;
-          fvs[c] = k0 + c < kend ? sl[TTHREADS + tid] : 0.0;
+          evs[c] = k0 + c < kend ? ld_l2(sl + tid, pf) : 0.0;
+          fvs[c] = k0 + c < kend ? ld_l2(sl + TTHREADS + tid, pf) : 0.0;
         }
 #pragma unroll
       for (int c = 0; c < SUB; ++c) {
@@ -1438,7 +1440,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           v = fv;
         }
         if (DIAG) {
-          const double d8 = sl[2 * TTHREADS + tid];
+          const double d8 = ld_l2(sl + 2 * TTHREADS + tid, pf);
           const double vit_k = k < kz ? 1.0 : 0.0;
           const double at_old = at_in[cg];
           a.tend[n * F + cg] = (v - at_old) / dts * vit_k;
@@ -1446,8 +1448,8 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
           else a.dt_diff[n * F + cg] = (v - d8) / dts * vit_k;
           if (j == 2 && a.tripole) a.fold_save[((long)(n * km + k)) * imt + i] = d8;
         }
-        at_out[cg] = v;
-        atb_out[(long)(k + 1) * A + qo] = v;
+        __stcs(at_out + cg, v);
+        __stcs(atb_out + (long)(k + 1) * A + qo, v);
       }
       }
     }

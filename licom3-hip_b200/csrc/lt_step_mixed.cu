@@ -918,8 +918,8 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
         if (k0 + c < km)
 #pragma unroll
           for (int n = 0; n < 2; ++n) {
-            at_out[n * F + (long)(k0 + c) * A + qo] = v[c][n];
-            atb_out[n * FB + (long)(k0 + c + 1) * A + qo] = v[c][n];
+            __stcs(at_out + n * F + (long)(k0 + c) * A + qo, v[c][n]);
+            __stcs(atb_out + n * FB + (long)(k0 + c + 1) * A + qo, v[c][n]);
           }
     }
   }
@@ -1047,8 +1047,8 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
         const double c = Lk.at[n][rc];
-        a.at[a.cur ^ 1][n * F + (long)k * A + qo] = c;
-        a.atb[a.cur ^ 1][n * FB + (long)(k + 1) * A + qo] = c;
+        __stcs(a.at[a.cur ^ 1] + n * F + (long)k * A + qo, c);
+        __stcs(a.atb[a.cur ^ 1] + n * FB + (long)(k + 1) * A + qo, c);
         cs[n].carry = 0.0;
         cs[n].wbelow = 0.0;
       }
@@ -1147,7 +1147,8 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
           const double g0 = 1.0 / (b8 - c8 * st.e);
           st.e = a8 * g0;
           st.f = (d8 + c8 * st.f) * g0;
-          reinterpret_cast<double2*>(scr)[((long)k * 2 + n) * MTH + tid] = make_double2(st.e, st.f);
+          st_l2(reinterpret_cast<double2*>(scr) + ((long)k * 2 + n) * MTH + tid, make_double2(st.e, st.f),
+                l2_evict_last());
         }
       }
     }
@@ -1167,13 +1168,14 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
     double x[2] = {0.0, 0.0};
     constexpr int SUB = 4;
     const double2* sc2 = reinterpret_cast<const double2*>(scr);
+    const uint64_t pf = l2_evict_first();
     for (int k0 = 0; k0 < kz; k0 += SUB) {
       double2 ef[SUB][2];
 #pragma unroll
       for (int c = 0; c < SUB; ++c)
 #pragma unroll
         for (int n = 0; n < 2; ++n)
-          ef[c][n] = k0 + c < kz ? sc2[((long)(k0 + c) * 2 + n) * MTH + tid] : make_double2(0.0, 0.0);
+          ef[c][n] = k0 + c < kz ? ld_l2(sc2 + ((long)(k0 + c) * 2 + n) * MTH + tid, pf) : make_double2(0.0, 0.0);
 #pragma unroll
       for (int c = 0; c < SUB; ++c) {
         const int k = k0 + c;
@@ -1182,8 +1184,8 @@ __device__ __forceinline__ bool mixed_item(bool tma, MxSmem& S, const MxLevel* _
         for (int n = 0; n < 2; ++n) {
           const double v = (k == 0) ? ef[c][n].x * cs[n].stf + ef[c][n].y : ef[c][n].x * x[n] + ef[c][n].y;
           x[n] = v;
-          at_out[n * F + (long)k * A + qo] = v;
-          atb_out[n * FB + (long)(k + 1) * A + qo] = v;
+          __stcs(at_out + n * F + (long)k * A + qo, v);
+          __stcs(atb_out + n * FB + (long)(k + 1) * A + qo, v);
         }
       }
     }
