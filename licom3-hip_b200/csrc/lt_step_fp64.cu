@@ -396,15 +396,15 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
       const double* uk = s_uk[b];
       const double* vk = s_vk[b];
       const long c = (long)k * A + qo;
-      a.utf_out[c] = own_utf * p.oncc;
-      a.vtf_out[c] = own_vtf * p.oncc;
+      __stcs(a.utf_out + c, own_utf * p.oncc);
+      __stcs(a.vtf_out + c, own_vtf * p.oncc);
       double uwv = 0.0, vsv = 0.0;   // the faces outside these ranges stay zero
       if (flux) {
-        if (j >= 1 && j < jmt - 1) a.uwf[c] = uwv = (wd[mn] * dyu_n + wd[m0] * dyu_o) * 0.25;
-        if (i >= 1 && i < imt - 1) a.vsf[c] = vsv = (wb[m0] * dxu_o + wb[m0 + 1] * dxu_e) * 0.25;
+        if (j >= 1 && j < jmt - 1) __stcs(a.uwf + c, uwv = (wd[mn] * dyu_n + wd[m0] * dyu_o) * 0.25);
+        if (i >= 1 && i < imt - 1) __stcs(a.vsf + c, vsv = (wb[m0] * dxu_o + wb[m0 + 1] * dxu_e) * 0.25);
       } else {
-        if (j >= 1 && j < jmt - 1) a.uwf[c] = uwv = (wd[mn] + wd[m0]) * htw_o * 0.25;
-        if (i >= 1 && i < imt - 1) a.vsf[c] = vsv = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25;
+        if (j >= 1 && j < jmt - 1) __stcs(a.uwf + c, uwv = (wd[mn] + wd[m0]) * htw_o * 0.25);
+        if (i >= 1 && i < imt - 1) __stcs(a.vsf + c, vsv = (wb[m0] + wb[m0 + 1]) * hts_o * 0.25);
       }
       if (uwv != 0.0 || vsv != 0.0) kf = k + 1;
       double wka = 0.0;
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
         const double north = (vk[mn + 1] + vk[mn]) * hts_n;
         wka = 0.5 * (east - west + south - north) * trr;
       }
-      a.wka[c] = wka;
+      st_l2(a.wka + c, wka, l2_evict_last());
       if (col) W = W - dzp_c * wka * (k < kz ? 1.0 : 0.0);
     }
     if (k + 1 < km) {
@@ -432,19 +432,21 @@ __global__ void __launch_bounds__(32 * BY) k_cont_march64(Arena a) {
   const double fac = 1.0 / (1.0 + a.stf_ssh[qo] * ohbt);
   double wsp = a.ws[qo];
   // upward integration; the wka of CH levels are loaded together ahead of
-  // their stores (one round trip per CH levels)
+  // their stores (one round trip per CH levels).  The march wrote wka with
+  // an L2 evict-last policy (the tile's levels stay in L2 until read here,
+  // then leave it); the outputs go out as streaming stores.
   constexpr int CH = 8;
   for (int k0 = 1; k0 < km; k0 += CH) {
     double wk[CH];
 #pragma unroll
-    for (int c = 0; c < CH; ++c) wk[c] = k0 + c < km ? a.wka[(long)(k0 + c - 1) * A + qo] : 0.0;
+    for (int c = 0; c < CH; ++c) wk[c] = k0 + c < km ? ld_l2(a.wka + (long)(k0 + c - 1) * A + qo, l2_evict_first()) : 0.0;
 #pragma unroll
     for (int c = 0; c < CH; ++c) {
       const int k = k0 + c;
       if (k >= km) break;
       const double raw = (k < kz ? 1.0 : 0.0) * (wsp + a.dzp[k - 1] * (W * ohbt + wk[c]));
       const double wv = raw * fac;
-      a.ws[(long)k * A + qo] = wv;
+      __stcs(a.ws + (long)k * A + qo, wv);
       if (wv != 0.0) kf = max(kf, k + 1);
       wsp = raw;
     }
