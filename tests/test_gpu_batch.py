@@ -12,8 +12,9 @@ pytestmark = pytest.mark.gpu
 SIZES = [(64, 40, 20), (96, 60, 30), (48, 32, 20)]   # uneven members (nx + 4 a multiple of 4)
 
 
-def members(lt, precision, seed0=11):
-    syns = [lt.Synth(nx, ny, km, seed=seed0 + i, forced=1) for i, (nx, ny, km) in enumerate(SIZES)]
+def members(lt, precision, seed0=11, hypsometry=0):
+    syns = [lt.Synth(nx, ny, km, seed=seed0 + i, forced=1, hypsometry=hypsometry)
+            for i, (nx, ny, km) in enumerate(SIZES)]
     return syns, [s.domain(precision=precision) for s in syns]
 
 
@@ -23,10 +24,12 @@ def assert_same(doms_a, doms_b):
             np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
 
 
+@pytest.mark.parametrize("hypsometry", [0, 1])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_batch_equals_members_stepped_alone(lt, precision):
+def test_batch_equals_members_stepped_alone(lt, precision, hypsometry):
+    """hypsometry 1: most tiles march from a wet bottom level."""
     prec = lt.PREC_MIXED if precision == "mixed" else lt.PREC_FP64
-    syns, doms = members(lt, prec)
+    syns, doms = members(lt, prec, hypsometry=hypsometry)
     alone = [s.domain(precision=prec) for s in syns]
     for d in alone:
         d.step(5)
