@@ -96,6 +96,9 @@ typedef enum {
   LT_F_DMC, LT_F_DMN, LT_F_DMS, LT_F_DME, LT_F_DMW,
   LT_F_AMF,                         /* [jmt][imt] resolution factor of the viscosity */
   LT_F_UAREA_R, LT_F_DXUR, LT_F_DYUR,  /* [jmt][imt] U-cell metrics */
+  /* tracer_7's nudging (simple_assm), f64; held by domains created with it */
+  LT_F_RESTORE_AT,                  /* [2][km][jmt][imt] nudging target (d_restore_at) */
+  LT_F_DT_RESTORE,                  /* [2][km][jmt][imt] the nudging term of the last step (d_dt_restore) */
   LT_F_COUNT
 } lt_field;
 
@@ -140,6 +143,11 @@ typedef struct {
   int nss;               /* pconst_mod nss */
   int boundary_restore;  /* pconst_mod boundary_restore (1 = 15-day restoring) */
   int adv_tracer;        /* lt_adv_scheme from pconst_mod adv_tracer (0 = tspas) */
+  int simple_assm;       /* 1 = tracer_7's nudging toward LT_F_RESTORE_AT in the levels k < ktv
+                            (tracer.cpp:1595-1611; 5-day time scale, weaker below level 45), with
+                            its term written to LT_F_DT_RESTORE; FP64 form only.  The reference's
+                            tracer_ passes 0 (tracer.cpp:1877-1879). */
+  int ktv;               /* levels the nudging reaches (the reference's d_ktv) */
 } lt_params;
 
 typedef struct lt_domain lt_domain;

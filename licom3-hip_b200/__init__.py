@@ -43,7 +43,8 @@ class Grid(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("dts", "oncc", "onbc", "dwndmix", "gamma", "od0", "od0cp", "ah", "area_t")] + [
-        ("nss", C.c_int), ("boundary_restore", C.c_int), ("adv_tracer", C.c_int)]
+        ("nss", C.c_int), ("boundary_restore", C.c_int), ("adv_tracer", C.c_int), ("simple_assm", C.c_int),
+        ("ktv", C.c_int)]
 
 
 class IcesnowParams(C.Structure):
@@ -258,7 +259,8 @@ INT_FIELDS = {n for n in FIELDS if lib.lt_field_is_int(FIELD_ID[n])}
 # (WS, NET and QICE are model state the step or icesnow reads and rewrites;
 # they start at zero)
 INPUT_FIELDS = [n for n in FIELDS if n not in (
-    "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE")
+    "UTF_OUT", "VTF_OUT", "H0F_OUT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE",
+    "RESTORE_AT", "DT_RESTORE")
     and not lib.lt_field_on_demand(FIELD_ID[n])]
 # fields a domain allocates on first use: the turbulence closure's and the
 # momentum friction's

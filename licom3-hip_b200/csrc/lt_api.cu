@@ -113,6 +113,8 @@ void* field_ptr(lt_domain* d, int f, int which_state) {
     case LT_F_SO: return a.so;
     case LT_F_C: return a.cc;
     case LT_F_RESTORE: return a.restore;
+    case LT_F_RESTORE_AT: return a.restore_at;
+    case LT_F_DT_RESTORE: return a.dt_restore;
     case LT_F_AX: return a.ax;
     case LT_F_AY: return a.ay;
     case LT_F_AZ: return a.az;
@@ -206,6 +208,7 @@ void plan_arena(Arena& a, Plan& pl) {
   D(&a.scalars, 16);
   I(&a.status, 16);
   if (a.p.boundary_restore == 1) D(&a.restore, 2 * F);
+  if (a.p.simple_assm) { D(&a.restore_at, 2 * F); D(&a.dt_restore, 2 * F); }
   if (a.diagnostics) {
     D(&a.ax, 2 * F); D(&a.ay, 2 * F); D(&a.az, 2 * F); D(&a.dzd, 2 * F);
     D(&a.tend, 2 * F); D(&a.dt_diff, 2 * F); D(&a.dt_conv, 2 * F); D(&a.penetrate, F);
@@ -419,7 +422,7 @@ static const char* const k_field_names[LT_F_COUNT] = {
     "DT_DIFF", "DT_CONV", "PENETRATE", "QICE", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY", "FZ_TIDE",
     "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "ZKP", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON", "FZTIDAL",
     "WP3_TIDAL", "UP", "VP", "DLU", "DLV", "WKA_DRAG", "DUC", "DUM", "DUN", "DUS", "DUE", "DUW", "DMC", "DMN",
-    "DMS", "DME", "DMW", "AMF", "UAREA_R", "DXUR", "DYUR"};
+    "DMS", "DME", "DMW", "AMF", "UAREA_R", "DXUR", "DYUR", "RESTORE_AT", "DT_RESTORE"};
 
 const char* lt_field_name(int f) { return (f >= 0 && f < LT_F_COUNT) ? k_field_names[f] : nullptr; }
 long lt_field_count(int f, int nx, int ny, int km) {
@@ -494,6 +497,18 @@ static bool scheme_ok(int precision, const lt_params* p, const char* where) {
   }
   if (precision == LT_PREC_MIXED && p->adv_tracer != LT_ADV_TSPAS) {
     set_error("%s: the centred and flux advection schemes run in the FP64 form only", where);
+    return false;
+  }
+  if (p->simple_assm != 0 && p->simple_assm != 1) {
+    set_error("%s: simple_assm %d is not 0 or 1", where, p->simple_assm);
+    return false;
+  }
+  if (p->simple_assm && precision == LT_PREC_MIXED) {
+    set_error("%s: tracer_7's nudging (simple_assm) runs in the FP64 form only", where);
+    return false;
+  }
+  if (p->simple_assm && p->ktv < 0) {
+    set_error("%s: ktv %d is negative", where, p->ktv);
     return false;
   }
   return true;
@@ -595,6 +610,10 @@ int lt_set_params(lt_domain* d, const lt_params* p) {
   if (!scheme_ok(d->a.precision, p, "lt_set_params")) return LT_E_INVALID;
   if (p->boundary_restore == 1 && !d->a.restore) {
     set_error("lt_set_params: boundary_restore needs a domain created with it");
+    return LT_E_STATE;
+  }
+  if (p->simple_assm && !d->a.restore_at) {
+    set_error("lt_set_params: simple_assm needs a domain created with it");
     return LT_E_STATE;
   }
   d->a.p = *p;

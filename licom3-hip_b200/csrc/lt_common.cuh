@@ -58,6 +58,7 @@ struct alignas(16) Arena {   // copied into shared memory as 16-byte words
   double *au0, *aus, *auw, *ausw;
   int *kmt, *kmu, *kmtn, *kmts, *kmte, *kmtw;
   double *dzp, *odzp, *odzt, *pen, *to, *so, *cc, *restore;
+  double *restore_at, *dt_restore;   // tracer_7's nudging (simple_assm)
   double *qice;               // [jmt][imt] ice formed by icesnow (tracer_mod licomqice)
   // turbulence closure (lt_turb): inputs and outputs, null until the domain
   // first uses one of them

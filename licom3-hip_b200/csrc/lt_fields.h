@@ -21,7 +21,7 @@ enum FieldShape {
 inline int field_shape(int f) {
   switch (f) {
     case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE: case LT_F_AX: case LT_F_AY: case LT_F_AZ:
-    case LT_F_DZ: case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV:
+    case LT_F_DZ: case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV: case LT_F_RESTORE_AT: case LT_F_DT_RESTORE:
       return SH_TRACER3;
     case LT_F_ATB: return SH_TRACERB;
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:

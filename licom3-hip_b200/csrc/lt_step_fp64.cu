@@ -79,6 +79,43 @@ __device__ __forceinline__ void surface_col(const Arena& a, int i, int j) {
   flux_col(a, i, j, q, ssh_col(a, q));
 }
 
+// tracer_7's nudging toward restore_at (simple_assm; tracer.cpp:1587-1611):
+// the rate of level k, 1/(5 days) down to level 45 and smaller by
+// ((k+1)/5)^2 below, in the reference's operation order
+__device__ __forceinline__ double assm_rate(int k) {
+  return k < 45 ? 1.0e0 / (5.e0 * 86400.e0) : 1.0e0 / (5.e0 * 86400.e0) / ((k + 1) * (k + 1) / 5.0 / 5.0);
+}
+
+// The nudging term of every inner cell of the levels k < ktv, written to
+// dt_restore as tracer_7 writes it (land and below-bottom cells included:
+// their vit of 0 makes it a signed zero).  It reads only the step's inputs
+// (restore_at, the previous time level atb, kmt), so it runs beside the
+// column kernel, which adds the same term to the wet cells' tendencies.
+// Grid: x over the cells of a level, y the level, z the tracer.
+__global__ void k_assm_dt_restore(Arena a) {
+  const int k = blockIdx.y, n = blockIdx.z;
+  const int imt = a.imt, jmt = a.jmt;
+  const long A = a.A, F = a.F, FB = a.FB;
+  const double rate = assm_rate(k);
+  const double* atb = a.atb[a.cur] + n * FB + (long)(k + 1) * A;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < A; q += (long)gridDim.x * blockDim.x) {
+    const int j = (int)(q / imt), i = (int)(q % imt);
+    if (j < 2 || j >= jmt - 2 || i < 2 || i >= imt - 2) continue;
+    const double vit = k < a.kmt[q] ? 1.0 : 0.0;
+    const long c = n * F + (long)k * A + q;
+    a.dt_restore[c] = vit * (a.restore_at[c] - atb[q]) * rate;
+  }
+}
+
+int launch_assm_dt_restore(const Arena& a, cudaStream_t s) {
+  const int levels = a.p.ktv < a.km ? a.p.ktv : a.km;
+  if (!a.p.simple_assm || levels <= 0) return LT_OK;
+  const int bx = (int)((a.A + 255) / 256 < 64 ? (a.A + 255) / 256 : 64);
+  k_assm_dt_restore<<<dim3(bx, levels, 2), 256, 0, s>>>(a);
+  LT_LAUNCHED();
+  return LT_OK;
+}
+
 __global__ void k_ssh(Arena a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i >= a.imt || j >= a.jmt) return;
@@ -693,7 +730,8 @@ __global__ void __launch_bounds__(TTHREADS) k_tracer64(Arena a, int ntx, long nt
               tf = tf + stf * odzp[0] * 0.5;
             }
           }
-          // restoring (tracer_7, boundary_restore == 1)
+          // nudging (tracer_7, simple_assm), then restoring (boundary_restore == 1)
+          if (p.simple_assm && k < p.ktv) tf = tf + vit_k * (a.restore_at[n * F + cg] - atb_k) * assm_rate(k);
           if (p.boundary_restore == 1 && k >= 1) {
             const double lamda = 1.0 / (15.0 * 86400.0);
             tf = tf + vit_k * (a.restore[n * F + cg] - atb_k) * lamda;
@@ -1363,6 +1401,7 @@ __global__ void __launch_bounds__(TTHREADS, kFp64CtasPerSm)
               tf = tf + stf * odzp[0] * 0.5;
             }
           }
+          if (p.simple_assm && k < p.ktv) tf = tf + vit_k * (a.restore_at[n * F + cg] - atb_k) * assm_rate(k);
           if (p.boundary_restore == 1 && k >= 1) {
             const double lamda = 1.0 / (15.0 * 86400.0);
             tf = tf + vit_k * (a.restore[n * F + cg] - atb_k) * lamda;
@@ -1739,6 +1778,7 @@ int launch_tracer_fp64(const Arena& a, cudaStream_t s, int slots) {
   }
   const int adv = a.p.adv_tracer;
   if (adv != LT_ADV_CENTERED && adv != LT_ADV_FLUX) return LT_E_INVALID;
+  if (int rc = launch_assm_dt_restore(a, s)) return rc;
   kern[adv - 1][a.diagnostics ? 1 : 0]<<<slots, TTHREADS, sm, s>>>(a, ntx, ntiles);
   LT_LAUNCHED();
   return LT_OK;
@@ -1754,6 +1794,7 @@ int launch_tracer_tma64(const Arena& a, const TracerMaps& maps, cudaStream_t s, 
     LT_CUDA_OK(cudaFuncSetAttribute(k_tracer_tma64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     attr = true;
   }
+  if (int rc = launch_assm_dt_restore(a, s)) return rc;
   if (a.diagnostics) {
     k_tracer_tma64<true><<<grid, TTHREADS, sm, s>>>(a, maps, ntx, ntiles, tma ? 1 : 0);
     LT_LAUNCHED();

@@ -67,6 +67,8 @@ int lt_synth_params(const lt_synth* s, lt_params* p) {
   p->od0 = d.od0; p->od0cp = d.od0cp; p->ah = d.ah; p->area_t = d.area_t; p->nss = d.nss;
   p->boundary_restore = 0;
   p->adv_tracer = LT_ADV_TSPAS;
+  p->simple_assm = 0;
+  p->ktv = 0;
   return LT_OK;
 }
 

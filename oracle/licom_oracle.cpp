@@ -46,7 +46,7 @@ struct FieldInfo { int kind; bool is_int; };
 
 FieldInfo field_info(int f) {
   switch (f) {
-    case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE:
+    case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE: case LT_F_RESTORE_AT: case LT_F_DT_RESTORE:
     case LT_F_AX: case LT_F_AY: case LT_F_AZ: case LT_F_DZ: case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV:
       return {K3N, false};
     case LT_F_ATB: return {KB3N, false};
@@ -65,6 +65,41 @@ FieldInfo field_info(int f) {
       return {K1, false};
     case LT_F_C: return {K1C, false};
     default: return {K2, false};
+  }
+}
+
+// tracer_7 (tracer.cpp:1571-1626) for tracer n: the nudging toward
+// restore_at of the levels k < ktv (simple_assm), whose rate is 1/(5 days)
+// down to level 45 and smaller by ((k+1)/5)^2 below, with its term also
+// written to dt_restore; then the 15-day restoring toward restore
+// (boundary_restore == 1) of the levels k >= 1.  Inner cells only.  tf, vit:
+// [km][jmt][imt]; atbn: this tracer's [km+1][jmt][imt]; restore, restore_at,
+// dt_restore: [2][km][jmt][imt].
+void tracer7(const lt_params& p, int n, int imt, int jmt, int km, double* tf, const double* vit, const double* atbn,
+             const double* restore, const double* restore_at, double* dt_restore) {
+  const long A = (long)imt * jmt, F = A * km;
+  if (p.simple_assm) {
+#pragma omp parallel for
+    for (int k = 0; k < std::min(p.ktv, km); ++k) {
+      const double lamda1 = k < 45 ? 1.0e0 / (5.e0 * 86400.e0)
+                                   : 1.0e0 / (5.e0 * 86400.e0) / ((k + 1) * (k + 1) / 5.0 / 5.0);
+      for (int j = 2; j < jmt - 2; ++j)
+        for (int i = 2; i < imt - 2; ++i) {
+          const long c = (long)k * A + (long)j * imt + i;
+          tf[c] = tf[c] + vit[c] * (restore_at[n * F + c] - atbn[c + A]) * lamda1;
+          dt_restore[n * F + c] = vit[c] * (restore_at[n * F + c] - atbn[c + A]) * lamda1;
+        }
+    }
+  }
+  if (p.boundary_restore == 1) {
+    const double lamda = 1.0 / (15.0 * 86400.0);
+#pragma omp parallel for
+    for (int k = 1; k < km; ++k)
+      for (int j = 2; j < jmt - 2; ++j)
+        for (int i = 2; i < imt - 2; ++i) {
+          const long c = (long)k * A + (long)j * imt + i;
+          tf[c] = tf[c] + vit[c] * (restore[n * F + c] - atbn[c + A]) * lamda;
+        }
   }
 }
 
@@ -319,6 +354,9 @@ void tracer_call(Oracle& o) {
   const double* pen = o.fd[LT_F_PEN].data();
   if (o.p.boundary_restore == 1) o.ensure(LT_F_RESTORE);
   const double* restore = o.fd[LT_F_RESTORE].data();
+  if (o.p.simple_assm) { o.ensure(LT_F_RESTORE_AT); o.ensure(LT_F_DT_RESTORE); }
+  const double* restore_at = o.fd[LT_F_RESTORE_AT].data();
+  double* dt_restore = o.fd[LT_F_DT_RESTORE].data();
   const bool dg = o.diagnostics != 0;   // diagnostic fields are written only while on
   double* ax = o.fd[LT_F_AX].data();
   double* ay = o.fd[LT_F_AY].data();
@@ -672,17 +710,8 @@ void tracer_call(Oracle& o) {
         }
       }
     halo_r8(net, 2, imt, jmt, o.ew_cyclic, o.tripole);
-    // tracer_7: restoring (boundary_restore == 1), 15-day time scale
-    if (p.boundary_restore == 1) {
-      const double lamda = 1.0 / (15.0 * 86400.0);
-#pragma omp parallel for
-      for (int k = 1; k < km; ++k)
-        for (int j = 2; j < jmt - 2; ++j)
-          for (int i = 2; i < imt - 2; ++i) {
-            const long c = C(k, j, i);
-            tf[c] = tf[c] + vit[c] * (restore[n * F + c] - atbn[c + A]) * lamda;
-          }
-    }
+    // tracer_7: nudging (simple_assm) and restoring (boundary_restore)
+    tracer7(p, n, imt, jmt, km, tf, vit, atb + n * FB, restore, restore_at, dt_restore);
     // tracer_8: explicit update into vtl (used as scratch), copy to ori
 #pragma omp parallel for
     for (int k = 0; k < km; ++k)
@@ -1540,6 +1569,14 @@ int or_halo(double* a, int nz, int imt, int jmt, int ew_cyclic, int tripole) {
 }
 int or_set_sum_order(void* h, int tree) {
   static_cast<Oracle*>(h)->tree_sum = tree != 0;
+  return 0;
+}
+// tracer_7 alone on caller arrays (the nudging branch is pinned with it
+// against the reference's own tracer_7, which the reference's tracer_ never
+// runs with simple_assm on)
+int or_tracer7(const lt_params* p, int n, int imt, int jmt, int km, double* tf, const double* vit,
+               const double* atb, const double* restore, const double* restore_at, double* dt_restore) {
+  tracer7(*p, n, imt, jmt, km, tf, vit, atb + (long)n * imt * jmt * (km + 1), restore, restore_at, dt_restore);
   return 0;
 }
 int or_set_threads(int n) {

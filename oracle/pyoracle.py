@@ -27,14 +27,15 @@ FIELDS = ["AT", "ATB", "UTF", "VTF", "UTL", "VTL", "H0F", "H0L", "AKT", "WS", "N
           "DZ", "TEND", "DT_DIFF", "DT_CONV", "PENETRATE", "QICE", "RIT", "RICDTTMS", "S2T", "RICT", "PDENSITY",
           "FZ_TIDE", "BUOYTUR", "BUOYSOL", "FCORT", "WAVE_DIS", "ZKP", "AKMT", "AK_TIDE", "AMLD", "RICHARDSON",
           "FZTIDAL", "WP3_TIDAL", "UP", "VP", "DLU", "DLV", "WKA_DRAG", "DUC", "DUM", "DUN", "DUS", "DUE", "DUW",
-          "DMC", "DMN", "DMS", "DME", "DMW", "AMF", "UAREA_R", "DXUR", "DYUR"]
+          "DMC", "DMN", "DMS", "DME", "DMW", "AMF", "UAREA_R", "DXUR", "DYUR", "RESTORE_AT", "DT_RESTORE"]
 FID = {n: i for i, n in enumerate(FIELDS)}
 INT = {"KMT", "KMU", "KMTN", "KMTS", "KMTE", "KMTW"}
 
 
 def shape_of(name, nx, ny, km):
     imt, jmt = nx + 4, ny + 4
-    if name in ("AT", "AKT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV"):
+    if name in ("AT", "AKT", "RESTORE", "AX", "AY", "AZ", "DZ", "TEND", "DT_DIFF", "DT_CONV", "RESTORE_AT",
+                "DT_RESTORE"):
         return (2, km, jmt, imt)
     if name == "ATB":
         return (2, km + 1, jmt, imt)
@@ -63,7 +64,8 @@ def _dtype(name):
 class Params(C.Structure):
     """lt_params (include/licom_tracer.h)."""
     _fields_ = [(n, C.c_double) for n in ("dts", "oncc", "onbc", "dwndmix", "gamma", "od0", "od0cp", "ah", "area_t")] + [
-        ("nss", C.c_int), ("boundary_restore", C.c_int), ("adv_tracer", C.c_int)]
+        ("nss", C.c_int), ("boundary_restore", C.c_int), ("adv_tracer", C.c_int), ("simple_assm", C.c_int),
+        ("ktv", C.c_int)]
 
 
 class SynthConfig(C.Structure):
@@ -239,6 +241,17 @@ class Oracle:
         return a
 
 
+def oracle_tracer7(params, n, tf, vit, atb, restore, restore_at, dt_restore):
+    """The oracle's restatement of tracer_7 alone (tf and dt_restore updated in
+    place): tf, vit [km][jmt][imt]; atb [2][km+1][jmt][imt]; restore,
+    restore_at, dt_restore [2][km][jmt][imt]."""
+    lib = C.CDLL(ORACLE_LIB)
+    lib.or_tracer7.argtypes = [C.c_void_p] + [C.c_int] * 4 + [C.c_void_p] * 6
+    km, jmt, imt = tf.shape
+    lib.or_tracer7(C.byref(params), int(n), imt, jmt, km, tf.ctypes.data, vit.ctypes.data, atb.ctypes.data,
+                   restore.ctypes.data, restore_at.ctypes.data, dt_restore.ctypes.data)
+
+
 def reference_available():
     return os.path.exists(REF_LIB)
 
@@ -289,6 +302,14 @@ class Reference:
 
     def fw_norm2(self):
         return self.lib.ref_fw_norm2()
+
+    def tracer7(self, n, tf, vit, atb, restore, restore_at, dt_restore, boundary_restore, simple_assm, ktv):
+        """The reference's tracer_7 kernel alone on the given arrays (tf and
+        dt_restore updated in place; float64, C order, the block size)."""
+        f = self.lib.ref_tracer7_call
+        f.argtypes = [C.c_int] + [C.c_void_p] * 6 + [C.c_int] * 3
+        f(int(n), tf.ctypes.data, vit.ctypes.data, atb.ctypes.data, restore.ctypes.data, restore_at.ctypes.data,
+          dt_restore.ctypes.data, int(boundary_restore), int(simple_assm), int(ktv))
 
 
 def reference_readyc_available():

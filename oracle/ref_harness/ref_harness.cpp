@@ -30,6 +30,9 @@ static const int R_IMT = BLCKX + 4, R_JMT = BLCKY + 4, R_KM = NKM;
 thread_local dim3 threadIdx, blockIdx, blockDim, gridDim;
 
 extern "C" void tracer_(int ii);
+// tracer.cpp's tracer_7 kernel (__global__ is empty in the CPU stand-in)
+void tracer_7(int d_imt, int d_jmt, int d_km, int n, double* d_tf, double* d_vit, double* d_atb, double* d_restore,
+              double* d_restore_at, double* d_dt_restore, int d_boundary_restore, int d_simple_assm, int d_ktv);
 extern "C" void convadj_();
 extern "C" void icesnow_();
 extern "C" void icesnow_nofrc_();
@@ -79,7 +82,8 @@ bool ready = false;
 
 long field_count(int f) {
   switch (f) {
-    case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE: case LT_F_AX: case LT_F_AY: case LT_F_AZ: case LT_F_DZ:
+    case LT_F_AT: case LT_F_AKT: case LT_F_RESTORE: case LT_F_RESTORE_AT: case LT_F_DT_RESTORE:
+    case LT_F_AX: case LT_F_AY: case LT_F_AZ: case LT_F_DZ:
     case LT_F_TEND: case LT_F_DT_DIFF: case LT_F_DT_CONV: return 2 * F;
     case LT_F_ATB: return 2 * FB;
     case LT_F_UTF: case LT_F_VTF: case LT_F_UTL: case LT_F_VTL: case LT_F_UTF_OUT: case LT_F_VTF_OUT:
@@ -235,5 +239,18 @@ int ref_icesnow_call(double tbice, double cp, int frc_core) {
   return 0;
 }
 double ref_fw_norm2(void) { return tracer_mod_mp_fw_norm2_; }
+// tracer_7 alone on the caller's arrays of the reference's block size,
+// launched as tracer_ launches it (8x8x4 threads).  tracer_ passes
+// simple_assm = 0 (tracer.cpp:1877-1879); this runs the nudging branch too.
+int ref_tracer7_call(int n, double* tf, double* vit, double* atb, double* restore, double* restore_at,
+                     double* dt_restore, int boundary_restore, int simple_assm, int ktv) {
+  setup();
+  dim3 threads(8, 8, 4);
+  dim3 blocks((R_IMT + threads.x - 1) / threads.x, (R_JMT + threads.y - 1) / threads.y,
+              (R_KM + threads.z - 1) / threads.z);
+  hipLaunchKernelGGL(tracer_7, dim3(blocks), dim3(threads), 0, 0, R_IMT, R_JMT, R_KM, n, tf, vit, atb, restore,
+                     restore_at, dt_restore, boundary_restore, simple_assm, ktv);
+  return 0;
+}
 
 }  // extern "C"

@@ -5,7 +5,8 @@ Runs LICOM3-HIP's tracer.cpp, convadj.cpp, icesnow.cpp and readyc.cpp
 reference tree, on seeded
 synthetic inputs (with the restoring branch on in the cases of
 tests/restore_case.py, the centred and flux advection schemes in those of
-tests/scheme_case.py) at the reference's built-in block size (36 x 40 physical, 55
+tests/scheme_case.py; tracer_7 alone with its nudging branch on, in the
+cases of tests/assm_case.py) at the reference's built-in block size (36 x 40 physical, 55
 levels) and records SHA-256 digests of every output field plus fw_norm2.  The
 icesnow cases start from the cold states of tests/icesnow_state.py; the
 turbulence cases use the closure inputs and stand-in tables of
@@ -28,6 +29,7 @@ from conftest import load_package  # noqa: E402
 import pyoracle  # noqa: E402
 from icesnow_state import ICE_CASES, cold_state  # noqa: E402
 from turb_case import DFRICMX, NCC, TURB_CASES, case, tables  # noqa: E402
+import assm_case  # noqa: E402
 import del4u_case  # noqa: E402
 import restore_case  # noqa: E402
 import scheme_case  # noqa: E402
@@ -129,6 +131,17 @@ def main():
                 "inputs": {n: digest(f[n]) for n in ("UP", "DUC", "DMS")},
                 "outputs": {n: digest(ref.get(n)) for n in ("DLU", "DLV", "WKA_DRAG")},
             }
+    # tracer_7 alone, nudging branch included (tests/assm_case.py)
+    ref = pyoracle.Reference(lt.Synth(36, 40, 55).params)
+    for br, sa, ktv, seed in assm_case.ASSM_CASES:
+        tf, vit, atb, restore, restore_at = assm_case.arrays(ref.nx, ref.ny, ref.km, seed)
+        res = {}
+        for n in (0, 1):
+            t, d = tf.copy(), np.zeros_like(restore)
+            ref.tracer7(n, t, vit, atb, restore, restore_at, d, br, sa, ktv)
+            res["TF%d" % n], res["DT_RESTORE%d" % n] = digest(t), digest(d)
+        out[assm_case.key(br, sa, ktv, seed)] = {"inputs": {"ATB": digest(atb), "RESTORE_AT": digest(restore_at)},
+                                                 "outputs": res}
     with open(os.path.join(HERE, "reference_digests.json"), "w") as f:
         json.dump(out, f, indent=1, sort_keys=True)
     print("wrote", len(out), "cases")

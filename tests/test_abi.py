@@ -97,3 +97,18 @@ def test_advection_scheme_checked_before_device_work(lt):
         rc = lt.lib.lt_create(C.byref(g), C.byref(p), C.byref(h))
         assert rc == lt.LT_E_INVALID, (prec, adv)
         assert b"adv" in lt.lib.lt_last_error() or b"FP64 form only" in lt.lib.lt_last_error()
+
+
+def test_nudging_checked_before_device_work(lt):
+    """tracer_7's nudging (simple_assm) runs in the FP64 form only, with a
+    flag of 0 or 1 and ktv >= 0: anything else is LT_E_INVALID from
+    lt_create, before any device work."""
+    syn = lt.Synth(16, 12, 5)
+    h = C.c_void_p()
+    for prec, sa, ktv in ((lt.PREC_MIXED, 1, 5), (lt.PREC_FP64, 2, 5), (lt.PREC_FP64, 1, -1)):
+        p = type(syn.params).from_buffer_copy(syn.params)
+        p.simple_assm, p.ktv = sa, ktv
+        g = lt.Grid(16, 12, 5, prec, 0, 1, 1)
+        rc = lt.lib.lt_create(C.byref(g), C.byref(p), C.byref(h))
+        assert rc == lt.LT_E_INVALID, (prec, sa, ktv)
+        assert b"simple_assm" in lt.lib.lt_last_error() or b"ktv" in lt.lib.lt_last_error()

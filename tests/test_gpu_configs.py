@@ -127,3 +127,32 @@ def test_restoring_one_degree(lt):
     dt, ds = ocean_errors(f, syn.km, r, mix.get("AT"))
     print("restoring, mixed vs oracle after 10 steps: %.3e K, %.3e psu" % (dt, ds))
     assert dt <= 1e-5 and ds <= 1e-6, (dt, ds)
+
+
+@pytest.mark.parametrize("diagnostics,tma,scheme", [(False, True, 0), (True, True, 0), (False, False, 0),
+                                                    (True, None, 1)])
+def test_nudging_fp64_bitexact(lt, diagnostics, tma, scheme):
+    """tracer_7's nudging toward RESTORE_AT (simple_assm) in the levels
+    k < ktv = 50 (the deep ones at the weaker rate), with the 15-day
+    restoring on as well: the FP64 step and DT_RESTORE bit for bit against
+    the oracle, whose tracer_7 is pinned to the reference's own kernel.
+    Both column kernels (TMA boxes, copy fill) and the centred scheme's."""
+    syn, p, f = restore_case.case(lt, 1, 23)
+    p.simple_assm, p.ktv, p.adv_tracer = 1, 50, scheme
+    f["RESTORE_AT"] = 2.0 * f["AT"] - restore_case.restore_target(f["AT"])
+    o = pyoracle.Oracle(syn.nx, syn.ny, syn.km, p, ew_cyclic=syn.cfg.ew_cyclic, tripole=syn.cfg.tripole)
+    o.load(f)
+    o.sum_order(1)
+    o.step(3)
+    dom = lt.TracerDomain(syn.nx, syn.ny, syn.km, p, precision=lt.PREC_FP64, diagnostics=diagnostics,
+                          ew_cyclic=bool(syn.cfg.ew_cyclic), tripole=bool(syn.cfg.tripole))
+    for n in lt.INPUT_FIELDS + ["RESTORE", "RESTORE_AT"]:
+        dom.set(n, f[n])
+    if tma is not None:
+        dom.use_tma(tma)
+    dom.step(3)
+    names = ["AT", "ATB", "WS", "DT_RESTORE"] + (["TEND", "DT_DIFF"] if diagnostics else [])
+    for n in names:
+        g, r = dom.get(n), o.get(n)
+        assert bits_equal(g, r), n + ": " + mismatch(g, r)
+    assert np.count_nonzero(dom.get("DT_RESTORE")[0, 45:50]) > 0

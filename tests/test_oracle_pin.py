@@ -18,6 +18,7 @@ import pytest
 from conftest import REPO
 
 import pyoracle
+import assm_case
 import restore_case
 import scheme_case
 
@@ -319,3 +320,45 @@ def test_tree_order_reproduces_reference_temperature(lt, forced, nsteps, seed):
     o.convadj()
     for n in ("AT", "ATB"):
         assert digest(o.get(n)[0]) == gold["outputs_T"][n], n
+
+
+def _tracer7_oracle(params, br, sa, ktv, tf, vit, atb, restore, restore_at):
+    p = type(params).from_buffer_copy(params)
+    p.boundary_restore, p.simple_assm, p.ktv = br, sa, ktv
+    out = {}
+    for n in (0, 1):
+        t, d = tf.copy(), np.zeros_like(restore)
+        pyoracle.oracle_tracer7(p, n, t, vit, atb, restore, restore_at, d)
+        out[n] = (t, d)
+    return out
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference tree not built here")
+@pytest.mark.parametrize("br,sa,ktv,seed", assm_case.ASSM_CASES)
+def test_oracle_tracer7_bitexact_vs_reference(lt, br, sa, ktv, seed):
+    """tracer_7 with its nudging branch (simple_assm), which the reference's
+    tracer_ never runs: the reference's own kernel against the oracle."""
+    syn = lt.Synth(36, 40, 55)
+    ref = pyoracle.Reference(syn.params)
+    tf, vit, atb, restore, restore_at = assm_case.arrays(ref.nx, ref.ny, ref.km, seed)
+    mine = _tracer7_oracle(syn.params, br, sa, ktv, tf, vit, atb, restore, restore_at)
+    for n in (0, 1):
+        t, d = tf.copy(), np.zeros_like(restore)
+        ref.tracer7(n, t, vit, atb, restore, restore_at, d, br, sa, ktv)
+        assert np.array_equal(t.view(np.uint64), mine[n][0].view(np.uint64)), n
+        assert np.array_equal(d.view(np.uint64), mine[n][1].view(np.uint64)), n
+        if sa and n == 0:
+            assert np.count_nonzero(d[0, :min(ktv, ref.km)]) > 0 and not d[0, ktv:].any()
+
+
+@pytest.mark.parametrize("br,sa,ktv,seed", assm_case.ASSM_CASES)
+def test_oracle_tracer7_matches_golden_digests(lt, br, sa, ktv, seed):
+    gold = json.load(open(os.path.join(REPO, "tests", "golden", "reference_digests.json")))[
+        assm_case.key(br, sa, ktv, seed)]
+    syn = lt.Synth(36, 40, 55)
+    tf, vit, atb, restore, restore_at = assm_case.arrays(36, 40, 55, seed)
+    assert hashlib.sha256(atb.tobytes()).hexdigest() == gold["inputs"]["ATB"]
+    mine = _tracer7_oracle(syn.params, br, sa, ktv, tf, vit, atb, restore, restore_at)
+    for n in (0, 1):
+        assert hashlib.sha256(mine[n][0].tobytes()).hexdigest() == gold["outputs"]["TF%d" % n]
+        assert hashlib.sha256(mine[n][1].tobytes()).hexdigest() == gold["outputs"]["DT_RESTORE%d" % n]
