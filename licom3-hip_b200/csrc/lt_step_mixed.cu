@@ -456,8 +456,10 @@ struct MxLevel {
 
 struct MxSmem {
   MxSlot slot[NSM];
-  float2 fd[FN];                       // predictor's level: face difference (T, S), 0 where a side is land
-  float fu[FN], fq[FN];                // predictor's level: f32 transport u and Lax-Wendroff factor u*u*cf
+  // predictor's level, per face: the difference (T, S), 0 where a side is
+  // land, and u + u*u*cf, u - u*u*cf of the f32 transport u (the cell east /
+  // south of the face takes the first, the other cell the second)
+  float4 fdq[FN];
   double ou[OXN + OYN], oq[OXN + OYN]; // column phase's level: the tile's f64 transports and u*u*cf
   double d2[2][MHN];                   // column phase's level: first Laplacian times ahf (T, S)
   unsigned char flag[NSM][MHN];        // bit n: tracer n's predictor leaves its local bounds
@@ -583,9 +585,8 @@ __device__ __forceinline__ void face_f32(MxSmem& S, const MxSlot& L, int kk, con
   float2 d;
   d.x = wet ? (float)(L.at[0][r2] - L.at[0][r1]) : 0.f;
   d.y = wet ? (float)(L.at[1][r2] - L.at[1][r1]) : 0.f;
-  S.fd[q.f] = d;
-  S.fu[q.f] = u;
-  S.fq[q.f] = u * u * S.cf[q.f];
+  const float lw = u * u * S.cf[q.f];
+  S.fdq[q.f] = make_float4(d.x, d.y, u + lw, u - lw);
 }
 
 // border faces of the region beyond each thread's own west x face and north
@@ -692,10 +693,12 @@ __device__ __forceinline__ unsigned pred_cell(const MxSmem& S, const HCell& h, i
   // land cells need no flag: every face of a land cell carries no transport
   if (!h.valid || kk >= kr) return 0u;
   const int fe = h.fw + 1, fw = h.fw, fs = h.fn + HQX, fn = h.fn;
-  const float2 de = S.fd[fe], dw = S.fd[fw], ds = S.fd[fs], dn = S.fd[fn];
+  const float4 qe = S.fdq[fe], qw = S.fdq[fw], qs = S.fdq[fs], qn = S.fdq[fn];
+  const float2 de = make_float2(qe.x, qe.y), dw = make_float2(qw.x, qw.y);
+  const float2 ds = make_float2(qs.x, qs.y), dn = make_float2(qn.x, qn.y);
   // east face: this cell is the lower one, d*(u - q); west face: upper, d*(u + q)
-  const float2 sx = __ffma2_rn(dw, f2(S.fu[fw] + S.fq[fw]), __fmul2_rn(de, f2(S.fu[fe] - S.fq[fe])));
-  const float2 sy = __ffma2_rn(dn, f2(S.fu[fn] + S.fq[fn]), __fmul2_rn(ds, f2(S.fu[fs] - S.fq[fs])));
+  const float2 sx = __ffma2_rn(dw, f2(qw.z), __fmul2_rn(de, f2(qe.w)));
+  const float2 sy = __ffma2_rn(dn, f2(qn.z), __fmul2_rn(ds, f2(qs.w)));
   // vertical faces: above (kk-1|kk) with w(kk), below (kk|kk+1) with w(kk+1)
   const MxSlot& C = S.slot[sc];
   const MxSlot& U = S.slot[kk > 0 ? su : sc];
